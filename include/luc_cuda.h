@@ -1,0 +1,188 @@
+/*
+ * luc_cuda.h — the C ABI of liblucida_cuda.so, the B200 (sm_100a) drop-in for
+ * Lucida's wgpu harness (crate `pt-gpu`, crates/gpu/src).
+ *
+ * Plain pointers and sizes only; every struct crossing the boundary is one of
+ * the `#[repr(C)]` layouts from crates/core/src/gpu_layout.rs restated in
+ * lucida_layout.h, so a Rust `crates/cuda` shim passes `bytemuck` slices of
+ * its `SceneBlob` straight through.
+ *
+ * Conventions
+ *   - Ownership: the caller owns every host array and only lends it for the
+ *     duration of the call. The context owns all device memory it allocates.
+ *     A `*_dev` pointer argument is caller-owned device memory on the
+ *     context's device.
+ *   - Errors: every entry point returns 0 on success or a negative LUC_ERR_*
+ *     code, which map one-to-one onto pt_gpu::GpuError (crates/gpu/src/
+ *     lib.rs:100-112); luc_last_error() has the message. Nothing aborts.
+ *   - Threading: one context per host thread; a context is not re-entrant.
+ *     All work is queued on the context's stream (its own, or the one given
+ *     to luc_set_stream) and every entry point that returns host data
+ *     synchronises that stream before returning.
+ */
+#ifndef LUC_CUDA_H
+#define LUC_CUDA_H
+
+#include <stdint.h>
+#include "lucida_layout.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* GpuError (crates/gpu/src/lib.rs:100-112) */
+#define LUC_OK 0
+#define LUC_ERR_NO_DEVICE (-1)  /* GpuError::NoAdapter / NoDevice */
+#define LUC_ERR_LAUNCH (-2)     /* GpuError::Shader: module load or kernel launch failed */
+#define LUC_ERR_READBACK (-3)   /* GpuError::Readback: device->host copy failed */
+#define LUC_ERR_VALIDATION (-4) /* GpuError::Validation: bad argument, layout, size, or device status word */
+#define LUC_ERR_OUT_OF_MEMORY (-5)
+
+/* luc_render arch_flags (Architecture, crates/gpu/src/lib.rs:38-66). */
+#define LUC_ARCH_WAVEFRONT 0x0u
+/* Skip the first-hit guide channels (albedo/normal/depth) of the
+ * accumulator: they are needed only by the denoiser. */
+#define LUC_FLAG_NO_GUIDES 0x100u
+/* Record per-stage CUDA events during the render (luc_get_stats). */
+#define LUC_FLAG_PROFILE 0x200u
+
+typedef struct luc_ctx luc_ctx;
+
+/* The SceneBlob upload (crates/core/src/gpu_layout.rs:706-770 plus the
+ * environment textures of crates/gpu/src/lib.rs:263-359). */
+typedef struct luc_scene_view {
+    const GpuMaterial* materials;
+    uint32_t num_materials;
+    /* Analytic primitives (spheres, quads) followed by `num_instances`
+     * GpuInstance rows, as SceneBlob::primitives_upload lays them out. */
+    const GpuPrimitive* primitives;
+    uint32_t num_primitives; /* analytic only */
+    uint32_t num_instances;
+    const GpuLight* lights;
+    uint32_t num_lights;
+    const float* positions; /* [x, y, z, w] per vertex */
+    const GpuVertexAttr* vertex_attrs;
+    uint32_t num_vertices;
+    const GpuTriangle* triangles;
+    uint32_t num_triangles;
+    /* The caller's BVH over `triangles` (leaves index triangles directly,
+     * i.e. compacted as Bvh::compact_primitives leaves them). When
+     * num_bvh_nodes == 0 and there are triangles, the context builds an LBVH
+     * on the device (30-bit Morton, radix sort, Karras, fit, relayout) and
+     * reorders its own copy of the triangles into leaf order. */
+    const GpuBvhNode* bvh_nodes;
+    uint32_t num_bvh_nodes;
+    uint32_t tlas_root;
+    /* Equirectangular environment: RGBA32F texels, row 0 = zenith, and the
+     * packed CDF rectangle (cdf_width x (env_height + 1)): rows 0..h-1 hold
+     * the per-row conditionals (env_width + 1 entries), row h the marginal
+     * (env_height + 1 entries). env_width == 0 means no map. */
+    const float* env_pixels;
+    uint32_t env_width, env_height;
+    const float* env_cdf;
+    uint32_t env_cdf_width;
+    float env_total_weight;
+} luc_scene_view;
+
+/* LbvhBuilder output (crates/gpu/src/lbvh.rs:724-733 GpuBuildOutput, plus
+ * the relaid-out tree Lbvh::from_parts produces). Every pointer is a
+ * caller-allocated host array or null (skipped). Sizes for n primitives:
+ * codes/order: n; karras: 2(n-1); parent: 2n-1; node_bounds: 6(2n-1) floats;
+ * subtree_size: n-1; scene_bounds: 6 floats (centroid box);
+ * nodes: up to 2n-1 GpuBvhNode (count returned in *num_nodes);
+ * prim_indices: n. */
+typedef struct luc_lbvh_out {
+    uint32_t* codes;        /* Morton code per primitive, input order */
+    uint32_t* order;        /* sorted permutation */
+    uint32_t* karras;       /* (left, right) per internal node */
+    uint32_t* parent;       /* per node id, 0xFFFFFFFF for the root */
+    float* node_bounds;     /* (min xyz, max xyz) per node id */
+    uint32_t* subtree_size; /* per internal node */
+    float* scene_bounds;    /* centroid bounds */
+    GpuBvhNode* nodes;      /* relaid-out tree */
+    uint32_t* prim_indices;
+    uint32_t num_nodes;     /* out */
+} luc_lbvh_out;
+
+/* DenoiseParams (crates/core/src/denoise.rs:62-94). */
+typedef struct luc_denoise_params {
+    uint32_t iterations;
+    float sigma_normal, sigma_depth, sigma_luminance, sigma_albedo;
+} luc_denoise_params;
+
+/* Per-render statistics (filled by luc_render; stage times only under
+ * LUC_FLAG_PROFILE). */
+typedef struct luc_render_stats {
+    double ms_total;       /* device time of the whole render, CUDA events */
+    double ms_generate, ms_extend, ms_shade, ms_connect, ms_resolve;
+    uint64_t launches;     /* kernels this library launched */
+    uint64_t rays_extend;  /* closest-hit rays traced */
+    uint64_t rays_shadow;  /* shadow rays traced */
+    uint64_t paths;        /* camera paths started */
+} luc_render_stats;
+
+/* Layout contract: returns LUC_LAYOUT_VERSION. */
+uint32_t luc_layout_version(void);
+/* Byte size of each boundary struct, for a caller's own layout assertion
+ * (gpu_layout.rs:993-1166): which = 0 material, 1 primitive, 2 light,
+ * 3 vertex attr, 4 triangle, 5 bvh node, 6 accum, 7 uniforms, 8 instance. */
+uint32_t luc_sizeof(uint32_t which);
+
+/* Gpu::new (crates/gpu/src/lib.rs:133-242). */
+int32_t luc_create(int32_t device, luc_ctx** out);
+void luc_destroy(luc_ctx* ctx);
+const char* luc_last_error(const luc_ctx* ctx);
+/* Queue this context's work on a caller stream (a cudaStream_t); null
+ * restores the context's own stream. */
+int32_t luc_set_stream(luc_ctx* ctx, void* cuda_stream);
+
+/* Upload a scene (replaces the previous one). */
+int32_t luc_upload_scene(luc_ctx* ctx, const luc_scene_view* scene);
+
+/* render(scene, camera, spp, bounces) -> HDR accumulator:
+ * pt_gpu::render_with(.., Architecture::Wavefront) / wavefront::
+ * render_native_on (crates/gpu/src/lib.rs:69-79, wavefront.rs:134-140).
+ * `u` carries camera, resolution, frame_seed, sample_offset, sampling_mode,
+ * sampler_kind and background, exactly as integrator::build_uniforms writes
+ * them; its samples_per_launch and max_depth fields are ignored in favour of
+ * `spp` and `max_depth`. Samples sample_offset .. sample_offset+spp-1 of
+ * every pixel are traced and summed into the accumulator with the
+ * semantics of RESOLVE (shaders/wavefront/resolve.wgsl:36-47).
+ * Exactly one of out_host / out_dev is non-null:
+ *   out_host — width*height GpuAccum, overwritten with this render alone;
+ *   out_dev  — caller device array of width*height GpuAccum, accumulated
+ *              into (progressive rendering). */
+int32_t luc_render(luc_ctx* ctx, const GpuUniforms* u, uint32_t spp, uint32_t max_depth, uint32_t arch_flags,
+                   GpuAccum* out_host, void* out_dev);
+int32_t luc_get_stats(const luc_ctx* ctx, luc_render_stats* out);
+
+/* Camera::write_uniforms (crates/core/src/camera.rs:344-365): fills the
+ * camera block plus width/height of `out` (all other fields zeroed) from a
+ * look-at camera with vertical field of view in degrees; aspect = w/h. */
+int32_t luc_camera_uniforms(const float* eye, const float* look_at, const float* up, float vfov_deg,
+                            float aperture, float focus_distance, uint32_t width, uint32_t height,
+                            GpuUniforms* out);
+
+/* LbvhBuilder::build / build_parts (crates/gpu/src/lbvh.rs:369-665). */
+int32_t luc_lbvh_build(luc_ctx* ctx, const GpuTriangle* triangles, uint32_t n, const float* positions,
+                       uint32_t num_vertices, luc_lbvh_out* out);
+/* LBVH over arbitrary boxes (min xyz, max xyz per box): the per-frame TLAS
+ * over instance world bounds. Outputs as luc_lbvh_build. */
+int32_t luc_lbvh_build_boxes(luc_ctx* ctx, const float* boxes, uint32_t n, luc_lbvh_out* out);
+/* LbvhBuilder::sort (crates/gpu/src/lbvh.rs:669-714): stable ascending sort
+ * of (key, value) pairs by key. Host arrays. */
+int32_t luc_sort_u32(luc_ctx* ctx, const uint32_t* keys, const uint32_t* vals, uint32_t n, uint32_t* keys_out,
+                     uint32_t* vals_out);
+/* Device-resident variant: sorts keys_dev/vals_dev in place (n pairs). */
+int32_t luc_sort_u32_dev(luc_ctx* ctx, void* keys_dev, void* vals_dev, uint32_t n);
+
+/* Denoiser::run (crates/gpu/src/denoise.rs:103-210): edge-avoiding à-trous
+ * over an accumulator (radiance/albedo/normal/depth sums and samples);
+ * writes an Accum-shaped image with samples = 1. Host arrays. */
+int32_t luc_denoise(luc_ctx* ctx, const GpuAccum* accum, uint32_t width, uint32_t height,
+                    const luc_denoise_params* params, GpuAccum* out);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+#endif /* LUC_CUDA_H */

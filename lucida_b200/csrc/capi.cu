@@ -1,0 +1,462 @@
+// The C ABI of liblucida_cuda.so (include/luc_cuda.h): context, scene
+// residency, and the render(scene, camera, spp, bounces) entry point.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include "ctx.cuh"
+
+using namespace luc;
+
+int32_t luc_fail(luc_ctx* c, int32_t code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+int32_t luc_cuda_fail(luc_ctx* c, cudaError_t e, const char* what) {
+    int32_t code = e == cudaErrorMemoryAllocation ? LUC_ERR_OUT_OF_MEMORY : LUC_ERR_LAUNCH;
+    return luc_fail(c, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+// The white-Fresnel single-scattering GGX directional albedo table that the
+// Turquin compensation interpolates (crates/core/src/bsdf.rs:1210-1225,
+// 760-777): 32x32 entries over (roughness, sqrt(cos_o)), each a 128x128
+// midpoint quadrature over the VNDF sampler's unit square, summed in double.
+// Computed once per context on the host, with the same f32 operations (and
+// the same libm) the reference's CPU build uses, so the GPU interpolates the
+// identical table.
+std::vector<float> energy_table_host() {
+    const float PI = 3.14159265358979323846f;
+    auto alpha_of = [](float r) { return std::fmax(r * r, 2.0e-3f); };
+    auto lambda = [](float a, float ct) {
+        float c = std::fabs(ct);
+        if (c >= 1.0f) return 0.0f;
+        float c2 = c * c;
+        float tan2 = (1.0f - c2) / std::fmax(c2, 1.0e-12f);
+        return 0.5f * (-1.0f + std::sqrt(1.0f + a * a * tan2));
+    };
+    auto ggx = [&](float a, float c) {
+        if (c <= 0.0f) return 0.0f;
+        float a2 = a * a, c2 = c * c, s2 = std::fmax(1.0f - c2, 0.0f), den = a2 * c2 + s2;
+        return a2 / (PI * den * den);
+    };
+    std::vector<float> t(32 * 32);
+    for (int ri = 0; ri < 32; ++ri) {
+        float roughness = (float)ri / 31.0f;
+        float a = alpha_of(roughness);
+        for (int ci = 0; ci < 32; ++ci) {
+            float rm = (float)ci / 31.0f;
+            float mu = std::fmax(rm * rm, 1.0e-4f);
+            float st = std::sqrt(std::fmax(1.0f - mu * mu, 0.0f));
+            float wo[3] = {st, 0.0f, mu};
+            double sum = 0.0;
+            for (int i = 0; i < 128; ++i) {
+                for (int j = 0; j < 128; ++j) {
+                    float ux = ((float)i + 0.5f) / 128.0f, uy = ((float)j + 0.5f) / 128.0f;
+                    // sample_ggx_vndf (bsdf.rs:187-216)
+                    float vx = a * wo[0], vy = a * wo[1], vz = wo[2];
+                    float il = 1.0f / std::sqrt(((vx * vx) + (vy * vy)) + (vz * vz));
+                    vx = vx * il; vy = vy * il; vz = vz * il;
+                    float lensq = vx * vx + vy * vy;
+                    float t1x = 1.0f, t1y = 0.0f, t1z = 0.0f;
+                    if (lensq > 0.0f) {
+                        float sl = std::sqrt(lensq);
+                        t1x = -vy / sl; t1y = vx / sl; t1z = 0.0f / sl;
+                    }
+                    float t2x = vy * t1z - t1y * vz, t2y = vz * t1x - t1z * vx, t2z = vx * t1y - t1x * vy;
+                    float r = std::sqrt(ux);
+                    float phi = 2.0f * PI * uy;
+                    float p1 = r * std::cos(phi);
+                    float p2 = r * std::sin(phi);
+                    float s = 0.5f * (1.0f + vz);
+                    p2 = (1.0f - s) * std::sqrt(std::fmax(1.0f - p1 * p1, 0.0f)) + s * p2;
+                    float q = std::sqrt(std::fmax(1.0f - p1 * p1 - p2 * p2, 0.0f));
+                    float nx = p1 * t1x + p2 * t2x + q * vx, ny = p1 * t1y + p2 * t2y + q * vy,
+                          nz = p1 * t1z + p2 * t2z + q * vz;
+                    float mx = a * nx, my = a * ny, mz = std::fmax(nz, 0.0f);
+                    float im = 1.0f / std::sqrt(((mx * mx) + (my * my)) + (mz * mz));
+                    mx = mx * im; my = my * im; mz = mz * im;
+                    // reflect (bsdf.rs:699-701) and specular::sample_single (488-511)
+                    float dm = ((wo[0] * mx) + (wo[1] * my)) + (wo[2] * mz);
+                    float k2 = 2.0f * dm;
+                    float wiz = -wo[2] + k2 * mz;
+                    if (wiz <= 0.0f) continue;
+                    float g1 = 1.0f / (1.0f + lambda(a, mu));
+                    float pdf = g1 * ggx(a, mz) / (4.0f * mu);
+                    if (pdf <= 0.0f) continue;
+                    float g2 = 1.0f / (1.0f + lambda(a, mu) + lambda(a, wiz));
+                    float f = 1.0f + (1.0f - 1.0f) * 0.0f;  // white Schlick: F == 1
+                    sum += (double)(f * (g2 / g1));
+                }
+            }
+            t[ri * 32 + ci] = (float)(sum / (128.0 * 128.0));
+        }
+    }
+    return t;
+}
+
+const std::vector<float>& energy_table_cached() {
+    static std::vector<float> t = energy_table_host();
+    return t;
+}
+
+template <class T>
+cudaError_t upload(DevBuf& b, const T* src, size_t n, cudaStream_t s) {
+    cudaError_t e = b.ensure(n * sizeof(T));
+    if (e != cudaSuccess || n == 0 || !src) return e;
+    return cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t luc_layout_version(void) { return LUC_LAYOUT_VERSION; }
+uint32_t luc_sizeof(uint32_t which) {
+    switch (which) {
+        case 0: return sizeof(GpuMaterial);
+        case 1: return sizeof(GpuPrimitive);
+        case 2: return sizeof(GpuLight);
+        case 3: return sizeof(GpuVertexAttr);
+        case 4: return sizeof(GpuTriangle);
+        case 5: return sizeof(GpuBvhNode);
+        case 6: return sizeof(GpuAccum);
+        case 7: return sizeof(GpuUniforms);
+        case 8: return sizeof(GpuInstance);
+    }
+    return 0;
+}
+
+int32_t luc_create(int32_t device, luc_ctx** out) {
+    if (!out) return LUC_ERR_VALIDATION;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return LUC_ERR_NO_DEVICE;
+    if (device < 0 || device >= count) return LUC_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return LUC_ERR_NO_DEVICE;
+    luc_ctx* c = new luc_ctx();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    c->rs.num_sms = c->num_sms;
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return LUC_ERR_NO_DEVICE;
+    }
+    c->stream = c->own_stream;
+    if (const char* b = std::getenv("LUC_PATH_BUDGET")) c->path_budget = std::strtoull(b, nullptr, 10);
+    const std::vector<float>& et = energy_table_cached();
+    if (upload(c->energy, et.data(), et.size(), c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        cudaStreamDestroy(c->own_stream);
+        delete c;
+        return LUC_ERR_OUT_OF_MEMORY;
+    }
+    *out = c;
+    return LUC_OK;
+}
+
+void luc_destroy(luc_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    DevBuf* bufs[] = {&c->materials, &c->prims,    &c->lights,   &c->positions, &c->attrs,     &c->tris,
+                      &c->nodes,     &c->env_px,   &c->env_cond, &c->env_marg,  &c->env_row_sin, &c->energy,
+                      &c->pool,      &c->accum_tmp, &c->lb_tris, &c->lb_pos,    &c->lb_boxes,  &c->lb_keys,
+                      &c->lb_vals,   &c->lb_keys2, &c->lb_vals2, &c->lb_hist,   &c->lb_karras, &c->lb_parent,
+                      &c->lb_nbounds, &c->lb_subtree, &c->lb_flags, &c->lb_nodes, &c->lb_rank, &c->lb_misc,
+                      &c->lb_icount, &c->lb_look, &c->dn_in,  &c->dn_out,    &c->dn_a,      &c->dn_b,
+                      &c->dn_dev};
+    for (DevBuf* b : bufs) b->release();
+    cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+const char* luc_last_error(const luc_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int32_t luc_set_stream(luc_ctx* c, void* stream) {
+    if (!c) return LUC_ERR_VALIDATION;
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return LUC_OK;
+}
+
+int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) {
+    if (!c || !v) return LUC_ERR_VALIDATION;
+    cudaSetDevice(c->device);
+    if (v->num_materials == 0 || !v->materials) return luc_fail(c, LUC_ERR_VALIDATION, "scene has no materials");
+    if (v->num_primitives && !v->primitives) return luc_fail(c, LUC_ERR_VALIDATION, "null primitives");
+    if (v->num_lights && !v->lights) return luc_fail(c, LUC_ERR_VALIDATION, "null lights");
+    if (v->num_triangles && (!v->triangles || !v->positions || !v->vertex_attrs || v->num_vertices == 0))
+        return luc_fail(c, LUC_ERR_VALIDATION, "triangles without positions/attributes");
+    if (v->num_instances) return luc_fail(c, LUC_ERR_VALIDATION, "instanced scenes are not supported by this build");
+    for (uint32_t i = 0; i < v->num_primitives; ++i)
+        if (v->primitives[i].material >= v->num_materials || v->primitives[i].kind > PRIM_KIND_QUAD)
+            return luc_fail(c, LUC_ERR_VALIDATION, "primitive " + std::to_string(i) + " has a bad kind or material");
+    for (uint32_t i = 0; i < v->num_lights; ++i)
+        if (v->lights[i].material >= v->num_materials)
+            return luc_fail(c, LUC_ERR_VALIDATION, "light " + std::to_string(i) + " has a bad material");
+    for (uint32_t i = 0; i < v->num_triangles; ++i) {
+        const GpuTriangle& t = v->triangles[i];
+        if (t.i0 >= v->num_vertices || t.i1 >= v->num_vertices || t.i2 >= v->num_vertices ||
+            t.material >= v->num_materials)
+            return luc_fail(c, LUC_ERR_VALIDATION, "triangle " + std::to_string(i) + " indexes out of range");
+    }
+    for (uint32_t i = 0; i < v->num_bvh_nodes; ++i) {
+        const GpuBvhNode& n = v->bvh_nodes[i];
+        bool bad = n.count == 0 ? (uint64_t)n.left_first + 1 >= v->num_bvh_nodes
+                                : (uint64_t)n.left_first + n.count > v->num_triangles;
+        if (bad) return luc_fail(c, LUC_ERR_VALIDATION, "bvh node " + std::to_string(i) + " out of range");
+    }
+    if (v->env_width && (!v->env_pixels || !v->env_cdf || v->env_height == 0 ||
+                         v->env_cdf_width < std::max(v->env_width, v->env_height) + 1))
+        return luc_fail(c, LUC_ERR_VALIDATION, "environment map without pixels or a packed CDF");
+    cudaStream_t s = c->stream;
+    c->has_scene = false;
+    LUC_CUDA(c, upload(c->materials, v->materials, v->num_materials, s), "upload materials");
+    LUC_CUDA(c, upload(c->prims, v->primitives, v->num_primitives, s), "upload primitives");
+    LUC_CUDA(c, upload(c->lights, v->lights, v->num_lights, s), "upload lights");
+    LUC_CUDA(c, upload(c->positions, v->positions, 4 * (size_t)v->num_vertices, s), "upload positions");
+    LUC_CUDA(c, upload(c->attrs, v->vertex_attrs, v->num_vertices, s), "upload vertex attrs");
+    uint32_t num_nodes = v->num_bvh_nodes;
+    if (v->num_triangles && v->num_bvh_nodes == 0) {
+        // No caller tree: build an LBVH on the device and reorder our copy of
+        // the triangles into leaf order (Bvh::compact_primitives).
+        LUC_CUDA(c, upload(c->lb_tris, v->triangles, v->num_triangles, s), "upload triangles");
+        int32_t rc = luc_triangle_boxes_device(c, c->lb_tris.as<GpuTriangle>(), c->positions.as<float4>(),
+                                               v->num_triangles);
+        if (rc) return rc;
+        rc = luc_lbvh_device(c, v->num_triangles, &num_nodes);
+        if (rc) return rc;
+        LUC_CUDA(c, c->tris.ensure((size_t)v->num_triangles * sizeof(GpuTriangle)), "alloc triangles");
+        rc = luc_gather_triangles(c, c->lb_tris.as<GpuTriangle>(), c->tris.as<GpuTriangle>(), c->lb_vals.as<uint32_t>(),
+                                  v->num_triangles);
+        if (rc) return rc;
+        LUC_CUDA(c, c->nodes.ensure((size_t)num_nodes * sizeof(GpuBvhNode)), "alloc nodes");
+        LUC_CUDA(c, cudaMemcpyAsync(c->nodes.p, c->lb_nodes.p, (size_t)num_nodes * sizeof(GpuBvhNode),
+                                    cudaMemcpyDeviceToDevice, s), "copy nodes");
+    } else {
+        LUC_CUDA(c, upload(c->tris, v->triangles, v->num_triangles, s), "upload triangles");
+        LUC_CUDA(c, upload(c->nodes, v->bvh_nodes, v->num_bvh_nodes, s), "upload bvh nodes");
+    }
+    // Environment: pixels, the packed CDF split into conditional rows and
+    // the marginal, and the per-row sin(theta) the pdf divides by.
+    std::vector<float> cond, marg, rsin;
+    if (v->env_width) {
+        uint32_t w = v->env_width, h = v->env_height, cw = v->env_cdf_width;
+        cond.resize((size_t)(w + 1) * h);
+        for (uint32_t j = 0; j < h; ++j)
+            std::memcpy(&cond[(size_t)j * (w + 1)], v->env_cdf + (size_t)j * cw, (w + 1) * sizeof(float));
+        marg.assign(v->env_cdf + (size_t)h * cw, v->env_cdf + (size_t)h * cw + h + 1);
+        rsin.resize(h);
+        const float PI = 3.14159265358979323846f;
+        for (uint32_t j = 0; j < h; ++j) rsin[j] = std::sin(((float)j + 0.5f) / (float)h * PI);
+    }
+    LUC_CUDA(c, upload(c->env_px, v->env_pixels, 4 * (size_t)v->env_width * v->env_height, s), "upload env");
+    LUC_CUDA(c, upload(c->env_cond, cond.data(), cond.size(), s), "upload env cdf");
+    LUC_CUDA(c, upload(c->env_marg, marg.data(), marg.size(), s), "upload env marginal");
+    LUC_CUDA(c, upload(c->env_row_sin, rsin.data(), rsin.size(), s), "upload env rows");
+    LUC_CUDA(c, cudaStreamSynchronize(s), "scene upload");
+
+    DevScene& d = c->scene;
+    d.materials = c->materials.as<GpuMaterial>();
+    d.prims = c->prims.as<GpuPrimitive>();
+    d.num_prims = v->num_primitives;
+    d.lights = c->lights.as<GpuLight>();
+    d.num_lights = v->num_lights;
+    d.positions = c->positions.as<float4>();
+    d.attrs = c->attrs.as<GpuVertexAttr>();
+    d.tris = c->tris.as<GpuTriangle>();
+    d.num_tris = v->num_triangles;
+    d.nodes = c->nodes.as<float4>();
+    d.num_nodes = v->num_triangles ? num_nodes : 0;
+    d.env_px = c->env_px.as<float4>();
+    d.env_cond = c->env_cond.as<float>();
+    d.env_marg = c->env_marg.as<float>();
+    d.env_row_sin = c->env_row_sin.as<float>();
+    d.env_w = v->env_width;
+    d.env_h = v->env_width ? v->env_height : 0;
+    d.env_total = v->env_total_weight;
+    d.energy = c->energy.as<float>();
+    d.has_env = v->env_width > 0 && v->env_total_weight > 0.0f;  // EnvMap::is_empty
+    d.light_strategies = v->num_lights + (d.has_env ? 1u : 0u);
+    c->num_materials = v->num_materials;
+    c->has_scene = true;
+    return LUC_OK;
+}
+
+static int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth) {
+    RenderState& rs = c->rs;
+    uint32_t ctrs = kCtrStride * (max_depth + 2);
+    if (paths <= rs.capacity && ctrs <= rs.ctr_capacity) return LUC_OK;
+    paths = std::max(paths, rs.capacity);
+    ctrs = std::max(ctrs, rs.ctr_capacity);
+    const size_t f4 = sizeof(float4);
+    size_t bytes = paths * (11 * f4 + 2 * sizeof(uint32_t)) + ctrs * sizeof(uint32_t) + 16 * 256;
+    LUC_CUDA(c, c->pool.ensure(bytes), "allocate path pool");
+    char* p = (char*)c->pool.p;
+    auto take = [&](size_t n) {
+        char* r = p;
+        p += (n + 255) & ~size_t(255);
+        return r;
+    };
+    PathState& ps = rs.ps;
+    ps.o_pdf = (float4*)take(paths * f4);
+    ps.dir = (float4*)take(paths * f4);
+    ps.thr = (float4*)take(paths * f4);
+    ps.rad = (float4*)take(paths * f4);
+    ps.prev = (float4*)take(paths * f4);
+    ps.hit = (float4*)take(paths * f4);
+    ps.galb = (float4*)take(paths * f4);
+    ps.gnrm = (float4*)take(paths * f4);
+    ps.sh_o = (float4*)take(paths * f4);
+    ps.sh_d = (float4*)take(paths * f4);
+    ps.sh_c = (float4*)take(paths * f4);
+    ps.queue[0] = (uint32_t*)take(paths * 4);
+    ps.queue[1] = (uint32_t*)take(paths * 4);
+    ps.ctr = (uint32_t*)take(ctrs * 4);
+    if ((size_t)(p - (char*)c->pool.p) > c->pool.bytes) return luc_fail(c, LUC_ERR_VALIDATION, "path pool carve");
+    rs.capacity = paths;
+    rs.ctr_capacity = ctrs;
+    return LUC_OK;
+}
+
+int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_depth, uint32_t flags,
+                   GpuAccum* out_host, void* out_dev) {
+    if (!c || !u) return LUC_ERR_VALIDATION;
+    cudaSetDevice(c->device);
+    if (!c->has_scene) return luc_fail(c, LUC_ERR_VALIDATION, "no scene uploaded");
+    if (u->width == 0 || u->height == 0) return luc_fail(c, LUC_ERR_VALIDATION, "zero-sized image");
+    if (spp == 0) return luc_fail(c, LUC_ERR_VALIDATION, "spp must be positive");
+    if (max_depth == 0 || max_depth > 256) return luc_fail(c, LUC_ERR_VALIDATION, "max_depth must be in 1..=256");
+    if ((out_host == nullptr) == (out_dev == nullptr))
+        return luc_fail(c, LUC_ERR_VALIDATION, "exactly one of out_host / out_dev must be given");
+    if ((flags & 0xFFu) != LUC_ARCH_WAVEFRONT) return luc_fail(c, LUC_ERR_VALIDATION, "unknown architecture");
+    if (u->sampling_mode > 2 || u->sampler_kind > 1) return luc_fail(c, LUC_ERR_VALIDATION, "bad sampling mode");
+    const uint64_t pixels = (uint64_t)u->width * u->height;
+    if (pixels > 0xFFFFFFFFull) return luc_fail(c, LUC_ERR_VALIDATION, "image too large");
+    cudaStream_t s = c->stream;
+
+    GpuAccum* accum = (GpuAccum*)out_dev;
+    if (out_host) {
+        LUC_CUDA(c, c->accum_tmp.ensure(pixels * sizeof(GpuAccum)), "allocate accumulator");
+        accum = c->accum_tmp.as<GpuAccum>();
+        LUC_CUDA(c, cudaMemsetAsync(accum, 0, pixels * sizeof(GpuAccum), s), "clear accumulator");
+    }
+    uint64_t per_batch = std::max<uint64_t>(1, std::min<uint64_t>(spp, c->path_budget / pixels));
+    int32_t rc = ensure_pool(c, per_batch * pixels, max_depth);
+    if (rc) return rc;
+
+    FrameParams fp{};
+    fp.pixels = (uint32_t)pixels;
+    fp.width = u->width;
+    fp.height = u->height;
+    fp.frame_seed = u->frame_seed;
+    fp.sampler_kind = u->sampler_kind;
+    fp.sampling = u->sampling_mode;
+    fp.max_depth = max_depth;
+    fp.guides = (flags & LUC_FLAG_NO_GUIDES) ? 0u : 1u;
+    fp.lens_radius = u->lens_radius;
+    fp.cam_origin = ld3(u->cam_origin);
+    fp.cam_upper_left = ld3(u->cam_upper_left);
+    fp.cam_horizontal = ld3(u->cam_horizontal);
+    fp.cam_vertical = ld3(u->cam_vertical);
+    DevScene sc = c->scene;
+    sc.background = ld3(u->background);
+
+    c->stats = luc_render_stats{};
+    c->rs.launches = 0;
+    StageTimer timer;
+    StageTimer* tp = (flags & LUC_FLAG_PROFILE) ? &timer : nullptr;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    for (uint32_t done = 0; done < spp;) {
+        uint32_t n = (uint32_t)std::min<uint64_t>(per_batch, spp - done);
+        fp.sample_base = u->sample_offset + done;
+        fp.batch_samples = n;
+        fp.num_paths = (uint64_t)n * pixels;
+        record_batch(c->rs, sc, fp, accum, s, tp);
+        done += n;
+        c->stats.paths += fp.num_paths;
+    }
+    cudaEventRecord(e1, s);
+    cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) return luc_cuda_fail(c, le, "render launch");
+    if (out_host) {
+        LUC_CUDA(c, cudaMemcpyAsync(out_host, accum, pixels * sizeof(GpuAccum), cudaMemcpyDeviceToHost, s),
+                 "read back accumulator");
+    }
+    cudaError_t se = cudaStreamSynchronize(s);
+    if (se != cudaSuccess) {
+        int32_t code = out_host ? LUC_ERR_READBACK : LUC_ERR_LAUNCH;
+        return luc_fail(c, code, std::string("render: ") + cudaGetErrorString(se));
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->stats.ms_total = ms;
+    c->stats.launches = c->rs.launches;
+    if (tp) {
+        double st[StageTimer::kCount] = {0};
+        tp->collect(st);
+        c->stats.ms_generate = st[StageTimer::kGenerate];
+        c->stats.ms_extend = st[StageTimer::kExtend];
+        c->stats.ms_shade = st[StageTimer::kShade];
+        c->stats.ms_connect = st[StageTimer::kConnect];
+        c->stats.ms_resolve = st[StageTimer::kResolve];
+    }
+    return LUC_OK;
+}
+
+int32_t luc_get_stats(const luc_ctx* c, luc_render_stats* out) {
+    if (!c || !out) return LUC_ERR_VALIDATION;
+    *out = c->stats;
+    return LUC_OK;
+}
+
+}  // extern "C"
+
+// Camera::write_uniforms + integrator::build_uniforms (crates/core/src/
+// camera.rs:344-365, integrator.rs:153-178) for callers that hold a camera
+// rather than baked uniforms. f32 throughout, glibc tanf, no contraction.
+extern "C" int32_t luc_camera_uniforms(const float* eye, const float* look_at, const float* up, float vfov_deg,
+                                       float aperture, float focus_distance, uint32_t width, uint32_t height,
+                                       GpuUniforms* out) {
+    if (!eye || !look_at || !up || !out || width == 0 || height == 0) return LUC_ERR_VALIDATION;
+    auto sub = [](const float* a, const float* b, float* o) { o[0] = a[0] - b[0]; o[1] = a[1] - b[1]; o[2] = a[2] - b[2]; };
+    auto dotf = [](const float* a, const float* b) { return ((a[0] * b[0]) + (a[1] * b[1])) + (a[2] * b[2]); };
+    auto crossf = [](const float* a, const float* b, float* o) {
+        o[0] = a[1] * b[2] - b[1] * a[2];
+        o[1] = a[2] * b[0] - b[2] * a[0];
+        o[2] = a[0] * b[1] - b[0] * a[1];
+    };
+    auto norm = [&](float* a) {
+        float r = 1.0f / std::sqrt(dotf(a, a));
+        a[0] = a[0] * r; a[1] = a[1] * r; a[2] = a[2] * r;
+    };
+    float fwd[3], right[3], upv[3], down[3];
+    sub(look_at, eye, fwd);
+    norm(fwd);
+    crossf(fwd, up, right);
+    norm(right);
+    crossf(right, fwd, upv);
+    down[0] = -upv[0]; down[1] = -upv[1]; down[2] = -upv[2];
+    const float PI = 3.14159265358979323846f;
+    float aspect = (float)width / (float)height;
+    float half_h = std::tan(vfov_deg * (PI / 180.0f) * 0.5f) * focus_distance;
+    float half_w = half_h * aspect;
+    std::memset(out, 0, sizeof(GpuUniforms));
+    for (int k = 0; k < 3; ++k) {
+        out->cam_origin[k] = eye[k];
+        out->cam_horizontal[k] = right[k] * (2.0f * half_w);
+        out->cam_vertical[k] = down[k] * (2.0f * half_h);
+        out->cam_upper_left[k] = ((eye[k] + fwd[k] * focus_distance) - right[k] * half_w) - down[k] * half_h;
+    }
+    out->lens_radius = aperture * 0.5f;
+    out->focus_distance = focus_distance;
+    out->width = width;
+    out->height = height;
+    return LUC_OK;
+}

@@ -1,0 +1,79 @@
+// Shared host/device declarations for the wavefront integrator.
+#pragma once
+#include <algorithm>
+#include <cstdint>
+#include <vector>
+#include "scene_dev.cuh"
+
+namespace luc {
+
+// Per-depth device counters: queue length entering the depth, shadow rays
+// appended at the depth.
+constexpr uint32_t kCtrStride = 4;
+constexpr uint32_t kCtrQueue = 0;
+constexpr uint32_t kCtrShadow = 1;
+
+// SoA path pool, one float4 per field per path (128-bit accesses).
+struct PathState {
+    float4* o_pdf;  // ray origin, prev_bsdf_pdf
+    float4* dir;    // ray direction, -
+    float4* thr;    // throughput, sampler state (u32 bits)
+    float4* rad;    // radiance accumulated along the path
+    float4* prev;   // previous vertex (for the MIS light pdf)
+    float4* hit;    // t, u, v, id (u32 bits)
+    float4* galb;   // first-hit albedo, depth
+    float4* gnrm;   // first-hit shading normal
+    float4* sh_o;   // shadow ray origin, t_max
+    float4* sh_d;   // shadow ray direction, path id (u32 bits)
+    float4* sh_c;   // shadow ray contribution
+    uint32_t* queue[2];
+    uint32_t* ctr;
+};
+
+struct FrameParams {
+    uint64_t num_paths;  // pixels * batch_samples
+    uint32_t pixels, width, height;
+    uint32_t sample_base, batch_samples;
+    uint32_t frame_seed, sampler_kind, sampling, max_depth;
+    uint32_t guides;
+    float lens_radius;
+    V3 cam_origin, cam_upper_left, cam_horizontal, cam_vertical;
+};
+
+// CUDA-event marks between stages, accumulated per stage.
+struct StageTimer {
+    enum Stage { kGenerate = 0, kExtend, kShade, kConnect, kResolve, kEnd, kCount };
+    std::vector<cudaEvent_t> events;
+    std::vector<int> stages;
+    void mark(cudaStream_t s, int stage) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, s);
+        events.push_back(e);
+        stages.push_back(stage);
+    }
+    // Adds the elapsed time of each interval to ms[stage of its start].
+    void collect(double* ms) {
+        for (size_t i = 0; i + 1 < events.size(); ++i) {
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, events[i], events[i + 1]);
+            if (stages[i] < kEnd) ms[stages[i]] += t;
+        }
+        for (auto e : events) cudaEventDestroy(e);
+        events.clear();
+        stages.clear();
+    }
+};
+
+struct RenderState {
+    PathState ps{};
+    uint64_t capacity = 0;  // paths
+    uint32_t ctr_capacity = 0;
+    int num_sms = 148;
+    uint64_t launches = 0;
+};
+
+void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream,
+                  StageTimer* timer);
+
+}  // namespace luc

@@ -1,0 +1,364 @@
+// Wavefront path integrator on sm_100a: GENERATE -> (EXTEND -> SHADE ->
+// CONNECT) x max_depth -> RESOLVE, the stage split of Lucida's
+// crates/gpu/src/wavefront.rs:152-676 with the per-path semantics of the CPU
+// reference integrator (crates/core/src/integrator.rs:209-589).
+//
+// Design (B200-first, not a translation of the WGSL):
+//   * path state is SoA in HBM, one 16-byte float4 per field, so every stage
+//     does 128-bit coalesced loads/stores; the whole spp x pixel pool is in
+//     flight at once when it fits (a 1024^2 x 16 spp frame is 3.4 GB);
+//   * stages are persistent grid-stride kernels sized to the SM count; queue
+//     lengths live on the device and are read by the next stage, so the host
+//     never synchronises inside a frame and the whole frame is captured into
+//     one CUDA graph;
+//   * SHADE compacts survivors and shadow rays with warp-aggregated atomics
+//     (one atomicAdd per warp, ballot + popc for the slot);
+//   * CONNECT adds each shadow ray's contribution into its own path (one
+//     shadow ray per path per bounce), so no atomics and the radiance sum keeps
+//     the CPU's accumulation order: emission(d), NEE(d), emission(d+1), ...;
+//   * RESOLVE sums a pixel's samples in sample order onto the accumulator,
+//     which makes batched and progressive renders bit-identical to one shot.
+#include "render.cuh"
+
+namespace luc {
+
+__device__ __forceinline__ void store4(float4* p, V3 v, float w) { *p = make_float4(v.x, v.y, v.z, w); }
+__device__ __forceinline__ V3 xyz(float4 a) { return V3{a.x, a.y, a.z}; }
+
+// GENERATE (shaders/wavefront/generate.wgsl:35-88; camera.rs:373-405).
+__global__ void __launch_bounds__(256) k_generate(PathState ps, FrameParams fp) {
+    const uint64_t n = fp.num_paths;
+    for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t pixel = (uint32_t)(p % fp.pixels);
+        uint32_t sample = fp.sample_base + (uint32_t)(p / fp.pixels);
+        uint32_t x = pixel % fp.width, y = pixel / fp.width;
+        Sampler smp = make_sampler(fp.sampler_kind, fp.frame_seed, pixel, sample);
+        float pu, pv, lu, lv;
+        smp.next_vec2(pu, pv);
+        smp.next_vec2(lu, lv);
+        float s = ((float)x + pu) / (float)fp.width;
+        float t = ((float)y + pv) / (float)fp.height;
+        V3 origin = fp.cam_origin;
+        V3 target = fp.cam_upper_left + s * fp.cam_horizontal + t * fp.cam_vertical;
+        V3 dir;
+        if (fp.lens_radius <= 0.0f) {
+            dir = normalize(target - origin);
+        } else {
+            float dx, dy;
+            concentric_disk(lu, lv, dx, dy);
+            dx = dx * fp.lens_radius;
+            dy = dy * fp.lens_radius;
+            V3 right = normalize(fp.cam_horizontal), down = normalize(fp.cam_vertical);
+            origin = origin + (right * dx + down * dy);
+            dir = normalize(target - origin);
+        }
+        store4(ps.o_pdf + p, origin, 0.0f);
+        store4(ps.dir + p, dir, 0.0f);
+        ps.thr[p] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(smp.state));
+        ps.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        store4(ps.prev + p, origin, 0.0f);
+        if (fp.guides) {
+            ps.galb[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            ps.gnrm[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+    }
+}
+
+// EXTEND (shaders/wavefront/extend.wgsl:35-68): closest hit per queued path.
+__global__ void __launch_bounds__(128) k_extend(PathState ps, DevScene sc, FrameParams fp, uint32_t depth) {
+    const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
+    const uint32_t* queue = ps.queue[depth & 1];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
+        uint32_t p = depth == 0 ? i : queue[i];
+        float4 o4 = ps.o_pdf[p], d4 = ps.dir[p];
+        float t, u, v;
+        uint32_t id = closest_hit(sc, xyz(o4), xyz(d4), t, u, v);
+        ps.hit[p] = make_float4(t, u, v, __uint_as_float(id));
+    }
+}
+
+// Warp-aggregated append: one atomicAdd per warp. Every lane of the warp must
+// call this (it uses full-warp ballots).
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t mask = __ballot_sync(0xFFFFFFFFu, pred);
+    if (mask == 0) return 0xFFFFFFFFu;
+    uint32_t leader = __ffs(mask) - 1u;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    return pred ? base + (uint32_t)__popc(mask & ((1u << lane) - 1u)) : 0xFFFFFFFFu;
+}
+
+// SHADE (shaders/wavefront/shade.wgsl:119-348), one bounce of
+// integrator.rs:227-400 per queued path.
+__global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameParams fp, uint32_t depth) {
+    const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
+    const uint32_t* queue = ps.queue[depth & 1];
+    uint32_t* next_queue = ps.queue[(depth + 1) & 1];
+    uint32_t* next_len = ps.ctr + (depth + 1) * kCtrStride + kCtrQueue;
+    uint32_t* shadow_len = ps.ctr + depth * kCtrStride + kCtrShadow;
+    const bool last = depth + 1 >= fp.max_depth;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // Warp-uniform trip count so the ballots below see every lane.
+    const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;
+    for (uint32_t base = warp0; base < len; base += stride) {
+        const uint32_t i = base + (threadIdx.x & 31u);
+        bool active = i < len;
+        bool survive = false, cast = false;
+        uint32_t p = 0;
+        V3 sh_o{0, 0, 0}, sh_d{0, 0, 0}, sh_c{0, 0, 0};
+        float sh_t = 0.0f;
+        if (active) {
+            p = depth == 0 ? i : queue[i];
+            float4 o4 = ps.o_pdf[p], d4 = ps.dir[p], h4 = ps.hit[p], t4 = ps.thr[p], r4 = ps.rad[p];
+            V3 dir = xyz(d4), thr = xyz(t4), rad = xyz(r4);
+            float prev_pdf = o4.w;
+            uint32_t id = __float_as_uint(h4.w);
+            uint32_t pixel = (uint32_t)(p % fp.pixels);
+            Sampler smp;
+            smp.kind = fp.sampler_kind;
+            smp.state = __float_as_uint(t4.w);
+            smp.index = fp.sample_base + (uint32_t)(p / fp.pixels);
+            smp.seed = sobol_pixel_seed(pixel, fp.frame_seed);
+            bool rad_changed = false;
+            if (id == kMiss) {
+                // Escaped (integrator.rs:228-263).
+                if (sc.has_env) {
+                    V3 l = env_radiance(sc, dir);
+                    float weight;
+                    if (depth == 0 || fp.sampling == LUC_SAMPLING_BSDF) weight = 1.0f;
+                    else if (fp.sampling == LUC_SAMPLING_NEE) weight = 0.0f;
+                    else {
+                        uint32_t total = max(sc.light_strategies, 1u);
+                        weight = power_heuristic(prev_pdf, env_pdf(sc, dir) / (float)total);
+                    }
+                    if (weight > 0.0f) {
+                        rad = rad + thr * l * weight;
+                        rad_changed = true;
+                    }
+                } else {
+                    rad = rad + thr * sc.background;
+                    rad_changed = true;
+                }
+            } else {
+                V3 org = xyz(o4);
+                SurfaceHit hit = surface_hit(sc, id, h4.x, h4.y, h4.z, org, dir);
+                const GpuMaterial m = sc.materials[hit.material];
+                V3 emissive = ld3(m.emissive);
+                // Emission with MIS (integrator.rs:271-309).
+                if (hit.front && max_elem(emissive) > 0.0f) {
+                    float weight;
+                    if (depth == 0 || fp.sampling == LUC_SAMPLING_BSDF) weight = 1.0f;
+                    else if (fp.sampling == LUC_SAMPLING_NEE) weight = 0.0f;
+                    else {
+                        uint32_t n = sc.num_lights, total = sc.light_strategies;
+                        float pdf_light = 0.0f;
+                        V3 prev = xyz(ps.prev[p]);
+                        if (n != 0 && hit.light_area > 0.0f) {  // light.rs:241-263
+                            V3 tl = hit.position - prev;
+                            float d2 = dot(tl, tl);
+                            if (d2 > 0.0f) {
+                                V3 wi = tl / sqrtf(d2);
+                                float cl = dot(hit.gnormal, -wi);
+                                if (cl > 1.0e-6f) pdf_light = 1.0f / ((float)n * hit.light_area) * d2 / cl;
+                            }
+                        }
+                        pdf_light = pdf_light * ((float)n / (float)max(total, 1u));
+                        weight = power_heuristic(prev_pdf, pdf_light);
+                    }
+                    if (weight > 0.0f) {
+                        rad = rad + thr * emissive * weight;
+                        rad_changed = true;
+                    }
+                }
+                Surface surf = make_surface(m, hit.front);
+                if (depth == 0 && fp.guides) {
+                    V3 alb = vmax(surf.diffuse_albedo + surf.f0 + emissive, splat(1.0e-3f));
+                    store4(ps.galb + p, alb, h4.x);
+                    store4(ps.gnrm + p, hit.normal, 0.0f);
+                }
+                V3 wo = to_local(-dir, hit.normal);
+                if (wo.z > 0.0f) {
+                    // Next event estimation (integrator.rs:349-354, 418-532).
+                    if ((fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) && !last &&
+                        sc.light_strategies > 0) {
+                        float u_sel = smp.next_f32();
+                        float ua, ub;
+                        smp.next_vec2(ua, ub);
+                        uint32_t nl = sc.num_lights, total = sc.light_strategies;
+                        uint32_t pick = min(f2u(u_sel * (float)total), total - 1u);
+                        bool ok = true;
+                        V3 wiw{0, 0, 0}, lrad{0, 0, 0};
+                        float dist = 0.0f, lpdf = 0.0f;
+                        if (pick < nl) {
+                            float u_light = ((float)pick + 0.5f) / (float)nl;
+                            uint32_t idx = min(f2u(u_light * (float)nl), nl - 1u);
+                            const GpuLight L = sc.lights[idx];
+                            V3 lo = ld3(L.origin), eu = ld3(L.edge_u), ev = ld3(L.edge_v);
+                            V3 point;
+                            if (L.kind == LIGHT_KIND_TRIANGLE) {
+                                float su = sqrtf(ua);
+                                float b1 = 1.0f - su, b2 = ub * su;
+                                point = lo + b1 * eu + b2 * ev;
+                            } else {
+                                point = lo + ua * eu + ub * ev;
+                            }
+                            V3 tl = point - hit.position;
+                            float d2 = dot(tl, tl);
+                            if (d2 <= 0.0f) ok = false;
+                            else {
+                                dist = sqrtf(d2);
+                                wiw = tl / dist;
+                                float cl = dot(ld3(L.normal), -wiw);
+                                if (cl <= 1.0e-6f) ok = false;
+                                else {
+                                    float pa = 1.0f / ((float)nl * L.area);
+                                    float pw = pa * d2 / cl;
+                                    if (!isfinite(pw) || pw <= 0.0f) ok = false;
+                                    else {
+                                        lrad = ld3(sc.materials[L.material].emissive);
+                                        lpdf = pw * ((float)nl / (float)total);
+                                    }
+                                }
+                            }
+                        } else {
+                            EnvSample es = env_sample(sc, ua, ub);
+                            if (es.pdf <= 0.0f) ok = false;
+                            else {
+                                wiw = es.dir;
+                                lrad = es.rad;
+                                dist = __int_as_float(0x7f800000);
+                                lpdf = es.pdf / (float)total;
+                            }
+                        }
+                        if (ok && lpdf > 0.0f) {
+                            V3 wi = to_local(wiw, hit.normal);
+                            if (!(wi.z == 0.0f || (wi.z < 0.0f && surf.transmission <= 0.0f))) {
+                                V3 f = bsdf_eval(surf, sc.energy, wo, wi);
+                                if (max_elem(f) > 0.0f) {
+                                    float mis = fp.sampling == LUC_SAMPLING_MIS
+                                                    ? power_heuristic(lpdf, bsdf_pdf(surf, sc.energy, wo, wi))
+                                                    : 1.0f;
+                                    if (mis > 0.0f) {
+                                        sh_o = offset_ray_origin(hit.position, wi.z < 0.0f ? -hit.gnormal : hit.gnormal);
+                                        sh_d = wiw;
+                                        sh_t = dist * (1.0f - 1.0e-3f);
+                                        sh_c = thr * (f * fabsf(wi.z) * lrad * (mis / lpdf));
+                                        cast = true;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    // BSDF sampling (integrator.rs:360-399). Skipped on the last
+                    // bounce, where its result would never be read.
+                    if (!last) {
+                        float u_lobe = smp.next_f32();
+                        float ux, uy;
+                        smp.next_vec2(ux, uy);
+                        BsdfSample bs = bsdf_sample(surf, sc.energy, wo, u_lobe, ux, uy);
+                        if (bs.pdf > 0.0f) {
+                            thr = thr * bs.weight;
+                            if (max_elem(thr) > 0.0f) {
+                                V3 ndir = to_world(bs.wi, hit.normal);
+                                V3 norg = offset_ray_origin(hit.position, bs.wi.z < 0.0f ? -hit.gnormal : hit.gnormal);
+                                store4(ps.o_pdf + p, norg, bs.pdf);
+                                store4(ps.dir + p, ndir, 0.0f);
+                                ps.thr[p] = make_float4(thr.x, thr.y, thr.z, __uint_as_float(smp.state));
+                                store4(ps.prev + p, hit.position, 0.0f);
+                                survive = true;
+                            }
+                        }
+                    }
+                }
+            }
+            if (rad_changed) store4(ps.rad + p, rad, 0.0f);
+        }
+        uint32_t slot = warp_append(next_len, survive);
+        if (survive) next_queue[slot] = p;
+        uint32_t sslot = warp_append(shadow_len, cast);
+        if (cast) {
+            store4(ps.sh_o + sslot, sh_o, sh_t);
+            store4(ps.sh_d + sslot, sh_d, __uint_as_float(p));
+            store4(ps.sh_c + sslot, sh_c, 0.0f);
+        }
+    }
+}
+
+// CONNECT (shaders/wavefront/connect.wgsl:58-84): any-hit shadow rays.
+__global__ void __launch_bounds__(128) k_connect(PathState ps, DevScene sc, uint32_t depth) {
+    const uint32_t len = ps.ctr[depth * kCtrStride + kCtrShadow];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
+        float4 o4 = ps.sh_o[i], d4 = ps.sh_d[i];
+        if (!occluded(sc, xyz(o4), xyz(d4), o4.w)) {
+            uint32_t p = __float_as_uint(d4.w);
+            float4 c4 = ps.sh_c[i], r4 = ps.rad[p];
+            ps.rad[p] = make_float4(r4.x + c4.x, r4.y + c4.y, r4.z + c4.z, 0.0f);
+        }
+    }
+}
+
+// RESOLVE (shaders/wavefront/resolve.wgsl:14-48): per pixel, this batch's
+// samples in sample order, added one at a time onto the accumulator.
+__global__ void __launch_bounds__(256) k_resolve(PathState ps, FrameParams fp, GpuAccum* accum) {
+    for (uint32_t px = blockIdx.x * blockDim.x + threadIdx.x; px < fp.pixels; px += gridDim.x * blockDim.x) {
+        GpuAccum a = accum[px];
+        V3 r = ld3(a.radiance), r2 = ld3(a.radiance_sq), al = ld3(a.albedo), nn = ld3(a.normal);
+        float dep = a.depth;
+        for (uint32_t j = 0; j < fp.batch_samples; ++j) {
+            uint64_t p = (uint64_t)px + (uint64_t)j * fp.pixels;
+            V3 q = xyz(ps.rad[p]);
+            r = r + q;
+            r2 = r2 + q * q;
+            if (fp.guides) {
+                float4 g = ps.galb[p];
+                al = al + xyz(g);
+                dep = dep + g.w;
+                nn = nn + xyz(ps.gnrm[p]);
+            }
+        }
+        a.radiance[0] = r.x; a.radiance[1] = r.y; a.radiance[2] = r.z;
+        a.radiance_sq[0] = r2.x; a.radiance_sq[1] = r2.y; a.radiance_sq[2] = r2.z;
+        a.albedo[0] = al.x; a.albedo[1] = al.y; a.albedo[2] = al.z;
+        a.normal[0] = nn.x; a.normal[1] = nn.y; a.normal[2] = nn.z;
+        a.depth = dep;
+        a.samples = a.samples + (float)fp.batch_samples;
+        accum[px] = a;
+    }
+}
+
+// Host side: record one batch of the frame on `stream` (graph-capturable:
+// fixed launch shapes, device-resident lengths).
+void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream,
+                  StageTimer* timer) {
+    const int sms = rs.num_sms;
+    const uint32_t stride_ctr = kCtrStride * (fp.max_depth + 2);
+    cudaMemsetAsync(rs.ps.ctr, 0, stride_ctr * sizeof(uint32_t), stream);
+    if (timer) timer->mark(stream, StageTimer::kGenerate);
+    {
+        uint64_t blocks = (fp.num_paths + 255) / 256;
+        int grid = (int)std::min<uint64_t>(blocks, (uint64_t)sms * 16);
+        k_generate<<<grid, 256, 0, stream>>>(rs.ps, fp);
+        rs.launches++;
+    }
+    for (uint32_t d = 0; d < fp.max_depth; ++d) {
+        if (timer) timer->mark(stream, StageTimer::kExtend);
+        k_extend<<<sms * 8, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        if (timer) timer->mark(stream, StageTimer::kShade);
+        k_shade<<<sms * 8, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        rs.launches += 2;
+        if (d + 1 < fp.max_depth && (fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) &&
+            sc.light_strategies > 0) {
+            if (timer) timer->mark(stream, StageTimer::kConnect);
+            k_connect<<<sms * 8, 128, 0, stream>>>(rs.ps, sc, d);
+            rs.launches++;
+        }
+    }
+    if (timer) timer->mark(stream, StageTimer::kResolve);
+    k_resolve<<<sms * 8, 256, 0, stream>>>(rs.ps, fp, accum);
+    rs.launches++;
+    if (timer) timer->mark(stream, StageTimer::kEnd);
+}
+
+}  // namespace luc

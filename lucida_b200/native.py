@@ -1,0 +1,131 @@
+"""ctypes binding of liblucida_cuda.so (include/luc_cuda.h).
+
+The library is built in-tree by lucida_b200/build.py. Loading fails loudly
+when it is missing: there is no CPU fallback anywhere in this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import layout as L
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liblucida_cuda.so")
+
+LUC_OK = 0
+ERRORS = {-1: "NoDevice", -2: "Launch", -3: "Readback", -4: "Validation", -5: "OutOfMemory"}
+LUC_FLAG_NO_GUIDES = 0x100
+LUC_FLAG_PROFILE = 0x200
+
+
+class GpuError(RuntimeError):
+    """pt_gpu::GpuError (crates/gpu/src/lib.rs:100-112): `kind` is one of
+    NoDevice, Launch (Shader), Readback, Validation, OutOfMemory."""
+
+    def __init__(self, code: int, message: str):
+        self.code = code
+        self.kind = ERRORS.get(code, f"Unknown({code})")
+        super().__init__(f"{self.kind}: {message}")
+
+
+class SceneView(C.Structure):
+    _fields_ = [("materials", C.c_void_p), ("num_materials", C.c_uint32),
+                ("primitives", C.c_void_p), ("num_primitives", C.c_uint32), ("num_instances", C.c_uint32),
+                ("lights", C.c_void_p), ("num_lights", C.c_uint32),
+                ("positions", C.c_void_p), ("vertex_attrs", C.c_void_p), ("num_vertices", C.c_uint32),
+                ("triangles", C.c_void_p), ("num_triangles", C.c_uint32),
+                ("bvh_nodes", C.c_void_p), ("num_bvh_nodes", C.c_uint32), ("tlas_root", C.c_uint32),
+                ("env_pixels", C.c_void_p), ("env_width", C.c_uint32), ("env_height", C.c_uint32),
+                ("env_cdf", C.c_void_p), ("env_cdf_width", C.c_uint32), ("env_total_weight", C.c_float)]
+
+
+class LbvhOut(C.Structure):
+    _fields_ = [("codes", C.c_void_p), ("order", C.c_void_p), ("karras", C.c_void_p), ("parent", C.c_void_p),
+                ("node_bounds", C.c_void_p), ("subtree_size", C.c_void_p), ("scene_bounds", C.c_void_p),
+                ("nodes", C.c_void_p), ("prim_indices", C.c_void_p), ("num_nodes", C.c_uint32)]
+
+
+class DenoiseParams(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("sigma_normal", C.c_float), ("sigma_depth", C.c_float),
+                ("sigma_luminance", C.c_float), ("sigma_albedo", C.c_float)]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("ms_total", C.c_double), ("ms_generate", C.c_double), ("ms_extend", C.c_double),
+                ("ms_shade", C.c_double), ("ms_connect", C.c_double), ("ms_resolve", C.c_double),
+                ("launches", C.c_uint64), ("rays_extend", C.c_uint64), ("rays_shadow", C.c_uint64),
+                ("paths", C.c_uint64)]
+
+
+# Every entry point include/luc_cuda.h declares, with its ctypes signature.
+_SIGS = {
+    "luc_layout_version": (C.c_uint32, []),
+    "luc_sizeof": (C.c_uint32, [C.c_uint32]),
+    "luc_create": (C.c_int32, [C.c_int32, C.POINTER(C.c_void_p)]),
+    "luc_destroy": (None, [C.c_void_p]),
+    "luc_last_error": (C.c_char_p, [C.c_void_p]),
+    "luc_set_stream": (C.c_int32, [C.c_void_p, C.c_void_p]),
+    "luc_upload_scene": (C.c_int32, [C.c_void_p, C.POINTER(SceneView)]),
+    "luc_render": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+                               C.c_void_p]),
+    "luc_get_stats": (C.c_int32, [C.c_void_p, C.POINTER(RenderStats)]),
+    "luc_camera_uniforms": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float,
+                                        C.c_uint32, C.c_uint32, C.c_void_p]),
+    "luc_lbvh_build": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
+                                   C.POINTER(LbvhOut)]),
+    "luc_lbvh_build_boxes": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(LbvhOut)]),
+    "luc_sort_u32": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "luc_sort_u32_dev": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    "luc_denoise": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(DenoiseParams),
+                                C.c_void_p]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load liblucida_cuda.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m lucida_b200.build` "
+                               "(there is no CPU fallback)")
+        h = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(h, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = h
+    return _lib
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def check(ctx, rc: int):
+    if rc != LUC_OK:
+        msg = lib().luc_last_error(ctx).decode(errors="replace") if ctx else ""
+        raise GpuError(rc, msg)
+
+
+def camera_uniforms(eye, look_at, vfov_deg, width, height, up=(0.0, 1.0, 0.0), aperture=0.0,
+                    focus_distance=None) -> L.Uniforms:
+    e = np.asarray(eye, np.float32)
+    a = np.asarray(look_at, np.float32)
+    u = np.asarray(up, np.float32)
+    if focus_distance is None:  # Camera::look_at (camera.rs:318-327): |look_at - eye| in f32
+        d = (a - e).astype(np.float32)
+        focus_distance = np.float32(np.sqrt(np.float32(np.float32(d[0] * d[0]) + np.float32(d[1] * d[1]))
+                                            + np.float32(d[2] * d[2])))
+    out = L.Uniforms()
+    check(None, lib().luc_camera_uniforms(ptr(e), ptr(a), ptr(u), float(vfov_deg), float(aperture),
+                                          float(focus_distance), int(width), int(height), C.byref(out)))
+    return out
