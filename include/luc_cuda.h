@@ -119,6 +119,8 @@ typedef struct luc_render_stats {
     uint64_t rays_extend;  /* closest-hit rays traced */
     uint64_t rays_shadow;  /* shadow rays traced */
     uint64_t paths;        /* camera paths started */
+    uint64_t nodes_extend, tris_extend; /* BVH node visits / triangle tests, closest hit */
+    uint64_t nodes_shadow, tris_shadow; /* the same for shadow rays */
 } luc_render_stats;
 
 /* Layout contract: returns LUC_LAYOUT_VERSION. */

@@ -165,7 +165,7 @@ void luc_destroy(luc_ctx* c) {
                       &c->pool,      &c->accum_tmp, &c->lb_tris, &c->lb_pos,    &c->lb_boxes,  &c->lb_keys,
                       &c->lb_vals,   &c->lb_keys2, &c->lb_vals2, &c->lb_hist,   &c->lb_karras, &c->lb_parent,
                       &c->lb_nbounds, &c->lb_subtree, &c->lb_flags, &c->lb_nodes, &c->lb_rank, &c->lb_misc,
-                      &c->lb_icount, &c->lb_look, &c->dn_in,  &c->dn_out,    &c->dn_a,      &c->dn_b,
+                      &c->lb_icount, &c->lb_look, &c->lb_codes, &c->dn_in,  &c->dn_out,    &c->dn_a,      &c->dn_b,
                       &c->dn_dev};
     for (DevBuf* b : bufs) b->release();
     cudaStreamDestroy(c->own_stream);
@@ -314,6 +314,7 @@ static int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth) {
     ps.queue[0] = (uint32_t*)take(paths * 4);
     ps.queue[1] = (uint32_t*)take(paths * 4);
     ps.ctr = (uint32_t*)take(ctrs * 4);
+    ps.stat = (unsigned long long*)take(8 * sizeof(unsigned long long));
     if ((size_t)(p - (char*)c->pool.p) > c->pool.bytes) return luc_fail(c, LUC_ERR_VALIDATION, "path pool carve");
     rs.capacity = paths;
     rs.ctr_capacity = ctrs;
@@ -370,6 +371,7 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    cudaMemsetAsync(c->rs.ps.stat, 0, 8 * sizeof(unsigned long long), s);
     cudaEventRecord(e0, s);
     for (uint32_t done = 0; done < spp;) {
         uint32_t n = (uint32_t)std::min<uint64_t>(per_batch, spp - done);
@@ -387,6 +389,8 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
         LUC_CUDA(c, cudaMemcpyAsync(out_host, accum, pixels * sizeof(GpuAccum), cudaMemcpyDeviceToHost, s),
                  "read back accumulator");
     }
+    unsigned long long counts[8] = {0};
+    LUC_CUDA(c, cudaMemcpyAsync(counts, c->rs.ps.stat, sizeof(counts), cudaMemcpyDeviceToHost, s), "read counters");
     cudaError_t se = cudaStreamSynchronize(s);
     if (se != cudaSuccess) {
         int32_t code = out_host ? LUC_ERR_READBACK : LUC_ERR_LAUNCH;
@@ -398,6 +402,12 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     cudaEventDestroy(e1);
     c->stats.ms_total = ms;
     c->stats.launches = c->rs.launches;
+    c->stats.rays_extend = counts[0];
+    c->stats.nodes_extend = counts[1];
+    c->stats.tris_extend = counts[2];
+    c->stats.rays_shadow = counts[3];
+    c->stats.nodes_shadow = counts[4];
+    c->stats.tris_shadow = counts[5];
     if (tp) {
         double st[StageTimer::kCount] = {0};
         tp->collect(st);

@@ -44,7 +44,7 @@ struct luc_ctx {
     uint64_t path_budget = 1ull << 25;
     // LBVH / sort scratch.
     DevBuf lb_tris, lb_pos, lb_boxes, lb_keys, lb_vals, lb_keys2, lb_vals2, lb_hist, lb_karras, lb_parent,
-        lb_nbounds, lb_subtree, lb_flags, lb_nodes, lb_rank, lb_misc, lb_icount, lb_look;
+        lb_nbounds, lb_subtree, lb_flags, lb_nodes, lb_rank, lb_misc, lb_icount, lb_look, lb_codes;
     // Denoiser scratch.
     DevBuf dn_in, dn_out, dn_a, dn_b, dn_dev;
 };

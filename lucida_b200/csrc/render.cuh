@@ -28,6 +28,9 @@ struct PathState {
     float4* sh_c;   // shadow ray contribution
     uint32_t* queue[2];
     uint32_t* ctr;
+    // [0] extend rays, [1] extend node visits, [2] extend triangle tests,
+    // [3] shadow rays, [4] shadow node visits, [5] shadow triangle tests.
+    unsigned long long* stat;
 };
 
 struct FrameParams {

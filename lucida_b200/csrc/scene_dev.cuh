@@ -130,8 +130,11 @@ constexpr uint32_t kMiss = 0xFFFFFFFFu;
 
 // Closest hit over the BVH (bvh.rs:1045-1130): near-child-first with a
 // 64-entry stack, ties resolved toward the later-tested triangle.
+struct TravCount {
+    uint32_t nodes = 0, tris = 0;
+};
 LUC_D bool bvh_closest(const DevScene& s, V3 o, V3 d, float tmin, float& closest, float& bu, float& bv,
-                       uint32_t& btri) {
+                       uint32_t& btri, TravCount& tc) {
     if (s.num_nodes == 0) return false;
     V3 inv = safe_inv_dir(d);
     bool found = false;
@@ -141,7 +144,9 @@ LUC_D bool bvh_closest(const DevScene& s, V3 o, V3 d, float tmin, float& closest
     for (;;) {
         float4 a = __ldg(s.nodes + 2 * node), b = __ldg(s.nodes + 2 * node + 1);
         uint32_t count = __float_as_uint(b.w), lf = __float_as_uint(a.w);
+        tc.nodes++;
         if (count > 0) {
+            tc.tris += count;
             for (uint32_t k = lf; k < lf + count; ++k) {
                 GpuTriangle t = s.tris[k];
                 float th, uh, vh;
@@ -182,7 +187,7 @@ LUC_D bool bvh_closest(const DevScene& s, V3 o, V3 d, float tmin, float& closest
 }
 
 // Any hit within [tmin, tmax] (bvh.rs:1137-1193).
-LUC_D bool bvh_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax) {
+LUC_D bool bvh_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax, TravCount& tc) {
     if (s.num_nodes == 0) return false;
     V3 inv = safe_inv_dir(d);
     uint32_t stack[64];
@@ -191,7 +196,9 @@ LUC_D bool bvh_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax) {
     for (;;) {
         float4 a = __ldg(s.nodes + 2 * node), b = __ldg(s.nodes + 2 * node + 1);
         uint32_t count = __float_as_uint(b.w), lf = __float_as_uint(a.w);
+        tc.nodes++;
         if (count > 0) {
+            tc.tris += count;
             for (uint32_t k = lf; k < lf + count; ++k) {
                 GpuTriangle t = s.tris[k];
                 float th, uh, vh;
@@ -223,7 +230,7 @@ LUC_D bool bvh_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax) {
 
 // Scene::intersect (scene.rs:452-527): analytic primitives by brute force,
 // then triangles bounded by the analytic hit. Returns the id (kMiss on miss).
-LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, float& v) {
+LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, float& v, TravCount& tc) {
     float best_t = kTMax;
     uint32_t id = kMiss;
     for (uint32_t i = 0; i < s.num_prims; ++i) {
@@ -239,7 +246,7 @@ LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, fl
     }
     float bu = 0.0f, bv = 0.0f;
     uint32_t tri;
-    if (bvh_closest(s, o, d, kTMin, best_t, bu, bv, tri)) {
+    if (bvh_closest(s, o, d, kTMin, best_t, bu, bv, tri, tc)) {
         id = tri;
     } else if (s.num_nodes == 0 && s.num_tris > 0) {
         // No BVH: brute force over every triangle (bvh.rs:975-997).
@@ -261,7 +268,7 @@ LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, fl
 }
 
 // Scene::occluded (scene.rs:577-606).
-LUC_D bool occluded(const DevScene& s, V3 o, V3 d, float tmax) {
+LUC_D bool occluded(const DevScene& s, V3 o, V3 d, float tmax, TravCount& tc) {
     for (uint32_t i = 0; i < s.num_prims; ++i) {
         const GpuPrimitive& p = s.prims[i];
         float th;
@@ -278,7 +285,7 @@ LUC_D bool occluded(const DevScene& s, V3 o, V3 d, float tmax) {
         }
         return false;
     }
-    return bvh_any(s, o, d, kTMin, tmax);
+    return bvh_any(s, o, d, kTMin, tmax, tc);
 }
 
 struct SurfaceHit {

@@ -23,6 +23,21 @@
 namespace luc {
 
 __device__ __forceinline__ void store4(float4* p, V3 v, float w) { *p = make_float4(v.x, v.y, v.z, w); }
+
+// One atomic per warp: fold this thread's traversal counters into stat[k..k+2].
+__device__ __forceinline__ void flush_counts(unsigned long long* stat, uint32_t rays, const TravCount& tc) {
+    unsigned long long r = rays, nv = tc.nodes, tt = tc.tris;
+    for (int off = 16; off > 0; off >>= 1) {
+        r += __shfl_down_sync(0xFFFFFFFFu, r, off);
+        nv += __shfl_down_sync(0xFFFFFFFFu, nv, off);
+        tt += __shfl_down_sync(0xFFFFFFFFu, tt, off);
+    }
+    if ((threadIdx.x & 31u) == 0 && r) {
+        atomicAdd(stat + 0, r);
+        atomicAdd(stat + 1, nv);
+        atomicAdd(stat + 2, tt);
+    }
+}
 __device__ __forceinline__ V3 xyz(float4 a) { return V3{a.x, a.y, a.z}; }
 
 // GENERATE (shaders/wavefront/generate.wgsl:35-88; camera.rs:373-405).
@@ -68,13 +83,17 @@ __global__ void __launch_bounds__(256) k_generate(PathState ps, FrameParams fp) 
 __global__ void __launch_bounds__(128) k_extend(PathState ps, DevScene sc, FrameParams fp, uint32_t depth) {
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
     const uint32_t* queue = ps.queue[depth & 1];
+    TravCount tc;
+    uint32_t rays = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
         uint32_t p = depth == 0 ? i : queue[i];
         float4 o4 = ps.o_pdf[p], d4 = ps.dir[p];
         float t, u, v;
-        uint32_t id = closest_hit(sc, xyz(o4), xyz(d4), t, u, v);
+        uint32_t id = closest_hit(sc, xyz(o4), xyz(d4), t, u, v, tc);
         ps.hit[p] = make_float4(t, u, v, __uint_as_float(id));
+        ++rays;
     }
+    flush_counts(ps.stat, rays, tc);
 }
 
 // Warp-aggregated append: one atomicAdd per warp. Every lane of the warp must
@@ -289,14 +308,18 @@ __global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameP
 // CONNECT (shaders/wavefront/connect.wgsl:58-84): any-hit shadow rays.
 __global__ void __launch_bounds__(128) k_connect(PathState ps, DevScene sc, uint32_t depth) {
     const uint32_t len = ps.ctr[depth * kCtrStride + kCtrShadow];
+    TravCount tc;
+    uint32_t rays = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
         float4 o4 = ps.sh_o[i], d4 = ps.sh_d[i];
-        if (!occluded(sc, xyz(o4), xyz(d4), o4.w)) {
+        if (!occluded(sc, xyz(o4), xyz(d4), o4.w, tc)) {
             uint32_t p = __float_as_uint(d4.w);
             float4 c4 = ps.sh_c[i], r4 = ps.rad[p];
             ps.rad[p] = make_float4(r4.x + c4.x, r4.y + c4.y, r4.z + c4.z, 0.0f);
         }
+        ++rays;
     }
+    flush_counts(ps.stat + 3, rays, tc);
 }
 
 // RESOLVE (shaders/wavefront/resolve.wgsl:14-48): per pixel, this batch's

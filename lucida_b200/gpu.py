@@ -107,7 +107,7 @@ class Gpu:
         h = C.c_void_p()
         check(None, self._lib.luc_create(device, C.byref(h)))
         self._h = h
-        self._scene_key = None
+        self._scene = None  # strong reference: an id() could be reused after a free
 
     @property
     def handle(self):
@@ -127,10 +127,10 @@ class Gpu:
     def set_stream(self, stream_handle: int | None):
         check(self._h, self._lib.luc_set_stream(self._h, C.c_void_p(stream_handle or 0)))
 
-    def upload(self, scene: SceneDef):
-        """Make `scene` resident (re-uploads only when it changed)."""
-        key = id(scene)
-        if self._scene_key == key:
+    def upload(self, scene: SceneDef, force: bool = False):
+        """Make `scene` resident. A SceneDef already resident is not sent
+        again unless `force` (use it after mutating the arrays in place)."""
+        if self._scene is scene and not force:
             return
         v = SceneView()
         keep = []
@@ -161,8 +161,9 @@ class Gpu:
             v.env_pixels, v.env_width, v.env_height = ptr(px), w, h
             v.env_cdf, v.env_cdf_width = ptr(cdf), cdf.shape[1]
             v.env_total_weight = float(scene.env_total_weight)
+        self._scene = None
         check(self._h, self._lib.luc_upload_scene(self._h, C.byref(v)))
-        self._scene_key = key
+        self._scene = scene
 
     def stats(self) -> RenderStats:
         s = RenderStats()

@@ -57,7 +57,8 @@ class RenderStats(C.Structure):
     _fields_ = [("ms_total", C.c_double), ("ms_generate", C.c_double), ("ms_extend", C.c_double),
                 ("ms_shade", C.c_double), ("ms_connect", C.c_double), ("ms_resolve", C.c_double),
                 ("launches", C.c_uint64), ("rays_extend", C.c_uint64), ("rays_shadow", C.c_uint64),
-                ("paths", C.c_uint64)]
+                ("paths", C.c_uint64), ("nodes_extend", C.c_uint64), ("tris_extend", C.c_uint64),
+                ("nodes_shadow", C.c_uint64), ("tris_shadow", C.c_uint64)]
 
 
 # Every entry point include/luc_cuda.h declares, with its ctypes signature.

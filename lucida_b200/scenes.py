@@ -82,7 +82,7 @@ def _lattice_hash(ix, iy, iz, seed):
     """Integer lattice hash -> [0, 1): a 32-bit avalanche of the cell
     coordinates and the octave seed (the value-noise lattice of DESIGN.md)."""
     h = (ix.astype(np.uint32) * np.uint32(0x8DA6B343) ^ iy.astype(np.uint32) * np.uint32(0xD8163841)
-         ^ iz.astype(np.uint32) * np.uint32(0xCB1AB31F) ^ np.uint32(seed))
+         ^ iz.astype(np.uint32) * np.uint32(0xCB1AB31F) ^ np.uint32(seed & 0xFFFFFFFF))
     h ^= h >> np.uint32(16)
     h *= np.uint32(0x7FEB352D)
     h ^= h >> np.uint32(15)

@@ -79,7 +79,7 @@ def lib():
         L.orc_scene_get_camera.argtypes = [vp, vp]
         L.orc_scene_get_misc.argtypes = [vp, vp, vp, vp]
         L.orc_build_uniforms.argtypes = [vp, u32, u32, u32, u32, u32, u32, u32, u32, vp]
-        L.orc_render_sums.argtypes = [vp, vp, u32, u32, u32, vp]
+        L.orc_render_sums.argtypes = [vp, vp, u32, u32, u32, u32, vp]
         L.orc_intersect_batch.argtypes = [vp, vp, u32, vp]
         for f in ("orc_pcg_hash", "orc_hash_u32", "orc_expand_bits"):
             getattr(L, f).restype = u32
@@ -229,11 +229,12 @@ class Scene:
                                  sampler, C.byref(u))
         return u
 
-    def render_sums(self, u: Uniforms, threads: int = 0, rows=None) -> np.ndarray:
-        """Per-pixel [radiance sum 3, radiance^2 sum 3, albedo 3, normal 3, depth 1] in sample order."""
+    def render_sums(self, u: Uniforms, threads: int = 0, rows=None, band: int = 32) -> np.ndarray:
+        """Per-pixel [radiance sum 3, radiance^2 sum 3, albedo 3, normal 3, depth 1] in sample order,
+        rows [r0, r1) handed to `threads` workers in `band`-row bands (integrator.rs:635-699 uses 32)."""
         r0, r1 = (0, u.height) if rows is None else rows
         out = np.zeros(((r1 - r0) * u.width, 13), np.float32)
-        lib().orc_render_sums(self._h, C.byref(u), threads, r0, r1, _p(out))
+        lib().orc_render_sums(self._h, C.byref(u), threads, r0, r1, band, _p(out))
         return out
 
     def intersect(self, rays: np.ndarray) -> np.ndarray:

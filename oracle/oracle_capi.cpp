@@ -127,9 +127,10 @@ void orc_build_uniforms(void* h, uint32_t w, uint32_t ht, uint32_t spp, uint32_t
 
 // Per pixel of rows [row0, row1): 13 floats — radiance sum (3), squared
 // radiance sum (3), albedo sum (3), normal sum (3), depth sum (1).
-void orc_render_sums(void* h, const GpuUniforms* u, uint32_t threads, uint32_t row0, uint32_t row1, float* out) {
+void orc_render_sums(void* h, const GpuUniforms* u, uint32_t threads, uint32_t row0, uint32_t row1, uint32_t band,
+                     float* out) {
     std::vector<PixelSums> ps;
-    render_sums(*(Scene*)h, *u, threads, ps, row0, row1);
+    render_sums(*(Scene*)h, *u, threads, ps, row0, row1, band);
     for (size_t i = 0; i < ps.size(); ++i) {
         float* o = out + 13 * i;
         ps[i].radiance.to(o);

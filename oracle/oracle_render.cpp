@@ -317,8 +317,8 @@ Vec3 radiance_with_guide(const Scene& scene, Ray ray, Sampler& rng, uint32_t max
 // kept (not multiplied by 1/spp) so the caller can compare against an
 // accumulator.
 void render_sums(const Scene& s, const GpuUniforms& u, uint32_t threads, std::vector<PixelSums>& out,
-                 uint32_t row0, uint32_t row1) {
-    const uint32_t BAND = 32;
+                 uint32_t row0, uint32_t row1, uint32_t band) {
+    const uint32_t BAND = band == 0 ? 32 : band;
     out.assign((size_t)u.width * (row1 - row0), PixelSums{});
     uint32_t rows = row1 - row0;
     uint32_t num_bands = (rows + BAND - 1) / BAND;

@@ -178,7 +178,7 @@ struct PixelSums {
     float depth;
 };
 void render_sums(const Scene& s, const GpuUniforms& u, uint32_t threads, std::vector<PixelSums>& out,
-                 uint32_t row0, uint32_t row1);
+                 uint32_t row0, uint32_t row1, uint32_t band = 32);
 
 // ---------------------------------------------------------------- denoise.rs
 struct DenoiseParams {
