@@ -178,6 +178,21 @@ int32_t luc_sort_u32(luc_ctx* ctx, const uint32_t* keys, const uint32_t* vals, u
 /* Device-resident variant: sorts keys_dev/vals_dev in place (n pairs). */
 int32_t luc_sort_u32_dev(luc_ctx* ctx, void* keys_dev, void* vals_dev, uint32_t n);
 
+/* Sort without allocating: the variant of luc_sort_u32_dev for callers that
+ * cannot call cudaMalloc (a host that reserves all device memory up front, or
+ * a frame loop where an allocation would synchronise the device). It has no
+ * counterpart in the reference. Sorts n <= luc_sort_u32_static_max() = 2^20
+ * (key, value) pairs of caller device memory in place on `stream` (a
+ * cudaStream_t of the current device; null = the legacy default stream) and
+ * returns when the sort is done. Scratch is a file-scope device array (about
+ * 8.3 MiB, held on every GPU that loads the library until exit), shared by
+ * every call: calls that overlap on the GPU race. The first call on a device
+ * resolves the array's address, so make it before any stream capture.
+ * Larger n returns LUC_ERR_VALIDATION; messages go to err_msg (may be null). */
+int32_t luc_sort_u32_static(void* keys_dev, void* vals_dev, uint32_t n, void* stream, char* err_msg,
+                            uint32_t err_len);
+uint32_t luc_sort_u32_static_max(void);
+
 /* Denoiser::run (crates/gpu/src/denoise.rs:103-210): edge-avoiding à-trous
  * over an accumulator (radiance/albedo/normal/depth sums and samples);
  * writes an Accum-shaped image with samples = 1. Host arrays. */

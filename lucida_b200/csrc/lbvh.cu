@@ -18,6 +18,7 @@
 // which the reference runs on the host after a readback (Lbvh::from_parts),
 // runs on the device here.
 #include "ctx.cuh"
+#include "sort_kernels.cuh"
 
 namespace luc {
 
@@ -137,11 +138,6 @@ __global__ void k_morton(const float* __restrict__ boxes, uint32_t n, const floa
 // input order), publishes per-digit tile counts, and resolves its global
 // prefix by decoupled look-back over the preceding tiles. Tile ids come from
 // an atomic counter, so every tile a block waits on has already started.
-constexpr int kSortThreads = 256;
-constexpr int kSortKpt = 16;
-constexpr uint32_t kTile = kSortThreads * kSortKpt;  // 4096
-constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kCountMask = (1u << 30) - 1u;
-constexpr uint32_t kSpinLimit = 1u << 24;
 
 __global__ void k_hist4(const uint32_t* __restrict__ keys, uint32_t n, uint32_t* __restrict__ hist) {
     __shared__ uint32_t sh[4][256];

@@ -1,0 +1,25 @@
+// The onesweep radix-sort kernels (defined in lbvh.cu), for the files that
+// drive them.
+#pragma once
+#include <cstdint>
+
+namespace luc {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortKpt = 16;
+constexpr uint32_t kTile = kSortThreads * kSortKpt;  // keys per block tile
+constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kCountMask = (1u << 30) - 1u;
+constexpr uint32_t kSpinLimit = 1u << 24;
+
+// Digit histograms of all four 8-bit passes (hist: 4 x 256, zeroed by the caller).
+__global__ void k_hist4(const uint32_t* __restrict__ keys, uint32_t n, uint32_t* __restrict__ hist);
+// Exclusive scan of each pass's 256 counts into offsets (one block of 256 threads).
+__global__ void k_hist_scan(const uint32_t* __restrict__ hist, uint32_t* __restrict__ offsets);
+// One stable pass over digit (key >> shift) & 255; `status` (tiles x 256) and
+// `tile_counter` must be zero on entry; *err is set if a look-back wait gives up.
+__global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                           uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t n, int shift,
+                           const uint32_t* __restrict__ digit_offsets, uint32_t* status, uint32_t* tile_counter,
+                           uint32_t* err);
+
+}  // namespace luc
