@@ -139,6 +139,7 @@ int32_t luc_create(int32_t device, luc_ctx** out) {
     c->device = device;
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
     c->rs.num_sms = c->num_sms;
+    query_occupancy(c->rs);
     if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
         return LUC_ERR_NO_DEVICE;
@@ -162,6 +163,7 @@ void luc_destroy(luc_ctx* c) {
     cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->materials, &c->prims,    &c->lights,   &c->positions, &c->attrs,     &c->tris,
                       &c->nodes,     &c->env_px,   &c->env_cond, &c->env_marg,  &c->env_row_sin, &c->energy,
+                      &c->tnodes,    &c->soup,
                       &c->pool,      &c->accum_tmp, &c->lb_tris, &c->lb_pos,    &c->lb_boxes,  &c->lb_keys,
                       &c->lb_vals,   &c->lb_keys2, &c->lb_vals2, &c->lb_hist,   &c->lb_karras, &c->lb_parent,
                       &c->lb_nbounds, &c->lb_subtree, &c->lb_flags, &c->lb_nodes, &c->lb_rank, &c->lb_misc,
@@ -255,6 +257,10 @@ int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) {
     LUC_CUDA(c, upload(c->env_cond, cond.data(), cond.size(), s), "upload env cdf");
     LUC_CUDA(c, upload(c->env_marg, marg.data(), marg.size(), s), "upload env marginal");
     LUC_CUDA(c, upload(c->env_row_sin, rsin.data(), rsin.size(), s), "upload env rows");
+    if (v->num_triangles && num_nodes) {
+        int32_t rc2 = luc_build_traversal(c, num_nodes, v->num_triangles);
+        if (rc2) return rc2;
+    }
     LUC_CUDA(c, cudaStreamSynchronize(s), "scene upload");
 
     DevScene& d = c->scene;
@@ -269,6 +275,18 @@ int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) {
     d.num_tris = v->num_triangles;
     d.nodes = c->nodes.as<float4>();
     d.num_nodes = v->num_triangles ? num_nodes : 0;
+    d.tnodes = c->tnodes.as<float4>();
+    d.soup = c->soup.as<float4>();
+    d.root_first = 0;
+    d.root_count = 0;
+    if (d.num_nodes) {
+        GpuBvhNode root;
+        LUC_CUDA(c, cudaMemcpy(&root, c->nodes.p, sizeof(root), cudaMemcpyDeviceToHost), "read root");
+        if (root.count > 0) {
+            d.root_first = root.left_first;
+            d.root_count = root.count;
+        }
+    }
     d.env_px = c->env_px.as<float4>();
     d.env_cond = c->env_cond.as<float>();
     d.env_marg = c->env_marg.as<float>();

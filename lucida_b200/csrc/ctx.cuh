@@ -34,6 +34,7 @@ struct luc_ctx {
     int num_sms = 148;
     // Resident scene.
     DevBuf materials, prims, lights, positions, attrs, tris, nodes, env_px, env_cond, env_marg, env_row_sin, energy;
+    DevBuf tnodes, soup;  // traversal layout derived from nodes / tris
     luc::DevScene scene{};
     bool has_scene = false;
     uint32_t num_materials = 0;
@@ -71,6 +72,9 @@ int32_t luc_triangle_boxes_device(luc_ctx* c, const GpuTriangle* tris_dev, const
 int32_t luc_radix_sort_device(luc_ctx* c, uint32_t n);
 // Gather triangles into leaf order on the device: dst[i] = src[order[i]].
 int32_t luc_gather_triangles(luc_ctx* c, const GpuTriangle* src, GpuTriangle* dst, const uint32_t* order, uint32_t n);
+// Implemented in wavefront.cu: derive the traversal layout (child-pair
+// records, triangle soup) from the resident nodes and triangles.
+int32_t luc_build_traversal(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris);
 // Implemented in denoise.cu.
 int32_t luc_denoise_device(luc_ctx* c, const GpuAccum* accum_dev, uint32_t w, uint32_t h,
                            const luc_denoise_params* p, GpuAccum* out_dev);

@@ -12,6 +12,8 @@ namespace luc {
 constexpr uint32_t kCtrStride = 4;
 constexpr uint32_t kCtrQueue = 0;
 constexpr uint32_t kCtrShadow = 1;
+constexpr uint32_t kCtrPullExtend = 2;  // ray-pull cursor of EXTEND at this depth
+constexpr uint32_t kCtrPullConnect = 3;  // ray-pull cursor of CONNECT at this depth
 
 // SoA path pool, one float4 per field per path (128-bit accesses).
 struct PathState {
@@ -73,9 +75,11 @@ struct RenderState {
     uint64_t capacity = 0;  // paths
     uint32_t ctr_capacity = 0;
     int num_sms = 148;
+    int extend_blocks = 0, connect_blocks = 0, shade_blocks = 0;  // resident blocks per SM
     uint64_t launches = 0;
 };
 
+void query_occupancy(RenderState& rs);
 void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream,
                   StageTimer* timer);
 

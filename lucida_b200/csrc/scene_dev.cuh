@@ -18,6 +18,9 @@ struct DevScene {
     uint32_t num_tris;
     const float4* nodes;  // GpuBvhNode as two float4 each
     uint32_t num_nodes;
+    const float4* tnodes;  // child-pair records, 4 float4 per internal node id
+    const float4* soup;    // (p0, e1, e2) per triangle, leaf order
+    uint32_t root_first, root_count;  // the root when it is itself a leaf
     const float4* env_px;
     const float* env_cond;   // (w+1) per row
     const float* env_marg;   // h+1
@@ -128,29 +131,118 @@ LUC_D V3 vtx(const DevScene& s, uint32_t i) {
 constexpr uint32_t kAnalytic = 0x80000000u;
 constexpr uint32_t kMiss = 0xFFFFFFFFu;
 
-// Closest hit over the BVH (bvh.rs:1045-1130): near-child-first with a
-// 64-entry stack, ties resolved toward the later-tested triangle.
 struct TravCount {
     uint32_t nodes = 0, tris = 0;
 };
+
+// Traversal layout, derived on the device from the GpuBvhNode tree:
+//   * child-pair nodes: for each internal node, both children's boxes and
+//     references in one 64-byte record (4 x float4), so descending never
+//     re-reads the node it just tested and one record serves both slab tests;
+//     a reference is (node id, 0) for an internal child or (first triangle,
+//     count) for a leaf;
+//   * a triangle soup in leaf order: (p0, p1 - p0, p2 - p0), the exact
+//     values Möller–Trumbore computes from the indexed vertices, so the test is
+//     bit-identical with three independent loads instead of four dependent ones.
+struct TRef {
+    uint32_t a, cnt;
+};
+constexpr uint32_t kNoNode = 0xFFFFFFFFu;
+
+// Slab tests of both children of a child-pair node. The FMA form
+// (b * inv - o * inv) differs from the reference's (b - o) * inv by a few
+// ULPs; boxes are padded by 1e-6 relative (bvh.rs:100-111), far above that,
+// so no hit is ever culled. Only the visiting order of equal-entry boxes can
+// change, which matters solely for exactly tied triangle distances.
+LUC_D void test_pair(const float4* __restrict__ tn, V3 oi, V3 inv, float tmin, float tmax, bool& h0, bool& h1,
+                     float& e0, float& e1, TRef& r0, TRef& r1) {
+    float4 a = __ldg(tn), b = __ldg(tn + 1), c = __ldg(tn + 2);
+    uint4 r = __ldg(reinterpret_cast<const uint4*>(tn + 3));
+    float lx = __fmaf_rn(a.x, inv.x, -oi.x), hx = __fmaf_rn(a.w, inv.x, -oi.x);
+    float ly = __fmaf_rn(a.y, inv.y, -oi.y), hy = __fmaf_rn(b.x, inv.y, -oi.y);
+    float lz = __fmaf_rn(a.z, inv.z, -oi.z), hz = __fmaf_rn(b.y, inv.z, -oi.z);
+    e0 = fmaxf(fmaxf(fminf(lx, hx), fminf(ly, hy)), fmaxf(fminf(lz, hz), tmin));
+    float x0 = fminf(fminf(fmaxf(lx, hx), fmaxf(ly, hy)), fminf(fmaxf(lz, hz), tmax));
+    lx = __fmaf_rn(b.z, inv.x, -oi.x); hx = __fmaf_rn(c.y, inv.x, -oi.x);
+    ly = __fmaf_rn(b.w, inv.y, -oi.y); hy = __fmaf_rn(c.z, inv.y, -oi.y);
+    lz = __fmaf_rn(c.x, inv.z, -oi.z); hz = __fmaf_rn(c.w, inv.z, -oi.z);
+    e1 = fmaxf(fmaxf(fminf(lx, hx), fminf(ly, hy)), fmaxf(fminf(lz, hz), tmin));
+    float x1 = fminf(fminf(fmaxf(lx, hx), fmaxf(ly, hy)), fminf(fmaxf(lz, hz), tmax));
+    h0 = e0 <= x0;
+    h1 = e1 <= x1;
+    r0 = TRef{r.x, r.y};
+    r1 = TRef{r.z, r.w};
+}
+
+// Möller–Trumbore from (p0, e1, e2) (bvh.rs:930-968, same operation order).
+LUC_D bool hit_soup(const float4* __restrict__ soup, uint32_t k, V3 o, V3 d, float tmin, float tmax, float& tout,
+                    float& uout, float& vout) {
+    float4 q0 = __ldg(soup + 3 * k), q1 = __ldg(soup + 3 * k + 1), q2 = __ldg(soup + 3 * k + 2);
+    V3 p0{q0.x, q0.y, q0.z}, e1{q1.x, q1.y, q1.z}, e2{q2.x, q2.y, q2.z};
+    V3 pv = cross(d, e2);
+    float det = dot(e1, pv);
+    if (fabsf(det) < 1.0e-12f) return false;
+    float inv_det = 1.0f / det;
+    V3 tv = o - p0;
+    float u = dot(tv, pv) * inv_det;
+    if (!(u >= 0.0f && u <= 1.0f)) return false;
+    V3 qv = cross(tv, e1);
+    float v = dot(d, qv) * inv_det;
+    if (v < 0.0f || u + v > 1.0f) return false;
+    float t = dot(e2, qv) * inv_det;
+    if (t < tmin || t > tmax) return false;
+    tout = t;
+    uout = u;
+    vout = v;
+    return true;
+}
+
+// Closest hit (bvh.rs:1045-1130 semantics: the nearest t wins; among exact
+// ties the later-tested triangle). While-while traversal (Aila & Laine):
+// descend internal nodes near-child-first, postponing the first leaf met so
+// lanes of a warp run the node loop and the triangle loop together.
 LUC_D bool bvh_closest(const DevScene& s, V3 o, V3 d, float tmin, float& closest, float& bu, float& bv,
                        uint32_t& btri, TravCount& tc) {
     if (s.num_nodes == 0) return false;
-    V3 inv = safe_inv_dir(d);
+    const V3 inv = safe_inv_dir(d);
+    const V3 oi = V3{o.x * inv.x, o.y * inv.y, o.z * inv.z};
     bool found = false;
-    uint32_t stack[64];
+    TRef stack[64];
     int sp = 0;
-    uint32_t node = 0;
+    TRef cur{0u, 0u}, leaf{0u, 0u};
+    if (s.root_count > 0) {
+        leaf = TRef{s.root_first, s.root_count};
+        cur = TRef{kNoNode, 0u};
+    }
     for (;;) {
-        float4 a = __ldg(s.nodes + 2 * node), b = __ldg(s.nodes + 2 * node + 1);
-        uint32_t count = __float_as_uint(b.w), lf = __float_as_uint(a.w);
-        tc.nodes++;
-        if (count > 0) {
-            tc.tris += count;
-            for (uint32_t k = lf; k < lf + count; ++k) {
-                GpuTriangle t = s.tris[k];
+        while (cur.a != kNoNode && cur.cnt == 0) {
+            bool h0, h1;
+            float e0, e1;
+            TRef r0, r1;
+            test_pair(s.tnodes + 4 * (size_t)cur.a, oi, inv, tmin, closest, h0, h1, e0, e1, r0, r1);
+            tc.nodes++;
+            if (h0 && h1) {
+                bool first = e0 <= e1;
+                if (sp < 64) stack[sp++] = first ? r1 : r0;
+                cur = first ? r0 : r1;
+            } else if (h0) {
+                cur = r0;
+            } else if (h1) {
+                cur = r1;
+            } else {
+                cur = sp > 0 ? stack[--sp] : TRef{kNoNode, 0u};
+            }
+            if (cur.cnt > 0 && leaf.cnt == 0) {
+                leaf = cur;
+                cur = sp > 0 ? stack[--sp] : TRef{kNoNode, 0u};
+            }
+            if (__all_sync(__activemask(), leaf.cnt > 0)) break;
+        }
+        while (leaf.cnt > 0) {
+            tc.tris += leaf.cnt;
+            for (uint32_t k = leaf.a; k < leaf.a + leaf.cnt; ++k) {
                 float th, uh, vh;
-                if (hit_triangle(vtx(s, t.i0), vtx(s, t.i1), vtx(s, t.i2), o, d, tmin, closest, th, uh, vh)) {
+                if (hit_soup(s.soup, k, o, d, tmin, closest, th, uh, vh)) {
                     closest = th;
                     bu = uh;
                     bv = vh;
@@ -158,30 +250,13 @@ LUC_D bool bvh_closest(const DevScene& s, V3 o, V3 d, float tmin, float& closest
                     found = true;
                 }
             }
-        } else {
-            uint32_t c0 = lf;
-            float4 a0 = __ldg(s.nodes + 2 * c0), b0 = __ldg(s.nodes + 2 * c0 + 1);
-            float4 a1 = __ldg(s.nodes + 2 * c0 + 2), b1 = __ldg(s.nodes + 2 * c0 + 3);
-            V3 t0 = (V3{a0.x, a0.y, a0.z} - o) * inv, t1 = (V3{b0.x, b0.y, b0.z} - o) * inv;
-            float e0 = fmaxf(max_elem(vmin(t0, t1)), tmin), x0 = fminf(min_elem(vmax(t0, t1)), closest);
-            V3 u0 = (V3{a1.x, a1.y, a1.z} - o) * inv, u1 = (V3{b1.x, b1.y, b1.z} - o) * inv;
-            float e1 = fmaxf(max_elem(vmin(u0, u1)), tmin), x1 = fminf(min_elem(vmax(u0, u1)), closest);
-            bool h0 = e0 <= x0, h1 = e1 <= x1;
-            if (h0 && h1) {
-                uint32_t nearc = e0 <= e1 ? c0 : c0 + 1, farc = e0 <= e1 ? c0 + 1 : c0;
-                if (sp < 64) stack[sp++] = farc;
-                node = nearc;
-                continue;
-            } else if (h0) {
-                node = c0;
-                continue;
-            } else if (h1) {
-                node = c0 + 1;
-                continue;
+            leaf.cnt = 0;
+            if (cur.a != kNoNode && cur.cnt > 0) {
+                leaf = cur;
+                cur = sp > 0 ? stack[--sp] : TRef{kNoNode, 0u};
             }
         }
-        if (sp == 0) break;
-        node = stack[--sp];
+        if (cur.a == kNoNode) break;
     }
     return found;
 }
@@ -189,42 +264,51 @@ LUC_D bool bvh_closest(const DevScene& s, V3 o, V3 d, float tmin, float& closest
 // Any hit within [tmin, tmax] (bvh.rs:1137-1193).
 LUC_D bool bvh_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax, TravCount& tc) {
     if (s.num_nodes == 0) return false;
-    V3 inv = safe_inv_dir(d);
-    uint32_t stack[64];
+    const V3 inv = safe_inv_dir(d);
+    const V3 oi = V3{o.x * inv.x, o.y * inv.y, o.z * inv.z};
+    TRef stack[64];
     int sp = 0;
-    uint32_t node = 0;
+    TRef cur{0u, 0u}, leaf{0u, 0u};
+    if (s.root_count > 0) {
+        leaf = TRef{s.root_first, s.root_count};
+        cur = TRef{kNoNode, 0u};
+    }
     for (;;) {
-        float4 a = __ldg(s.nodes + 2 * node), b = __ldg(s.nodes + 2 * node + 1);
-        uint32_t count = __float_as_uint(b.w), lf = __float_as_uint(a.w);
-        tc.nodes++;
-        if (count > 0) {
-            tc.tris += count;
-            for (uint32_t k = lf; k < lf + count; ++k) {
-                GpuTriangle t = s.tris[k];
+        while (cur.a != kNoNode && cur.cnt == 0) {
+            bool h0, h1;
+            float e0, e1;
+            TRef r0, r1;
+            test_pair(s.tnodes + 4 * (size_t)cur.a, oi, inv, tmin, tmax, h0, h1, e0, e1, r0, r1);
+            tc.nodes++;
+            if (h0 && h1) {
+                if (sp < 64) stack[sp++] = r1;
+                cur = r0;
+            } else if (h0) {
+                cur = r0;
+            } else if (h1) {
+                cur = r1;
+            } else {
+                cur = sp > 0 ? stack[--sp] : TRef{kNoNode, 0u};
+            }
+            if (cur.cnt > 0 && leaf.cnt == 0) {
+                leaf = cur;
+                cur = sp > 0 ? stack[--sp] : TRef{kNoNode, 0u};
+            }
+            if (__all_sync(__activemask(), leaf.cnt > 0)) break;
+        }
+        while (leaf.cnt > 0) {
+            tc.tris += leaf.cnt;
+            for (uint32_t k = leaf.a; k < leaf.a + leaf.cnt; ++k) {
                 float th, uh, vh;
-                if (hit_triangle(vtx(s, t.i0), vtx(s, t.i1), vtx(s, t.i2), o, d, tmin, tmax, th, uh, vh)) return true;
+                if (hit_soup(s.soup, k, o, d, tmin, tmax, th, uh, vh)) return true;
             }
-        } else {
-            uint32_t c0 = lf;
-            float4 a0 = __ldg(s.nodes + 2 * c0), b0 = __ldg(s.nodes + 2 * c0 + 1);
-            float4 a1 = __ldg(s.nodes + 2 * c0 + 2), b1 = __ldg(s.nodes + 2 * c0 + 3);
-            V3 t0 = (V3{a0.x, a0.y, a0.z} - o) * inv, t1 = (V3{b0.x, b0.y, b0.z} - o) * inv;
-            float e0 = fmaxf(max_elem(vmin(t0, t1)), tmin), x0 = fminf(min_elem(vmax(t0, t1)), tmax);
-            V3 u0 = (V3{a1.x, a1.y, a1.z} - o) * inv, u1 = (V3{b1.x, b1.y, b1.z} - o) * inv;
-            float e1 = fmaxf(max_elem(vmin(u0, u1)), tmin), x1 = fminf(min_elem(vmax(u0, u1)), tmax);
-            bool h0 = e0 <= x0, h1 = e1 <= x1;
-            if (h0) {
-                if (h1 && sp < 64) stack[sp++] = c0 + 1;
-                node = c0;
-                continue;
-            }
-            if (h1) {
-                node = c0 + 1;
-                continue;
+            leaf.cnt = 0;
+            if (cur.a != kNoNode && cur.cnt > 0) {
+                leaf = cur;
+                cur = sp > 0 ? stack[--sp] : TRef{kNoNode, 0u};
             }
         }
-        if (sp == 0) return false;
-        node = stack[--sp];
+        if (cur.a == kNoNode) return false;
     }
 }
 

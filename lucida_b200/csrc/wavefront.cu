@@ -18,7 +18,7 @@
 //     the CPU's accumulation order: emission(d), NEE(d), emission(d+1), ...;
 //   * RESOLVE sums a pixel's samples in sample order onto the accumulator,
 //     which makes batched and progressive renders bit-identical to one shot.
-#include "render.cuh"
+#include "ctx.cuh"
 
 namespace luc {
 
@@ -80,18 +80,31 @@ __global__ void __launch_bounds__(256) k_generate(PathState ps, FrameParams fp) 
 }
 
 // EXTEND (shaders/wavefront/extend.wgsl:35-68): closest hit per queued path.
+// Persistent ray pull: each warp claims 32 queue entries at a time from the
+// depth's cursor until the queue is drained, so fast warps keep taking work
+// instead of idling behind slow ones.
 __global__ void __launch_bounds__(128) k_extend(PathState ps, DevScene sc, FrameParams fp, uint32_t depth) {
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
     const uint32_t* queue = ps.queue[depth & 1];
+    uint32_t* pull = ps.ctr + depth * kCtrStride + kCtrPullExtend;
+    const uint32_t lane = threadIdx.x & 31u;
     TravCount tc;
     uint32_t rays = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
-        uint32_t p = depth == 0 ? i : queue[i];
-        float4 o4 = ps.o_pdf[p], d4 = ps.dir[p];
-        float t, u, v;
-        uint32_t id = closest_hit(sc, xyz(o4), xyz(d4), t, u, v, tc);
-        ps.hit[p] = make_float4(t, u, v, __uint_as_float(id));
-        ++rays;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(pull, 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= len) break;
+        const uint32_t i = base + lane;
+        if (i < len) {
+            uint32_t p = depth == 0 ? i : queue[i];
+            float4 o4 = ps.o_pdf[p], d4 = ps.dir[p];
+            float t, u, v;
+            uint32_t id = closest_hit(sc, xyz(o4), xyz(d4), t, u, v, tc);
+            ps.hit[p] = make_float4(t, u, v, __uint_as_float(id));
+            ++rays;
+        }
+        __syncwarp();
     }
     flush_counts(ps.stat, rays, tc);
 }
@@ -305,19 +318,30 @@ __global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameP
     }
 }
 
-// CONNECT (shaders/wavefront/connect.wgsl:58-84): any-hit shadow rays.
+// CONNECT (shaders/wavefront/connect.wgsl:58-84): any-hit shadow rays, with
+// the same persistent ray pull as EXTEND.
 __global__ void __launch_bounds__(128) k_connect(PathState ps, DevScene sc, uint32_t depth) {
     const uint32_t len = ps.ctr[depth * kCtrStride + kCtrShadow];
+    uint32_t* pull = ps.ctr + depth * kCtrStride + kCtrPullConnect;
+    const uint32_t lane = threadIdx.x & 31u;
     TravCount tc;
     uint32_t rays = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
-        float4 o4 = ps.sh_o[i], d4 = ps.sh_d[i];
-        if (!occluded(sc, xyz(o4), xyz(d4), o4.w, tc)) {
-            uint32_t p = __float_as_uint(d4.w);
-            float4 c4 = ps.sh_c[i], r4 = ps.rad[p];
-            ps.rad[p] = make_float4(r4.x + c4.x, r4.y + c4.y, r4.z + c4.z, 0.0f);
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(pull, 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= len) break;
+        const uint32_t i = base + lane;
+        if (i < len) {
+            float4 o4 = ps.sh_o[i], d4 = ps.sh_d[i];
+            if (!occluded(sc, xyz(o4), xyz(d4), o4.w, tc)) {
+                uint32_t p = __float_as_uint(d4.w);
+                float4 c4 = ps.sh_c[i], r4 = ps.rad[p];
+                ps.rad[p] = make_float4(r4.x + c4.x, r4.y + c4.y, r4.z + c4.z, 0.0f);
+            }
+            ++rays;
         }
-        ++rays;
+        __syncwarp();
     }
     flush_counts(ps.stat + 3, rays, tc);
 }
@@ -351,6 +375,44 @@ __global__ void __launch_bounds__(256) k_resolve(PathState ps, FrameParams fp, G
     }
 }
 
+// Traversal layout (see scene_dev.cuh): child-pair records per internal
+// node and the (p0, e1, e2) triangle soup.
+__global__ void k_make_tnodes(const float4* __restrict__ nodes, uint32_t n, float4* __restrict__ tn) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 b = nodes[2 * i + 1];
+        if (__float_as_uint(b.w) != 0u) continue;  // leaves have no record
+        uint32_t c0 = __float_as_uint(nodes[2 * i].w);
+        float4 a0 = nodes[2 * c0], b0 = nodes[2 * c0 + 1], a1 = nodes[2 * c0 + 2], b1 = nodes[2 * c0 + 3];
+        uint32_t n0 = __float_as_uint(b0.w), n1 = __float_as_uint(b1.w);
+        float4* o = tn + 4 * (size_t)i;
+        o[0] = make_float4(a0.x, a0.y, a0.z, b0.x);
+        o[1] = make_float4(b0.y, b0.z, a1.x, a1.y);
+        o[2] = make_float4(a1.z, b1.x, b1.y, b1.z);
+        uint4 r = make_uint4(n0 ? __float_as_uint(a0.w) : c0, n0, n1 ? __float_as_uint(a1.w) : c0 + 1, n1);
+        reinterpret_cast<uint4*>(o)[3] = r;
+    }
+}
+__global__ void k_make_soup(const GpuTriangle* __restrict__ tris, const float4* __restrict__ pos, uint32_t n,
+                            float4* __restrict__ soup) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        GpuTriangle t = tris[k];
+        float4 p0 = pos[t.i0], p1 = pos[t.i1], p2 = pos[t.i2];
+        soup[3 * (size_t)k] = make_float4(p0.x, p0.y, p0.z, 0.0f);
+        soup[3 * (size_t)k + 1] = make_float4(p1.x - p0.x, p1.y - p0.y, p1.z - p0.z, 0.0f);
+        soup[3 * (size_t)k + 2] = make_float4(p2.x - p0.x, p2.y - p0.y, p2.z - p0.z, 0.0f);
+    }
+}
+
+void query_occupancy(RenderState& rs) {
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend, 128, 0);
+    rs.extend_blocks = b > 0 ? b : 8;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_connect, 128, 0);
+    rs.connect_blocks = b > 0 ? b : 8;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade, 128, 0);
+    rs.shade_blocks = b > 0 ? b : 8;
+}
+
 // Host side: record one batch of the frame on `stream` (graph-capturable:
 // fixed launch shapes, device-resident lengths).
 void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream,
@@ -367,14 +429,14 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
     }
     for (uint32_t d = 0; d < fp.max_depth; ++d) {
         if (timer) timer->mark(stream, StageTimer::kExtend);
-        k_extend<<<sms * 8, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        k_extend<<<sms * rs.extend_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
         if (timer) timer->mark(stream, StageTimer::kShade);
-        k_shade<<<sms * 8, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        k_shade<<<sms * rs.shade_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
         rs.launches += 2;
         if (d + 1 < fp.max_depth && (fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) &&
             sc.light_strategies > 0) {
             if (timer) timer->mark(stream, StageTimer::kConnect);
-            k_connect<<<sms * 8, 128, 0, stream>>>(rs.ps, sc, d);
+            k_connect<<<sms * rs.connect_blocks, 128, 0, stream>>>(rs.ps, sc, d);
             rs.launches++;
         }
     }
@@ -385,3 +447,16 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
 }
 
 }  // namespace luc
+
+int32_t luc_build_traversal(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris) {
+    using namespace luc;
+    LUC_CUDA(c, c->tnodes.ensure((size_t)num_nodes * 64), "alloc traversal nodes");
+    LUC_CUDA(c, c->soup.ensure((size_t)num_tris * 48), "alloc triangle soup");
+    int g1 = (int)std::min<uint64_t>((num_nodes + 255) / 256, (uint64_t)c->num_sms * 32);
+    int g2 = (int)std::min<uint64_t>((num_tris + 255) / 256, (uint64_t)c->num_sms * 32);
+    k_make_tnodes<<<g1, 256, 0, c->stream>>>(c->nodes.as<float4>(), num_nodes, c->tnodes.as<float4>());
+    k_make_soup<<<g2, 256, 0, c->stream>>>(c->tris.as<GpuTriangle>(), c->positions.as<float4>(), num_tris,
+                                           c->soup.as<float4>());
+    LUC_CUDA(c, cudaGetLastError(), "traversal layout");
+    return LUC_OK;
+}
