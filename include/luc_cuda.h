@@ -178,6 +178,21 @@ int32_t luc_sort_u32(luc_ctx* ctx, const uint32_t* keys, const uint32_t* vals, u
 /* Device-resident variant: sorts keys_dev/vals_dev in place (n pairs). */
 int32_t luc_sort_u32_dev(luc_ctx* ctx, void* keys_dev, void* vals_dev, uint32_t n);
 
+/* Per-function device evaluation, as Lucida's shader eval harness
+ * (crates/gpu/src/eval.rs, shaders/test/eval_bsdf.wgsl) does for WGSL.
+ * luc_eval_bsdf: material `m` seen from the front (front != 0) or back.
+ *   mode 0 = surface::sample (bsdf.rs:1571-1661): in3 = (u_lobe, u.x, u.y),
+ *            outputs wi, weight (f|cos|/pdf) and pdf;
+ *   mode 1 = surface::eval + surface::pdf at (wo, wi = in3): outputs f, pdf.
+ * luc_eval_env: the resident scene's environment map.
+ *   mode 0 = EnvMap::sample (envmap.rs:235-275): in = u (2 floats), outputs
+ *            direction, radiance, pdf;
+ *   mode 1 = EnvMap::radiance + pdf at direction in (3 floats).
+ * n entries, host arrays, 3 floats per vector. */
+int32_t luc_eval_bsdf(luc_ctx* ctx, const GpuMaterial* m, int32_t front, const float* wo3, const float* in3,
+                      uint32_t n, int32_t mode, float* out_wi3, float* out_f3, float* out_pdf);
+int32_t luc_eval_env(luc_ctx* ctx, const float* in, uint32_t n, int32_t mode, float* dir3, float* rad3, float* pdf);
+
 /* Sort without allocating: the variant of luc_sort_u32_dev for callers that
  * cannot call cudaMalloc (a host that reserves all device memory up front, or
  * a frame loop where an allocation would synchronise the device). It has no

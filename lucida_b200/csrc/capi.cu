@@ -146,6 +146,7 @@ int32_t luc_create(int32_t device, luc_ctx** out) {
     }
     c->stream = c->own_stream;
     if (const char* b = std::getenv("LUC_PATH_BUDGET")) c->path_budget = std::strtoull(b, nullptr, 10);
+    if (const char* g = std::getenv("LUC_NO_GRAPHS")) c->use_graphs = g[0] == '\0' || g[0] == '0';
     const std::vector<float>& et = energy_table_cached();
     if (upload(c->energy, et.data(), et.size(), c->stream) != cudaSuccess ||
         cudaStreamSynchronize(c->stream) != cudaSuccess) {
@@ -170,6 +171,8 @@ void luc_destroy(luc_ctx* c) {
                       &c->lb_icount, &c->lb_look, &c->lb_codes, &c->dn_in,  &c->dn_out,    &c->dn_a,      &c->dn_b,
                       &c->dn_dev};
     for (DevBuf* b : bufs) b->release();
+    if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
+    c->graph.timer.release();
     cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -299,6 +302,7 @@ int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) {
     d.light_strategies = v->num_lights + (d.has_env ? 1u : 0u);
     c->num_materials = v->num_materials;
     c->has_scene = true;
+    c->scene_version++;
     return LUC_OK;
 }
 
@@ -391,14 +395,53 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     cudaEventCreate(&e1);
     cudaMemsetAsync(c->rs.ps.stat, 0, 8 * sizeof(unsigned long long), s);
     cudaEventRecord(e0, s);
-    for (uint32_t done = 0; done < spp;) {
-        uint32_t n = (uint32_t)std::min<uint64_t>(per_batch, spp - done);
-        fp.sample_base = u->sample_offset + done;
-        fp.batch_samples = n;
-        fp.num_paths = (uint64_t)n * pixels;
-        record_batch(c->rs, sc, fp, accum, s, tp);
-        done += n;
+    const bool one_batch = per_batch >= spp;
+    if (one_batch && c->use_graphs) {
+        // Single-batch frame: capture it once as a CUDA graph and replay it
+        // while the frame parameters, scene, pool and accumulator repeat.
+        fp.sample_base = u->sample_offset;
+        fp.batch_samples = spp;
+        fp.num_paths = (uint64_t)spp * pixels;
+        std::vector<unsigned char> key(sizeof(FrameParams) + sizeof(DevScene) + 4 * sizeof(uint64_t));
+        uint64_t extra[4] = {(uint64_t)(uintptr_t)accum, c->scene_version, (uint64_t)(uintptr_t)c->rs.ps.o_pdf,
+                             (uint64_t)(tp != nullptr)};
+        std::memcpy(key.data(), &fp, sizeof(FrameParams));
+        std::memcpy(key.data() + sizeof(FrameParams), &sc, sizeof(DevScene));
+        std::memcpy(key.data() + sizeof(FrameParams) + sizeof(DevScene), extra, sizeof(extra));
+        FrameGraph& g = c->graph;
+        if (g.exec == nullptr || g.key != key) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+            g.timer.release();
+            cudaGraph_t graph = nullptr;
+            uint64_t before = c->rs.launches;
+            LUC_CUDA(c, cudaStreamBeginCapture(c->own_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            record_batch(c->rs, sc, fp, accum, c->own_stream, tp ? &g.timer : nullptr);
+            LUC_CUDA(c, cudaStreamEndCapture(c->own_stream, &graph), "end capture");
+            cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ie != cudaSuccess) {
+                g.exec = nullptr;
+                return luc_cuda_fail(c, ie, "instantiate frame graph");
+            }
+            g.launches = c->rs.launches - before;
+            c->rs.launches = before;
+            g.key = key;
+            g.profiled = tp != nullptr;
+        }
+        LUC_CUDA(c, cudaGraphLaunch(g.exec, s), "launch frame graph");
+        c->rs.launches += g.launches;
         c->stats.paths += fp.num_paths;
+    } else {
+        for (uint32_t done = 0; done < spp;) {
+            uint32_t n = (uint32_t)std::min<uint64_t>(per_batch, spp - done);
+            fp.sample_base = u->sample_offset + done;
+            fp.batch_samples = n;
+            fp.num_paths = (uint64_t)n * pixels;
+            record_batch(c->rs, sc, fp, accum, s, tp);
+            done += n;
+            c->stats.paths += fp.num_paths;
+        }
     }
     cudaEventRecord(e1, s);
     cudaError_t le = cudaGetLastError();
@@ -428,7 +471,8 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     c->stats.tris_shadow = counts[5];
     if (tp) {
         double st[StageTimer::kCount] = {0};
-        tp->collect(st);
+        if (one_batch && c->use_graphs) c->graph.timer.accumulate(st);
+        else tp->collect(st);
         c->stats.ms_generate = st[StageTimer::kGenerate];
         c->stats.ms_extend = st[StageTimer::kExtend];
         c->stats.ms_shade = st[StageTimer::kShade];

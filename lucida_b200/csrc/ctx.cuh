@@ -26,8 +26,21 @@ struct DevBuf {
     T* as() const { return (T*)p; }
 };
 
+// One captured frame: the whole GENERATE..RESOLVE sequence of a single-batch
+// render as a CUDA graph, replayed while the frame's parameters repeat.
+struct FrameGraph {
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec = nullptr;
+    luc::StageTimer timer;  // event nodes inside the graph (profiled frames)
+    uint64_t launches = 0;
+    bool profiled = false;
+};
+
 struct luc_ctx {
     int device = 0;
+    uint64_t scene_version = 0;
+    FrameGraph graph;
+    bool use_graphs = true;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     std::string err;

@@ -58,15 +58,21 @@ struct StageTimer {
         stages.push_back(stage);
     }
     // Adds the elapsed time of each interval to ms[stage of its start].
-    void collect(double* ms) {
+    void accumulate(double* ms) const {
         for (size_t i = 0; i + 1 < events.size(); ++i) {
             float t = 0.0f;
             cudaEventElapsedTime(&t, events[i], events[i + 1]);
             if (stages[i] < kEnd) ms[stages[i]] += t;
         }
+    }
+    void release() {
         for (auto e : events) cudaEventDestroy(e);
         events.clear();
         stages.clear();
+    }
+    void collect(double* ms) {
+        accumulate(ms);
+        release();
     }
 };
 

@@ -80,6 +80,10 @@ _SIGS = {
     "luc_lbvh_build_boxes": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(LbvhOut)]),
     "luc_sort_u32": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     "luc_sort_u32_dev": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    "luc_eval_bsdf": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_uint32,
+                                  C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "luc_eval_env": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p, C.c_void_p,
+                                 C.c_void_p]),
     "luc_sort_u32_static": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_char_p,
                                         C.c_uint32]),
     "luc_sort_u32_static_max": (C.c_uint32, []),
