@@ -45,6 +45,12 @@ extern "C" {
 #define LUC_FLAG_NO_GUIDES 0x100u
 /* Record per-stage CUDA events during the render (luc_get_stats). */
 #define LUC_FLAG_PROFILE 0x200u
+/* Learned path guiding (no reference counterpart): one-sample MIS between
+ * the BSDF and the guide's vMF mixture (fraction 0.5 each) at opaque,
+ * non-specular vertices, with the mixture pdf in both MIS sites; after each
+ * batch of samples the guide takes one Adam step on the batch's records
+ * (luc_guide_configure). Requires luc_guide_init. */
+#define LUC_FLAG_GUIDED 0x400u
 
 typedef struct luc_ctx luc_ctx;
 
@@ -121,6 +127,7 @@ typedef struct luc_render_stats {
     uint64_t paths;        /* camera paths started */
     uint64_t nodes_extend, tris_extend; /* BVH node visits / triangle tests, closest hit */
     uint64_t nodes_shadow, tris_shadow; /* the same for shadow rays */
+    double ms_guide, ms_train; /* guide inference and training (LUC_FLAG_GUIDED) */
 } luc_render_stats;
 
 /* Layout contract: returns LUC_LAYOUT_VERSION. */
@@ -207,6 +214,50 @@ int32_t luc_eval_env(luc_ctx* ctx, const float* in, uint32_t n, int32_t mode, fl
 int32_t luc_sort_u32_static(void* keys_dev, void* vals_dev, uint32_t n, void* stream, char* err_msg,
                             uint32_t err_len);
 uint32_t luc_sort_u32_static_max(void);
+
+/* ---- Learned path-guiding proposal (no reference counterpart) ----
+ * Model: frequency-encoded position (12 frequencies per axis over the guide's
+ * box), shading normal and outgoing direction (4 each), 120 features padded to
+ * 128 -> 64 -> 64 -> 64 -> 40 ReLU MLP, BF16 weights and FP32 accumulation on
+ * the tensor cores; outputs 8 vMF lobes (direction, kappa = min(1 +
+ * softplus, 1e4), softmax weight). Parameters: kGParams = 19176 floats in the
+ * order W1[64][128], b1[64], W2[64][64], b2, W3[64][64], b3, W4[40][64], b4[40].
+ * Training: loss -sum F log q(wi) / sum F over path-vertex records, Adam
+ * (0.9, 0.999, 1e-8). */
+typedef struct luc_guide_info {
+    uint32_t steps;        /* Adam steps taken */
+    uint32_t last_records; /* records in the last step */
+    float last_loss;       /* loss of the last step */
+    uint32_t threshold;    /* current recording fraction, out of 65536 */
+    uint32_t num_params;   /* 19176 */
+} luc_guide_info;
+
+/* Initialise the guide: params (num_params floats) or, when null, a seeded
+ * uniform +-sqrt(6 / (fan_in + fan_out)) initialisation; the position box
+ * lo/hi (3 floats each) or, when both are null, the uploaded scene's bounds.
+ * Resets the Adam state. */
+int32_t luc_guide_init(luc_ctx* ctx, const float* params, uint64_t seed, const float* lo, const float* hi);
+/* train != 0: one Adam step after every batch of a LUC_FLAG_GUIDED render on
+ * up to records_per_step path vertices (default 2^18), learning rate lr
+ * (default 1e-2). train == 0 renders with the guide frozen. */
+int32_t luc_guide_configure(luc_ctx* ctx, uint32_t train, uint32_t records_per_step, float lr);
+int32_t luc_guide_get_params(luc_ctx* ctx, float* out);
+int32_t luc_guide_stats(luc_ctx* ctx, luc_guide_info* out);
+/* Raw network outputs (40 floats per row) for rows of 9 floats: position,
+ * shading normal, outgoing direction. Host arrays. */
+int32_t luc_guide_forward(luc_ctx* ctx, const float* in9, uint32_t n, float* out40);
+/* Host training records, 20 floats each: position, F, normal, -, outgoing
+ * direction, -, sampled direction, -, 4 unused. steps == 0: the gradient of
+ * the loss (num_params floats into grad_out) at the current parameters, which
+ * stay unchanged; steps > 0: that many Adam steps on these records. loss_out
+ * (may be null) receives the loss of the last evaluation. */
+int32_t luc_guide_train_records(luc_ctx* ctx, const float* records, uint32_t n, uint32_t steps, float* grad_out,
+                                float* loss_out);
+/* vMF mixture of given raw outputs (40 floats per row): mode 0 samples it
+ * with in3 = 3 uniforms per row (lobe choice, then the lobe) into dir3 and
+ * its pdf; mode 1 evaluates the pdf at the unit directions in3. */
+int32_t luc_guide_mixture(luc_ctx* ctx, const float* raw40, const float* in3, uint32_t n, int32_t mode, float* dir3,
+                          float* pdf);
 
 /* Denoiser::run (crates/gpu/src/denoise.rs:103-210): edge-avoiding à-trous
  * over an accumulator (radiance/albedo/normal/depth sums and samples);

@@ -169,7 +169,8 @@ void luc_destroy(luc_ctx* c) {
                       &c->lb_vals,   &c->lb_keys2, &c->lb_vals2, &c->lb_hist,   &c->lb_karras, &c->lb_parent,
                       &c->lb_nbounds, &c->lb_subtree, &c->lb_flags, &c->lb_nodes, &c->lb_rank, &c->lb_misc,
                       &c->lb_icount, &c->lb_look, &c->lb_codes, &c->dn_in,  &c->dn_out,    &c->dn_a,      &c->dn_b,
-                      &c->dn_dev};
+                      &c->dn_dev,    &c->g_params, &c->g_m,     &c->g_v,       &c->g_grad,    &c->g_wbf,
+                      &c->g_bias,    &c->g_misc,   &c->g_lobes, &c->g_rec,     &c->g_io};
     for (DevBuf* b : bufs) b->release();
     if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
     c->graph.timer.release();
@@ -215,6 +216,38 @@ int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) {
     if (v->env_width && (!v->env_pixels || !v->env_cdf || v->env_height == 0 ||
                          v->env_cdf_width < std::max(v->env_width, v->env_height) + 1))
         return luc_fail(c, LUC_ERR_VALIDATION, "environment map without pixels or a packed CDF");
+    // Scene bounds (the guide's default position box): vertices, spheres,
+    // quad corners.
+    {
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        auto grow = [&](float x, float y, float z) {
+            const float q[3] = {x, y, z};
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = std::min(lo[a], q[a]);
+                hi[a] = std::max(hi[a], q[a]);
+            }
+        };
+        for (uint32_t i = 0; i < v->num_vertices && v->num_triangles; ++i)
+            grow(v->positions[4 * i], v->positions[4 * i + 1], v->positions[4 * i + 2]);
+        for (uint32_t i = 0; i < v->num_primitives; ++i) {
+            const GpuPrimitive& p = v->primitives[i];
+            const float* o = p.position;
+            if (p.kind == PRIM_KIND_QUAD) {
+                for (int k = 0; k < 4; ++k) {
+                    float su = (k & 1) ? 1.0f : 0.0f, sv = (k & 2) ? 1.0f : 0.0f;
+                    grow(o[0] + su * p.edge_u[0] + sv * p.edge_v[0], o[1] + su * p.edge_u[1] + sv * p.edge_v[1],
+                         o[2] + su * p.edge_u[2] + sv * p.edge_v[2]);
+                }
+            } else {
+                grow(o[0] - p.radius, o[1] - p.radius, o[2] - p.radius);
+                grow(o[0] + p.radius, o[1] + p.radius, o[2] + p.radius);
+            }
+        }
+        for (int a = 0; a < 3; ++a) {
+            c->scene_lo[a] = lo[a] <= hi[a] ? lo[a] : 0.0f;
+            c->scene_hi[a] = lo[a] <= hi[a] ? hi[a] : 1.0f;
+        }
+    }
     cudaStream_t s = c->stream;
     c->has_scene = false;
     LUC_CUDA(c, upload(c->materials, v->materials, v->num_materials, s), "upload materials");
@@ -354,6 +387,11 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     if ((out_host == nullptr) == (out_dev == nullptr))
         return luc_fail(c, LUC_ERR_VALIDATION, "exactly one of out_host / out_dev must be given");
     if ((flags & 0xFFu) != LUC_ARCH_WAVEFRONT) return luc_fail(c, LUC_ERR_VALIDATION, "unknown architecture");
+    if (flags & ~(0xFFu | LUC_FLAG_NO_GUIDES | LUC_FLAG_PROFILE | LUC_FLAG_GUIDED))
+        return luc_fail(c, LUC_ERR_VALIDATION, "unknown render flag");
+    const bool guided = (flags & LUC_FLAG_GUIDED) != 0;
+    if (guided && !c->guide_ready)
+        return luc_fail(c, LUC_ERR_VALIDATION, "LUC_FLAG_GUIDED needs luc_guide_init first");
     if (u->sampling_mode > 2 || u->sampler_kind > 1) return luc_fail(c, LUC_ERR_VALIDATION, "bad sampling mode");
     const uint64_t pixels = (uint64_t)u->width * u->height;
     if (pixels > 0xFFFFFFFFull) return luc_fail(c, LUC_ERR_VALIDATION, "image too large");
@@ -368,6 +406,14 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     uint64_t per_batch = std::max<uint64_t>(1, std::min<uint64_t>(spp, c->path_budget / pixels));
     int32_t rc = ensure_pool(c, per_batch * pixels, max_depth);
     if (rc) return rc;
+    if (guided) {
+        rc = luc_guide_prepare_frame(c, c->rs.capacity);
+        if (rc) return rc;
+        c->rs.ps.lobes = c->g_lobes.as<float4>();
+        c->rs.ps.rec = c->g_rec.as<float4>();
+        c->rs.ps.gmisc = c->g_misc.as<uint32_t>();
+    }
+    const GuideTrain gt = guided ? luc_guide_train_state(c) : GuideTrain{};
 
     FrameParams fp{};
     fp.pixels = (uint32_t)pixels;
@@ -378,6 +424,11 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     fp.sampling = u->sampling_mode;
     fp.max_depth = max_depth;
     fp.guides = (flags & LUC_FLAG_NO_GUIDES) ? 0u : 1u;
+    if (guided) {
+        fp.guided = 1u;
+        fp.rec_cap = c->guide_train ? c->guide_rec_cap : 0u;
+        fp.guide = luc_guide_dev(c);
+    }
     fp.lens_radius = u->lens_radius;
     fp.cam_origin = ld3(u->cam_origin);
     fp.cam_upper_left = ld3(u->cam_upper_left);
@@ -402,9 +453,14 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
         fp.sample_base = u->sample_offset;
         fp.batch_samples = spp;
         fp.num_paths = (uint64_t)spp * pixels;
-        std::vector<unsigned char> key(sizeof(FrameParams) + sizeof(DevScene) + 4 * sizeof(uint64_t));
-        uint64_t extra[4] = {(uint64_t)(uintptr_t)accum, c->scene_version, (uint64_t)(uintptr_t)c->rs.ps.o_pdf,
-                             (uint64_t)(tp != nullptr)};
+        uint32_t lr_bits = 0;
+        std::memcpy(&lr_bits, &gt.lr, 4);
+        const uint64_t extra[10] = {(uint64_t)(uintptr_t)accum,        c->scene_version,
+                                    (uint64_t)(uintptr_t)c->rs.ps.o_pdf, (uint64_t)(tp != nullptr),
+                                    (uint64_t)(uintptr_t)c->rs.ps.lobes, (uint64_t)(uintptr_t)c->rs.ps.rec,
+                                    (uint64_t)(uintptr_t)c->rs.ps.gmisc, (uint64_t)(uintptr_t)gt.params,
+                                    (uint64_t)gt.train,                  (uint64_t)lr_bits};
+        std::vector<unsigned char> key(sizeof(FrameParams) + sizeof(DevScene) + sizeof(extra));
         std::memcpy(key.data(), &fp, sizeof(FrameParams));
         std::memcpy(key.data() + sizeof(FrameParams), &sc, sizeof(DevScene));
         std::memcpy(key.data() + sizeof(FrameParams) + sizeof(DevScene), extra, sizeof(extra));
@@ -416,7 +472,7 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
             cudaGraph_t graph = nullptr;
             uint64_t before = c->rs.launches;
             LUC_CUDA(c, cudaStreamBeginCapture(c->own_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-            record_batch(c->rs, sc, fp, accum, c->own_stream, tp ? &g.timer : nullptr);
+            record_batch(c->rs, sc, fp, accum, c->own_stream, tp ? &g.timer : nullptr, &gt);
             LUC_CUDA(c, cudaStreamEndCapture(c->own_stream, &graph), "end capture");
             cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
             cudaGraphDestroy(graph);
@@ -438,7 +494,7 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
             fp.sample_base = u->sample_offset + done;
             fp.batch_samples = n;
             fp.num_paths = (uint64_t)n * pixels;
-            record_batch(c->rs, sc, fp, accum, s, tp);
+            record_batch(c->rs, sc, fp, accum, s, tp, &gt);
             done += n;
             c->stats.paths += fp.num_paths;
         }
@@ -478,6 +534,8 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
         c->stats.ms_shade = st[StageTimer::kShade];
         c->stats.ms_connect = st[StageTimer::kConnect];
         c->stats.ms_resolve = st[StageTimer::kResolve];
+        c->stats.ms_guide = st[StageTimer::kGuide];
+        c->stats.ms_train = st[StageTimer::kTrain];
     }
     return LUC_OK;
 }

@@ -61,6 +61,15 @@ struct luc_ctx {
         lb_nbounds, lb_subtree, lb_flags, lb_nodes, lb_rank, lb_misc, lb_icount, lb_look, lb_codes;
     // Denoiser scratch.
     DevBuf dn_in, dn_out, dn_a, dn_b, dn_dev;
+    // Learned guide: FP32 master, Adam moments, gradient, packed weights,
+    // bookkeeping words, per-path mixtures, training records, host-call io.
+    DevBuf g_params, g_m, g_v, g_grad, g_wbf, g_bias, g_misc, g_lobes, g_rec, g_io;
+    bool guide_ready = false, guide_train = true;
+    uint32_t guide_rec_cap = 1u << 18;
+    float guide_lr = 1.0e-2f;
+    float guide_lo[3] = {0, 0, 0}, guide_hi[3] = {1, 1, 1};
+    // Bounds of the uploaded scene (vertices and analytic primitives).
+    float scene_lo[3] = {0, 0, 0}, scene_hi[3] = {0, 0, 0};
 };
 
 // Error helpers: record a message and return a LUC_ERR_* code.
@@ -88,6 +97,11 @@ int32_t luc_gather_triangles(luc_ctx* c, const GpuTriangle* src, GpuTriangle* ds
 // Implemented in wavefront.cu: derive the traversal layout (child-pair
 // records, triangle soup) from the resident nodes and triangles.
 int32_t luc_build_traversal(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris);
+// Implemented in guide.cu: the guide's device view and training buffers,
+// and per-frame allocations (mixtures for `paths` paths, records).
+luc::GuideDev luc_guide_dev(const luc_ctx* c);
+luc::GuideTrain luc_guide_train_state(luc_ctx* c);
+int32_t luc_guide_prepare_frame(luc_ctx* c, uint64_t paths);
 // Implemented in denoise.cu.
 int32_t luc_denoise_device(luc_ctx* c, const GpuAccum* accum_dev, uint32_t w, uint32_t h,
                            const luc_denoise_params* p, GpuAccum* out_dev);

@@ -1,0 +1,907 @@
+// Learned path-guiding proposal on sm_100a: fused BF16 tensor-core MLP
+// kernels (inference per bounce over the path queue; forward + backward +
+// weight-gradient accumulation for training), record finalisation and Adam.
+// The model and the record layout are described in guide.cuh.
+//
+// Matrix products use mma.sync m16n8k16 (BF16 inputs, FP32 accumulate) with
+// operands staged in shared memory and fed by ldmatrix (.trans where the
+// product needs the transposed operand), so one row-major copy of every
+// weight and activation tile serves the forward, input-gradient and
+// weight-gradient products. A CTA of 4 warps owns a 64-row tile, one warp per
+// 16 rows; weight gradients accumulate in shared-memory FP32 across all the
+// tiles a persistent CTA processes and reach global memory once per CTA.
+//
+// Every kernel reads its row count and normalisers from device memory, so the
+// per-batch training step (finalise -> train -> Adam -> pack) is captured in
+// the frame's CUDA graph with the rest of the batch.
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <cuda_bf16.h>
+#include "ctx.cuh"
+
+namespace luc {
+
+// Shared-memory row strides (elements), padded by 8 bf16 (16 B) so the eight
+// row addresses of an ldmatrix fall in distinct banks.
+constexpr int kSIn = kGIn + 8, kSHid = kGHid + 8, kSOut = kGOutPad + 8;
+constexpr int kTileRows = 64;
+constexpr int kGuideThreads = 128;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t (&r)[4], const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldsm_x2(uint32_t (&r)[2], const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n" : "=r"(r[0]), "=r"(r[1]) : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldsm_x2_t(uint32_t (&r)[2], const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n"
+                 : "=r"(r[0]), "=r"(r[1])
+                 : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ uint16_t to_bf16(float x) {
+    __nv_bfloat16 h = __float2bfloat16_rn(x);
+    return *reinterpret_cast<uint16_t*>(&h);
+}
+__device__ __forceinline__ float bf16_to_f(uint16_t h) { return __uint_as_float(((uint32_t)h) << 16); }
+__device__ __forceinline__ float u2f(uint32_t u) { return __uint_as_float(u); }
+
+// Shared-memory image of the network (weight row = output unit).
+struct NetSmem {
+    uint16_t w1[kGHid * kSIn], w2[kGHid * kSHid], w3[kGHid * kSHid], w4[kGOutPad * kSHid];
+    float b[kGBias];
+};
+
+__device__ __forceinline__ void load_net(NetSmem& s, const uint16_t* __restrict__ wbf, const float* __restrict__ bias) {
+    const int t = threadIdx.x, nt = blockDim.x;
+    for (int i = t; i < kGHid * kGIn; i += nt) s.w1[(i / kGIn) * kSIn + i % kGIn] = wbf[i];
+    const uint16_t* w2 = wbf + kGHid * kGIn;
+    for (int i = t; i < kGHid * kGHid; i += nt) s.w2[(i / kGHid) * kSHid + i % kGHid] = w2[i];
+    const uint16_t* w3 = w2 + kGHid * kGHid;
+    for (int i = t; i < kGHid * kGHid; i += nt) s.w3[(i / kGHid) * kSHid + i % kGHid] = w3[i];
+    const uint16_t* w4 = w3 + kGHid * kGHid;
+    for (int i = t; i < kGOutPad * kGHid; i += nt) s.w4[(i / kGHid) * kSHid + i % kGHid] = w4[i];
+    for (int i = t; i < kGBias; i += nt) s.b[i] = bias[i];
+}
+
+// Features of one row into shared memory (bf16); lane l writes features
+// l, l + 32, l + 64, l + 96. Order: position axis a, frequency k, (sin, cos)
+// at 24a + 2k; then normal and outgoing direction at 72 + 24v + 8a + 2k.
+__device__ __forceinline__ void encode_row(uint16_t* __restrict__ xrow, const float (&in)[9], const GuideDev& g, int lane) {
+#pragma unroll
+    for (int f0 = 0; f0 < kGIn; f0 += 32) {
+        const int f = f0 + lane;
+        float v = 0.0f;
+        if (f < 72) {
+            int a = f / 24, k = (f % 24) >> 1;
+            float q = fminf(fmaxf((in[a] - g.lo[a]) / g.ext[a], 0.0f), 1.0f);
+            float arg = q * (kPi * (float)(1 << k));
+            v = (f & 1) ? cosf(arg) : sinf(arg);
+        } else if (f < kGFeatures) {
+            int r = f - 72, which = r / 24, a = (r % 24) / 8, k = (r % 8) >> 1;
+            float arg = in[3 + 3 * which + a] * (kPi * (float)(1 << k));
+            v = (f & 1) ? cosf(arg) : sinf(arg);
+        }
+        xrow[f] = to_bf16(v);
+    }
+}
+
+// Broadcast lanes 0..15's row inputs in turn and encode the warp's 16 rows.
+__device__ __forceinline__ void encode_rows(uint16_t* __restrict__ x, const float (&mine)[9], const GuideDev& g, int r0, int lane) {
+    for (int r = 0; r < 16; ++r) {
+        float v[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v[k] = __shfl_sync(0xFFFFFFFFu, mine[k], r);
+        encode_row(x + (r0 + r) * kSIn, v, g, lane);
+    }
+}
+
+// out[rows r0..r0+15][0..N) = act(A[rows][0..K) W^T + b); A, W and out bf16.
+template <int K, int SA, int N, bool RELU>
+__device__ void dense_fwd_bf16(const uint16_t* __restrict__ A, const uint16_t* __restrict__ W, const float* __restrict__ b,
+                               uint16_t* __restrict__ out, int r0, int lane) {
+    uint32_t af[K / 16][4];
+#pragma unroll
+    for (int kt = 0; kt < K / 16; ++kt)
+        ldsm_x4(af[kt], A + (r0 + (lane & 7) + 8 * ((lane >> 3) & 1)) * SA + kt * 16 + 8 * (lane >> 4));
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < N / 8; ++nt) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int kt = 0; kt < K / 16; ++kt) {
+            uint32_t bf[2];
+            ldsm_x2(bf, W + (nt * 8 + (lane & 7)) * SA + kt * 16 + 8 * ((lane >> 3) & 1));
+            mma16816(c, af[kt], bf);
+        }
+        const int n = nt * 8 + 2 * t;
+        float b0 = b[n], b1 = b[n + 1];
+        float v0 = c[0] + b0, v1 = c[1] + b1, v2 = c[2] + b0, v3 = c[3] + b1;
+        if (RELU) {
+            v0 = fmaxf(v0, 0.f);
+            v1 = fmaxf(v1, 0.f);
+            v2 = fmaxf(v2, 0.f);
+            v3 = fmaxf(v3, 0.f);
+        }
+        *reinterpret_cast<uint32_t*>(out + (r0 + g) * kSHid + n) = pack_bf16(v0, v1);
+        *reinterpret_cast<uint32_t*>(out + (r0 + g + 8) * kSHid + n) = pack_bf16(v2, v3);
+    }
+}
+
+// Last layer: FP32 outputs (rows r0..r0+15, 48 columns) into O[64][48].
+__device__ void dense_out_f32(const uint16_t* __restrict__ A, const NetSmem& net, float* __restrict__ O, int r0,
+                              int lane) {
+    uint32_t af[kGHid / 16][4];
+#pragma unroll
+    for (int kt = 0; kt < kGHid / 16; ++kt)
+        ldsm_x4(af[kt], A + (r0 + (lane & 7) + 8 * ((lane >> 3) & 1)) * kSHid + kt * 16 + 8 * (lane >> 4));
+    const int g = lane >> 2, t = lane & 3;
+    const float* b = net.b + 3 * kGHid;
+#pragma unroll
+    for (int nt = 0; nt < kGOutPad / 8; ++nt) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int kt = 0; kt < kGHid / 16; ++kt) {
+            uint32_t bf[2];
+            ldsm_x2(bf, net.w4 + (nt * 8 + (lane & 7)) * kSHid + kt * 16 + 8 * ((lane >> 3) & 1));
+            mma16816(c, af[kt], bf);
+        }
+        const int n = nt * 8 + 2 * t;
+        O[(r0 + g) * kGOutPad + n] = c[0] + b[n];
+        O[(r0 + g) * kGOutPad + n + 1] = c[1] + b[n + 1];
+        O[(r0 + g + 8) * kGOutPad + n] = c[2] + b[n];
+        O[(r0 + g + 8) * kGOutPad + n + 1] = c[3] + b[n + 1];
+    }
+}
+
+// The whole forward pass of the warp's 16 rows: X -> H1 -> H2 -> H3 -> O.
+__device__ __forceinline__ void forward_rows(const NetSmem& net, const uint16_t* x, uint16_t* h1, uint16_t* h2, uint16_t* h3, float* o,
+                             int r0, int lane) {
+    dense_fwd_bf16<kGIn, kSIn, kGHid, true>(x, net.w1, net.b, h1, r0, lane);
+    __syncwarp();
+    dense_fwd_bf16<kGHid, kSHid, kGHid, true>(h1, net.w2, net.b + kGHid, h2, r0, lane);
+    __syncwarp();
+    dense_fwd_bf16<kGHid, kSHid, kGHid, true>(h2, net.w3, net.b + 2 * kGHid, h3, r0, lane);
+    __syncwarp();
+    dense_out_f32(h3, net, o, r0, lane);
+    __syncwarp();
+}
+
+__device__ __forceinline__ float softplus_f(float x) { return x > 20.0f ? x : log1pf(expf(x)); }
+
+// Raw outputs -> (mu, kappa) x 8 and softmax weights.
+__device__ __forceinline__ void decode_row(const float* __restrict__ o, float4* __restrict__ lobes, float* __restrict__ w) {
+    float mx = -INFINITY;
+    for (int j = 0; j < kGLobes; ++j) mx = fmaxf(mx, o[5 * j + 4]);
+    float s = 0.0f;
+    for (int j = 0; j < kGLobes; ++j) {
+        w[j] = expf(o[5 * j + 4] - mx);
+        s += w[j];
+    }
+    for (int j = 0; j < kGLobes; ++j) {
+        w[j] /= s;
+        float x = o[5 * j], y = o[5 * j + 1], z = o[5 * j + 2];
+        float ln = sqrtf(x * x + y * y + z * z);
+        float kappa = fminf(1.0f + softplus_f(o[5 * j + 3]), kGKappaMax);
+        lobes[j] = ln > 0.0f ? make_float4(x / ln, y / ln, z / ln, kappa) : make_float4(0.f, 0.f, 1.f, kappa);
+    }
+}
+
+struct InferSmem {
+    NetSmem net;
+    uint16_t x[kTileRows * kSIn];
+    uint16_t h[2][kTileRows * kSHid];
+    float o[kTileRows * kGOutPad];
+};
+
+// Per bounce: the decoded mixture of every queued path whose ray hit a
+// surface, into ps.lobes. Inputs are the hit point, the shading normal and the
+// outgoing direction -dir, as SHADE computes them.
+__global__ void __launch_bounds__(kGuideThreads) k_guide_infer(PathState ps, DevScene sc, FrameParams fp,
+                                                                uint32_t depth) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    InferSmem& S = *reinterpret_cast<InferSmem*>(smem_raw);
+    load_net(S.net, fp.guide.wbf, fp.guide.bias);
+    __syncthreads();
+    const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
+    const uint32_t* queue = ps.queue[depth & 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r0 = warp * 16;
+    for (uint32_t base = blockIdx.x * kTileRows; base < len; base += gridDim.x * kTileRows) {
+        float in[9] = {0, 0, 0, 0, 0, 1, 0, 0, 1};
+        uint32_t p = 0xFFFFFFFFu;
+        if (lane < 16 && base + r0 + lane < len) {
+            const uint32_t i = base + r0 + lane;
+            const uint32_t q = depth == 0 ? i : queue[i];
+            float4 h4 = ps.hit[q];
+            uint32_t id = __float_as_uint(h4.w);
+            if (id != kMiss) {
+                p = q;
+                float4 o4 = ps.o_pdf[q], d4 = ps.dir[q];
+                V3 dir{d4.x, d4.y, d4.z};
+                SurfaceHit hit = surface_hit(sc, id, h4.x, h4.y, h4.z, V3{o4.x, o4.y, o4.z}, dir);
+                in[0] = hit.position.x;
+                in[1] = hit.position.y;
+                in[2] = hit.position.z;
+                in[3] = hit.normal.x;
+                in[4] = hit.normal.y;
+                in[5] = hit.normal.z;
+                in[6] = -dir.x;
+                in[7] = -dir.y;
+                in[8] = -dir.z;
+            }
+        }
+        // A warp whose 16 rows all missed has nothing to infer.
+        if (__ballot_sync(0xFFFFFFFFu, p != 0xFFFFFFFFu) == 0) continue;
+        encode_rows(S.x, in, fp.guide, r0, lane);
+        __syncwarp();
+        forward_rows(S.net, S.x, S.h[0], S.h[1], S.h[0], S.o, r0, lane);
+        if (p != 0xFFFFFFFFu) {
+            float4 lobes[kGLobes];
+            float w[kGLobes];
+            decode_row(S.o + (r0 + lane) * kGOutPad, lobes, w);
+            float4* dst = ps.lobes + (size_t)p * kGLobeF4;
+#pragma unroll
+            for (int j = 0; j < kGLobes; ++j) dst[j] = lobes[j];
+            dst[8] = make_float4(w[0], w[1], w[2], w[3]);
+            dst[9] = make_float4(w[4], w[5], w[6], w[7]);
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------- training
+struct TrainSmem {
+    NetSmem net;
+    float dw1[kGHid * kGIn], dw2[kGHid * kGHid], dw3[kGHid * kGHid], dw4[kGOutPad * kGHid];
+    float db[kGBias];
+    uint16_t x[kTileRows * kSIn];
+    uint16_t h[3][kTileRows * kSHid];
+    uint16_t dy[kTileRows * kSOut];
+    uint16_t dh[2][kTileRows * kSHid];
+    float o[kTileRows * kGOutPad];
+    float loss;
+};
+
+// dW[m][n] += sum_r G[r][m] H[r][n] over the tile's 64 rows for the 16 output
+// rows m0..m0+15. G is [64][SG] (m contiguous), H is [64][SH]; both operands
+// come through ldmatrix.trans, so neither is ever stored transposed.
+template <int NIN, int SH, int SG>
+__device__ void acc_weight_grad(const uint16_t* __restrict__ G, const uint16_t* __restrict__ H, float* __restrict__ dW,
+                                int m0, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    uint32_t af[kTileRows / 16][4];
+#pragma unroll
+    for (int kt = 0; kt < kTileRows / 16; ++kt)
+        ldsm_x4_t(af[kt], G + (kt * 16 + (lane & 7) + 8 * (lane >> 4)) * SG + m0 + 8 * ((lane >> 3) & 1));
+#pragma unroll 4
+    for (int nt = 0; nt < NIN / 8; ++nt) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int kt = 0; kt < kTileRows / 16; ++kt) {
+            uint32_t bf[2];
+            ldsm_x2_t(bf, H + (kt * 16 + (lane & 7) + 8 * ((lane >> 3) & 1)) * SH + nt * 8);
+            mma16816(c, af[kt], bf);
+        }
+        const int n = nt * 8 + 2 * t;
+        float2* d0 = reinterpret_cast<float2*>(dW + (m0 + g) * NIN + n);
+        float2* d1 = reinterpret_cast<float2*>(dW + (m0 + g + 8) * NIN + n);
+        float2 a0 = *d0, a1 = *d1;
+        *d0 = make_float2(a0.x + c[0], a0.y + c[1]);
+        *d1 = make_float2(a1.x + c[2], a1.y + c[3]);
+    }
+}
+
+// dH[r][k] = (sum_n G[r][n] W[n][k]) * (Hprev[r][k] > 0) for the warp's 16
+// rows, and db[k] += the column sums of that FP32 value.
+template <int NOUT, int SG>
+__device__ void input_grad(const uint16_t* __restrict__ G, const uint16_t* __restrict__ W, const uint16_t* __restrict__ Hp,
+                           uint16_t* __restrict__ dH, float* __restrict__ db, int r0, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    uint32_t af[NOUT / 16][4];
+#pragma unroll
+    for (int kt = 0; kt < NOUT / 16; ++kt)
+        ldsm_x4(af[kt], G + (r0 + (lane & 7) + 8 * ((lane >> 3) & 1)) * SG + kt * 16 + 8 * (lane >> 4));
+#pragma unroll
+    for (int nt = 0; nt < kGHid / 8; ++nt) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int kt = 0; kt < NOUT / 16; ++kt) {
+            uint32_t bf[2];
+            ldsm_x2_t(bf, W + (kt * 16 + (lane & 7) + 8 * ((lane >> 3) & 1)) * kSHid + nt * 8);
+            mma16816(c, af[kt], bf);
+        }
+        const int n = nt * 8 + 2 * t;
+        const uint16_t* h0 = Hp + (r0 + g) * kSHid + n;
+        const uint16_t* h1 = Hp + (r0 + g + 8) * kSHid + n;
+        float v0 = bf16_to_f(h0[0]) > 0.f ? c[0] : 0.f, v1 = bf16_to_f(h0[1]) > 0.f ? c[1] : 0.f;
+        float v2 = bf16_to_f(h1[0]) > 0.f ? c[2] : 0.f, v3 = bf16_to_f(h1[1]) > 0.f ? c[3] : 0.f;
+        *reinterpret_cast<uint32_t*>(dH + (r0 + g) * kSHid + n) = pack_bf16(v0, v1);
+        *reinterpret_cast<uint32_t*>(dH + (r0 + g + 8) * kSHid + n) = pack_bf16(v2, v3);
+        float s0 = v0 + v2, s1 = v1 + v3;
+#pragma unroll
+        for (int off = 4; off < 32; off <<= 1) {
+            s0 += __shfl_xor_sync(0xFFFFFFFFu, s0, off);
+            s1 += __shfl_xor_sync(0xFFFFFFFFu, s1, off);
+        }
+        if (g == 0) {
+            atomicAdd(db + n, s0);
+            atomicAdd(db + n + 1, s1);
+        }
+    }
+}
+
+// Loss term of one row, -F/S log q(d), and its gradient w.r.t. the raw
+// outputs (the same closed forms as the oracle).
+__device__ __forceinline__ float row_loss_grad(const float* __restrict__ o, V3 d, float F, float invS, float* __restrict__ go) {
+    float mx = -INFINITY;
+    for (int j = 0; j < kGLobes; ++j) mx = fmaxf(mx, o[5 * j + 4]);
+    float w[kGLobes], pj[kGLobes];
+    float ws = 0.f;
+    for (int j = 0; j < kGLobes; ++j) {
+        w[j] = expf(o[5 * j + 4] - mx);
+        ws += w[j];
+    }
+    float q = 0.f;
+    for (int j = 0; j < kGLobes; ++j) {
+        w[j] /= ws;
+        float x = o[5 * j], y = o[5 * j + 1], z = o[5 * j + 2];
+        float ln = fmaxf(sqrtf(x * x + y * y + z * z), 1e-30f);
+        float c = (x * d.x + y * d.y + z * d.z) / ln;
+        float kap = fminf(1.0f + softplus_f(o[5 * j + 3]), kGKappaMax);
+        pj[j] = kap / (2.0f * kPi * (1.0f - expf(-2.0f * kap))) * expf(kap * (c - 1.0f));
+        q += w[j] * pj[j];
+    }
+    q = fmaxf(q, 1e-30f);
+    const float scale = -F * invS;
+    for (int j = 0; j < kGLobes; ++j) {
+        float x = o[5 * j], y = o[5 * j + 1], z = o[5 * j + 2];
+        float ln = fmaxf(sqrtf(x * x + y * y + z * z), 1e-30f);
+        float mu[3] = {x / ln, y / ln, z / ln};
+        float c = mu[0] * d.x + mu[1] * d.y + mu[2] * d.z;
+        float kr = 1.0f + softplus_f(o[5 * j + 3]);
+        float kap = fminf(kr, kGKappaMax);
+        float ex = expf(-2.0f * kap);
+        float r = w[j] * pj[j] / q;
+        go[5 * j + 4] = scale * (r - w[j]);
+        float dk = r * (1.0f / kap - 2.0f * ex / (1.0f - ex) + c - 1.0f);
+        float sig = 1.0f / (1.0f + expf(-fminf(fmaxf(o[5 * j + 3], -60.f), 60.f)));
+        go[5 * j + 3] = kr >= kGKappaMax ? 0.0f : scale * dk * sig;
+        float gm[3] = {r * kap * d.x, r * kap * d.y, r * kap * d.z};
+        float dotm = gm[0] * mu[0] + gm[1] * mu[1] + gm[2] * mu[2];
+        for (int a = 0; a < 3; ++a) go[5 * j + a] = scale * (gm[a] - dotm * mu[a]) / ln;
+    }
+    return scale * logf(q);
+}
+
+// One gradient evaluation over the records (count gmisc[kGmRecords], capped
+// at `cap`; normaliser 1 / gmisc[kGmWeightSum]) added into grad (FP32, master
+// layout), and the loss into gmisc[kGmLoss].
+__global__ void __launch_bounds__(kGuideThreads) k_guide_train(const float4* __restrict__ rec, uint32_t cap,
+                                                                uint32_t* __restrict__ gmisc, GuideDev g,
+                                                                float* __restrict__ grad) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
+    const uint32_t n = min(gmisc[kGmRecords], cap);
+    const float wsum = u2f(gmisc[kGmWeightSum]);
+    const float invS = wsum > 0.0f ? 1.0f / wsum : 0.0f;
+    if (blockIdx.x * kTileRows >= n) return;
+    load_net(S.net, g.wbf, g.bias);
+    for (int i = threadIdx.x; i < kGHid * kGIn; i += blockDim.x) S.dw1[i] = 0.f;
+    for (int i = threadIdx.x; i < kGHid * kGHid; i += blockDim.x) {
+        S.dw2[i] = 0.f;
+        S.dw3[i] = 0.f;
+    }
+    for (int i = threadIdx.x; i < kGOutPad * kGHid; i += blockDim.x) S.dw4[i] = 0.f;
+    for (int i = threadIdx.x; i < kGBias; i += blockDim.x) S.db[i] = 0.f;
+    if (threadIdx.x == 0) S.loss = 0.f;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r0 = warp * 16;
+    for (uint32_t base = blockIdx.x * kTileRows; base < n; base += gridDim.x * kTileRows) {
+        const uint32_t i = base + r0 + lane;
+        const bool mine = lane < 16 && i < n;
+        float in[9] = {0, 0, 0, 0, 0, 1, 0, 0, 1};
+        float4 a4{0, 0, 0, 0}, d4{0, 0, 0, 0};
+        if (mine) {
+            a4 = rec[kGRecF4 * (size_t)i];
+            float4 b4 = rec[kGRecF4 * (size_t)i + 1], c4 = rec[kGRecF4 * (size_t)i + 2];
+            d4 = rec[kGRecF4 * (size_t)i + 3];
+            in[0] = a4.x;
+            in[1] = a4.y;
+            in[2] = a4.z;
+            in[3] = b4.x;
+            in[4] = b4.y;
+            in[5] = b4.z;
+            in[6] = c4.x;
+            in[7] = c4.y;
+            in[8] = c4.z;
+        }
+        encode_rows(S.x, in, g, r0, lane);
+        __syncwarp();
+        forward_rows(S.net, S.x, S.h[0], S.h[1], S.h[2], S.o, r0, lane);
+        // Loss epilogue: lanes 0..15, one row each.
+        if (lane < 16) {
+            const int r = r0 + lane;
+            float go[kGOut];
+            float lrow = 0.f;
+            if (mine && a4.w > 0.0f) {
+                lrow = row_loss_grad(S.o + r * kGOutPad, V3{d4.x, d4.y, d4.z}, a4.w, invS, go);
+            } else {
+                for (int k = 0; k < kGOut; ++k) go[k] = 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < kGOutPad; k += 2) {
+                float v0 = k < kGOut ? go[k] : 0.f, v1 = k + 1 < kGOut ? go[k + 1] : 0.f;
+                *reinterpret_cast<uint32_t*>(S.dy + r * kSOut + k) = pack_bf16(v0, v1);
+            }
+            // Output-bias gradient: reduce over the 16 rows, then one atomic.
+#pragma unroll
+            for (int k = 0; k < kGOut; ++k) {
+                float v = go[k];
+                for (int off = 8; off > 0; off >>= 1) v += __shfl_xor_sync(0x0000FFFFu, v, off);
+                if (lane == 0) atomicAdd(S.db + 3 * kGHid + k, v);
+            }
+            for (int off = 8; off > 0; off >>= 1) lrow += __shfl_xor_sync(0x0000FFFFu, lrow, off);
+            if (lane == 0) atomicAdd(&S.loss, lrow);
+        }
+        __syncthreads();
+        // Layer 4: dW4 (48 rows: warps 0..2, 16 each) and dH3.
+        if (warp < 3) acc_weight_grad<kGHid, kSHid, kSOut>(S.dy, S.h[2], S.dw4, warp * 16, lane);
+        input_grad<kGOutPad, kSOut>(S.dy, S.net.w4, S.h[2], S.dh[0], S.db + 2 * kGHid, r0, lane);
+        __syncthreads();
+        acc_weight_grad<kGHid, kSHid, kSHid>(S.dh[0], S.h[1], S.dw3, warp * 16, lane);
+        input_grad<kGHid, kSHid>(S.dh[0], S.net.w3, S.h[1], S.dh[1], S.db + kGHid, r0, lane);
+        __syncthreads();
+        acc_weight_grad<kGHid, kSHid, kSHid>(S.dh[1], S.h[0], S.dw2, warp * 16, lane);
+        input_grad<kGHid, kSHid>(S.dh[1], S.net.w2, S.h[0], S.dh[0], S.db, r0, lane);
+        __syncthreads();
+        acc_weight_grad<kGIn, kSIn, kSHid>(S.dh[0], S.x, S.dw1, warp * 16, lane);
+        __syncthreads();
+    }
+    // Fold this CTA's gradients into the global FP32 gradient.
+    float* gW1 = grad;
+    float* gb1 = gW1 + kGHid * kGIn;
+    float* gW2 = gb1 + kGHid;
+    float* gb2 = gW2 + kGHid * kGHid;
+    float* gW3 = gb2 + kGHid;
+    float* gb3 = gW3 + kGHid * kGHid;
+    float* gW4 = gb3 + kGHid;
+    float* gb4 = gW4 + kGOut * kGHid;
+    for (int i = threadIdx.x; i < kGHid * kGIn; i += blockDim.x) atomicAdd(gW1 + i, S.dw1[i]);
+    for (int i = threadIdx.x; i < kGHid * kGHid; i += blockDim.x) {
+        atomicAdd(gW2 + i, S.dw2[i]);
+        atomicAdd(gW3 + i, S.dw3[i]);
+    }
+    for (int i = threadIdx.x; i < kGOut * kGHid; i += blockDim.x) atomicAdd(gW4 + i, S.dw4[i]);
+    for (int i = threadIdx.x; i < kGHid; i += blockDim.x) {
+        atomicAdd(gb1 + i, S.db[i]);
+        atomicAdd(gb2 + i, S.db[kGHid + i]);
+        atomicAdd(gb3 + i, S.db[2 * kGHid + i]);
+    }
+    for (int i = threadIdx.x; i < kGOut; i += blockDim.x) atomicAdd(gb4 + i, S.db[3 * kGHid + i]);
+    if (threadIdx.x == 0) atomicAdd(reinterpret_cast<float*>(gmisc + kGmLoss), S.loss);
+}
+
+// Records of a rendered batch: F = luminance of the radiance that arrived
+// along the sampled direction (the path radiance gained after the vertex,
+// divided per channel by the throughput after scattering) over the mixture
+// pdf, into rec[0].w; the sum of F into gmisc[kGmWeightSum].
+__global__ void k_guide_finalize(PathState ps, uint32_t cap) {
+    const uint32_t n = min(ps.gmisc[kGmRecords], cap);
+    float s = 0.f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4* r = ps.rec + kGRecF4 * (size_t)i;
+        float4 a = r[0], b = r[1], c = r[2], d = r[3], e = r[4];
+        const uint32_t p = __float_as_uint(a.w);
+        float4 rf = ps.rad[p];
+        const float T[3] = {b.w, c.w, d.w};
+        const float dR[3] = {rf.x - e.x, rf.y - e.y, rf.z - e.z};
+        const float lw[3] = {0.2126f, 0.7152f, 0.0722f};
+        float L = 0.f;
+        for (int k = 0; k < 3; ++k)
+            if (T[k] > 0.f) L += lw[k] * dR[k] / T[k];
+        float F = L > 0.f && e.w > 0.f ? L / e.w : 0.f;
+        if (!isfinite(F)) F = 0.f;
+        r[0].w = F;
+        s += F;
+    }
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, off);
+    if ((threadIdx.x & 31) == 0 && s != 0.f) atomicAdd(reinterpret_cast<float*>(ps.gmisc + kGmWeightSum), s);
+}
+
+// Sum of F over host-given records.
+__global__ void k_guide_weight_sum(const float4* __restrict__ rec, uint32_t n, uint32_t* __restrict__ gmisc) {
+    float s = 0.f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        s += fmaxf(rec[kGRecF4 * (size_t)i].w, 0.f);
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, off);
+    if ((threadIdx.x & 31) == 0 && s != 0.f) atomicAdd(reinterpret_cast<float*>(gmisc + kGmWeightSum), s);
+}
+
+// Adam (beta1 0.9, beta2 0.999, eps 1e-8) on the FP32 master; the step
+// number comes from gmisc[kGmStep] (advanced by k_guide_pack).
+__global__ void k_guide_adam(float* __restrict__ p, float* __restrict__ m, float* __restrict__ v,
+                             const float* __restrict__ grad, const uint32_t* __restrict__ gmisc, float lr) {
+    const float t = (float)(gmisc[kGmStep] + 1u);
+    const float c1 = 1.0f - powf(0.9f, t), c2 = 1.0f - powf(0.999f, t);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGParams; i += gridDim.x * blockDim.x) {
+        float gi = grad[i];
+        float mi = 0.9f * m[i] + 0.1f * gi;
+        float vi = 0.999f * v[i] + 0.001f * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + 1e-8f);
+    }
+}
+
+// Pack the master into BF16 weights (W4 zero-padded to 48 rows) and FP32
+// biases. With `advance`, block 0 thread 0 also closes the step: step count,
+// last loss and record count, the recording threshold for the next batch
+// (aiming at `cap` records from this batch's candidate count) and the
+// per-batch counters reset.
+__global__ void k_guide_pack(const float* __restrict__ p, uint16_t* __restrict__ wbf, float* __restrict__ bias,
+                             uint32_t* __restrict__ gmisc, uint32_t cap, uint32_t advance) {
+    const float* W1 = p;
+    const float* b1 = W1 + kGHid * kGIn;
+    const float* W2 = b1 + kGHid;
+    const float* b2 = W2 + kGHid * kGHid;
+    const float* W3 = b2 + kGHid;
+    const float* b3 = W3 + kGHid * kGHid;
+    const float* W4 = b3 + kGHid;
+    const float* b4 = W4 + kGOut * kGHid;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGBf16; i += gridDim.x * blockDim.x) {
+        float x;
+        if (i < kGHid * kGIn) x = W1[i];
+        else if (i < kGHid * kGIn + kGHid * kGHid) x = W2[i - kGHid * kGIn];
+        else if (i < kGHid * kGIn + 2 * kGHid * kGHid) x = W3[i - kGHid * kGIn - kGHid * kGHid];
+        else {
+            int j = i - kGHid * kGIn - 2 * kGHid * kGHid;
+            x = j < kGOut * kGHid ? W4[j] : 0.0f;
+        }
+        wbf[i] = to_bf16(x);
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGBias; i += gridDim.x * blockDim.x) {
+        float x;
+        if (i < kGHid) x = b1[i];
+        else if (i < 2 * kGHid) x = b2[i - kGHid];
+        else if (i < 3 * kGHid) x = b3[i - 2 * kGHid];
+        else x = (i - 3 * kGHid) < kGOut ? b4[i - 3 * kGHid] : 0.0f;
+        bias[i] = x;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && advance) {
+        gmisc[kGmStep] += 1u;
+        gmisc[kGmLastLoss] = gmisc[kGmLoss];
+        gmisc[kGmLastRecords] = min(gmisc[kGmRecords], cap);
+        const uint32_t cand = gmisc[kGmCandidates];
+        if (cand > 0) {
+            uint64_t t = (uint64_t)65536 * cap * 15 / 16 / cand;
+            gmisc[kGmThreshold] = (uint32_t)(t > 65536 ? 65536 : (t == 0 ? 1 : t));
+        }
+        gmisc[kGmCandidates] = 0;
+        gmisc[kGmRecords] = 0;
+    }
+}
+
+// Raw outputs for host-given inputs (x, n, wo per row).
+__global__ void __launch_bounds__(kGuideThreads) k_guide_forward(const float* __restrict__ in9, uint32_t n, GuideDev g,
+                                                                  float* __restrict__ out40) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    InferSmem& S = *reinterpret_cast<InferSmem*>(smem_raw);
+    load_net(S.net, g.wbf, g.bias);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r0 = warp * 16;
+    for (uint32_t base = blockIdx.x * kTileRows; base < n; base += gridDim.x * kTileRows) {
+        float in[9] = {0, 0, 0, 0, 0, 1, 0, 0, 1};
+        const uint32_t i = base + r0 + lane;
+        if (lane < 16 && i < n)
+            for (int k = 0; k < 9; ++k) in[k] = in9[9 * (size_t)i + k];
+        encode_rows(S.x, in, g, r0, lane);
+        __syncwarp();
+        forward_rows(S.net, S.x, S.h[0], S.h[1], S.h[0], S.o, r0, lane);
+        for (int k = lane; k < 16 * kGOut; k += 32) {
+            const int r = k / kGOut, c = k % kGOut;
+            if (base + r0 + r < n) out40[(size_t)(base + r0 + r) * kGOut + c] = S.o[(r0 + r) * kGOutPad + c];
+        }
+        __syncwarp();
+    }
+}
+
+// Mixture sampling (mode 0: in3 = uniforms; out dir3 and pdf) and density
+// (mode 1: in3 = directions; out pdf) for given raw outputs.
+__global__ void k_guide_mixture_eval(const float* __restrict__ raw40, const float* __restrict__ in3, uint32_t n, int mode,
+                                     float* __restrict__ dir3, float* __restrict__ pdf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 lobes[kGLobes];
+    float w[kGLobes];
+    decode_row(raw40 + (size_t)i * kGOut, lobes, w);
+    Mixture m;
+    for (int j = 0; j < kGLobes; ++j) {
+        m.lobe[j] = lobes[j];
+        m.w[j] = w[j];
+    }
+    V3 d;
+    if (mode == 0) {
+        d = mixture_sample(m, in3[3 * i], in3[3 * i + 1], in3[3 * i + 2]);
+        dir3[3 * i] = d.x;
+        dir3[3 * i + 1] = d.y;
+        dir3[3 * i + 2] = d.z;
+    } else {
+        d = V3{in3[3 * i], in3[3 * i + 1], in3[3 * i + 2]};
+    }
+    pdf[i] = mixture_pdf(m, d);
+}
+
+static int g_infer_blocks = 1;
+
+// Dynamic shared memory above 48 KB needs an opt-in per kernel; done once
+// per device, before any launch (never inside a stream capture).
+static cudaError_t guide_kernel_setup(int device) {
+    static bool done[64] = {false};
+    if (device >= 0 && device < 64 && done[device]) return cudaSuccess;
+    cudaError_t e =
+        cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InferSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_guide_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InferSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem));
+    if (e != cudaSuccess) return e;
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_guide_infer, kGuideThreads, sizeof(InferSmem));
+    g_infer_blocks = b > 0 ? b : 1;
+    if (device >= 0 && device < 64) done[device] = true;
+    return cudaSuccess;
+}
+
+void launch_guide_infer(const RenderState& rs, const DevScene& sc, const FrameParams& fp, uint32_t depth,
+                        cudaStream_t s) {
+    k_guide_infer<<<rs.num_sms * g_infer_blocks, kGuideThreads, sizeof(InferSmem), s>>>(rs.ps, sc, fp, depth);
+}
+
+void launch_guide_train(const RenderState& rs, const FrameParams& fp, const GuideTrain& gt, cudaStream_t s) {
+    cudaMemsetAsync(gt.grad, 0, kGParams * sizeof(float), s);
+    cudaMemsetAsync(rs.ps.gmisc + kGmWeightSum, 0, 2 * sizeof(uint32_t), s);  // weight sum, loss
+    k_guide_finalize<<<rs.num_sms * 4, 256, 0, s>>>(rs.ps, fp.rec_cap);
+    k_guide_train<<<rs.num_sms, kGuideThreads, sizeof(TrainSmem), s>>>(rs.ps.rec, fp.rec_cap, rs.ps.gmisc, fp.guide,
+                                                                         gt.grad);
+    k_guide_adam<<<(kGParams + 255) / 256, 256, 0, s>>>(gt.params, gt.m, gt.v, gt.grad, rs.ps.gmisc, gt.lr);
+    k_guide_pack<<<(kGBf16 + 255) / 256, 256, 0, s>>>(gt.params, gt.wbf, gt.bias, rs.ps.gmisc, fp.rec_cap, 1u);
+}
+
+}  // namespace luc
+
+using namespace luc;
+
+// ------------------------------------------------------------------ context side
+static int32_t require_guide(luc_ctx* c) {
+    if (!c->guide_ready) return luc_fail(c, LUC_ERR_VALIDATION, "guide not initialised (luc_guide_init)");
+    return LUC_OK;
+}
+
+GuideDev luc_guide_dev(const luc_ctx* c) {
+    GuideDev g{};
+    g.wbf = c->g_wbf.as<uint16_t>();
+    g.bias = c->g_bias.as<float>();
+    for (int a = 0; a < 3; ++a) {
+        g.lo[a] = c->guide_lo[a];
+        g.ext[a] = c->guide_hi[a] > c->guide_lo[a] ? c->guide_hi[a] - c->guide_lo[a] : 1.0f;
+    }
+    return g;
+}
+
+GuideTrain luc_guide_train_state(luc_ctx* c) {
+    GuideTrain gt{};
+    gt.params = c->g_params.as<float>();
+    gt.m = c->g_m.as<float>();
+    gt.v = c->g_v.as<float>();
+    gt.grad = c->g_grad.as<float>();
+    gt.wbf = c->g_wbf.as<uint16_t>();
+    gt.bias = c->g_bias.as<float>();
+    gt.lr = c->guide_lr;
+    gt.train = c->guide_train;
+    return gt;
+}
+
+int32_t luc_guide_prepare_frame(luc_ctx* c, uint64_t paths) {
+    if (int32_t rc = require_guide(c)) return rc;
+    LUC_CUDA(c, guide_kernel_setup(c->device), "guide kernel attributes");
+    LUC_CUDA(c, c->g_lobes.ensure(paths * kGLobeF4 * sizeof(float4)), "allocate guide lobes");
+    LUC_CUDA(c, c->g_rec.ensure((size_t)std::max<uint32_t>(c->guide_rec_cap, 1) * kGRecF4 * sizeof(float4)),
+             "allocate guide records");
+    return LUC_OK;
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+int32_t luc_guide_init(luc_ctx* c, const float* params, uint64_t seed, const float* lo, const float* hi) {
+    if (!c) return LUC_ERR_VALIDATION;
+    cudaSetDevice(c->device);
+    if ((lo == nullptr) != (hi == nullptr)) return luc_fail(c, LUC_ERR_VALIDATION, "give both lo and hi or neither");
+    if (!lo && !c->has_scene) return luc_fail(c, LUC_ERR_VALIDATION, "no scene bounds: upload a scene or give lo/hi");
+    for (int a = 0; a < 3; ++a) {
+        c->guide_lo[a] = lo ? lo[a] : c->scene_lo[a];
+        c->guide_hi[a] = hi ? hi[a] : c->scene_hi[a];
+        if (!std::isfinite(c->guide_lo[a]) || !std::isfinite(c->guide_hi[a]))
+            return luc_fail(c, LUC_ERR_VALIDATION, "guide bounds must be finite");
+    }
+    LUC_CUDA(c, guide_kernel_setup(c->device), "guide kernel attributes");
+    std::vector<float> p(kGParams, 0.0f);
+    if (params) {
+        std::memcpy(p.data(), params, kGParams * sizeof(float));
+    } else {
+        // Uniform +-sqrt(6 / (fan_in + fan_out)) weights, zero biases, W1's
+        // padding columns zero.
+        std::mt19937_64 rng(seed);
+        const int fan[4][2] = {{kGHid, kGIn}, {kGHid, kGHid}, {kGHid, kGHid}, {kGOut, kGHid}};
+        size_t o = 0;
+        for (int l = 0; l < 4; ++l) {
+            float lim = std::sqrt(6.0f / (float)(fan[l][0] + fan[l][1]));
+            std::uniform_real_distribution<float> U(-lim, lim);
+            for (int r = 0; r < fan[l][0]; ++r)
+                for (int k = 0; k < fan[l][1]; ++k)
+                    p[o + (size_t)r * fan[l][1] + k] = (l == 0 && k >= kGFeatures) ? 0.0f : U(rng);
+            o += (size_t)fan[l][0] * fan[l][1] + fan[l][0];
+        }
+    }
+    for (float x : p)
+        if (!std::isfinite(x)) return luc_fail(c, LUC_ERR_VALIDATION, "guide parameters must be finite");
+    cudaStream_t s = c->stream;
+    LUC_CUDA(c, c->g_params.ensure(kGParams * sizeof(float)), "allocate guide");
+    LUC_CUDA(c, c->g_m.ensure(kGParams * sizeof(float)), "allocate guide");
+    LUC_CUDA(c, c->g_v.ensure(kGParams * sizeof(float)), "allocate guide");
+    LUC_CUDA(c, c->g_grad.ensure(kGParams * sizeof(float)), "allocate guide");
+    LUC_CUDA(c, c->g_wbf.ensure(kGBf16 * sizeof(uint16_t)), "allocate guide");
+    LUC_CUDA(c, c->g_bias.ensure(kGBias * sizeof(float)), "allocate guide");
+    LUC_CUDA(c, c->g_misc.ensure(kGmWords * sizeof(uint32_t)), "allocate guide");
+    LUC_CUDA(c, cudaMemcpyAsync(c->g_params.p, p.data(), kGParams * sizeof(float), cudaMemcpyHostToDevice, s),
+             "upload guide");
+    LUC_CUDA(c, cudaMemsetAsync(c->g_m.p, 0, kGParams * sizeof(float), s), "clear guide");
+    LUC_CUDA(c, cudaMemsetAsync(c->g_v.p, 0, kGParams * sizeof(float), s), "clear guide");
+    uint32_t misc[kGmWords] = {0};
+    misc[kGmThreshold] = 65536;
+    LUC_CUDA(c, cudaMemcpyAsync(c->g_misc.p, misc, sizeof(misc), cudaMemcpyHostToDevice, s), "upload guide");
+    k_guide_pack<<<(kGBf16 + 255) / 256, 256, 0, s>>>(c->g_params.as<float>(), c->g_wbf.as<uint16_t>(),
+                                                      c->g_bias.as<float>(), c->g_misc.as<uint32_t>(), 0, 0);
+    LUC_CUDA(c, cudaGetLastError(), "pack guide");
+    LUC_CUDA(c, cudaStreamSynchronize(s), "guide init");
+    c->guide_ready = true;
+    return LUC_OK;
+}
+
+int32_t luc_guide_configure(luc_ctx* c, uint32_t train, uint32_t records_per_step, float lr) {
+    if (!c) return LUC_ERR_VALIDATION;
+    if (records_per_step == 0 || records_per_step > (1u << 24))
+        return luc_fail(c, LUC_ERR_VALIDATION, "records_per_step must be in 1..=2^24");
+    if (!(lr > 0.0f) || !std::isfinite(lr)) return luc_fail(c, LUC_ERR_VALIDATION, "lr must be positive and finite");
+    c->guide_train = train != 0;
+    c->guide_rec_cap = records_per_step;
+    c->guide_lr = lr;
+    return LUC_OK;
+}
+
+int32_t luc_guide_get_params(luc_ctx* c, float* out) {
+    if (!c || !out) return LUC_ERR_VALIDATION;
+    if (int32_t rc = require_guide(c)) return rc;
+    cudaSetDevice(c->device);
+    LUC_CUDA(c, cudaMemcpyAsync(out, c->g_params.p, kGParams * sizeof(float), cudaMemcpyDeviceToHost, c->stream),
+             "read guide");
+    LUC_CUDA(c, cudaStreamSynchronize(c->stream), "read guide");
+    return LUC_OK;
+}
+
+int32_t luc_guide_stats(luc_ctx* c, luc_guide_info* out) {
+    if (!c || !out) return LUC_ERR_VALIDATION;
+    if (int32_t rc = require_guide(c)) return rc;
+    cudaSetDevice(c->device);
+    uint32_t misc[kGmWords];
+    LUC_CUDA(c, cudaMemcpyAsync(misc, c->g_misc.p, sizeof(misc), cudaMemcpyDeviceToHost, c->stream), "read guide");
+    LUC_CUDA(c, cudaStreamSynchronize(c->stream), "read guide");
+    out->steps = misc[kGmStep];
+    out->last_records = misc[kGmLastRecords];
+    std::memcpy(&out->last_loss, &misc[kGmLastLoss], 4);
+    out->threshold = misc[kGmThreshold];
+    out->num_params = kGParams;
+    return LUC_OK;
+}
+
+int32_t luc_guide_forward(luc_ctx* c, const float* in9, uint32_t n, float* out40) {
+    if (!c || (n && (!in9 || !out40))) return LUC_ERR_VALIDATION;
+    if (int32_t rc = require_guide(c)) return rc;
+    if (n == 0) return LUC_OK;
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    LUC_CUDA(c, c->g_io.ensure((size_t)n * (9 + kGOut) * sizeof(float)), "allocate guide io");
+    float* din = c->g_io.as<float>();
+    float* dout = din + (size_t)n * 9;
+    LUC_CUDA(c, cudaMemcpyAsync(din, in9, (size_t)n * 9 * sizeof(float), cudaMemcpyHostToDevice, s), "upload");
+    int grid = (int)std::min<uint64_t>((n + kTileRows - 1) / kTileRows, (uint64_t)c->num_sms * 2);
+    k_guide_forward<<<grid, kGuideThreads, sizeof(InferSmem), s>>>(din, n, luc_guide_dev(c), dout);
+    LUC_CUDA(c, cudaGetLastError(), "guide forward");
+    LUC_CUDA(c, cudaMemcpyAsync(out40, dout, (size_t)n * kGOut * sizeof(float), cudaMemcpyDeviceToHost, s), "readback");
+    LUC_CUDA(c, cudaStreamSynchronize(s), "guide forward");
+    return LUC_OK;
+}
+
+int32_t luc_guide_train_records(luc_ctx* c, const float* records, uint32_t n, uint32_t steps, float* grad_out,
+                                float* loss_out) {
+    if (!c || (n && !records)) return LUC_ERR_VALIDATION;
+    if (int32_t rc = require_guide(c)) return rc;
+    if (n == 0) return luc_fail(c, LUC_ERR_VALIDATION, "no records");
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    LUC_CUDA(c, c->g_io.ensure((size_t)n * kGRecF4 * sizeof(float4)), "allocate guide io");
+    float4* rec = c->g_io.as<float4>();
+    LUC_CUDA(c, cudaMemcpyAsync(rec, records, (size_t)n * kGRecF4 * sizeof(float4), cudaMemcpyHostToDevice, s),
+             "upload records");
+    uint32_t* gm = c->g_misc.as<uint32_t>();
+    const uint32_t rounds = steps == 0 ? 1 : steps;
+    const int grid = (int)std::min<uint64_t>((n + kTileRows - 1) / kTileRows, (uint64_t)c->num_sms);
+    const uint32_t count = n;
+    for (uint32_t it = 0; it < rounds; ++it) {
+        LUC_CUDA(c, cudaMemcpyAsync(gm + kGmRecords, &count, sizeof(count), cudaMemcpyHostToDevice, s), "upload count");
+        LUC_CUDA(c, cudaMemsetAsync(gm + kGmWeightSum, 0, 2 * sizeof(uint32_t), s), "clear sums");
+        LUC_CUDA(c, cudaMemsetAsync(c->g_grad.p, 0, kGParams * sizeof(float), s), "clear gradient");
+        k_guide_weight_sum<<<c->num_sms * 2, 256, 0, s>>>(rec, n, gm);
+        k_guide_train<<<grid, kGuideThreads, sizeof(TrainSmem), s>>>(rec, n, gm, luc_guide_dev(c),
+                                                                     c->g_grad.as<float>());
+        if (steps > 0) {
+            k_guide_adam<<<(kGParams + 255) / 256, 256, 0, s>>>(c->g_params.as<float>(), c->g_m.as<float>(),
+                                                                c->g_v.as<float>(), c->g_grad.as<float>(), gm,
+                                                                c->guide_lr);
+            k_guide_pack<<<(kGBf16 + 255) / 256, 256, 0, s>>>(c->g_params.as<float>(), c->g_wbf.as<uint16_t>(),
+                                                              c->g_bias.as<float>(), gm, n, 1u);
+        }
+        LUC_CUDA(c, cudaGetLastError(), "guide train");
+    }
+    uint32_t misc[kGmWords];
+    LUC_CUDA(c, cudaMemcpyAsync(misc, gm, sizeof(misc), cudaMemcpyDeviceToHost, s), "read guide");
+    if (grad_out)
+        LUC_CUDA(c, cudaMemcpyAsync(grad_out, c->g_grad.p, kGParams * sizeof(float), cudaMemcpyDeviceToHost, s),
+                 "read gradient");
+    LUC_CUDA(c, cudaStreamSynchronize(s), "guide train");
+    if (loss_out) std::memcpy(loss_out, &misc[steps > 0 ? kGmLastLoss : kGmLoss], 4);
+    return LUC_OK;
+}
+
+int32_t luc_guide_mixture(luc_ctx* c, const float* raw40, const float* in3, uint32_t n, int32_t mode, float* dir3,
+                          float* pdf) {
+    if (!c || (n && (!raw40 || !in3 || !pdf || (mode == 0 && !dir3)))) return LUC_ERR_VALIDATION;
+    if (mode != 0 && mode != 1) return luc_fail(c, LUC_ERR_VALIDATION, "mode must be 0 (sample) or 1 (pdf)");
+    if (n == 0) return LUC_OK;
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    LUC_CUDA(c, c->g_io.ensure((size_t)n * (kGOut + 3 + 3 + 1) * sizeof(float)), "allocate guide io");
+    float* draw = c->g_io.as<float>();
+    float* din = draw + (size_t)n * kGOut;
+    float* ddir = din + (size_t)n * 3;
+    float* dpdf = ddir + (size_t)n * 3;
+    LUC_CUDA(c, cudaMemcpyAsync(draw, raw40, (size_t)n * kGOut * 4, cudaMemcpyHostToDevice, s), "upload");
+    LUC_CUDA(c, cudaMemcpyAsync(din, in3, (size_t)n * 3 * 4, cudaMemcpyHostToDevice, s), "upload");
+    k_guide_mixture_eval<<<(n + 255) / 256, 256, 0, s>>>(draw, din, n, mode, ddir, dpdf);
+    LUC_CUDA(c, cudaGetLastError(), "guide mixture");
+    if (mode == 0) LUC_CUDA(c, cudaMemcpyAsync(dir3, ddir, (size_t)n * 3 * 4, cudaMemcpyDeviceToHost, s), "readback");
+    LUC_CUDA(c, cudaMemcpyAsync(pdf, dpdf, (size_t)n * 4, cudaMemcpyDeviceToHost, s), "readback");
+    LUC_CUDA(c, cudaStreamSynchronize(s), "guide mixture");
+    return LUC_OK;
+}
+
+}  // extern "C"

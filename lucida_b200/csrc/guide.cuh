@@ -21,12 +21,44 @@ constexpr int kGBf16 = kGHid * kGIn + 2 * kGHid * kGHid + kGOutPad * kGHid;  // 
 constexpr int kGBias = 3 * kGHid + kGOutPad;
 constexpr float kGKappaMax = 1.0e4f;
 constexpr int kGLobeF4 = 10;  // per path: 8 x (mu, kappa) + 2 x 4 weights
+constexpr int kGRecF4 = 5;    // per training record, see below
+// Vertices are guided when opaque and not near-specular; sharper lobes and
+// transmission stay BSDF-sampled.
+constexpr float kGuideMinRoughness = 0.2f;
+
+// Device bookkeeping words (u32, floats stored as bits).
+constexpr int kGmRecords = 0;     // records appended this batch
+constexpr int kGmStep = 1;        // Adam steps taken
+constexpr int kGmWeightSum = 2;   // sum of F over the batch's records (f32)
+constexpr int kGmLoss = 3;        // loss accumulated by the training kernel (f32)
+constexpr int kGmCandidates = 4;  // guided, surviving vertices this batch
+constexpr int kGmThreshold = 5;   // recording threshold, 16-bit fraction
+constexpr int kGmLastLoss = 6;    // loss of the last step (f32)
+constexpr int kGmLastRecords = 7; // records used by the last step
+constexpr int kGmWords = 16;
+
+// Training record, 5 float4 per guided vertex:
+//   [0] position, F (written by the finalize kernel; path id bits before)
+//   [1] shading normal, throughput after scattering .x
+//   [2] outgoing direction (world), throughput .y
+//   [3] sampled direction (world), throughput .z
+//   [4] path radiance when the continuation started, mixture pdf p(wi)
 
 struct GuideDev {
     const uint16_t* wbf;   // packed bf16 weights
     const float* bias;     // packed fp32 biases
-    float lo[3], inv_ext[3];  // scene box for the position encoding
+    float lo[3], ext[3];  // scene box for the position encoding (ext = hi - lo, or 1)
 };
+
+// 32-bit integer mix (Wellons' "lowbias32" constants) for record selection.
+LUC_D uint32_t mix32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
 
 // Decoded mixture of one vertex, as stored for SHADE.
 struct Mixture {
@@ -58,7 +90,20 @@ LUC_D float mixture_pdf(const Mixture& m, V3 d) {
     return p;
 }
 
-// Pick a lobe with u0, then sample it (Wood 1994 inversion in the lobe frame).
+// Sample one vMF lobe (Wood 1994 inversion of the cosine's CDF, in the
+// Duff et al. frame around the lobe direction).
+LUC_D V3 vmf_sample(float4 l, float u1, float u2) {
+    float kappa = l.w;
+    float W = 1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * kappa)) / kappa;
+    W = fminf(fmaxf(W, -1.0f), 1.0f);
+    float s = sqrtf(fmaxf(1.0f - W * W, 0.0f));
+    float sp, cp;
+    sincosf(2.0f * kPi * u2, &sp, &cp);
+    V3 local{s * cp, s * sp, W};
+    return normalize(to_world(local, V3{l.x, l.y, l.z}));
+}
+
+// Pick a lobe with u0 by weight, then sample it with (u1, u2).
 LUC_D V3 mixture_sample(const Mixture& m, float u0, float u1, float u2) {
     int j = kGLobes - 1;
     float acc = 0.0f;
@@ -70,15 +115,36 @@ LUC_D V3 mixture_sample(const Mixture& m, float u0, float u1, float u2) {
             break;
         }
     }
-    float4 l = m.lobe[j];
-    float kappa = l.w;
-    float W = 1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * kappa)) / kappa;
-    W = fminf(fmaxf(W, -1.0f), 1.0f);
-    float s = sqrtf(fmaxf(1.0f - W * W, 0.0f));
-    float sp, cp;
-    __sincosf(2.0f * kPi * u2, &sp, &cp);
-    V3 local{s * cp, s * sp, W};
-    return normalize(to_world(local, V3{l.x, l.y, l.z}));
+    return vmf_sample(m.lobe[j], u1, u2);
+}
+
+// The same two operations reading the stored mixture (kGLobeF4 float4 per
+// path) from memory lobe by lobe, so SHADE holds no mixture in registers.
+LUC_D float mixture_pdf_mem(const float4* __restrict__ L, V3 d) {
+    const float4 wa = L[8], wb = L[9];
+    const float w[kGLobes] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+    float p = 0.0f;
+#pragma unroll
+    for (int j = 0; j < kGLobes; ++j) {
+        float4 l = L[j];
+        p += w[j] * vmf_pdf(l.w, l.x * d.x + l.y * d.y + l.z * d.z);
+    }
+    return p;
+}
+LUC_D V3 mixture_sample_mem(const float4* __restrict__ L, float u0, float u1, float u2) {
+    const float4 wa = L[8], wb = L[9];
+    const float w[kGLobes] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+    int j = kGLobes - 1;
+    float acc = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kGLobes; ++k) {
+        acc += w[k];
+        if (u0 < acc) {
+            j = k;
+            break;
+        }
+    }
+    return vmf_sample(L[j], u1, u2);
 }
 
 }  // namespace luc

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <vector>
+#include "guide.cuh"
 #include "scene_dev.cuh"
 
 namespace luc {
@@ -33,6 +34,11 @@ struct PathState {
     // [0] extend rays, [1] extend node visits, [2] extend triangle tests,
     // [3] shadow rays, [4] shadow node visits, [5] shadow triangle tests.
     unsigned long long* stat;
+    // Guided frames: the decoded mixture per path (kGLobeF4 float4), the
+    // training records and the guide's bookkeeping words.
+    float4* lobes;
+    float4* rec;
+    uint32_t* gmisc;
 };
 
 struct FrameParams {
@@ -41,13 +47,16 @@ struct FrameParams {
     uint32_t sample_base, batch_samples;
     uint32_t frame_seed, sampler_kind, sampling, max_depth;
     uint32_t guides;
+    uint32_t guided;   // one-sample MIS with the learned proposal
+    uint32_t rec_cap;  // training records per batch (0: no recording)
+    GuideDev guide;
     float lens_radius;
     V3 cam_origin, cam_upper_left, cam_horizontal, cam_vertical;
 };
 
 // CUDA-event marks between stages, accumulated per stage.
 struct StageTimer {
-    enum Stage { kGenerate = 0, kExtend, kShade, kConnect, kResolve, kEnd, kCount };
+    enum Stage { kGenerate = 0, kExtend, kShade, kConnect, kResolve, kGuide, kTrain, kEnd, kCount };
     std::vector<cudaEvent_t> events;
     std::vector<int> stages;
     void mark(cudaStream_t s, int stage) {
@@ -81,12 +90,26 @@ struct RenderState {
     uint64_t capacity = 0;  // paths
     uint32_t ctr_capacity = 0;
     int num_sms = 148;
-    int extend_blocks = 0, connect_blocks = 0, shade_blocks = 0;  // resident blocks per SM
+    int extend_blocks = 0, connect_blocks = 0, shade_blocks = 0, shade_blocks_guided = 0;  // resident blocks per SM
     uint64_t launches = 0;
 };
 
 void query_occupancy(RenderState& rs);
+// Guide training buffers (FP32 master weights, Adam moments, gradient) and
+// the packed copies the kernels read.
+struct GuideTrain {
+    float *params, *m, *v, *grad;
+    uint16_t* wbf;
+    float* bias;
+    float lr;
+    bool train;
+};
+
 void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream,
-                  StageTimer* timer);
+                  StageTimer* timer, const GuideTrain* gt);
+// guide.cu: per-depth inference and the post-batch training step.
+void launch_guide_infer(const RenderState& rs, const DevScene& sc, const FrameParams& fp, uint32_t depth,
+                        cudaStream_t s);
+void launch_guide_train(const RenderState& rs, const FrameParams& fp, const GuideTrain& gt, cudaStream_t s);
 
 }  // namespace luc

