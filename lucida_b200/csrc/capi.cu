@@ -164,7 +164,7 @@ void luc_destroy(luc_ctx* c) {
     cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->materials, &c->prims,    &c->lights,   &c->positions, &c->attrs,     &c->tris,
                       &c->nodes,     &c->env_px,   &c->env_cond, &c->env_marg,  &c->env_row_sin, &c->energy,
-                      &c->tnodes,    &c->soup,
+                      &c->tnodes,    &c->soup,     &c->frame_word,
                       &c->pool,      &c->accum_tmp, &c->lb_tris, &c->lb_pos,    &c->lb_boxes,  &c->lb_keys,
                       &c->lb_vals,   &c->lb_keys2, &c->lb_vals2, &c->lb_hist,   &c->lb_karras, &c->lb_parent,
                       &c->lb_nbounds, &c->lb_subtree, &c->lb_flags, &c->lb_nodes, &c->lb_rank, &c->lb_misc,
@@ -410,12 +410,15 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
         rc = luc_guide_prepare_frame(c, c->rs.capacity);
         if (rc) return rc;
         c->rs.ps.lobes = c->g_lobes.as<float4>();
+        c->rs.ps.lobe_stride = c->rs.capacity;
         c->rs.ps.rec = c->g_rec.as<float4>();
         c->rs.ps.gmisc = c->g_misc.as<uint32_t>();
     }
     const GuideTrain gt = guided ? luc_guide_train_state(c) : GuideTrain{};
 
+    LUC_CUDA(c, c->frame_word.ensure(256), "allocate frame word");
     FrameParams fp{};
+    fp.sbase = c->frame_word.as<uint32_t>();
     fp.pixels = (uint32_t)pixels;
     fp.width = u->width;
     fp.height = u->height;
@@ -450,7 +453,11 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     if (one_batch && c->use_graphs) {
         // Single-batch frame: capture it once as a CUDA graph and replay it
         // while the frame parameters, scene, pool and accumulator repeat.
-        fp.sample_base = u->sample_offset;
+        // The sample offset reaches the kernels through the frame word, so
+        // the graph (keyed on everything else) replays across offsets.
+        fp.sample_base = 0;
+        const uint32_t sbase = u->sample_offset;
+        LUC_CUDA(c, cudaMemcpyAsync(c->frame_word.p, &sbase, 4, cudaMemcpyHostToDevice, s), "upload sample base");
         fp.batch_samples = spp;
         fp.num_paths = (uint64_t)spp * pixels;
         uint32_t lr_bits = 0;
@@ -492,6 +499,8 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
         for (uint32_t done = 0; done < spp;) {
             uint32_t n = (uint32_t)std::min<uint64_t>(per_batch, spp - done);
             fp.sample_base = u->sample_offset + done;
+            LUC_CUDA(c, cudaMemcpyAsync(c->frame_word.p, &fp.sample_base, 4, cudaMemcpyHostToDevice, s),
+                     "upload sample base");
             fp.batch_samples = n;
             fp.num_paths = (uint64_t)n * pixels;
             record_batch(c->rs, sc, fp, accum, s, tp, &gt);

@@ -53,7 +53,7 @@ struct luc_ctx {
     uint32_t num_materials = 0;
     // Path pool and frame.
     luc::RenderState rs;
-    DevBuf pool, accum_tmp;
+    DevBuf pool, accum_tmp, frame_word;  // frame_word: the batch's first sample index (FrameParams::sbase)
     luc_render_stats stats{};
     uint64_t path_budget = 1ull << 25;
     // LBVH / sort scratch.

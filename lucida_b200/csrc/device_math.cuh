@@ -74,19 +74,26 @@ LUC_HD int32_t f2i(float x) {
     return (int32_t)x;
 }
 
-// Transcendentals: one rounding from a double evaluation.
-LUC_D float dsin(float x) { return (float)sin((double)x); }
-LUC_D float dcos(float x) { return (float)cos((double)x); }
-LUC_D void dsincos(float x, float& s, float& c) {
+// Transcendentals: one rounding from a double evaluation. Not inlined: the
+// double-precision routines are long, and one copy per kernel keeps the
+// shading kernels' instruction footprint inside the instruction cache.
+#define LUC_DN static __device__ __noinline__
+LUC_DN float dsin(float x) { return (float)sin((double)x); }
+LUC_DN float dcos(float x) { return (float)cos((double)x); }
+LUC_DN float2 dsincos2(float x) {
     double sd, cd;
     sincos((double)x, &sd, &cd);
-    s = (float)sd;
-    c = (float)cd;
+    return make_float2((float)sd, (float)cd);
 }
-LUC_D float dacos(float x) { return (float)acos((double)x); }
-LUC_D float datan2(float y, float x) { return (float)atan2((double)y, (double)x); }
-LUC_D float dexp(float x) { return (float)exp((double)x); }
-LUC_D float dpow(float x, float y) { return (float)pow((double)x, (double)y); }
+LUC_D void dsincos(float x, float& s, float& c) {
+    float2 r = dsincos2(x);
+    s = r.x;
+    c = r.y;
+}
+LUC_DN float dacos(float x) { return (float)acos((double)x); }
+LUC_DN float datan2(float y, float x) { return (float)atan2((double)y, (double)x); }
+LUC_DN float dexp(float x) { return (float)exp((double)x); }
+LUC_DN float dpow(float x, float y) { return (float)pow((double)x, (double)y); }
 
 // ------------------------------------------------------------------ samplers
 // PCG-RXS-M-XS with counter seeding (crates/core/src/rng.rs:28-86).
@@ -468,17 +475,17 @@ struct BsdfSample {
     V3 wi, weight;
     float pdf;
 };
-// surface::sample (bsdf.rs:1571-1661).
-LUC_D BsdfSample bsdf_sample(const Surface& s, const float* table, V3 wo, float u_lobe, float ux, float uy) {
-    BsdfSample bad{V3{0.0f, 0.0f, 1.0f}, splat(0.0f), 0.0f};
-    if (wo.z <= 0.0f) return bad;
+// The direction half of surface::sample (bsdf.rs:1571-1661): lobe choice by
+// u_lobe, then GGX reflection (VNDF), rough transmission or cosine-weighted
+// diffuse. False where surface::sample returns no sample.
+LUC_D bool bsdf_sample_dir(const Surface& s, const float* table, V3 wo, float u_lobe, float ux, float uy, V3& wi) {
+    if (wo.z <= 0.0f) return false;
     float p_spec = specular_probability(s, table, wo.z);
     float alpha = rough_to_alpha(s.roughness);
-    V3 wi;
     if (u_lobe < p_spec) {
         V3 m = sample_vndf(wo, alpha, ux, uy);
         V3 r = reflect(wo, m);
-        if (r.z <= 0.0f) return bad;
+        if (r.z <= 0.0f) return false;
         wi = r;
     } else if (u_lobe < p_spec + (1.0f - p_spec) * s.transmission) {
         V3 m = sample_vndf(wo, alpha, ux, uy);
@@ -486,16 +493,24 @@ LUC_D BsdfSample bsdf_sample(const Surface& s, const float* table, V3 wo, float 
         float ci = dot(wo, m);
         float sin2_i = fmaxf(1.0f - ci * ci, 0.0f);
         float sin2_t = sin2_i / (eta * eta);
-        if (sin2_t >= 1.0f) return bad;
+        if (sin2_t >= 1.0f) return false;
         float ct = sqrtf(1.0f - sin2_t);
         V3 wt = normalize_or(-wo / eta + (ci / eta - copysignf(ct, ci)) * m, splat(0.0f));
-        if (wt.z >= 0.0f) return bad;
+        if (wt.z >= 0.0f) return false;
         wi = wt;
     } else {
         wi = cosine_hemisphere(ux, uy);
     }
-    if (wi.z == 0.0f || wi == splat(0.0f)) return bad;
-    if (wi.z < 0.0f && s.transmission <= 0.0f) return bad;
+    if (wi.z == 0.0f || wi == splat(0.0f)) return false;
+    if (wi.z < 0.0f && s.transmission <= 0.0f) return false;
+    return true;
+}
+
+// surface::sample (bsdf.rs:1571-1661): direction, then f and the pdf there.
+LUC_D BsdfSample bsdf_sample(const Surface& s, const float* table, V3 wo, float u_lobe, float ux, float uy) {
+    BsdfSample bad{V3{0.0f, 0.0f, 1.0f}, splat(0.0f), 0.0f};
+    V3 wi;
+    if (!bsdf_sample_dir(s, table, wo, u_lobe, ux, uy, wi)) return bad;
     V3 f = bsdf_eval(s, table, wo, wi);
     float pdf = bsdf_pdf(s, table, wo, wi);
     if (pdf <= 0.0f) return bad;

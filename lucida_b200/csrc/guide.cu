@@ -3,13 +3,15 @@
 // weight-gradient accumulation for training), record finalisation and Adam.
 // The model and the record layout are described in guide.cuh.
 //
-// Matrix products use mma.sync m16n8k16 (BF16 inputs, FP32 accumulate) with
-// operands staged in shared memory and fed by ldmatrix (.trans where the
-// product needs the transposed operand), so one row-major copy of every
-// weight and activation tile serves the forward, input-gradient and
-// weight-gradient products. A CTA of 4 warps owns a 64-row tile, one warp per
-// 16 rows; weight gradients accumulate in shared-memory FP32 across all the
-// tiles a persistent CTA processes and reach global memory once per CTA.
+// Matrix products use mma.sync m16n8k16 (BF16 inputs, FP32 accumulate). The
+// forward pass (inference and training alike) runs a warp's 16 rows entirely
+// in registers, layer to layer, with the weights in shared memory fed by
+// ldmatrix. Training stores the forward activations as row-major BF16 tiles;
+// the backward products read them through ldmatrix (.trans where the product
+// needs the transposed operand), so one copy of every tile serves the
+// input-gradient and weight-gradient products. A training CTA of 4 warps owns
+// a 64-row tile; weight gradients accumulate in shared-memory FP32 across all
+// the tiles a persistent CTA processes and reach global memory once per CTA.
 //
 // Every kernel reads its row count and normalisers from device memory, so the
 // per-batch training step (finalise -> train -> Adam -> pack) is captured in
@@ -83,109 +85,6 @@ __device__ __forceinline__ void load_net(NetSmem& s, const uint16_t* __restrict_
     for (int i = t; i < kGBias; i += nt) s.b[i] = bias[i];
 }
 
-// Features of one row into shared memory (bf16); lane l writes features
-// l, l + 32, l + 64, l + 96. Order: position axis a, frequency k, (sin, cos)
-// at 24a + 2k; then normal and outgoing direction at 72 + 24v + 8a + 2k.
-__device__ __forceinline__ void encode_row(uint16_t* __restrict__ xrow, const float (&in)[9], const GuideDev& g, int lane) {
-#pragma unroll
-    for (int f0 = 0; f0 < kGIn; f0 += 32) {
-        const int f = f0 + lane;
-        float v = 0.0f;
-        if (f < 72) {
-            int a = f / 24, k = (f % 24) >> 1;
-            float q = fminf(fmaxf((in[a] - g.lo[a]) / g.ext[a], 0.0f), 1.0f);
-            float arg = q * (kPi * (float)(1 << k));
-            v = (f & 1) ? cosf(arg) : sinf(arg);
-        } else if (f < kGFeatures) {
-            int r = f - 72, which = r / 24, a = (r % 24) / 8, k = (r % 8) >> 1;
-            float arg = in[3 + 3 * which + a] * (kPi * (float)(1 << k));
-            v = (f & 1) ? cosf(arg) : sinf(arg);
-        }
-        xrow[f] = to_bf16(v);
-    }
-}
-
-// Broadcast lanes 0..15's row inputs in turn and encode the warp's 16 rows.
-__device__ __forceinline__ void encode_rows(uint16_t* __restrict__ x, const float (&mine)[9], const GuideDev& g, int r0, int lane) {
-    for (int r = 0; r < 16; ++r) {
-        float v[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) v[k] = __shfl_sync(0xFFFFFFFFu, mine[k], r);
-        encode_row(x + (r0 + r) * kSIn, v, g, lane);
-    }
-}
-
-// out[rows r0..r0+15][0..N) = act(A[rows][0..K) W^T + b); A, W and out bf16.
-template <int K, int SA, int N, bool RELU>
-__device__ void dense_fwd_bf16(const uint16_t* __restrict__ A, const uint16_t* __restrict__ W, const float* __restrict__ b,
-                               uint16_t* __restrict__ out, int r0, int lane) {
-    uint32_t af[K / 16][4];
-#pragma unroll
-    for (int kt = 0; kt < K / 16; ++kt)
-        ldsm_x4(af[kt], A + (r0 + (lane & 7) + 8 * ((lane >> 3) & 1)) * SA + kt * 16 + 8 * (lane >> 4));
-    const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int nt = 0; nt < N / 8; ++nt) {
-        float c[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int kt = 0; kt < K / 16; ++kt) {
-            uint32_t bf[2];
-            ldsm_x2(bf, W + (nt * 8 + (lane & 7)) * SA + kt * 16 + 8 * ((lane >> 3) & 1));
-            mma16816(c, af[kt], bf);
-        }
-        const int n = nt * 8 + 2 * t;
-        float b0 = b[n], b1 = b[n + 1];
-        float v0 = c[0] + b0, v1 = c[1] + b1, v2 = c[2] + b0, v3 = c[3] + b1;
-        if (RELU) {
-            v0 = fmaxf(v0, 0.f);
-            v1 = fmaxf(v1, 0.f);
-            v2 = fmaxf(v2, 0.f);
-            v3 = fmaxf(v3, 0.f);
-        }
-        *reinterpret_cast<uint32_t*>(out + (r0 + g) * kSHid + n) = pack_bf16(v0, v1);
-        *reinterpret_cast<uint32_t*>(out + (r0 + g + 8) * kSHid + n) = pack_bf16(v2, v3);
-    }
-}
-
-// Last layer: FP32 outputs (rows r0..r0+15, 48 columns) into O[64][48].
-__device__ void dense_out_f32(const uint16_t* __restrict__ A, const NetSmem& net, float* __restrict__ O, int r0,
-                              int lane) {
-    uint32_t af[kGHid / 16][4];
-#pragma unroll
-    for (int kt = 0; kt < kGHid / 16; ++kt)
-        ldsm_x4(af[kt], A + (r0 + (lane & 7) + 8 * ((lane >> 3) & 1)) * kSHid + kt * 16 + 8 * (lane >> 4));
-    const int g = lane >> 2, t = lane & 3;
-    const float* b = net.b + 3 * kGHid;
-#pragma unroll
-    for (int nt = 0; nt < kGOutPad / 8; ++nt) {
-        float c[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int kt = 0; kt < kGHid / 16; ++kt) {
-            uint32_t bf[2];
-            ldsm_x2(bf, net.w4 + (nt * 8 + (lane & 7)) * kSHid + kt * 16 + 8 * ((lane >> 3) & 1));
-            mma16816(c, af[kt], bf);
-        }
-        const int n = nt * 8 + 2 * t;
-        O[(r0 + g) * kGOutPad + n] = c[0] + b[n];
-        O[(r0 + g) * kGOutPad + n + 1] = c[1] + b[n + 1];
-        O[(r0 + g + 8) * kGOutPad + n] = c[2] + b[n];
-        O[(r0 + g + 8) * kGOutPad + n + 1] = c[3] + b[n + 1];
-    }
-}
-
-// The whole forward pass of the warp's 16 rows: X -> H1 -> H2 -> H3 -> O.
-__device__ __forceinline__ void forward_rows(const NetSmem& net, const uint16_t* x, uint16_t* h1, uint16_t* h2, uint16_t* h3, float* o,
-                             int r0, int lane) {
-    dense_fwd_bf16<kGIn, kSIn, kGHid, true>(x, net.w1, net.b, h1, r0, lane);
-    __syncwarp();
-    dense_fwd_bf16<kGHid, kSHid, kGHid, true>(h1, net.w2, net.b + kGHid, h2, r0, lane);
-    __syncwarp();
-    dense_fwd_bf16<kGHid, kSHid, kGHid, true>(h2, net.w3, net.b + 2 * kGHid, h3, r0, lane);
-    __syncwarp();
-    dense_out_f32(h3, net, o, r0, lane);
-    __syncwarp();
-}
-
 __device__ __forceinline__ float softplus_f(float x) { return x > 20.0f ? x : log1pf(expf(x)); }
 
 // Raw outputs -> (mu, kappa) x 8 and softmax weights.
@@ -206,38 +105,172 @@ __device__ __forceinline__ void decode_row(const float* __restrict__ o, float4* 
     }
 }
 
+// ---------------------------------------------------------------- inference
+// Inference keeps a warp's 16 rows in registers from the features to the
+// outputs: the m16n8 accumulator fragments of n-tiles 2j and 2j+1 are, after
+// bias, ReLU and BF16 packing, exactly the m16k16 A fragment of k-tile j of
+// the next layer, so hidden activations never touch shared memory. The
+// features are computed straight into the first layer's A fragments: lane
+// (g = lane / 4, t = lane % 4) holds feature pairs 16 kt + 8 h + 2 t of rows g
+// and g + 8, and every pair is (sin, cos) of one argument. Only the weights
+// (shared by the CTA) and a 16 x 48 FP32 output tile per warp live in shared
+// memory.
+constexpr int kInferWarps = 8;
+
 struct InferSmem {
     NetSmem net;
-    uint16_t x[kTileRows * kSIn];
-    uint16_t h[2][kTileRows * kSHid];
-    float o[kTileRows * kGOutPad];
+    float o[kInferWarps][16 * kGOutPad];
 };
 
-// Per bounce: the decoded mixture of every queued path whose ray hit a
-// surface, into ps.lobes. Inputs are the hit point, the shading normal and the
-// outgoing direction -dir, as SHADE computes them.
-__global__ void __launch_bounds__(kGuideThreads) k_guide_infer(PathState ps, DevScene sc, FrameParams fp,
-                                                                uint32_t depth) {
+// (sin, cos) of feature pair f0 + 2t of one row, packed as bf16x2. f0 is a
+// multiple of 8 known at compile time after unrolling, so the input component
+// each feature reads is a constant index.
+template <int F0>
+__device__ __forceinline__ uint32_t feature_pair(const float (&in)[9], const GuideDev& g, int t) {
+    if (F0 >= kGFeatures) return 0u;
+    float arg;
+    if (F0 < 72) {
+        constexpr int a = F0 / 24, k0 = (F0 % 24) / 2;
+        float q = fminf(fmaxf((in[a] - g.lo[a]) / g.ext[a], 0.0f), 1.0f);
+        arg = q * (kPi * (float)(1 << (k0 + t)));
+    } else {
+        constexpr int r = F0 - 72, comp = 3 + 3 * (r / 24) + (r % 24) / 8;
+        arg = in[comp] * (kPi * (float)(1 << t));
+    }
+    float sn, cs;
+    sincosf(arg, &sn, &cs);
+    return pack_bf16(sn, cs);
+}
+
+template <int KT>
+__device__ __forceinline__ void features_kt(uint32_t (&a)[4], const float (&r0)[9], const float (&r1)[9],
+                                            const GuideDev& g, int t) {
+    a[0] = feature_pair<16 * KT>(r0, g, t);
+    a[1] = feature_pair<16 * KT>(r1, g, t);
+    a[2] = feature_pair<16 * KT + 8>(r0, g, t);
+    a[3] = feature_pair<16 * KT + 8>(r1, g, t);
+}
+
+// One hidden layer from register A fragments (KT k-tiles) to the next
+// layer's A fragments (N / 16 k-tiles), with bias and ReLU.
+template <int KT, int N, int SW>
+__device__ __forceinline__ void layer_regs(const uint32_t (&a)[KT][4], const uint16_t* __restrict__ W,
+                                           const float* __restrict__ b, uint32_t (&out)[N / 16][4], int lane) {
+    const int t = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < N / 8; ++nt) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int kt = 0; kt < KT; ++kt) {
+            uint32_t bf[2];
+            ldsm_x2(bf, W + (nt * 8 + (lane & 7)) * SW + kt * 16 + 8 * ((lane >> 3) & 1));
+            mma16816(c, a[kt], bf);
+        }
+        const int n = nt * 8 + 2 * t;
+        const float b0 = b[n], b1 = b[n + 1];
+        out[nt >> 1][(nt & 1) * 2] = pack_bf16(fmaxf(c[0] + b0, 0.f), fmaxf(c[1] + b1, 0.f));
+        out[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16(fmaxf(c[2] + b0, 0.f), fmaxf(c[3] + b1, 0.f));
+    }
+}
+
+// Store an A-fragment set (KT k-tiles) of rows g, g + 8 as a row-major bf16
+// tile (row stride SX), the layout the backward pass reads.
+template <int KT, int SX>
+__device__ __forceinline__ void store_frags(const uint32_t (&a)[KT][4], uint16_t* __restrict__ x, int lane) {
+    const int t = lane & 3, gr = lane >> 2;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+        *reinterpret_cast<uint32_t*>(x + gr * SX + 16 * kt + 2 * t) = a[kt][0];
+        *reinterpret_cast<uint32_t*>(x + (gr + 8) * SX + 16 * kt + 2 * t) = a[kt][1];
+        *reinterpret_cast<uint32_t*>(x + gr * SX + 16 * kt + 8 + 2 * t) = a[kt][2];
+        *reinterpret_cast<uint32_t*>(x + (gr + 8) * SX + 16 * kt + 8 + 2 * t) = a[kt][3];
+    }
+}
+
+// The warp's forward pass: rows g and g + 8 of this lane's fragments have
+// inputs r0 and r1; raw outputs (+ bias) land in o[16][kGOutPad]. With kStore
+// the features and the three hidden activations are also written, row-major
+// BF16, to x (stride kSIn) and h1, h2, h3 (stride kSHid) for the backward pass.
+template <bool kStore>
+__device__ __forceinline__ void warp_forward(const NetSmem& net, const GuideDev& g, const float (&r0)[9],
+                                             const float (&r1)[9], float* __restrict__ o, int lane,
+                                             uint16_t* x = nullptr, uint16_t* h1 = nullptr, uint16_t* h2 = nullptr,
+                                             uint16_t* h3 = nullptr) {
+    const int t = lane & 3, gr = lane >> 2;
+    uint32_t a1[kGIn / 16][4];
+    features_kt<0>(a1[0], r0, r1, g, t);
+    features_kt<1>(a1[1], r0, r1, g, t);
+    features_kt<2>(a1[2], r0, r1, g, t);
+    features_kt<3>(a1[3], r0, r1, g, t);
+    features_kt<4>(a1[4], r0, r1, g, t);
+    features_kt<5>(a1[5], r0, r1, g, t);
+    features_kt<6>(a1[6], r0, r1, g, t);
+    features_kt<7>(a1[7], r0, r1, g, t);
+    if (kStore) store_frags<kGIn / 16, kSIn>(a1, x, lane);
+    uint32_t a2[kGHid / 16][4], a3[kGHid / 16][4];
+    layer_regs<kGIn / 16, kGHid, kSIn>(a1, net.w1, net.b, a2, lane);
+    if (kStore) store_frags<kGHid / 16, kSHid>(a2, h1, lane);
+    layer_regs<kGHid / 16, kGHid, kSHid>(a2, net.w2, net.b + kGHid, a3, lane);
+    if (kStore) store_frags<kGHid / 16, kSHid>(a3, h2, lane);
+    layer_regs<kGHid / 16, kGHid, kSHid>(a3, net.w3, net.b + 2 * kGHid, a2, lane);
+    if (kStore) store_frags<kGHid / 16, kSHid>(a2, h3, lane);
+    const float* b4 = net.b + 3 * kGHid;
+#pragma unroll
+    for (int nt = 0; nt < kGOutPad / 8; ++nt) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int kt = 0; kt < kGHid / 16; ++kt) {
+            uint32_t bf[2];
+            ldsm_x2(bf, net.w4 + (nt * 8 + (lane & 7)) * kSHid + kt * 16 + 8 * ((lane >> 3) & 1));
+            mma16816(c, a2[kt], bf);
+        }
+        const int n = nt * 8 + 2 * t;
+        *reinterpret_cast<float2*>(o + gr * kGOutPad + n) = make_float2(c[0] + b4[n], c[1] + b4[n + 1]);
+        *reinterpret_cast<float2*>(o + (gr + 8) * kGOutPad + n) = make_float2(c[2] + b4[n], c[3] + b4[n + 1]);
+    }
+}
+
+// Rows g and g + 8 of the inputs held by lanes 0..15 (one row each).
+__device__ __forceinline__ void gather_rows(const float (&mine)[9], float (&r0)[9], float (&r1)[9], int lane) {
+    const int gr = lane >> 2;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        r0[k] = __shfl_sync(0xFFFFFFFFu, mine[k], gr);
+        r1[k] = __shfl_sync(0xFFFFFFFFu, mine[k], gr + 8);
+    }
+}
+
+// Per bounce: the decoded mixture at every queue position whose ray hit a
+// surface (SoA planes of ps.lobe_stride). Inputs are the hit point, the
+// shading normal and the outgoing direction -dir, as SHADE computes them.
+// Each warp takes 32 queue positions at a time (every lane fetches one hit, so
+// the dependent loads of all 32 overlap), then runs them through the network
+// as two groups of 16 rows; two lanes decode a row (four lobes each, softmax
+// across the pair).
+__global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(PathState ps, DevScene sc, FrameParams fp,
+                                                                   uint32_t depth) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     InferSmem& S = *reinterpret_cast<InferSmem*>(smem_raw);
     load_net(S.net, fp.guide.wbf, fp.guide.bias);
     __syncthreads();
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
     const uint32_t* queue = ps.queue[depth & 1];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r0 = warp * 16;
-    for (uint32_t base = blockIdx.x * kTileRows; base < len; base += gridDim.x * kTileRows) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float* o = S.o[warp];
+    const uint32_t nwarps = gridDim.x * kInferWarps;
+    for (uint32_t base = (blockIdx.x * kInferWarps + warp) * 32u; base < len; base += nwarps * 32u) {
         float in[9] = {0, 0, 0, 0, 0, 1, 0, 0, 1};
-        uint32_t p = 0xFFFFFFFFu;
-        if (lane < 16 && base + r0 + lane < len) {
-            const uint32_t i = base + r0 + lane;
+        bool hit_row = false;
+        if (base + lane < len) {
+            const uint32_t i = base + lane;
             const uint32_t q = depth == 0 ? i : queue[i];
-            float4 h4 = ps.hit[q];
-            uint32_t id = __float_as_uint(h4.w);
+            const float4 h4 = ps.hit[q];
+            const uint32_t id = __float_as_uint(h4.w);
             if (id != kMiss) {
-                p = q;
-                float4 o4 = ps.o_pdf[q], d4 = ps.dir[q];
-                V3 dir{d4.x, d4.y, d4.z};
-                SurfaceHit hit = surface_hit(sc, id, h4.x, h4.y, h4.z, V3{o4.x, o4.y, o4.z}, dir);
+                hit_row = true;
+                const float4 o4 = ps.o_pdf[q], d4 = ps.dir[q];
+                const V3 dir{d4.x, d4.y, d4.z};
+                const SurfaceHit hit = surface_hit(sc, id, h4.x, h4.y, h4.z, V3{o4.x, o4.y, o4.z}, dir);
                 in[0] = hit.position.x;
                 in[1] = hit.position.y;
                 in[2] = hit.position.z;
@@ -249,22 +282,51 @@ __global__ void __launch_bounds__(kGuideThreads) k_guide_infer(PathState ps, Dev
                 in[8] = -dir.z;
             }
         }
-        // A warp whose 16 rows all missed has nothing to infer.
-        if (__ballot_sync(0xFFFFFFFFu, p != 0xFFFFFFFFu) == 0) continue;
-        encode_rows(S.x, in, fp.guide, r0, lane);
-        __syncwarp();
-        forward_rows(S.net, S.x, S.h[0], S.h[1], S.h[0], S.o, r0, lane);
-        if (p != 0xFFFFFFFFu) {
-            float4 lobes[kGLobes];
-            float w[kGLobes];
-            decode_row(S.o + (r0 + lane) * kGOutPad, lobes, w);
-            float4* dst = ps.lobes + (size_t)p * kGLobeF4;
+        const uint32_t hits = __ballot_sync(0xFFFFFFFFu, hit_row);
+#pragma unroll 1
+        for (int half = 0; half < 2; ++half) {
+            const uint32_t hh = (hits >> (16 * half)) & 0xFFFFu;
+            if (hh == 0) continue;  // uniform across the warp
+            float r0[9], r1[9];
+            const int gr = (lane >> 2) + 16 * half;
 #pragma unroll
-            for (int j = 0; j < kGLobes; ++j) dst[j] = lobes[j];
-            dst[8] = make_float4(w[0], w[1], w[2], w[3]);
-            dst[9] = make_float4(w[4], w[5], w[6], w[7]);
+            for (int k = 0; k < 9; ++k) {
+                r0[k] = __shfl_sync(0xFFFFFFFFu, in[k], gr);
+                r1[k] = __shfl_sync(0xFFFFFFFFu, in[k], gr + 8);
+            }
+            warp_forward<false>(S.net, fp.guide, r0, r1, o, lane);
+            __syncwarp();
+            // Decode: lanes 2r and 2r + 1 share row r, lobes 4h .. 4h + 3.
+            const int r = lane >> 1, h = lane & 1;
+            const float* orow = o + r * kGOutPad + 20 * h;
+            float lg[4], mx = -INFINITY;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                lg[j] = orow[5 * j + 4];
+                mx = fmaxf(mx, lg[j]);
+            }
+            mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, 1));
+            float e[4], sum = 0.f;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                e[j] = expf(lg[j] - mx);
+                sum += e[j];
+            }
+            sum += __shfl_xor_sync(0xFFFFFFFFu, sum, 1);
+            if ((hh >> r) & 1u) {
+                const size_t st = ps.lobe_stride, i = base + 16 * half + r;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float x = orow[5 * j], y = orow[5 * j + 1], z = orow[5 * j + 2];
+                    const float ln = sqrtf(x * x + y * y + z * z);
+                    const float kappa = fminf(1.0f + softplus_f(orow[5 * j + 3]), kGKappaMax);
+                    ps.lobes[(4 * h + j) * st + i] =
+                        ln > 0.0f ? make_float4(x / ln, y / ln, z / ln, kappa) : make_float4(0.f, 0.f, 1.f, kappa);
+                }
+                ps.lobes[(8 + h) * st + i] = make_float4(e[0] / sum, e[1] / sum, e[2] / sum, e[3] / sum);
+            }
+            __syncwarp();
         }
-        __syncwarp();
     }
 }
 
@@ -434,9 +496,11 @@ __global__ void __launch_bounds__(kGuideThreads) k_guide_train(const float4* __r
             in[7] = c4.y;
             in[8] = c4.z;
         }
-        encode_rows(S.x, in, g, r0, lane);
+        float ra[9], rb[9];
+        gather_rows(in, ra, rb, lane);
+        warp_forward<true>(S.net, g, ra, rb, S.o + r0 * kGOutPad, lane, S.x + r0 * kSIn, S.h[0] + r0 * kSHid,
+                           S.h[1] + r0 * kSHid, S.h[2] + r0 * kSHid);
         __syncwarp();
-        forward_rows(S.net, S.x, S.h[0], S.h[1], S.h[2], S.o, r0, lane);
         // Loss epilogue: lanes 0..15, one row each.
         if (lane < 16) {
             const int r = r0 + lane;
@@ -600,25 +664,28 @@ __global__ void k_guide_pack(const float* __restrict__ p, uint16_t* __restrict__
     }
 }
 
-// Raw outputs for host-given inputs (x, n, wo per row).
-__global__ void __launch_bounds__(kGuideThreads) k_guide_forward(const float* __restrict__ in9, uint32_t n, GuideDev g,
-                                                                  float* __restrict__ out40) {
+// Raw outputs for host-given inputs (x, n, wo per row): the inference
+// kernel's forward pass, without the decode.
+__global__ void __launch_bounds__(kInferWarps * 32) k_guide_forward(const float* __restrict__ in9, uint32_t n,
+                                                                     GuideDev g, float* __restrict__ out40) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     InferSmem& S = *reinterpret_cast<InferSmem*>(smem_raw);
     load_net(S.net, g.wbf, g.bias);
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r0 = warp * 16;
-    for (uint32_t base = blockIdx.x * kTileRows; base < n; base += gridDim.x * kTileRows) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float* o = S.o[warp];
+    const uint32_t nwarps = gridDim.x * kInferWarps;
+    for (uint32_t base = (blockIdx.x * kInferWarps + warp) * 16u; base < n; base += nwarps * 16u) {
         float in[9] = {0, 0, 0, 0, 0, 1, 0, 0, 1};
-        const uint32_t i = base + r0 + lane;
-        if (lane < 16 && i < n)
-            for (int k = 0; k < 9; ++k) in[k] = in9[9 * (size_t)i + k];
-        encode_rows(S.x, in, g, r0, lane);
+        if (lane < 16 && base + lane < n)
+            for (int k = 0; k < 9; ++k) in[k] = in9[9 * (size_t)(base + lane) + k];
+        float r0[9], r1[9];
+        gather_rows(in, r0, r1, lane);
+        warp_forward<false>(S.net, g, r0, r1, o, lane);
         __syncwarp();
-        forward_rows(S.net, S.x, S.h[0], S.h[1], S.h[0], S.o, r0, lane);
         for (int k = lane; k < 16 * kGOut; k += 32) {
             const int r = k / kGOut, c = k % kGOut;
-            if (base + r0 + r < n) out40[(size_t)(base + r0 + r) * kGOut + c] = S.o[(r0 + r) * kGOutPad + c];
+            if (base + r < n) out40[(size_t)(base + r) * kGOut + c] = o[r * kGOutPad + c];
         }
         __syncwarp();
     }
@@ -665,7 +732,7 @@ static cudaError_t guide_kernel_setup(int device) {
         e = cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem));
     if (e != cudaSuccess) return e;
     int b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_guide_infer, kGuideThreads, sizeof(InferSmem));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_guide_infer, kInferWarps * 32, sizeof(InferSmem));
     g_infer_blocks = b > 0 ? b : 1;
     if (device >= 0 && device < 64) done[device] = true;
     return cudaSuccess;
@@ -673,7 +740,7 @@ static cudaError_t guide_kernel_setup(int device) {
 
 void launch_guide_infer(const RenderState& rs, const DevScene& sc, const FrameParams& fp, uint32_t depth,
                         cudaStream_t s) {
-    k_guide_infer<<<rs.num_sms * g_infer_blocks, kGuideThreads, sizeof(InferSmem), s>>>(rs.ps, sc, fp, depth);
+    k_guide_infer<<<rs.num_sms * g_infer_blocks, kInferWarps * 32, sizeof(InferSmem), s>>>(rs.ps, sc, fp, depth);
 }
 
 void launch_guide_train(const RenderState& rs, const FrameParams& fp, const GuideTrain& gt, cudaStream_t s) {
@@ -833,8 +900,8 @@ int32_t luc_guide_forward(luc_ctx* c, const float* in9, uint32_t n, float* out40
     float* din = c->g_io.as<float>();
     float* dout = din + (size_t)n * 9;
     LUC_CUDA(c, cudaMemcpyAsync(din, in9, (size_t)n * 9 * sizeof(float), cudaMemcpyHostToDevice, s), "upload");
-    int grid = (int)std::min<uint64_t>((n + kTileRows - 1) / kTileRows, (uint64_t)c->num_sms * 2);
-    k_guide_forward<<<grid, kGuideThreads, sizeof(InferSmem), s>>>(din, n, luc_guide_dev(c), dout);
+    int grid = (int)std::min<uint64_t>((n + 16 * kInferWarps - 1) / (16 * kInferWarps), (uint64_t)c->num_sms * 2);
+    k_guide_forward<<<grid, kInferWarps * 32, sizeof(InferSmem), s>>>(din, n, luc_guide_dev(c), dout);
     LUC_CUDA(c, cudaGetLastError(), "guide forward");
     LUC_CUDA(c, cudaMemcpyAsync(out40, dout, (size_t)n * kGOut * sizeof(float), cudaMemcpyDeviceToHost, s), "readback");
     LUC_CUDA(c, cudaStreamSynchronize(s), "guide forward");

@@ -20,7 +20,7 @@ constexpr int kGParams = kGHid * kGIn + kGHid + kGHid * kGHid + kGHid + kGHid * 
 constexpr int kGBf16 = kGHid * kGIn + 2 * kGHid * kGHid + kGOutPad * kGHid;  // packed W1..W4 (row = output)
 constexpr int kGBias = 3 * kGHid + kGOutPad;
 constexpr float kGKappaMax = 1.0e4f;
-constexpr int kGLobeF4 = 10;  // per path: 8 x (mu, kappa) + 2 x 4 weights
+constexpr int kGLobeF4 = 10;  // per queued path: 8 x (mu, kappa) + 2 x 4 weights
 constexpr int kGRecF4 = 5;    // per training record, see below
 // Vertices are guided when opaque and not near-specular; sharper lobes and
 // transmission stay BSDF-sampled.
@@ -74,9 +74,11 @@ LUC_D void load_mixture(const float4* __restrict__ p, Mixture& m) {
     m.w[4] = b.x; m.w[5] = b.y; m.w[6] = b.z; m.w[7] = b.w;
 }
 
-// kappa / (2 pi (1 - e^{-2 kappa})) e^{kappa (c - 1)}
+// kappa / (2 pi (1 - e^{-2 kappa})) e^{kappa (c - 1)}. For kappa >= 9,
+// 1 - e^{-2 kappa} rounds to 1 in f32, so the exponential is skipped.
 LUC_D float vmf_pdf(float kappa, float c) {
-    float norm = kappa / (2.0f * kPi * (1.0f - expf(-2.0f * kappa)));
+    float e = kappa < 9.0f ? expf(-2.0f * kappa) : 0.0f;
+    float norm = kappa / (2.0f * kPi * (1.0f - e));
     return norm * expf(kappa * (c - 1.0f));
 }
 
@@ -118,21 +120,23 @@ LUC_D V3 mixture_sample(const Mixture& m, float u0, float u1, float u2) {
     return vmf_sample(m.lobe[j], u1, u2);
 }
 
-// The same two operations reading the stored mixture (kGLobeF4 float4 per
-// path) from memory lobe by lobe, so SHADE holds no mixture in registers.
-LUC_D float mixture_pdf_mem(const float4* __restrict__ L, V3 d) {
-    const float4 wa = L[8], wb = L[9];
+// The same two operations on a stored mixture: SoA by queue position, lobe j
+// (mu.xyz, kappa) at L[j * stride], the weights at L[8 * stride] (lobes
+// 0..3) and L[9 * stride] (4..7), so a warp's loads coalesce and SHADE holds
+// no mixture in registers.
+LUC_D float mixture_pdf_mem(const float4* __restrict__ L, size_t stride, V3 d) {
+    const float4 wa = L[8 * stride], wb = L[9 * stride];
     const float w[kGLobes] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
     float p = 0.0f;
 #pragma unroll
     for (int j = 0; j < kGLobes; ++j) {
-        float4 l = L[j];
+        float4 l = L[j * stride];
         p += w[j] * vmf_pdf(l.w, l.x * d.x + l.y * d.y + l.z * d.z);
     }
     return p;
 }
-LUC_D V3 mixture_sample_mem(const float4* __restrict__ L, float u0, float u1, float u2) {
-    const float4 wa = L[8], wb = L[9];
+LUC_D V3 mixture_sample_mem(const float4* __restrict__ L, size_t stride, float u0, float u1, float u2) {
+    const float4 wa = L[8 * stride], wb = L[9 * stride];
     const float w[kGLobes] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
     int j = kGLobes - 1;
     float acc = 0.0f;
@@ -144,7 +148,7 @@ LUC_D V3 mixture_sample_mem(const float4* __restrict__ L, float u0, float u1, fl
             break;
         }
     }
-    return vmf_sample(L[j], u1, u2);
+    return vmf_sample(L[j * stride], u1, u2);
 }
 
 }  // namespace luc

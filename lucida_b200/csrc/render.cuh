@@ -34,9 +34,11 @@ struct PathState {
     // [0] extend rays, [1] extend node visits, [2] extend triangle tests,
     // [3] shadow rays, [4] shadow node visits, [5] shadow triangle tests.
     unsigned long long* stat;
-    // Guided frames: the decoded mixture per path (kGLobeF4 float4), the
-    // training records and the guide's bookkeeping words.
+    // Guided frames: the decoded mixture per queue position (kGLobeF4 float4
+    // planes of lobe_stride entries), the training records and the guide's
+    // bookkeeping words.
     float4* lobes;
+    uint64_t lobe_stride;
     float4* rec;
     uint32_t* gmisc;
 };
@@ -44,7 +46,9 @@ struct PathState {
 struct FrameParams {
     uint64_t num_paths;  // pixels * batch_samples
     uint32_t pixels, width, height;
-    uint32_t sample_base, batch_samples;
+    uint32_t sample_base;  // host copy only: kernels read *sbase, so one captured graph serves every offset
+    const uint32_t* sbase;  // device word: the batch's first sample index
+    uint32_t batch_samples;
     uint32_t frame_seed, sampler_kind, sampling, max_depth;
     uint32_t guides;
     uint32_t guided;   // one-sample MIS with the learned proposal
@@ -62,7 +66,12 @@ struct StageTimer {
     void mark(cudaStream_t s, int stage) {
         cudaEvent_t e;
         cudaEventCreate(&e);
-        cudaEventRecord(e, s);
+        // Inside a stream capture a plain record only orders the capture; the
+        // external flag makes it an event-record node that fires on replay.
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(s, &cs);
+        if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+        else cudaEventRecord(e, s);
         events.push_back(e);
         stages.push_back(stage);
     }

@@ -43,9 +43,10 @@ __device__ __forceinline__ V3 xyz(float4 a) { return V3{a.x, a.y, a.z}; }
 // GENERATE (shaders/wavefront/generate.wgsl:35-88; camera.rs:373-405).
 __global__ void __launch_bounds__(256) k_generate(PathState ps, FrameParams fp) {
     const uint64_t n = fp.num_paths;
+    const uint32_t sbase = *fp.sbase;
     for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t pixel = (uint32_t)(p % fp.pixels);
-        uint32_t sample = fp.sample_base + (uint32_t)(p / fp.pixels);
+        uint32_t sample = sbase + (uint32_t)(p / fp.pixels);
         uint32_t x = pixel % fp.width, y = pixel / fp.width;
         Sampler smp = make_sampler(fp.sampler_kind, fp.frame_seed, pixel, sample);
         float pu, pv, lu, lv;
@@ -131,9 +132,10 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
 // both MIS sites (emission hit and NEE); plus training records for a
 // threshold-selected subset of those vertices.
 template <bool kGuided>
-__global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameParams fp, uint32_t depth) {
+__global__ void __launch_bounds__(128, 4) k_shade(PathState ps, DevScene sc, FrameParams fp, uint32_t depth) {
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
-    const uint32_t rec_threshold = kGuided ? ps.gmisc[kGmThreshold] : 0u;
+    const uint32_t rec_threshold = kGuided ? ps.gmisc[kGmThreshold] : 65536u;
+    const uint32_t sbase = *fp.sbase;
     const uint32_t* queue = ps.queue[depth & 1];
     uint32_t* next_queue = ps.queue[(depth + 1) & 1];
     uint32_t* next_len = ps.ctr + (depth + 1) * kCtrStride + kCtrQueue;
@@ -159,7 +161,7 @@ __global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameP
             Sampler smp;
             smp.kind = fp.sampler_kind;
             smp.state = __float_as_uint(t4.w);
-            smp.index = fp.sample_base + (uint32_t)(p / fp.pixels);
+            smp.index = sbase + (uint32_t)(p / fp.pixels);
             smp.seed = sobol_pixel_seed(pixel, fp.frame_seed);
             bool rad_changed = false;
             if (kGuided) {
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameP
                 V3 wo = to_local(-dir, hit.normal);
                 const bool gv = kGuided && fp.guided && !last && surf.transmission <= 0.0f &&
                                 surf.roughness >= kGuideMinRoughness;
-                const float4* lob = ps.lobes + (size_t)p * kGLobeF4;
+                const float4* lob = ps.lobes + i;  // this queue position's mixture (SoA planes)
                 if (wo.z > 0.0f) {
                     // Next event estimation (integrator.rs:349-354, 418-532).
                     if ((fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) && !last &&
@@ -294,7 +296,7 @@ __global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameP
                                     float mis = 1.0f;
                                     if (fp.sampling == LUC_SAMPLING_MIS) {
                                         float pb = bsdf_pdf(surf, sc.energy, wo, wi);
-                                        if (gv) pb = 0.5f * pb + 0.5f * mixture_pdf_mem(lob, wiw);
+                                        if (gv) pb = 0.5f * pb + 0.5f * mixture_pdf_mem(lob, ps.lobe_stride, wiw);
                                         mis = power_heuristic(lpdf, pb);
                                     }
                                     if (mis > 0.0f) {
@@ -310,31 +312,33 @@ __global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameP
                     }
                     // BSDF sampling (integrator.rs:360-399). Skipped on the last
                     // bounce, where its result would never be read.
-                    if (!last && gv) {
-                        float u_choice = smp.next_f32();
+                    if (kGuided && !last) {
+                        // Guided frames: one code path for every vertex; the
+                        // choice dimension is drawn only where the guide applies.
+                        float u_choice = gv ? smp.next_f32() : 0.0f;
                         float u_lobe = smp.next_f32();
                         float ux, uy;
                         smp.next_vec2(ux, uy);
-                        V3 wl{0.0f, 0.0f, 1.0f}, wd{0.0f, 0.0f, 1.0f}, fc{0.0f, 0.0f, 0.0f};
-                        float pb = 0.0f;
-                        if (u_choice < 0.5f) {
-                            BsdfSample bs = bsdf_sample(surf, sc.energy, wo, u_lobe, ux, uy);
-                            if (bs.pdf > 0.0f) {
-                                wl = bs.wi;
-                                wd = to_world(bs.wi, hit.normal);
-                                pb = bs.pdf;
-                                fc = bs.weight * bs.pdf;
-                            }
+                        // Only the direction depends on the choice; f and both
+                        // pdfs are then evaluated once, converged.
+                        V3 wl{0.0f, 0.0f, 1.0f}, wd{0.0f, 0.0f, 1.0f};
+                        bool ok;
+                        if (!gv || u_choice < 0.5f) {
+                            ok = bsdf_sample_dir(surf, sc.energy, wo, u_lobe, ux, uy, wl);
+                            wd = to_world(wl, hit.normal);
                         } else {
-                            wd = mixture_sample_mem(lob, u_lobe, ux, uy);
+                            wd = mixture_sample_mem(lob, ps.lobe_stride, u_lobe, ux, uy);
                             wl = to_local(wd, hit.normal);
-                            if (!(wl.z == 0.0f || (wl.z < 0.0f && surf.transmission <= 0.0f))) {
-                                fc = bsdf_eval(surf, sc.energy, wo, wl) * fabsf(wl.z);
-                                pb = bsdf_pdf(surf, sc.energy, wo, wl);
-                            }
+                            ok = !(wl.z == 0.0f || (wl.z < 0.0f && surf.transmission <= 0.0f));
+                        }
+                        V3 fc{0.0f, 0.0f, 0.0f};
+                        float pb = 0.0f;
+                        if (ok) {
+                            fc = bsdf_eval(surf, sc.energy, wo, wl) * fabsf(wl.z);
+                            pb = bsdf_pdf(surf, sc.energy, wo, wl);
                         }
                         if (max_elem(fc) > 0.0f) {
-                            const float pc = 0.5f * pb + 0.5f * mixture_pdf_mem(lob, wd);
+                            const float pc = gv ? 0.5f * pb + 0.5f * mixture_pdf_mem(lob, ps.lobe_stride, wd) : pb;
                             if (pc > 0.0f) {
                                 thr = thr * (fc / pc);
                                 if (max_elem(thr) > 0.0f) {
@@ -343,13 +347,13 @@ __global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameP
                                     store4(ps.dir + p, wd, 0.0f);
                                     ps.thr[p] = make_float4(thr.x, thr.y, thr.z, __uint_as_float(smp.state));
                                     uint32_t slot1 = 0u;
-                                    if (fp.rec_cap) {
+                                    if (gv && fp.rec_cap) {
                                         // Opportunistic warp aggregation of the two counters.
                                         const uint32_t lane = threadIdx.x & 31u;
                                         uint32_t am = __activemask();
                                         uint32_t leader = __ffs(am) - 1u;
                                         if (lane == leader) atomicAdd(ps.gmisc + kGmCandidates, (uint32_t)__popc(am));
-                                        uint32_t h = mix32(p * 0x9E3779B9u ^ (depth << 27) ^ (fp.sample_base * 0x85EBCA6Bu));
+                                        uint32_t h = mix32(p * 0x9E3779B9u ^ (depth << 27) ^ (sbase * 0x85EBCA6Bu));
                                         const bool want = (h & 0xFFFFu) < rec_threshold;
                                         uint32_t wm = __ballot_sync(am, want);
                                         if (want) {
@@ -374,7 +378,7 @@ __global__ void __launch_bounds__(128) k_shade(PathState ps, DevScene sc, FrameP
                                 }
                             }
                         }
-                    } else if (!last) {
+                    } else if (!kGuided && !last) {
                         float u_lobe = smp.next_f32();
                         float ux, uy;
                         smp.next_vec2(ux, uy);

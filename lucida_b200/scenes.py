@@ -211,8 +211,44 @@ def displaced_spheres(count: int = 256, level: int = 4, seed: int = 2024, env_si
     mats = np.array(mats, L.MATERIAL)
     prims = np.array([L.quad((-30, 0, -30), (0, 0, 60), (60, 0, 0), 0)], L.PRIMITIVE)
     w, h = env_size
-    px, cdf, total = procedural_sky(w, h, (-0.4, 0.55, -0.7), 1.0e4, 0.5)
+    px, cdf, total = procedural_sky(w, h, (-0.4, 0.55, -0.7), 1.0e4, 0.5) if w > 0 else (None, None, 0.0)
     return SceneDef(materials=mats, primitives=prims, lights=L.quad_lights(mats, prims), positions=positions,
                     vertex_attrs=attrs, triangles=tris, bvh_nodes=None,
                     camera=Camera(eye=(0.0, 7.0, 24.0), look_at=(0.0, 1.5, 0.0), vfov_deg=45.0),
                     env_pixels=px, env_cdf=cdf, env_total_weight=total, name=f"displaced-spheres-l{level}")
+
+
+def guided_room(count: int = 256, level: int = 4, seed: int = 2024, emission: float = 200.0) -> SceneDef:
+    """Path-guiding workload: the displaced-spheres geometry (same seed, so the
+    same meshes and materials) inside a half-closed room lit only by two
+    0.2 x 0.2 emitters of radiance `emission`.
+
+    Room: x in [-12, 12], y in [0, 9], z in [-12, 12]; floor (the ground quad),
+    ceiling, back, left and right walls, grey Lambertian 0.7; the front
+    (z = +12, towards the camera) is open. No environment map, black
+    background. The emitters sit 0.4 below the ceiling at (-5, 8.6, -4) and
+    (5, 8.6, 3) and face up, so nothing but the ceiling sees them directly:
+    every other surface is lit by light that has bounced at least once, which
+    a BSDF-sampled path reaches only by chance and a learned guide can aim at.
+    """
+    base = displaced_spheres(count=count, level=level, seed=seed, env_size=(0, 0))
+    mats = list(base.materials)
+    wall = len(mats)
+    mats.append(L.diffuse((0.7, 0.7, 0.7)))
+    lamp = len(mats)
+    mats.append(L.emissive((emission, emission, emission)))
+    mats = np.array(mats, L.MATERIAL)
+    x0, x1, y1, z0, z1 = -12.0, 12.0, 9.0, -12.0, 12.0
+    prims = [base.primitives[0],
+             L.quad((x0, y1, z0), (x1 - x0, 0, 0), (0, 0, z1 - z0), wall),   # ceiling
+             L.quad((x0, 0, z0), (0, y1, 0), (x1 - x0, 0, 0), wall),         # back
+             L.quad((x0, 0, z0), (0, 0, z1 - z0), (0, y1, 0), wall),         # left
+             L.quad((x1, 0, z0), (0, y1, 0), (0, 0, z1 - z0), wall)]         # right
+    s = 0.2
+    for cx, cz in ((-5.0, -4.0), (5.0, 3.0)):
+        # edge_u x edge_v = (0, s^2, 0): the emitting side faces +y.
+        prims.append(L.quad((cx - s / 2, 8.6, cz - s / 2), (0, 0, s), (s, 0, 0), lamp))
+    prims = np.array(prims, L.PRIMITIVE)
+    return SceneDef(materials=mats, primitives=prims, lights=L.quad_lights(mats, prims), positions=base.positions,
+                    vertex_attrs=base.vertex_attrs, triangles=base.triangles, bvh_nodes=None, camera=base.camera,
+                    name=f"guided-room-l{level}")

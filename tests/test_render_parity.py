@@ -75,6 +75,20 @@ def test_reference_scenes(gpu, name, mode):
     _check(acc, ref, f"{name}/{mode}")
 
 
+@pytest.mark.parametrize("which", ["displaced-spheres", "guided-room"])
+def test_triangle_workload_scenes(gpu, which):
+    """The throughput and path-guiding workloads at reduced size (24 meshes,
+    subdivision 3): the device's own LBVH against the oracle's SAH tree,
+    plain MIS render with the Sobol sampler."""
+    if which == "displaced-spheres":
+        s = scenes.displaced_spheres(count=24, level=3, env_size=(256, 128))
+    else:
+        s = scenes.guided_room(count=24, level=3)
+    osc = oracle_from_scene(s)
+    acc, ref = _render_both(gpu, osc, 64, 48, 8, 8, scene=s)
+    _check(acc, ref, which)
+
+
 def test_progressive_equals_one_shot(gpu):
     """Accumulating 4 + 4 samples into one device accumulator equals one 8-sample
     render bit for bit (cpu_gpu_agreement.rs:119-168 asks < 1e-5)."""
@@ -104,3 +118,25 @@ def test_depth_sweep_energy_monotone(gpu):
         f = lb.render_with(gpu, s, lb.RenderParams(width=48, height=48, samples=16, max_depth=d))
         means.append(float(f.data.mean()))
     assert all(b >= a - 1e-5 for a, b in zip(means, means[1:])), means
+
+
+def test_profiled_renders_time_every_stage(gpu):
+    """LUC_FLAG_PROFILE on the captured-graph path (event-record nodes) and on
+    the batched path: stage times are filled in and the image is unchanged."""
+    s = scenes.cornell_analytic()
+    params = lb.RenderParams(width=64, height=64, samples=4, max_depth=4, sampler="independent")
+    plain = lb.render_accum(gpu, s, params)
+    for _ in range(2):  # capture, then replay
+        prof = lb.render_accum(gpu, s, params, profile=True)
+        st = gpu.stats()
+        assert np.array_equal(prof["radiance"], plain["radiance"])
+        assert st.ms_generate > 0 and st.ms_extend > 0 and st.ms_shade > 0 and st.ms_resolve > 0
+        assert st.ms_total >= st.ms_extend + st.ms_shade
+    from lucida_b200 import Guide
+    guide = Guide(gpu, seed=1)
+    guide.configure(train=True, records_per_step=4096)
+    for _ in range(2):
+        lb.render_accum(gpu, s, params, profile=True, guided=True)
+        st = gpu.stats()
+        assert st.ms_guide > 0 and st.ms_train > 0 and st.ms_shade > 0
+    assert guide.stats().steps == 2
