@@ -78,6 +78,13 @@ def lib():
         L.orc_scene_set_camera.argtypes = [vp, vp, vp, vp, f32, f32, f32]
         L.orc_scene_get_camera.argtypes = [vp, vp]
         L.orc_scene_get_misc.argtypes = [vp, vp, vp, vp]
+        L.orc_scene_set_instancing.argtypes = [vp, vp, u32, u32, u32]
+        L.orc_scene_instancing.argtypes = [vp, vp]
+        L.orc_scene_set_reference_shadows.argtypes = [vp, i32]
+        L.orc_affine_inverse.argtypes = [vp, vp]
+        L.orc_pack_instance.argtypes = [vp, u32, u32, vp]
+        L.orc_instance_transform.argtypes = [vp, i32, vp, u32, vp]
+        L.orc_instance_world_bounds.argtypes = [vp, vp, vp]
         L.orc_build_uniforms.argtypes = [vp, u32, u32, u32, u32, u32, u32, u32, u32, vp]
         L.orc_render_sums.argtypes = [vp, vp, u32, u32, u32, u32, vp]
         L.orc_intersect_batch.argtypes = [vp, vp, u32, vp]
@@ -164,8 +171,10 @@ class Scene:
 
     @classmethod
     def from_arrays(cls, materials, primitives, positions, vertex_attrs, triangles, lights=None,
-                    env=None, background=(0.0, 0.0, 0.0), camera=None, bvh="sah") -> "Scene":
-        """`env` = (pixels[h*w,4], conditional[(w+1)*h], marginal[h+1], total_weight, w, h)."""
+                    env=None, background=(0.0, 0.0, 0.0), camera=None, bvh="sah", instancing=None) -> "Scene":
+        """`env` = (pixels[h*w,4], conditional[(w+1)*h], marginal[h+1], total_weight, w, h).
+        `instancing` = (flattened nodes, num_instances, tlas_root) for an
+        instanced scene whose last num_instances primitives are instance rows."""
         L = lib()
         materials = np.ascontiguousarray(materials, MATERIAL)
         primitives = np.ascontiguousarray(primitives, PRIMITIVE)
@@ -186,11 +195,26 @@ class Scene:
                                       _p(lights_arr), 0 if lights_arr is None else len(lights_arr),
                                       _p(positions), len(positions), _p(vertex_attrs), _p(triangles),
                                       len(triangles), _p(px), w, h, _p(cond), _p(marg), float(total), _p(bg),
-                                      1 if bvh == "lbvh" else 0)
+                                      2 if instancing is not None else (1 if bvh == "lbvh" else 0))
         s = cls(hnd)
+        if instancing is not None:
+            nodes, ni, root = instancing
+            nodes = np.ascontiguousarray(nodes, BVH_NODE)
+            L.orc_scene_set_instancing(hnd, _p(nodes), len(nodes), int(ni), int(root))
         if camera is not None:
             s.set_camera(**camera)
         return s
+
+    def instancing(self):
+        """(instance count, analytic primitive count, TLAS root)."""
+        out = np.zeros(3, np.uint32)
+        lib().orc_scene_instancing(self._h, _p(out))
+        return int(out[0]), int(out[1]), int(out[2])
+
+    def set_reference_shadows(self, on: bool):
+        """Shadow rays of an instanced scene as the reference casts them
+        (untransformed object-space triangles) instead of the two-level any-hit."""
+        lib().orc_scene_set_reference_shadows(self._h, 1 if on else 0)
 
     def set_camera(self, eye, look_at, vfov_deg, up=(0.0, 1.0, 0.0), aperture=0.0, focus_distance=None):
         eye = np.asarray(eye, np.float32)
@@ -382,4 +406,36 @@ def transcendental(fn: str, x, y=None) -> np.ndarray:
     y = np.ascontiguousarray(np.zeros_like(x) if y is None else y, np.float32)
     out = np.zeros_like(x)
     lib().orc_transcendental_batch(code, _p(x), _p(y), len(x), _p(out))
+    return out
+
+
+# ---------------------------------------------------------------- instance maths
+def affine_inverse(m34):
+    m = np.ascontiguousarray(m34, np.float32).reshape(3, 4)
+    out = np.zeros((3, 4), np.float32)
+    lib().orc_affine_inverse(_p(m), _p(out))
+    return out
+
+
+def pack_instance(world_to_object34, blas_root=0, material=0xFFFFFFFF):
+    m = np.ascontiguousarray(world_to_object34, np.float32).reshape(3, 4)
+    out = np.zeros(1, PRIMITIVE)
+    lib().orc_pack_instance(_p(m), int(blas_root), int(material), _p(out))
+    return out[0]
+
+
+def instance_transform(inst, v, mode):
+    """mode 0: points, 1: vectors (not normalised), 2: normals."""
+    g = np.ascontiguousarray(np.asarray(inst, PRIMITIVE).reshape(1))
+    a = np.ascontiguousarray(v, np.float32).reshape(-1, 3)
+    out = np.zeros_like(a)
+    lib().orc_instance_transform(_p(g), int(mode), _p(a), len(a), _p(out))
+    return out
+
+
+def instance_world_bounds(inst, box6):
+    g = np.ascontiguousarray(np.asarray(inst, PRIMITIVE).reshape(1))
+    b = np.ascontiguousarray(box6, np.float32).reshape(6)
+    out = np.zeros(6, np.float32)
+    lib().orc_instance_world_bounds(_p(g), _p(b), _p(out))
     return out

@@ -49,7 +49,7 @@ void* orc_scene_from_arrays(const GpuMaterial* mats, uint32_t nm, const GpuPrimi
         s->env.total_weight = env_total;
     }
     s->background = background ? Vec3::from(background) : Vec3();
-    if (!s->triangles.empty()) {
+    if (!s->triangles.empty() && bvh_kind != 2) {  // 2: the caller supplies the tree (orc_scene_set_instancing)
         if (bvh_kind == 1) s->bvh = lbvh_build(s->triangles, s->positions, 4).tree;
         else s->bvh = Bvh::build(s->triangles, s->positions);
         s->bvh.compact_primitives(s->triangles);
@@ -57,6 +57,59 @@ void* orc_scene_from_arrays(const GpuMaterial* mats, uint32_t nm, const GpuPrimi
     if (lights) s->lights.assign(lights, lights + nl);
     else s->lights = build_lights(s->materials, s->primitives, s->triangles, s->positions);
     return s;
+}
+
+// Instanced scene in the upload's form: the last `num_instances` primitives
+// are GpuInstance rows in TLAS-leaf order, `nodes` the flattened BLAS + TLAS
+// array, `tlas_root` the TLAS's first node.
+void orc_scene_set_instancing(void* h, const GpuBvhNode* nodes, uint32_t nn, uint32_t num_instances,
+                              uint32_t tlas_root) {
+    Scene* s = (Scene*)h;
+    size_t na = s->primitives.size() - num_instances;
+    s->instances.resize(num_instances);
+    if (num_instances) std::memcpy(s->instances.data(), s->primitives.data() + na, num_instances * sizeof(GpuInstance));
+    s->primitives.resize(na);
+    s->flat_nodes.assign(nodes, nodes + nn);
+    s->tlas_root = tlas_root;
+    s->bvh = Bvh();
+}
+// out3: instance count, analytic primitive count, TLAS root.
+void orc_scene_instancing(void* h, uint32_t* out3) {
+    Scene* s = (Scene*)h;
+    out3[0] = (uint32_t)s->instances.size();
+    out3[1] = (uint32_t)s->primitives.size();
+    out3[2] = s->tlas_root;
+}
+void orc_scene_set_reference_shadows(void* h, int on) { ((Scene*)h)->reference_instance_shadows = on != 0; }
+
+// Instance maths (instance.rs): affine inverse of a row-major 3x4; pack an
+// instance from a world-to-object transform; transform n points (mode 0),
+// vectors (1) or normals (2); world bounds of a box (6 floats: min, max).
+void orc_affine_inverse(const float* in12, float* out12) {
+    Affine a;
+    std::memcpy(a.m, in12, sizeof(a.m));
+    Affine r = affine_inverse(a);
+    std::memcpy(out12, r.m, sizeof(r.m));
+}
+void orc_pack_instance(const float* w2o12, uint32_t blas_root, uint32_t material, GpuInstance* out) {
+    Affine a;
+    std::memcpy(a.m, w2o12, sizeof(a.m));
+    *out = pack_instance(a, blas_root, material);
+}
+void orc_instance_transform(const GpuInstance* g, int mode, const float* in3, uint32_t n, float* out3) {
+    for (uint32_t i = 0; i < n; ++i) {
+        Vec3 v = Vec3::from(in3 + 3 * i);
+        Vec3 r = mode == 0 ? instance_point(*g, v) : mode == 1 ? instance_vector(*g, v) : instance_normal(*g, v);
+        r.to(out3 + 3 * i);
+    }
+}
+void orc_instance_world_bounds(const GpuInstance* g, const float* box6, float* out6) {
+    Aabb b;
+    b.min = Vec3::from(box6);
+    b.max = Vec3::from(box6 + 3);
+    Aabb w = instance_world_bounds(*g, b);
+    w.min.to(out6);
+    w.max.to(out6 + 3);
 }
 
 void orc_scene_set_camera(void* h, const float* eye, const float* at, const float* up, float vfov,
@@ -89,12 +142,12 @@ size_t orc_scene_count(void* h, int which) {
     Scene* s = (Scene*)h;
     switch (which) {
         case W_MATERIALS: return s->materials.size();
-        case W_PRIMITIVES: return s->primitives.size();
+        case W_PRIMITIVES: return s->primitives.size() + s->instances.size();
         case W_LIGHTS: return s->lights.size();
         case W_POSITIONS: return s->positions.size() / 4;
         case W_ATTRS: return s->vertex_attrs.size();
         case W_TRIANGLES: return s->triangles.size();
-        case W_BVH_NODES: return s->bvh.nodes.size();
+        case W_BVH_NODES: return s->instances.empty() ? s->bvh.nodes.size() : s->flat_nodes.size();
         case W_BVH_PRIMS: return s->bvh.prim_indices.size();
         case W_ENV_PIXELS: return s->env.pixels.size() / 4;
         case W_ENV_COND: return s->env.conditional.size();
@@ -107,12 +160,20 @@ void orc_scene_copy(void* h, int which, void* dst) {
     auto cp = [&](const void* src, size_t bytes) { if (bytes) std::memcpy(dst, src, bytes); };
     switch (which) {
         case W_MATERIALS: cp(s->materials.data(), s->materials.size() * sizeof(GpuMaterial)); break;
-        case W_PRIMITIVES: cp(s->primitives.data(), s->primitives.size() * sizeof(GpuPrimitive)); break;
+        case W_PRIMITIVES:
+            cp(s->primitives.data(), s->primitives.size() * sizeof(GpuPrimitive));
+            if (!s->instances.empty())
+                std::memcpy((char*)dst + s->primitives.size() * sizeof(GpuPrimitive), s->instances.data(),
+                            s->instances.size() * sizeof(GpuInstance));
+            break;
         case W_LIGHTS: cp(s->lights.data(), s->lights.size() * sizeof(GpuLight)); break;
         case W_POSITIONS: cp(s->positions.data(), s->positions.size() * 4); break;
         case W_ATTRS: cp(s->vertex_attrs.data(), s->vertex_attrs.size() * sizeof(GpuVertexAttr)); break;
         case W_TRIANGLES: cp(s->triangles.data(), s->triangles.size() * sizeof(GpuTriangle)); break;
-        case W_BVH_NODES: cp(s->bvh.nodes.data(), s->bvh.nodes.size() * sizeof(GpuBvhNode)); break;
+        case W_BVH_NODES:
+            if (s->instances.empty()) cp(s->bvh.nodes.data(), s->bvh.nodes.size() * sizeof(GpuBvhNode));
+            else cp(s->flat_nodes.data(), s->flat_nodes.size() * sizeof(GpuBvhNode));
+            break;
         case W_BVH_PRIMS: cp(s->bvh.prim_indices.data(), s->bvh.prim_indices.size() * 4); break;
         case W_ENV_PIXELS: cp(s->env.pixels.data(), s->env.pixels.size() * 4); break;
         case W_ENV_COND: cp(s->env.conditional.data(), s->env.conditional.size() * 4); break;

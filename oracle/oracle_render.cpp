@@ -97,14 +97,24 @@ bool Scene::intersect(const Ray& ray, Hit& out) const {
         }
     }
     TriHit th;
-    bool tri_hit = bvh.empty()
-                       ? brute_force_intersect(triangles.data(), triangles.size(), positions.data(), ray,
-                                               T_MIN, best_t, th)
-                       : bvh.intersect(triangles.data(), positions.data(), ray, T_MIN, best_t, st, th);
-    if (tri_hit) {
-        out = shade_triangle(th, ray);
-        out.steps = st.node_visits;
-        return true;
+    if (!instances.empty()) {
+        // Instances instead of the single-level path (scene.rs:489-501).
+        uint32_t inst = 0;
+        if (intersect_instances(ray, T_MIN, best_t, st, th, inst)) {
+            out = shade_instanced_triangle(th, inst, ray);
+            out.steps = st.node_visits;
+            return true;
+        }
+    } else {
+        bool tri_hit = bvh.empty()
+                           ? brute_force_intersect(triangles.data(), triangles.size(), positions.data(), ray,
+                                                   T_MIN, best_t, th)
+                           : bvh.intersect(triangles.data(), positions.data(), ray, T_MIN, best_t, st, th);
+        if (tri_hit) {
+            out = shade_triangle(th, ray);
+            out.steps = st.node_visits;
+            return true;
+        }
     }
     if (best < 0) return false;
     const GpuPrimitive& prim = primitives[best];
@@ -133,6 +143,7 @@ bool Scene::occluded(const Ray& ray, float tmax) const {
                                           : intersect_sphere(p, ray, T_MIN, tmax, t);
         if (h) return true;
     }
+    if (!instances.empty() && !reference_instance_shadows) return occluded_instances(ray, T_MIN, tmax);
     if (bvh.empty()) {
         TriHit th;
         return brute_force_intersect(triangles.data(), triangles.size(), positions.data(), ray, T_MIN,

@@ -135,6 +135,27 @@ struct Hit {
     float light_area;
 };
 
+// ---------------------------------------------------------------- instance.rs
+// A 3x4 affine transform, row-major: m[i][3] is the translation.
+struct Affine {
+    float m[3][4];
+};
+// glam's Mat4::transform_point3 / transform_vector3 sum the columns in order:
+// per component ((m[i][0]*p.x + m[i][1]*p.y) + m[i][2]*p.z) (+ m[i][3]).
+Vec3 affine_point(const Affine& a, Vec3 p);
+Vec3 affine_vector(const Affine& a, Vec3 v);
+// The inverse of an affine transform by the adjugate: each entry of the 3x3 is
+// its cofactor expression divided by the determinant (IEEE division, no
+// reciprocal), the translation is -(inverse 3x3 . t). The device computes the
+// same expression; glam's 4x4 inverse (used by the reference) agrees to
+// rounding.
+Affine affine_inverse(const Affine& a);
+Affine instance_world_to_object(const GpuInstance& g);
+GpuInstance pack_instance(const Affine& w2o, uint32_t blas_root, uint32_t material);  // gpu_layout.rs:513-529
+Vec3 instance_point(const GpuInstance& g, Vec3 p);    // Instance::transform_ray, origin
+Vec3 instance_vector(const GpuInstance& g, Vec3 v);   // Instance::transform_ray, direction (not normalised)
+Vec3 instance_normal(const GpuInstance& g, Vec3 n);   // Instance::transform_normal (instance.rs:137-141)
+
 bool intersect_sphere(const GpuPrimitive& s, const Ray& r, float tmin, float tmax, float& t);
 bool intersect_quad(const GpuPrimitive& q, const Ray& r, float tmin, float tmax, float& t);
 
@@ -146,6 +167,21 @@ struct Scene {
     std::vector<GpuTriangle> triangles;
     std::vector<GpuLight> lights;
     Bvh bvh;  // single-level BVH over `triangles` (compacted: prim_indices is identity)
+    // Instancing (instance.rs; scene.rs:252-345), in the upload's form: the
+    // instance rows in TLAS-leaf order (appended to the primitives on upload),
+    // the flattened node array (every BLAS, then the TLAS) and the TLAS root.
+    // `primitives` keeps the analytic primitives only.
+    std::vector<GpuInstance> instances;
+    std::vector<GpuBvhNode> flat_nodes;
+    uint32_t tlas_root = 0;
+    // Shadow rays in an instanced scene: true = the reference's behaviour
+    // (scene.rs:577-606 tests the analytic primitives and then every triangle
+    // untransformed, in object space); false = the two-level any-hit.
+    bool reference_instance_shadows = false;
+    struct Placement {
+        Affine object_to_world;
+        uint32_t mesh, material;
+    };
     EnvMap env;
     Vec3 background;
     Camera camera;
@@ -158,7 +194,26 @@ struct Scene {
     bool intersect(const Ray& ray, Hit& out) const;
     bool occluded(const Ray& ray, float tmax) const;
     Hit shade_triangle(const TriHit& h, const Ray& ray) const;
+    // scene.rs:252-345 with a binned-SAH BLAS per mesh range and a binned-SAH
+    // TLAS over the instances' world bounds.
+    void build_instances(const std::vector<std::pair<uint32_t, uint32_t>>& mesh_ranges,
+                         const std::vector<Placement>& placements);
+    // InstanceSet::intersect (instance.rs:342-421) over the flattened arrays.
+    bool intersect_instances(const Ray& ray, float tmin, float tmax, TraversalStats& st, TriHit& tri,
+                             uint32_t& instance) const;
+    bool occluded_instances(const Ray& ray, float tmin, float tmax) const;
+    Hit shade_instanced_triangle(const TriHit& h, uint32_t instance, const Ray& ray) const;  // scene.rs:375-402
 };
+// World bounds of a BLAS box under an instance: the eight corners through the
+// forward transform (the inverse of the stored world-to-object), then padded
+// (Instance::world_bounds, instance.rs:98-113).
+Aabb instance_world_bounds(const GpuInstance& g, const Aabb& object_bounds);
+// Bvh::intersect / occluded (bvh.rs:1045-1193) over a flattened node array
+// from an arbitrary root (absolute child and triangle indices).
+bool flat_bvh_intersect(const GpuBvhNode* nodes, uint32_t root, const GpuTriangle* tris, const float* pos4,
+                        const Ray& ray, float tmin, float tmax, TraversalStats& st, TriHit& out);
+bool flat_bvh_occluded(const GpuBvhNode* nodes, uint32_t root, const GpuTriangle* tris, const float* pos4,
+                       const Ray& ray, float tmin, float tmax);
 
 // ---------------------------------------------------------------- integrator.rs
 struct GuideSample {

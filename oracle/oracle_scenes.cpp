@@ -318,7 +318,51 @@ static Scene sunset() {
     return s;
 }
 
+// scenes.rs:733-812: forty-nine placements of one icosphere (rotation about
+// y and non-uniform scale), one BLAS under a TLAS.
+static Scene instance_forest() {
+    Scene s;
+    s.materials = {mat_diffuse(Vec3(0.34f, 0.32f, 0.29f)), mat_glossy(Vec3(0.70f, 0.35f, 0.25f), 0.35f),
+                   mat_metal(Vec3(0.95f, 0.80f, 0.40f), 0.18f)};
+    s.primitives = {prim_quad(Vec3(-30, 0, -30), Vec3(60, 0, 0), Vec3(0, 0, 60), 0)};
+    icosphere(Vec3(), 0.5f, 2).append_to(s, 1);
+    uint32_t tri_count = (uint32_t)s.triangles.size();
+    Rng rng(0x1057, 0, 0);
+    std::vector<Scene::Placement> placements;
+    for (int gx = 0; gx < 7; ++gx) {
+        for (int gz = 0; gz < 7; ++gz) {
+            float jx = rng.next_f32() - 0.5f;
+            float x = ((float)gx * 1.6f - 4.8f) + jx * 0.5f;
+            float jz = rng.next_f32() - 0.5f;
+            float z = ((float)gz * 1.6f - 4.8f) + jz * 0.5f;
+            float sx = 0.7f + rng.next_f32() * 0.7f;
+            float sy = 0.5f + rng.next_f32() * 1.1f;
+            float sz = 0.7f + rng.next_f32() * 0.7f;
+            float spin = rng.next_f32() * TAU;
+            float y = 0.5f * sy;
+            // translation * rotation_y(spin) * scale: the products are exact
+            // (every other term is a zero), leaving these columns.
+            float sn = std::sin(spin), cs = std::cos(spin);
+            Affine m;
+            float rows[3][4] = {{cs * sx, 0.0f, sn * sz, x}, {0.0f, sy, 0.0f, y}, {-sn * sx, 0.0f, cs * sz, z}};
+            std::memcpy(m.m, rows, sizeof(rows));
+            uint32_t material = (gx + gz) % 3 == 0 ? 2u : 0xFFFFFFFFu;
+            placements.push_back(Scene::Placement{m, 0u, material});
+        }
+    }
+    s.env = procedural_sky(256, 128, Vec3(-0.4f, 0.35f, -0.85f), 6000.0f, 1.0f);
+    s.camera = Camera::make(Vec3(0, 3.2f, -11.0f), Vec3(0, 0.7f, 0), 40.0f);
+    s.background = Vec3();
+    s.build_instances({{0u, tri_count}}, placements);
+    s.lights = build_lights(s.materials, s.primitives, s.triangles, s.positions);
+    return s;
+}
+
 bool scene_by_name(const std::string& name, Scene& out) {
+    if (name == "instance-forest") {
+        out = instance_forest();
+        return true;
+    }
     if (name == "cornell-box") out = cornell_box();
     else if (name == "cornell-mesh") out = cornell_mesh();
     else if (name == "furnace-test") out = furnace_test();

@@ -73,6 +73,12 @@ def main(root):
                 # the uv lanes carry the generating platform's libm rounding.
                 lanes = b"".join(data[i * 32:i * 32 + 16] for i in range(count))
                 entry["normal_lanes_sha256"] = hashlib.sha256(lanes).hexdigest()
+            if s == "bvhNodes" and rec["instancing"][0]:
+                # Instanced scene: the BLAS part (before the TLAS root) by
+                # digest, the TLAS nodes raw, so the two can be checked apart.
+                tlas_root = rec["instancing"][2]
+                entry["blas_sha256"] = hashlib.sha256(data[:tlas_root * 32]).hexdigest()
+                entry["tlas_raw"] = base64.b64encode(data[tlas_root * 32:]).decode()
             secs[s] = entry
         out[name] = {"sections": secs, "instancing": rec["instancing"], "env": rec["env"],
                      "background": rec["background"], "camera": rec["camera"]}
