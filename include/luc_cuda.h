@@ -51,6 +51,13 @@ extern "C" {
  * batch of samples the guide takes one Adam step on the batch's records
  * (luc_guide_configure). Requires luc_guide_init. */
 #define LUC_FLAG_GUIDED 0x400u
+/* Instanced scenes: cast shadow rays the way the reference does
+ * (crates/core/src/scene.rs:577-606, shaders/wavefront/connect.wgsl:36-55),
+ * testing the analytic primitives and then every mesh's triangles
+ * untransformed, in object space, instead of through the two-level
+ * hierarchy. For parity with the reference; the default is the two-level
+ * any-hit. No effect on scenes without instances. */
+#define LUC_FLAG_REFERENCE_SHADOWS 0x800u
 
 typedef struct luc_ctx luc_ctx;
 

@@ -164,7 +164,7 @@ void luc_destroy(luc_ctx* c) {
     cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->materials, &c->prims,    &c->lights,   &c->positions, &c->attrs,     &c->tris,
                       &c->nodes,     &c->env_px,   &c->env_cond, &c->env_marg,  &c->env_row_sin, &c->energy,
-                      &c->tnodes,    &c->soup,     &c->frame_word,
+                      &c->tnodes,    &c->soup,     &c->frame_word, &c->blas_roots,
                       &c->pool,      &c->accum_tmp, &c->lb_tris, &c->lb_pos,    &c->lb_boxes,  &c->lb_keys,
                       &c->lb_vals,   &c->lb_keys2, &c->lb_vals2, &c->lb_hist,   &c->lb_karras, &c->lb_parent,
                       &c->lb_nbounds, &c->lb_subtree, &c->lb_flags, &c->lb_nodes, &c->lb_rank, &c->lb_misc,
@@ -194,7 +194,20 @@ int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) {
     if (v->num_lights && !v->lights) return luc_fail(c, LUC_ERR_VALIDATION, "null lights");
     if (v->num_triangles && (!v->triangles || !v->positions || !v->vertex_attrs || v->num_vertices == 0))
         return luc_fail(c, LUC_ERR_VALIDATION, "triangles without positions/attributes");
-    if (v->num_instances) return luc_fail(c, LUC_ERR_VALIDATION, "instanced scenes are not supported by this build");
+    const uint32_t ni = v->num_instances, np_ = v->num_primitives;
+    if (ni) {
+        // Instanced scene (scene.rs:252-345 layout): instance rows appended
+        // after the analytic primitives, BLAS nodes then TLAS nodes, the TLAS
+        // from tlas_root on. The tree must come with the scene.
+        if (v->num_bvh_nodes == 0 || v->tlas_root >= v->num_bvh_nodes)
+            return luc_fail(c, LUC_ERR_VALIDATION, "instanced scene without its BLAS/TLAS nodes or a valid tlas_root");
+        for (uint32_t i = 0; i < ni; ++i) {
+            const GpuInstance& g = *reinterpret_cast<const GpuInstance*>(v->primitives + np_ + i);
+            if (g.kind != PRIM_KIND_INSTANCE || g.blas_root >= v->tlas_root ||
+                (g.material != 0xFFFFFFFFu && g.material >= v->num_materials))
+                return luc_fail(c, LUC_ERR_VALIDATION, "instance " + std::to_string(i) + " has a bad tag, BLAS root or material");
+        }
+    }
     for (uint32_t i = 0; i < v->num_primitives; ++i)
         if (v->primitives[i].material >= v->num_materials || v->primitives[i].kind > PRIM_KIND_QUAD)
             return luc_fail(c, LUC_ERR_VALIDATION, "primitive " + std::to_string(i) + " has a bad kind or material");
@@ -209,8 +222,14 @@ int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) {
     }
     for (uint32_t i = 0; i < v->num_bvh_nodes; ++i) {
         const GpuBvhNode& n = v->bvh_nodes[i];
-        bool bad = n.count == 0 ? (uint64_t)n.left_first + 1 >= v->num_bvh_nodes
-                                : (uint64_t)n.left_first + n.count > v->num_triangles;
+        const bool tlas = ni && i >= v->tlas_root;
+        // Children come after their parent (every builder here and in the
+        // reference emits them so), which also rules out cycles; TLAS leaves
+        // index instance rows, BLAS leaves triangles.
+        bool bad = n.count == 0 ? (n.left_first <= i || (uint64_t)n.left_first + 1 >= v->num_bvh_nodes ||
+                                   (ni && !tlas && n.left_first + 1 >= v->tlas_root))
+                 : tlas ? (n.left_first < np_ || (uint64_t)n.left_first + n.count > (uint64_t)np_ + ni)
+                        : (uint64_t)n.left_first + n.count > v->num_triangles;
         if (bad) return luc_fail(c, LUC_ERR_VALIDATION, "bvh node " + std::to_string(i) + " out of range");
     }
     if (v->env_width && (!v->env_pixels || !v->env_cdf || v->env_height == 0 ||
@@ -227,8 +246,13 @@ int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) {
                 hi[a] = std::max(hi[a], q[a]);
             }
         };
-        for (uint32_t i = 0; i < v->num_vertices && v->num_triangles; ++i)
+        for (uint32_t i = 0; i < v->num_vertices && v->num_triangles && !ni; ++i)
             grow(v->positions[4 * i], v->positions[4 * i + 1], v->positions[4 * i + 2]);
+        if (ni && v->num_triangles) {  // instanced: the TLAS root's box (world space)
+            const GpuBvhNode& r = v->bvh_nodes[v->tlas_root];
+            grow(r.bounds_min[0], r.bounds_min[1], r.bounds_min[2]);
+            grow(r.bounds_max[0], r.bounds_max[1], r.bounds_max[2]);
+        }
         for (uint32_t i = 0; i < v->num_primitives; ++i) {
             const GpuPrimitive& p = v->primitives[i];
             const float* o = p.position;
@@ -251,7 +275,12 @@ int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) {
     cudaStream_t s = c->stream;
     c->has_scene = false;
     LUC_CUDA(c, upload(c->materials, v->materials, v->num_materials, s), "upload materials");
-    LUC_CUDA(c, upload(c->prims, v->primitives, v->num_primitives, s), "upload primitives");
+    LUC_CUDA(c, upload(c->prims, v->primitives, (size_t)np_ + ni, s), "upload primitives");
+    std::vector<uint32_t> roots;
+    for (uint32_t i = 0; i < ni; ++i) roots.push_back(reinterpret_cast<const GpuInstance*>(v->primitives + np_ + i)->blas_root);
+    std::sort(roots.begin(), roots.end());
+    roots.erase(std::unique(roots.begin(), roots.end()), roots.end());
+    LUC_CUDA(c, upload(c->blas_roots, roots.data(), roots.size(), s), "upload blas roots");
     LUC_CUDA(c, upload(c->lights, v->lights, v->num_lights, s), "upload lights");
     LUC_CUDA(c, upload(c->positions, v->positions, 4 * (size_t)v->num_vertices, s), "upload positions");
     LUC_CUDA(c, upload(c->attrs, v->vertex_attrs, v->num_vertices, s), "upload vertex attrs");
@@ -311,6 +340,12 @@ int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) {
     d.num_tris = v->num_triangles;
     d.nodes = c->nodes.as<float4>();
     d.num_nodes = v->num_triangles ? num_nodes : 0;
+    d.inst = reinterpret_cast<const GpuInstance*>(c->prims.as<GpuPrimitive>() + np_);
+    d.num_instances = v->num_triangles ? ni : 0;
+    d.tlas_root = v->tlas_root;
+    d.blas_roots = c->blas_roots.as<uint32_t>();
+    d.num_blas = (uint32_t)roots.size();
+    d.reference_shadows = false;
     d.tnodes = c->tnodes.as<float4>();
     d.soup = c->soup.as<float4>();
     d.root_first = 0;
@@ -346,7 +381,7 @@ static int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth) {
     paths = std::max(paths, rs.capacity);
     ctrs = std::max(ctrs, rs.ctr_capacity);
     const size_t f4 = sizeof(float4);
-    size_t bytes = paths * (11 * f4 + 2 * sizeof(uint32_t)) + ctrs * sizeof(uint32_t) + 16 * 256;
+    size_t bytes = paths * (11 * f4 + 3 * sizeof(uint32_t)) + ctrs * sizeof(uint32_t) + 16 * 256;
     LUC_CUDA(c, c->pool.ensure(bytes), "allocate path pool");
     char* p = (char*)c->pool.p;
     auto take = [&](size_t n) {
@@ -368,6 +403,7 @@ static int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth) {
     ps.sh_c = (float4*)take(paths * f4);
     ps.queue[0] = (uint32_t*)take(paths * 4);
     ps.queue[1] = (uint32_t*)take(paths * 4);
+    ps.hinst = (uint32_t*)take(paths * 4);
     ps.ctr = (uint32_t*)take(ctrs * 4);
     ps.stat = (unsigned long long*)take(8 * sizeof(unsigned long long));
     if ((size_t)(p - (char*)c->pool.p) > c->pool.bytes) return luc_fail(c, LUC_ERR_VALIDATION, "path pool carve");
@@ -387,7 +423,7 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     if ((out_host == nullptr) == (out_dev == nullptr))
         return luc_fail(c, LUC_ERR_VALIDATION, "exactly one of out_host / out_dev must be given");
     if ((flags & 0xFFu) != LUC_ARCH_WAVEFRONT) return luc_fail(c, LUC_ERR_VALIDATION, "unknown architecture");
-    if (flags & ~(0xFFu | LUC_FLAG_NO_GUIDES | LUC_FLAG_PROFILE | LUC_FLAG_GUIDED))
+    if (flags & ~(0xFFu | LUC_FLAG_NO_GUIDES | LUC_FLAG_PROFILE | LUC_FLAG_GUIDED | LUC_FLAG_REFERENCE_SHADOWS))
         return luc_fail(c, LUC_ERR_VALIDATION, "unknown render flag");
     const bool guided = (flags & LUC_FLAG_GUIDED) != 0;
     if (guided && !c->guide_ready)
@@ -439,6 +475,7 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     fp.cam_vertical = ld3(u->cam_vertical);
     DevScene sc = c->scene;
     sc.background = ld3(u->background);
+    sc.reference_shadows = (flags & LUC_FLAG_REFERENCE_SHADOWS) != 0;
 
     c->stats = luc_render_stats{};
     c->rs.launches = 0;

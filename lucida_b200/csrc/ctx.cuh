@@ -48,6 +48,7 @@ struct luc_ctx {
     // Resident scene.
     DevBuf materials, prims, lights, positions, attrs, tris, nodes, env_px, env_cond, env_marg, env_row_sin, energy;
     DevBuf tnodes, soup;  // traversal layout derived from nodes / tris
+    DevBuf blas_roots;    // distinct BLAS roots of an instanced scene
     luc::DevScene scene{};
     bool has_scene = false;
     uint32_t num_materials = 0;

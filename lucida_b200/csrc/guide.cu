@@ -270,7 +270,8 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(PathState ps, 
                 hit_row = true;
                 const float4 o4 = ps.o_pdf[q], d4 = ps.dir[q];
                 const V3 dir{d4.x, d4.y, d4.z};
-                const SurfaceHit hit = surface_hit(sc, id, h4.x, h4.y, h4.z, V3{o4.x, o4.y, o4.z}, dir);
+                const SurfaceHit hit = surface_hit(sc, id, sc.num_instances ? ps.hinst[q] : 0u, h4.x, h4.y, h4.z,
+                                                   V3{o4.x, o4.y, o4.z}, dir);
                 in[0] = hit.position.x;
                 in[1] = hit.position.y;
                 in[2] = hit.position.z;

@@ -24,6 +24,7 @@ struct PathState {
     float4* rad;    // radiance accumulated along the path
     float4* prev;   // previous vertex (for the MIS light pdf)
     float4* hit;    // t, u, v, id (u32 bits)
+    uint32_t* hinst;  // instance of the hit (instanced scenes)
     float4* galb;   // first-hit albedo, depth
     float4* gnrm;   // first-hit shading normal
     float4* sh_o;   // shadow ray origin, t_max
@@ -99,7 +100,9 @@ struct RenderState {
     uint64_t capacity = 0;  // paths
     uint32_t ctr_capacity = 0;
     int num_sms = 148;
-    int extend_blocks = 0, connect_blocks = 0, shade_blocks = 0, shade_blocks_guided = 0;  // resident blocks per SM
+    // Resident blocks per SM of each stage kernel (single-level / instanced).
+    int extend_blocks = 0, connect_blocks = 0, shade_blocks = 0, shade_blocks_guided = 0;
+    int extend_blocks_inst = 0, connect_blocks_inst = 0, shade_blocks_inst = 0, shade_blocks_guided_inst = 0;
     uint64_t launches = 0;
 };
 

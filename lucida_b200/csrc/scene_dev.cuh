@@ -21,6 +21,14 @@ struct DevScene {
     const float4* tnodes;  // child-pair records, 4 float4 per internal node id
     const float4* soup;    // (p0, e1, e2) per triangle, leaf order
     uint32_t root_first, root_count;  // the root when it is itself a leaf
+    // Instancing (instance.rs): GpuInstance rows appended after the analytic
+    // primitives, in TLAS-leaf order; the TLAS's first node in `nodes`; the
+    // distinct BLAS roots (for the reference's shadow-ray behaviour).
+    const GpuInstance* inst;
+    uint32_t num_instances, tlas_root;
+    const uint32_t* blas_roots;
+    uint32_t num_blas;
+    bool reference_shadows;
     const float4* env_px;
     const float* env_cond;   // (w+1) per row
     const float* env_marg;   // h+1
@@ -201,17 +209,18 @@ LUC_D bool hit_soup(const float4* __restrict__ soup, uint32_t k, V3 o, V3 d, flo
 // ties the later-tested triangle). While-while traversal (Aila & Laine):
 // descend internal nodes near-child-first, postponing the first leaf met so
 // lanes of a warp run the node loop and the triangle loop together.
-LUC_D bool bvh_closest(const DevScene& s, V3 o, V3 d, float tmin, float& closest, float& bu, float& bv,
+// `root` is (node, 0) for an internal root or (first triangle, count) for a
+// root that is itself a leaf.
+LUC_D bool bvh_closest(const DevScene& s, TRef root, V3 o, V3 d, float tmin, float& closest, float& bu, float& bv,
                        uint32_t& btri, TravCount& tc) {
-    if (s.num_nodes == 0) return false;
     const V3 inv = safe_inv_dir(d);
     const V3 oi = V3{o.x * inv.x, o.y * inv.y, o.z * inv.z};
     bool found = false;
     TRef stack[64];
     int sp = 0;
-    TRef cur{0u, 0u}, leaf{0u, 0u};
-    if (s.root_count > 0) {
-        leaf = TRef{s.root_first, s.root_count};
+    TRef cur = root, leaf{0u, 0u};
+    if (root.cnt > 0) {
+        leaf = root;
         cur = TRef{kNoNode, 0u};
     }
     for (;;) {
@@ -262,15 +271,14 @@ LUC_D bool bvh_closest(const DevScene& s, V3 o, V3 d, float tmin, float& closest
 }
 
 // Any hit within [tmin, tmax] (bvh.rs:1137-1193).
-LUC_D bool bvh_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax, TravCount& tc) {
-    if (s.num_nodes == 0) return false;
+LUC_D bool bvh_any(const DevScene& s, TRef root, V3 o, V3 d, float tmin, float tmax, TravCount& tc) {
     const V3 inv = safe_inv_dir(d);
     const V3 oi = V3{o.x * inv.x, o.y * inv.y, o.z * inv.z};
     TRef stack[64];
     int sp = 0;
-    TRef cur{0u, 0u}, leaf{0u, 0u};
-    if (s.root_count > 0) {
-        leaf = TRef{s.root_first, s.root_count};
+    TRef cur = root, leaf{0u, 0u};
+    if (root.cnt > 0) {
+        leaf = root;
         cur = TRef{kNoNode, 0u};
     }
     for (;;) {
@@ -312,9 +320,129 @@ LUC_D bool bvh_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax, TravCo
     }
 }
 
+// ---------------------------------------------------------------- instancing
+// Root reference of the subtree at node i: (i, 0) if internal, else its leaf.
+LUC_D TRef node_ref(const DevScene& s, uint32_t i) {
+    float4 a = __ldg(s.nodes + 2 * (size_t)i), b = __ldg(s.nodes + 2 * (size_t)i + 1);
+    uint32_t count = __float_as_uint(b.w);
+    return count ? TRef{__float_as_uint(a.w), count} : TRef{i, 0u};
+}
+// Instance::transform_ray (instance.rs:119-125) through the stored rows:
+// ((r.x*p.x + r.y*p.y) + r.z*p.z) (+ t), the order glam sums the columns in.
+LUC_D V3 inst_point(const GpuInstance& g, V3 p) {
+    return V3{((g.inv_row0[0] * p.x + g.inv_row0[1] * p.y) + g.inv_row0[2] * p.z) + g.inv_translation[0],
+              ((g.inv_row1[0] * p.x + g.inv_row1[1] * p.y) + g.inv_row1[2] * p.z) + g.inv_translation[1],
+              ((g.inv_row2[0] * p.x + g.inv_row2[1] * p.y) + g.inv_row2[2] * p.z) + g.inv_translation[2]};
+}
+LUC_D V3 inst_vector(const GpuInstance& g, V3 v) {
+    return V3{(g.inv_row0[0] * v.x + g.inv_row0[1] * v.y) + g.inv_row0[2] * v.z,
+              (g.inv_row1[0] * v.x + g.inv_row1[1] * v.y) + g.inv_row1[2] * v.z,
+              (g.inv_row2[0] * v.x + g.inv_row2[1] * v.y) + g.inv_row2[2] * v.z};
+}
+// Instance::transform_normal (instance.rs:137-141): transpose of the stored
+// 3x3 times n, normalised (or +z).
+LUC_D V3 inst_normal(const GpuInstance& g, V3 n) {
+    V3 t{(g.inv_row0[0] * n.x + g.inv_row1[0] * n.y) + g.inv_row2[0] * n.z,
+         (g.inv_row0[1] * n.x + g.inv_row1[1] * n.y) + g.inv_row2[1] * n.z,
+         (g.inv_row0[2] * n.x + g.inv_row1[2] * n.y) + g.inv_row2[2] * n.z};
+    return normalize_or(t, V3{0.0f, 0.0f, 1.0f});
+}
+
+// InstanceSet::intersect (instance.rs:342-421): walk the TLAS in world space
+// with the child-pair records (near child first; leaves hold instance
+// rows), and at each instance walk its BLAS with the ray in object space and
+// the closest t so far — the transform keeps t, so one t_max serves both
+// levels. The returned triangle index is absolute; `instance` indexes s.inst.
+LUC_D bool instances_closest(const DevScene& s, V3 o, V3 d, float tmin, float& closest, float& bu, float& bv,
+                             uint32_t& btri, uint32_t& binst, TravCount& tc) {
+    const V3 inv = safe_inv_dir(d);
+    const V3 oi = V3{o.x * inv.x, o.y * inv.y, o.z * inv.z};
+    bool found = false;
+    TRef stack[32];
+    int sp = 0;
+    TRef cur = node_ref(s, s.tlas_root);
+    for (;;) {
+        if (cur.cnt == 0) {
+            bool h0, h1;
+            float e0, e1;
+            TRef r0, r1;
+            test_pair(s.tnodes + 4 * (size_t)cur.a, oi, inv, tmin, closest, h0, h1, e0, e1, r0, r1);
+            tc.nodes++;
+            if (h0 && h1) {
+                bool first = e0 <= e1;
+                if (sp < 32) stack[sp++] = first ? r1 : r0;
+                cur = first ? r0 : r1;
+                continue;
+            } else if (h0) {
+                cur = r0;
+                continue;
+            } else if (h1) {
+                cur = r1;
+                continue;
+            }
+        } else {
+            for (uint32_t ii = cur.a; ii < cur.a + cur.cnt; ++ii) {
+                const uint32_t k = ii - s.num_prims;
+                const GpuInstance g = s.inst[k];
+                if (bvh_closest(s, node_ref(s, g.blas_root), inst_point(g, o), inst_vector(g, d), tmin, closest, bu, bv,
+                                btri, tc)) {
+                    binst = k;
+                    found = true;
+                }
+            }
+        }
+        if (sp == 0) break;
+        cur = stack[--sp];
+    }
+    return found;
+}
+
+// Any hit through the two levels (the default for shadow rays).
+LUC_D bool instances_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax, TravCount& tc) {
+    const V3 inv = safe_inv_dir(d);
+    const V3 oi = V3{o.x * inv.x, o.y * inv.y, o.z * inv.z};
+    TRef stack[32];
+    int sp = 0;
+    TRef cur = node_ref(s, s.tlas_root);
+    for (;;) {
+        if (cur.cnt == 0) {
+            bool h0, h1;
+            float e0, e1;
+            TRef r0, r1;
+            test_pair(s.tnodes + 4 * (size_t)cur.a, oi, inv, tmin, tmax, h0, h1, e0, e1, r0, r1);
+            tc.nodes++;
+            if (h0 && h1) {
+                if (sp < 32) stack[sp++] = r1;
+                cur = r0;
+                continue;
+            } else if (h0) {
+                cur = r0;
+                continue;
+            } else if (h1) {
+                cur = r1;
+                continue;
+            }
+        } else {
+            for (uint32_t ii = cur.a; ii < cur.a + cur.cnt; ++ii) {
+                const GpuInstance g = s.inst[ii - s.num_prims];
+                if (bvh_any(s, node_ref(s, g.blas_root), inst_point(g, o), inst_vector(g, d), tmin, tmax, tc))
+                    return true;
+            }
+        }
+        if (sp == 0) return false;
+        cur = stack[--sp];
+    }
+}
+
 // Scene::intersect (scene.rs:452-527): analytic primitives by brute force,
 // then triangles bounded by the analytic hit. Returns the id (kMiss on miss).
-LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, float& v, TravCount& tc) {
+// In an instanced scene the instances replace the single-level triangle path
+// (scene.rs:489-501) and `inst` receives the hit's instance (s.inst index).
+// kInst selects the instanced code at compile time, so kernels launched for
+// single-level scenes carry none of its registers.
+template <bool kInst>
+LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, float& v, uint32_t& inst,
+                           TravCount& tc) {
     float best_t = kTMax;
     uint32_t id = kMiss;
     for (uint32_t i = 0; i < s.num_prims; ++i) {
@@ -330,7 +458,11 @@ LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, fl
     }
     float bu = 0.0f, bv = 0.0f;
     uint32_t tri;
-    if (bvh_closest(s, o, d, kTMin, best_t, bu, bv, tri, tc)) {
+    inst = 0u;
+    if (kInst) {
+        if (instances_closest(s, o, d, kTMin, best_t, bu, bv, tri, inst, tc)) id = tri;
+    } else if (s.num_nodes > 0 && bvh_closest(s, TRef{s.root_count ? s.root_first : 0u, s.root_count}, o, d, kTMin,
+                                              best_t, bu, bv, tri, tc)) {
         id = tri;
     } else if (s.num_nodes == 0 && s.num_tris > 0) {
         // No BVH: brute force over every triangle (bvh.rs:975-997).
@@ -352,6 +484,7 @@ LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, fl
 }
 
 // Scene::occluded (scene.rs:577-606).
+template <bool kInst>
 LUC_D bool occluded(const DevScene& s, V3 o, V3 d, float tmax, TravCount& tc) {
     for (uint32_t i = 0; i < s.num_prims; ++i) {
         const GpuPrimitive& p = s.prims[i];
@@ -361,6 +494,14 @@ LUC_D bool occluded(const DevScene& s, V3 o, V3 d, float tmax, TravCount& tc) {
                      : hit_sphere(ld3(p.position), p.radius, o, d, kTMin, tmax, th);
         if (h) return true;
     }
+    if (kInst) {
+        if (!s.reference_shadows) return instances_any(s, o, d, kTMin, tmax, tc);
+        // The reference's shadow rays (scene.rs:577-606) test every mesh's
+        // triangles untransformed, in object space.
+        for (uint32_t b = 0; b < s.num_blas; ++b)
+            if (bvh_any(s, node_ref(s, s.blas_roots[b]), o, d, kTMin, tmax, tc)) return true;
+        return false;
+    }
     if (s.num_nodes == 0) {
         for (uint32_t k = 0; k < s.num_tris; ++k) {
             GpuTriangle tr = s.tris[k];
@@ -369,7 +510,7 @@ LUC_D bool occluded(const DevScene& s, V3 o, V3 d, float tmax, TravCount& tc) {
         }
         return false;
     }
-    return bvh_any(s, o, d, kTMin, tmax, tc);
+    return bvh_any(s, TRef{s.root_count ? s.root_first : 0u, s.root_count}, o, d, kTMin, tmax, tc);
 }
 
 struct SurfaceHit {
@@ -379,7 +520,8 @@ struct SurfaceHit {
     float light_area;
 };
 // scene.rs:405-435 (triangles) and :533-573 (analytic).
-LUC_D SurfaceHit surface_hit(const DevScene& s, uint32_t id, float t, float u, float v, V3 o, V3 d) {
+template <bool kInst>
+LUC_D SurfaceHit surface_hit_t(const DevScene& s, uint32_t id, uint32_t inst, float t, float u, float v, V3 o, V3 d) {
     SurfaceHit h;
     if (id & kAnalytic) {
         const GpuPrimitive& p = s.prims[id & ~kAnalytic];
@@ -394,6 +536,16 @@ LUC_D SurfaceHit surface_hit(const DevScene& s, uint32_t id, float t, float u, f
         h.material = p.material;
         return h;
     }
+    // Instanced (scene.rs:375-402): shade in object space with the object-space
+    // direction, bring both normals back, then decide front and back in world
+    // space; the position is the world ray at t, which the transform keeps.
+    const bool instanced = kInst;
+    GpuInstance g;
+    V3 dl = d;
+    if (instanced) {
+        g = s.inst[inst];
+        dl = inst_vector(g, d);
+    }
     GpuTriangle tr = s.tris[id];
     V3 p0 = vtx(s, tr.i0), p1 = vtx(s, tr.i1), p2 = vtx(s, tr.i2);
     float w = 1.0f - u - v;
@@ -401,14 +553,30 @@ LUC_D SurfaceHit surface_hit(const DevScene& s, uint32_t id, float t, float u, f
     V3 shading = normalize_or(w * n0 + u * n1 + v * n2, V3{0.0f, 0.0f, 1.0f});
     V3 cr = cross(p1 - p0, p2 - p0);
     V3 geometric = normalize_or(cr, V3{0.0f, 0.0f, 1.0f});
-    h.front = dot(geometric, d) < 0.0f;
+    h.front = dot(geometric, dl) < 0.0f;
     float flip = h.front ? 1.0f : -1.0f;
-    h.position = o + t * d;
     h.normal = shading * flip;
     h.gnormal = geometric * flip;
     h.material = tr.material;
+    if (instanced) {
+        h.normal = inst_normal(g, h.normal);
+        h.gnormal = inst_normal(g, h.gnormal);
+        h.front = dot(h.gnormal, d) < 0.0f;
+        flip = h.front ? 1.0f : -1.0f;
+        h.normal = h.normal * flip;
+        h.gnormal = h.gnormal * flip;
+        if (g.material != 0xFFFFFFFFu) h.material = g.material;
+        h.position = o + t * d;
+        h.light_area = 0.0f;
+        return h;
+    }
+    h.position = o + t * d;
     h.light_area = 0.5f * length(cr);
     return h;
+}
+LUC_D SurfaceHit surface_hit(const DevScene& s, uint32_t id, uint32_t inst, float t, float u, float v, V3 o, V3 d) {
+    return s.num_instances ? surface_hit_t<true>(s, id, inst, t, u, v, o, d)
+                           : surface_hit_t<false>(s, id, inst, t, u, v, o, d);
 }
 
 }  // namespace luc

@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(256) k_generate(PathState ps, FrameParams fp) 
 // Persistent ray pull: each warp claims 32 queue entries at a time from the
 // depth's cursor until the queue is drained, so fast warps keep taking work
 // instead of idling behind slow ones.
+template <bool kInst>
 __global__ void __launch_bounds__(128) k_extend(PathState ps, DevScene sc, FrameParams fp, uint32_t depth) {
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
     const uint32_t* queue = ps.queue[depth & 1];
@@ -101,8 +102,10 @@ __global__ void __launch_bounds__(128) k_extend(PathState ps, DevScene sc, Frame
             uint32_t p = depth == 0 ? i : queue[i];
             float4 o4 = ps.o_pdf[p], d4 = ps.dir[p];
             float t, u, v;
-            uint32_t id = closest_hit(sc, xyz(o4), xyz(d4), t, u, v, tc);
+            uint32_t inst;
+            uint32_t id = closest_hit<kInst>(sc, xyz(o4), xyz(d4), t, u, v, inst, tc);
             ps.hit[p] = make_float4(t, u, v, __uint_as_float(id));
+            if (kInst) ps.hinst[p] = inst;
             ++rays;
         }
         __syncwarp();
@@ -131,7 +134,7 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
 // the choice), with p = 0.5 p_bsdf + 0.5 p_guide as the path's sampling pdf in
 // both MIS sites (emission hit and NEE); plus training records for a
 // threshold-selected subset of those vertices.
-template <bool kGuided>
+template <bool kGuided, bool kInst>
 __global__ void __launch_bounds__(128, 4) k_shade(PathState ps, DevScene sc, FrameParams fp, uint32_t depth) {
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
     const uint32_t rec_threshold = kGuided ? ps.gmisc[kGmThreshold] : 65536u;
@@ -196,7 +199,7 @@ __global__ void __launch_bounds__(128, 4) k_shade(PathState ps, DevScene sc, Fra
                 }
             } else {
                 V3 org = xyz(o4);
-                SurfaceHit hit = surface_hit(sc, id, h4.x, h4.y, h4.z, org, dir);
+                SurfaceHit hit = surface_hit_t<kInst>(sc, id, kInst ? ps.hinst[p] : 0u, h4.x, h4.y, h4.z, org, dir);
                 const GpuMaterial m = sc.materials[hit.material];
                 V3 emissive = ld3(m.emissive);
                 // Emission with MIS (integrator.rs:271-309).
@@ -413,6 +416,7 @@ __global__ void __launch_bounds__(128, 4) k_shade(PathState ps, DevScene sc, Fra
 
 // CONNECT (shaders/wavefront/connect.wgsl:58-84): any-hit shadow rays, with
 // the same persistent ray pull as EXTEND.
+template <bool kInst>
 __global__ void __launch_bounds__(128) k_connect(PathState ps, DevScene sc, uint32_t depth) {
     const uint32_t len = ps.ctr[depth * kCtrStride + kCtrShadow];
     uint32_t* pull = ps.ctr + depth * kCtrStride + kCtrPullConnect;
@@ -427,7 +431,7 @@ __global__ void __launch_bounds__(128) k_connect(PathState ps, DevScene sc, uint
         const uint32_t i = base + lane;
         if (i < len) {
             float4 o4 = ps.sh_o[i], d4 = ps.sh_d[i];
-            if (!occluded(sc, xyz(o4), xyz(d4), o4.w, tc)) {
+            if (!occluded<kInst>(sc, xyz(o4), xyz(d4), o4.w, tc)) {
                 uint32_t p = __float_as_uint(d4.w);
                 float4 c4 = ps.sh_c[i], r4 = ps.rad[p];
                 ps.rad[p] = make_float4(r4.x + c4.x, r4.y + c4.y, r4.z + c4.z, 0.0f);
@@ -497,15 +501,19 @@ __global__ void k_make_soup(const GpuTriangle* __restrict__ tris, const float4* 
 }
 
 void query_occupancy(RenderState& rs) {
-    int b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend, 128, 0);
-    rs.extend_blocks = b > 0 ? b : 8;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_connect, 128, 0);
-    rs.connect_blocks = b > 0 ? b : 8;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<false>, 128, 0);
-    rs.shade_blocks = b > 0 ? b : 8;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<true>, 128, 0);
-    rs.shade_blocks_guided = b > 0 ? b : 8;
+    auto occ = [](const void* k) {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, 128, 0);
+        return b > 0 ? b : 8;
+    };
+    rs.extend_blocks = occ((const void*)k_extend<false>);
+    rs.connect_blocks = occ((const void*)k_connect<false>);
+    rs.shade_blocks = occ((const void*)k_shade<false, false>);
+    rs.shade_blocks_guided = occ((const void*)k_shade<true, false>);
+    rs.extend_blocks_inst = occ((const void*)k_extend<true>);
+    rs.connect_blocks_inst = occ((const void*)k_connect<true>);
+    rs.shade_blocks_inst = occ((const void*)k_shade<false, true>);
+    rs.shade_blocks_guided_inst = occ((const void*)k_shade<true, true>);
 }
 
 // Host side: record one batch of the frame on `stream` (graph-capturable:
@@ -524,20 +532,29 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
     }
     for (uint32_t d = 0; d < fp.max_depth; ++d) {
         if (timer) timer->mark(stream, StageTimer::kExtend);
-        k_extend<<<sms * rs.extend_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        const bool inst = sc.num_instances > 0;
+        if (inst) k_extend<true><<<sms * rs.extend_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        else k_extend<false><<<sms * rs.extend_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
         if (fp.guided && d + 1 < fp.max_depth) {
             if (timer) timer->mark(stream, StageTimer::kGuide);
             launch_guide_infer(rs, sc, fp, d, stream);
             rs.launches++;
         }
         if (timer) timer->mark(stream, StageTimer::kShade);
-        if (fp.guided) k_shade<true><<<sms * rs.shade_blocks_guided, 128, 0, stream>>>(rs.ps, sc, fp, d);
-        else k_shade<false><<<sms * rs.shade_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        if (fp.guided && inst)
+            k_shade<true, true><<<sms * rs.shade_blocks_guided_inst, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        else if (fp.guided)
+            k_shade<true, false><<<sms * rs.shade_blocks_guided, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        else if (inst)
+            k_shade<false, true><<<sms * rs.shade_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        else
+            k_shade<false, false><<<sms * rs.shade_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
         rs.launches += 2;
         if (d + 1 < fp.max_depth && (fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) &&
             sc.light_strategies > 0) {
             if (timer) timer->mark(stream, StageTimer::kConnect);
-            k_connect<<<sms * rs.connect_blocks, 128, 0, stream>>>(rs.ps, sc, d);
+            if (inst) k_connect<true><<<sms * rs.connect_blocks_inst, 128, 0, stream>>>(rs.ps, sc, d);
+            else k_connect<false><<<sms * rs.connect_blocks, 128, 0, stream>>>(rs.ps, sc, d);
             rs.launches++;
         }
     }

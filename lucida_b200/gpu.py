@@ -21,8 +21,9 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import layout as L
-from .native import (LUC_FLAG_GUIDED, LUC_FLAG_NO_GUIDES, LUC_FLAG_PROFILE, DenoiseParams as _DP, GpuError, LbvhOut,
-                     RenderStats, SceneView, camera_uniforms, check, lib, ptr)
+from .native import (LUC_FLAG_GUIDED, LUC_FLAG_NO_GUIDES, LUC_FLAG_PROFILE, LUC_FLAG_REFERENCE_SHADOWS,
+                     DenoiseParams as _DP, GpuError, LbvhOut, RenderStats, SceneView, camera_uniforms, check, lib,
+                     ptr)
 
 __all__ = ["Gpu", "SceneDef", "Camera", "RenderParams", "Film", "render_with", "render_native_on",
            "render_accum", "render_native_denoised", "LbvhBuilder", "GpuBuildOutput", "DenoiseParams",
@@ -57,6 +58,11 @@ class SceneDef:
     env_cdf: np.ndarray | None = None  # (h + 1, cdf_w) float32, lib.rs:322-338 packing
     env_total_weight: float = 0.0
     name: str = "scene"
+    # Instanced scenes (scene.rs:252-345 layout): the last `num_instances`
+    # rows of `primitives` are GpuInstance rows in TLAS-leaf order and
+    # `bvh_nodes` holds every BLAS followed by the TLAS from `tlas_root` on.
+    num_instances: int = 0
+    tlas_root: int = 0
 
     @property
     def env_size(self):
@@ -143,7 +149,8 @@ class Gpu:
         m = arr(scene.materials, L.MATERIAL)
         v.materials, v.num_materials = ptr(m), len(m)
         p = arr(scene.primitives, L.PRIMITIVE)
-        v.primitives, v.num_primitives, v.num_instances = ptr(p), len(p), 0
+        v.primitives, v.num_primitives, v.num_instances = ptr(p), len(p) - scene.num_instances, scene.num_instances
+        v.tlas_root = scene.tlas_root
         li = arr(scene.lights, L.LIGHT)
         v.lights, v.num_lights = ptr(li), len(li)
         pos = arr(scene.positions, np.float32).reshape(-1, 4)
@@ -180,7 +187,9 @@ def build_uniforms(scene: SceneDef, params: RenderParams) -> L.Uniforms:
     u.samples_per_launch = params.samples
     u.max_depth = params.max_depth
     u.frame_seed = params.frame_seed & 0xFFFFFFFF
-    u.num_primitives = len(scene.primitives)
+    u.num_primitives = len(scene.primitives) - scene.num_instances
+    u.num_instances = scene.num_instances
+    u.tlas_root = scene.tlas_root
     u.num_lights = len(scene.lights)
     u.num_triangles = len(scene.triangles)
     u.num_bvh_nodes = 0 if scene.bvh_nodes is None else len(scene.bvh_nodes)
@@ -195,7 +204,8 @@ def build_uniforms(scene: SceneDef, params: RenderParams) -> L.Uniforms:
 
 
 def render_accum(gpu: Gpu, scene: SceneDef, params: RenderParams, uniforms: L.Uniforms | None = None,
-                 guides: bool = True, profile: bool = False, guided: bool = False) -> np.ndarray:
+                 guides: bool = True, profile: bool = False, guided: bool = False,
+                 reference_shadows: bool = False) -> np.ndarray:
     """Render and return the raw GpuAccum array, shape (height, width).
     guided=True samples with the context's learned guide (lucida_b200.guide),
     which must have been initialised, and trains it after every batch."""
@@ -203,7 +213,7 @@ def render_accum(gpu: Gpu, scene: SceneDef, params: RenderParams, uniforms: L.Un
     u = uniforms if uniforms is not None else build_uniforms(scene, params)
     out = np.zeros(params.width * params.height, L.ACCUM)
     flags = ((0 if guides else LUC_FLAG_NO_GUIDES) | (LUC_FLAG_PROFILE if profile else 0)
-             | (LUC_FLAG_GUIDED if guided else 0))
+             | (LUC_FLAG_GUIDED if guided else 0) | (LUC_FLAG_REFERENCE_SHADOWS if reference_shadows else 0))
     check(gpu.handle, lib().luc_render(gpu.handle, C.byref(u), params.samples, params.max_depth, flags, ptr(out),
                                        None))
     return out.reshape(params.height, params.width)

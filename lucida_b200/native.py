@@ -20,6 +20,7 @@ ERRORS = {-1: "NoDevice", -2: "Launch", -3: "Readback", -4: "Validation", -5: "O
 LUC_FLAG_NO_GUIDES = 0x100
 LUC_FLAG_PROFILE = 0x200
 LUC_FLAG_GUIDED = 0x400
+LUC_FLAG_REFERENCE_SHADOWS = 0x800
 
 
 class GpuError(RuntimeError):

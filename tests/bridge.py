@@ -21,7 +21,8 @@ def scene_from_oracle(osc: "O.Scene", with_bvh=True) -> SceneDef:
         env_cdf[:h, :w + 1] = osc.array(O.W_ENV_COND).reshape(h, w + 1)
         env_cdf[h, :h + 1] = osc.array(O.W_ENV_MARG)
     tris = osc.array(O.W_TRIANGLES)
-    return SceneDef(materials=osc.array(O.W_MATERIALS).view(L.MATERIAL),
+    ni, _, tlas_root = osc.instancing()
+    return SceneDef(num_instances=ni, tlas_root=tlas_root,materials=osc.array(O.W_MATERIALS).view(L.MATERIAL),
                     primitives=osc.array(O.W_PRIMITIVES).view(L.PRIMITIVE),
                     lights=osc.array(O.W_LIGHTS).view(L.LIGHT),
                     positions=osc.array(O.W_POSITIONS).reshape(-1, 4),
@@ -44,7 +45,8 @@ def oracle_from_scene(s: SceneDef, bvh="sah") -> "O.Scene":
                                s.vertex_attrs.view(O.VERTEX_ATTR), s.triangles.view(O.TRIANGLE),
                                lights=s.lights.view(O.LIGHT), env=env, background=s.background,
                                camera=dict(eye=cam.eye, look_at=cam.look_at, vfov_deg=cam.vfov_deg, up=cam.up,
-                                           aperture=cam.aperture, focus_distance=cam.focus_distance), bvh=bvh)
+                                           aperture=cam.aperture, focus_distance=cam.focus_distance), bvh=bvh,
+                               instancing=((s.bvh_nodes, s.num_instances, s.tlas_root) if s.num_instances else None))
 
 
 def compare(a: np.ndarray, b: np.ndarray) -> dict:

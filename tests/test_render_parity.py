@@ -89,6 +89,38 @@ def test_triangle_workload_scenes(gpu, which):
     _check(acc, ref, which)
 
 
+@pytest.mark.parametrize("mode", ["bsdf", "nee", "mis"])
+@pytest.mark.parametrize("shadows", ["two-level", "reference"])
+def test_instanced_scene(gpu, mode, shadows):
+    """The reference's instance-forest (one BLAS, 49 rotated and non-uniformly
+    scaled instances under a TLAS, material overrides): two-level closest hit
+    and shading, and shadow rays either through the two levels (the default)
+    or as the reference casts them (LUC_FLAG_REFERENCE_SHADOWS)."""
+    osc = O.Scene.builtin("instance-forest")
+    ref_shadows = shadows == "reference"
+    osc.set_reference_shadows(ref_shadows)
+    s = scene_from_oracle(osc)
+    u = osc.uniforms(64, 48, 8, 6, frame_seed=0x5EED1234, sampling=lb.layout.SAMPLING[mode],
+                     sampler=lb.layout.SAMPLER["sobol"])
+    params = lb.RenderParams(width=64, height=48, samples=8, max_depth=6, sampling=mode, sampler="sobol")
+    acc = lb.render_accum(gpu, s, params, uniforms=lb.layout.uniforms_from_bytes(bytes(u)),
+                          reference_shadows=ref_shadows).reshape(-1)
+    _check(acc, osc.render_sums(u), f"instance-forest/{mode}/{shadows}")
+
+
+def test_instanced_shadow_modes_differ(gpu):
+    """The two shadow-ray behaviours are really different on this scene (the
+    reference's untransformed mesh sits at the origin, the instances cast real
+    shadows), so the mode test above compares two distinct images."""
+    osc = O.Scene.builtin("instance-forest")
+    s = scene_from_oracle(osc)
+    params = lb.RenderParams(width=64, height=48, samples=16, max_depth=4, sampling="nee", sampler="sobol")
+    a = lb.render_accum(gpu, s, params)["radiance"]
+    b = lb.render_accum(gpu, s, params, reference_shadows=True)["radiance"]
+    assert np.mean(np.any(a != b, axis=-1)) > 0.05
+    assert b.sum() > a.sum()  # fewer blockers in the reference's shadow rays
+
+
 def test_progressive_equals_one_shot(gpu):
     """Accumulating 4 + 4 samples into one device accumulator equals one 8-sample
     render bit for bit (cpu_gpu_agreement.rs:119-168 asks < 1e-5)."""
