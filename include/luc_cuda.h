@@ -222,6 +222,28 @@ int32_t luc_sort_u32_static(void* keys_dev, void* vals_dev, uint32_t n, void* st
                             uint32_t err_len);
 uint32_t luc_sort_u32_static_max(void);
 
+/* ---- Device-built instancing (no reference counterpart: the reference
+ * builds its BLASes and TLAS once, on the CPU, with binned SAH in
+ * Scene::build_instances, crates/core/src/scene.rs:252-345) ----
+ * luc_upload_meshes uploads a scene like luc_upload_scene (no instances, no
+ * tree) whose triangles are grouped into meshes (ascending, disjoint ranges
+ * [first, first + count)) in object space, and builds one LBVH per mesh on the
+ * device. luc_set_instances then places the meshes: per instance a row-major
+ * 3x4 object-to-world transform (12 floats), a mesh index and a material
+ * override (UINT32_MAX keeps the triangles' own); the device inverts each
+ * transform, bounds each instance in world space and rebuilds the TLAS by
+ * LBVH over those boxes. Call it again whenever the placements change (per
+ * frame); rendering needs at least one call after the upload. */
+int32_t luc_upload_meshes(luc_ctx* ctx, const luc_scene_view* view, const uint32_t* mesh_first,
+                          const uint32_t* mesh_count, uint32_t num_meshes);
+int32_t luc_set_instances(luc_ctx* ctx, const float* object_to_world, const uint32_t* mesh, const uint32_t* material,
+                          uint32_t num_instances);
+/* Copy the resident scene's arrays to the host: which = 0 BVH nodes (every
+ * BLAS then the TLAS), 1 triangles (leaf order), 2 primitives (analytic, then
+ * instance rows in TLAS-leaf order). *bytes receives the size; out may be null
+ * to query it. */
+int32_t luc_read_scene(luc_ctx* ctx, uint32_t which, void* out, uint64_t capacity, uint64_t* bytes);
+
 /* ---- Learned path-guiding proposal (no reference counterpart) ----
  * Model: frequency-encoded position (12 frequencies per axis over the guide's
  * box), shading normal and outgoing direction (4 each), 120 features padded to

@@ -101,13 +101,6 @@ const std::vector<float>& energy_table_cached() {
     return t;
 }
 
-template <class T>
-cudaError_t upload(DevBuf& b, const T* src, size_t n, cudaStream_t s) {
-    cudaError_t e = b.ensure(n * sizeof(T));
-    if (e != cudaSuccess || n == 0 || !src) return e;
-    return cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, s);
-}
-
 }  // namespace
 
 extern "C" {
@@ -186,7 +179,17 @@ int32_t luc_set_stream(luc_ctx* c, void* stream) {
     return LUC_OK;
 }
 
-int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) {
+}  // extern "C"
+
+// Mesh ranges for device-built instancing (luc_upload_meshes); null for a
+// plain upload.
+struct MeshSpec {
+    const uint32_t* first;
+    const uint32_t* count;
+    uint32_t n;
+};
+
+static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec* meshes) {
     if (!c || !v) return LUC_ERR_VALIDATION;
     cudaSetDevice(c->device);
     if (v->num_materials == 0 || !v->materials) return luc_fail(c, LUC_ERR_VALIDATION, "scene has no materials");
@@ -285,7 +288,19 @@ int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) {
     LUC_CUDA(c, upload(c->positions, v->positions, 4 * (size_t)v->num_vertices, s), "upload positions");
     LUC_CUDA(c, upload(c->attrs, v->vertex_attrs, v->num_vertices, s), "upload vertex attrs");
     uint32_t num_nodes = v->num_bvh_nodes;
-    if (v->num_triangles && v->num_bvh_nodes == 0) {
+    c->num_meshes = 0;
+    c->needs_instances = false;
+    if (meshes) {
+        // One BLAS per mesh now; the TLAS comes with luc_set_instances.
+        LUC_CUDA(c, upload(c->lb_tris, v->triangles, v->num_triangles, s), "upload triangles");
+        int32_t rc = luc_build_blases(c, meshes->first, meshes->count, meshes->n, v->num_triangles, &num_nodes);
+        if (rc) return rc;
+        c->num_meshes = meshes->n;
+        c->blas_nodes = num_nodes;
+        c->inst_capacity = 0;
+        c->needs_instances = true;
+        c->host_prims.assign(v->primitives, v->primitives + np_);
+    } else if (v->num_triangles && v->num_bvh_nodes == 0) {
         // No caller tree: build an LBVH on the device and reorder our copy of
         // the triangles into leaf order (Bvh::compact_primitives).
         LUC_CUDA(c, upload(c->lb_tris, v->triangles, v->num_triangles, s), "upload triangles");
@@ -369,9 +384,31 @@ int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) {
     d.has_env = v->env_width > 0 && v->env_total_weight > 0.0f;  // EnvMap::is_empty
     d.light_strategies = v->num_lights + (d.has_env ? 1u : 0u);
     c->num_materials = v->num_materials;
+    c->total_nodes = num_nodes;
     c->has_scene = true;
     c->scene_version++;
     return LUC_OK;
+}
+
+extern "C" {
+
+int32_t luc_upload_scene(luc_ctx* c, const luc_scene_view* v) { return upload_scene(c, v, nullptr); }
+
+int32_t luc_upload_meshes(luc_ctx* c, const luc_scene_view* v, const uint32_t* mesh_first, const uint32_t* mesh_count,
+                          uint32_t num_meshes) {
+    if (!c || !v || !mesh_first || !mesh_count || num_meshes == 0) return LUC_ERR_VALIDATION;
+    if (v->num_instances || v->num_bvh_nodes)
+        return luc_fail(c, LUC_ERR_VALIDATION, "luc_upload_meshes takes no instances and no tree");
+    if (v->num_triangles == 0) return luc_fail(c, LUC_ERR_VALIDATION, "luc_upload_meshes needs triangles");
+    uint64_t end = 0;
+    for (uint32_t m = 0; m < num_meshes; ++m) {
+        if (mesh_count[m] == 0 || mesh_first[m] < end || (uint64_t)mesh_first[m] + mesh_count[m] > v->num_triangles)
+            return luc_fail(c, LUC_ERR_VALIDATION,
+                            "mesh " + std::to_string(m) + ": ranges must be non-empty, ascending, disjoint and inside the triangles");
+        end = (uint64_t)mesh_first[m] + mesh_count[m];
+    }
+    MeshSpec ms{mesh_first, mesh_count, num_meshes};
+    return upload_scene(c, v, &ms);
 }
 
 static int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth) {
@@ -417,6 +454,7 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     if (!c || !u) return LUC_ERR_VALIDATION;
     cudaSetDevice(c->device);
     if (!c->has_scene) return luc_fail(c, LUC_ERR_VALIDATION, "no scene uploaded");
+    if (c->needs_instances) return luc_fail(c, LUC_ERR_VALIDATION, "meshes uploaded but no instances set (luc_set_instances)");
     if (u->width == 0 || u->height == 0) return luc_fail(c, LUC_ERR_VALIDATION, "zero-sized image");
     if (spp == 0) return luc_fail(c, LUC_ERR_VALIDATION, "spp must be positive");
     if (max_depth == 0 || max_depth > 256) return luc_fail(c, LUC_ERR_VALIDATION, "max_depth must be in 1..=256");

@@ -49,6 +49,16 @@ struct luc_ctx {
     DevBuf materials, prims, lights, positions, attrs, tris, nodes, env_px, env_cond, env_marg, env_row_sin, energy;
     DevBuf tnodes, soup;  // traversal layout derived from nodes / tris
     DevBuf blas_roots;    // distinct BLAS roots of an instanced scene
+    // Meshes uploaded for device-built instancing (luc_upload_meshes): per
+    // mesh its BLAS root node and object-space bounds (6 floats), the BLAS
+    // node total (= the TLAS's first node), the analytic primitives, and the
+    // instance capacity the buffers are sized for.
+    DevBuf mesh_root, mesh_bounds, inst_in, inst_tmp;
+    std::vector<uint32_t> host_mesh_root;
+    std::vector<GpuPrimitive> host_prims;
+    uint32_t blas_nodes = 0, inst_capacity = 0, num_meshes = 0;
+    bool needs_instances = false;
+    uint32_t total_nodes = 0, tlas_nodes = 0;  // nodes as uploaded or built; TLAS nodes of the last luc_set_instances
     luc::DevScene scene{};
     bool has_scene = false;
     uint32_t num_materials = 0;
@@ -72,6 +82,14 @@ struct luc_ctx {
     // Bounds of the uploaded scene (vertices and analytic primitives).
     float scene_lo[3] = {0, 0, 0}, scene_hi[3] = {0, 0, 0};
 };
+
+// Host array -> DevBuf (grown to n elements), asynchronously on stream s.
+template <class T>
+cudaError_t upload(DevBuf& b, const T* src, size_t n, cudaStream_t s) {
+    cudaError_t e = b.ensure(n * sizeof(T));
+    if (e != cudaSuccess || n == 0 || !src) return e;
+    return cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, s);
+}
 
 // Error helpers: record a message and return a LUC_ERR_* code.
 int32_t luc_fail(luc_ctx* c, int32_t code, const std::string& msg);
@@ -98,6 +116,11 @@ int32_t luc_gather_triangles(luc_ctx* c, const GpuTriangle* src, GpuTriangle* ds
 // Implemented in wavefront.cu: derive the traversal layout (child-pair
 // records, triangle soup) from the resident nodes and triangles.
 int32_t luc_build_traversal(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris);
+int32_t luc_build_tnodes_range(luc_ctx* c, uint32_t begin, uint32_t end);
+// Implemented in instances.cu: one LBVH per mesh range of the triangles in
+// lb_tris into c->nodes / c->tris (see luc_upload_meshes).
+int32_t luc_build_blases(luc_ctx* c, const uint32_t* first, const uint32_t* count, uint32_t nm, uint32_t ntris,
+                         uint32_t* blas_nodes);
 // Implemented in guide.cu: the guide's device view and training buffers,
 // and per-frame allocations (mixtures for `paths` paths, records).
 luc::GuideDev luc_guide_dev(const luc_ctx* c);

@@ -474,8 +474,8 @@ __global__ void __launch_bounds__(256) k_resolve(PathState ps, FrameParams fp, G
 
 // Traversal layout (see scene_dev.cuh): child-pair records per internal
 // node and the (p0, e1, e2) triangle soup.
-__global__ void k_make_tnodes(const float4* __restrict__ nodes, uint32_t n, float4* __restrict__ tn) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+__global__ void k_make_tnodes(const float4* __restrict__ nodes, uint32_t begin, uint32_t end, float4* __restrict__ tn) {
+    for (uint32_t i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
         float4 b = nodes[2 * i + 1];
         if (__float_as_uint(b.w) != 0u) continue;  // leaves have no record
         uint32_t c0 = __float_as_uint(nodes[2 * i].w);
@@ -577,9 +577,20 @@ int32_t luc_build_traversal(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris) {
     LUC_CUDA(c, c->soup.ensure((size_t)num_tris * 48), "alloc triangle soup");
     int g1 = (int)std::min<uint64_t>((num_nodes + 255) / 256, (uint64_t)c->num_sms * 32);
     int g2 = (int)std::min<uint64_t>((num_tris + 255) / 256, (uint64_t)c->num_sms * 32);
-    k_make_tnodes<<<g1, 256, 0, c->stream>>>(c->nodes.as<float4>(), num_nodes, c->tnodes.as<float4>());
+    k_make_tnodes<<<g1, 256, 0, c->stream>>>(c->nodes.as<float4>(), 0u, num_nodes, c->tnodes.as<float4>());
     k_make_soup<<<g2, 256, 0, c->stream>>>(c->tris.as<GpuTriangle>(), c->positions.as<float4>(), num_tris,
                                            c->soup.as<float4>());
+    LUC_CUDA(c, cudaGetLastError(), "traversal layout");
+    return LUC_OK;
+}
+
+// Child-pair records for nodes [begin, end) only (a TLAS rebuilt after the
+// BLASes, whose records stay).
+int32_t luc_build_tnodes_range(luc_ctx* c, uint32_t begin, uint32_t end) {
+    using namespace luc;
+    if (end <= begin) return LUC_OK;
+    int g = (int)std::min<uint64_t>((end - begin + 255) / 256, (uint64_t)c->num_sms * 32);
+    k_make_tnodes<<<g, 256, 0, c->stream>>>(c->nodes.as<float4>(), begin, end, c->tnodes.as<float4>());
     LUC_CUDA(c, cudaGetLastError(), "traversal layout");
     return LUC_OK;
 }

@@ -63,6 +63,12 @@ class SceneDef:
     # `bvh_nodes` holds every BLAS followed by the TLAS from `tlas_root` on.
     num_instances: int = 0
     tlas_root: int = 0
+    # Device-built instancing: `meshes` (M, 2) = (first triangle, count) per
+    # mesh of object-space triangles (one LBVH each, luc_upload_meshes) and
+    # `placements` = (object_to_world (N, 3, 4), mesh (N,), material (N,),
+    # 0xFFFFFFFF keeping the triangles' own) for the TLAS (luc_set_instances).
+    meshes: np.ndarray | None = None
+    placements: tuple | None = None
 
     @property
     def env_size(self):
@@ -169,8 +175,37 @@ class Gpu:
             v.env_cdf, v.env_cdf_width = ptr(cdf), cdf.shape[1]
             v.env_total_weight = float(scene.env_total_weight)
         self._scene = None
-        check(self._h, self._lib.luc_upload_scene(self._h, C.byref(v)))
+        if scene.meshes is not None:
+            ms = np.ascontiguousarray(scene.meshes, np.uint32).reshape(-1, 2)
+            first, count = np.ascontiguousarray(ms[:, 0]), np.ascontiguousarray(ms[:, 1])
+            check(self._h, self._lib.luc_upload_meshes(self._h, C.byref(v), ptr(first), ptr(count), len(ms)))
+            if scene.placements is not None:
+                self.set_instances(*scene.placements)
+        else:
+            check(self._h, self._lib.luc_upload_scene(self._h, C.byref(v)))
         self._scene = scene
+
+    def set_instances(self, object_to_world, mesh, material=None):
+        """Place the uploaded meshes (luc_set_instances): rebuilds the TLAS on
+        the device. object_to_world (N, 3, 4) row-major; material None keeps
+        every triangle's own."""
+        m = np.ascontiguousarray(object_to_world, np.float32).reshape(-1, 12)
+        me = np.ascontiguousarray(mesh, np.uint32).reshape(-1)
+        mat = (np.full(len(m), 0xFFFFFFFF, np.uint32) if material is None
+               else np.ascontiguousarray(material, np.uint32).reshape(-1))
+        if not (len(m) == len(me) == len(mat)):
+            raise ValueError("object_to_world, mesh and material must have one entry per instance")
+        check(self._h, self._lib.luc_set_instances(self._h, ptr(m), ptr(me), ptr(mat), len(m)))
+
+    def read_scene(self, which: str) -> np.ndarray:
+        """The resident scene's 'nodes', 'triangles' or 'primitives' (instance
+        rows after the analytic primitives)."""
+        code, dt = {"nodes": (0, L.BVH_NODE), "triangles": (1, L.TRIANGLE), "primitives": (2, L.PRIMITIVE)}[which]
+        n = C.c_uint64(0)
+        check(self._h, self._lib.luc_read_scene(self._h, code, None, 0, C.byref(n)))
+        out = np.zeros(n.value // dt.itemsize, dt)
+        check(self._h, self._lib.luc_read_scene(self._h, code, ptr(out), out.nbytes, C.byref(n)))
+        return out
 
     def stats(self) -> RenderStats:
         s = RenderStats()

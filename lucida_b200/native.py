@@ -97,6 +97,9 @@ _SIGS = {
     "luc_sort_u32_static_max": (C.c_uint32, []),
     "luc_denoise": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(DenoiseParams),
                                 C.c_void_p]),
+    "luc_upload_meshes": (C.c_int32, [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_void_p, C.c_uint32]),
+    "luc_set_instances": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    "luc_read_scene": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
     "luc_guide_init": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     "luc_guide_configure": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
     "luc_guide_get_params": (C.c_int32, [C.c_void_p, C.c_void_p]),

@@ -252,3 +252,87 @@ def guided_room(count: int = 256, level: int = 4, seed: int = 2024, emission: fl
     return SceneDef(materials=mats, primitives=prims, lights=L.quad_lights(mats, prims), positions=base.positions,
                     vertex_attrs=base.vertex_attrs, triangles=base.triangles, bvh_nodes=None, camera=base.camera,
                     name=f"guided-room-l{level}")
+
+
+def _random_rotations(rng, n):
+    """Uniform random rotations (normalised Gaussian quaternions) as (n, 3, 3)."""
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    return np.stack([np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)], -1),
+                     np.stack([2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)], -1),
+                     np.stack([2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)], -1)], 1)
+
+
+def instanced_field(num_meshes: int = 16, tri_range=(50_000, 500_000), num_instances: int = 4096,
+                    extent=(100.0, 10.0, 100.0), seed: int = 5150, level: int = 4, env_size=(1024, 512)) -> SceneDef:
+    """Two-level workload: `num_meshes` base meshes whose triangle counts are
+    log-uniform in `tri_range`, each a cluster of displaced icospheres built
+    with the displaced-spheres recipe (value-noise amplitude 0.05, the same
+    material mix: 40% diffuse, 40% GGX metal, 20% rough glass), placed by
+    `num_instances` seeded affine transforms: uniform random rotation, uniform
+    scale U[0.5, 2], position uniform in an `extent` box (y from 0) above a
+    ground quad. The BLASes are built per mesh on the device and the TLAS by
+    LBVH (scene.meshes / scene.placements); the sky is the procedural one of
+    the displaced-spheres scene.
+    """
+    rng = np.random.default_rng(seed)
+    unit, faces = icosphere_unit(level)
+    nv, nf = len(unit), len(faces)
+    mats = [L.diffuse((0.5, 0.5, 0.5))]  # 0: ground
+    pos_all, nrm_all, tri_all, meshes = [], [], [], []
+    vbase = tbase = 0
+    lo, hi = np.log(tri_range[0]), np.log(tri_range[1])
+    for m in range(num_meshes):
+        target = float(np.exp(rng.uniform(lo, hi)))
+        k = max(1, int(round(target / nf)))
+        kind = rng.uniform()
+        if kind < 0.4:
+            mats.append(L.diffuse(tuple(rng.uniform(0.1, 0.9, 3))))
+        elif kind < 0.8:
+            mats.append(L.metal(tuple(rng.uniform(0.5, 1.0, 3)), rng.uniform(0.05, 0.8)))
+        else:
+            mats.append(L.glass((1.0, 1.0, 1.0), rng.uniform(0.0, 0.3), 1.5))
+        first = tbase
+        spread = 0.6 * k ** (1.0 / 3.0)
+        for s in range(k):
+            r = rng.uniform(0.3, 0.6)
+            c = rng.uniform(-spread, spread, 3)
+            disp = 1.0 + 0.05 * (2.0 * value_noise3(unit, seed * 7919 + m * 1000 + s) - 1.0)
+            p = c + unit * (r * disp)[:, None]
+            pos_all.append(p)
+            nrm_all.append(_vertex_normals(p, faces))
+            t = np.zeros(nf, L.TRIANGLE)
+            t["i0"], t["i1"], t["i2"] = faces[:, 0] + vbase, faces[:, 1] + vbase, faces[:, 2] + vbase
+            t["material"] = len(mats) - 1
+            tri_all.append(t)
+            vbase += nv
+            tbase += nf
+        meshes.append((first, tbase - first))
+    positions = np.zeros((vbase, 4), F32)
+    positions[:, :3] = np.concatenate(pos_all)
+    attrs = np.zeros(vbase, L.VERTEX_ATTR)
+    attrs["normal"] = np.concatenate(nrm_all)
+    rot = _random_rotations(rng, num_instances)
+    scale = rng.uniform(0.5, 2.0, num_instances)
+    xyz = rng.uniform((-extent[0] / 2, 0.0, -extent[2] / 2), (extent[0] / 2, extent[1], extent[2] / 2),
+                      (num_instances, 3))
+    o2w = np.zeros((num_instances, 3, 4), F32)
+    o2w[:, :, :3] = rot * scale[:, None, None]
+    o2w[:, :, 3] = xyz
+    mesh = rng.integers(0, num_meshes, num_instances).astype(np.uint32)
+    material = np.full(num_instances, 0xFFFFFFFF, np.uint32)
+    recolour = rng.uniform(size=num_instances) < 0.1  # every tenth or so: a material override
+    material[recolour] = rng.integers(1, len(mats), int(recolour.sum()))
+    mats = np.array(mats, L.MATERIAL)
+    g = 0.6 * max(extent[0], extent[2])
+    prims = np.array([L.quad((-g, 0, -g), (0, 0, 2 * g), (2 * g, 0, 0), 0)], L.PRIMITIVE)
+    w, h = env_size
+    px, cdf, total = procedural_sky(w, h, (-0.4, 0.55, -0.7), 1.0e4, 0.5) if w > 0 else (None, None, 0.0)
+    return SceneDef(materials=mats, primitives=prims, lights=L.quad_lights(mats, prims), positions=positions,
+                    vertex_attrs=attrs, triangles=np.concatenate(tri_all), bvh_nodes=None,
+                    camera=Camera(eye=(0.0, 0.35 * max(extent) + 5.0, 0.8 * max(extent)), look_at=(0.0, 2.0, 0.0),
+                                  vfov_deg=45.0),
+                    env_pixels=px, env_cdf=cdf, env_total_weight=total,
+                    meshes=np.array(meshes, np.uint32), placements=(o2w, mesh, material),
+                    name=f"instanced-field-{num_meshes}x{num_instances}")

@@ -82,6 +82,7 @@ def lib():
         L.orc_scene_instancing.argtypes = [vp, vp]
         L.orc_scene_set_reference_shadows.argtypes = [vp, i32]
         L.orc_affine_inverse.argtypes = [vp, vp]
+        L.orc_scene_build_instances_lbvh.argtypes = [vp, vp, vp, u32, vp, vp, vp, u32]
         L.orc_pack_instance.argtypes = [vp, u32, u32, vp]
         L.orc_instance_transform.argtypes = [vp, i32, vp, u32, vp]
         L.orc_instance_world_bounds.argtypes = [vp, vp, vp]
@@ -195,7 +196,7 @@ class Scene:
                                       _p(lights_arr), 0 if lights_arr is None else len(lights_arr),
                                       _p(positions), len(positions), _p(vertex_attrs), _p(triangles),
                                       len(triangles), _p(px), w, h, _p(cond), _p(marg), float(total), _p(bg),
-                                      2 if instancing is not None else (1 if bvh == "lbvh" else 0))
+                                      2 if (instancing is not None or bvh == "none") else (1 if bvh == "lbvh" else 0))
         s = cls(hnd)
         if instancing is not None:
             nodes, ni, root = instancing
@@ -210,6 +211,15 @@ class Scene:
         out = np.zeros(3, np.uint32)
         lib().orc_scene_instancing(self._h, _p(out))
         return int(out[0]), int(out[1]), int(out[2])
+
+    def build_instances_lbvh(self, meshes, object_to_world, mesh, material):
+        """The device's luc_upload_meshes + luc_set_instances, restated."""
+        ms = np.ascontiguousarray(meshes, np.uint32).reshape(-1, 2)
+        first, count = np.ascontiguousarray(ms[:, 0]), np.ascontiguousarray(ms[:, 1])
+        m = np.ascontiguousarray(object_to_world, np.float32).reshape(-1, 12)
+        me = np.ascontiguousarray(mesh, np.uint32)
+        mat = np.ascontiguousarray(material, np.uint32)
+        lib().orc_scene_build_instances_lbvh(self._h, _p(first), _p(count), len(ms), _p(m), _p(me), _p(mat), len(m))
 
     def set_reference_shadows(self, on: bool):
         """Shadow rays of an instanced scene as the reference casts them

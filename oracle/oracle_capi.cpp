@@ -80,6 +80,22 @@ void orc_scene_instancing(void* h, uint32_t* out3) {
     out3[1] = (uint32_t)s->primitives.size();
     out3[2] = s->tlas_root;
 }
+// Device-built instancing restated (Scene::build_instances_lbvh): mesh
+// ranges of the scene's (object-space) triangles and placements given by
+// row-major 3x4 object-to-world transforms.
+void orc_scene_build_instances_lbvh(void* h, const uint32_t* first, const uint32_t* count, uint32_t nm,
+                                    const float* o2w, const uint32_t* mesh, const uint32_t* material, uint32_t n) {
+    Scene* s = (Scene*)h;
+    std::vector<std::pair<uint32_t, uint32_t>> ranges;
+    for (uint32_t m = 0; m < nm; ++m) ranges.push_back({first[m], count[m]});
+    std::vector<Scene::Placement> pl(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        std::memcpy(pl[i].object_to_world.m, o2w + 12 * (size_t)i, 48);
+        pl[i].mesh = mesh[i];
+        pl[i].material = material[i];
+    }
+    s->build_instances_lbvh(ranges, pl);
+}
 void orc_scene_set_reference_shadows(void* h, int on) { ((Scene*)h)->reference_instance_shadows = on != 0; }
 
 // Instance maths (instance.rs): affine inverse of a row-major 3x4; pack an

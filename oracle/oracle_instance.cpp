@@ -314,4 +314,48 @@ void Scene::build_instances(const std::vector<std::pair<uint32_t, uint32_t>>& me
     bvh = Bvh();  // the single-level tree stays empty, as in the reference
 }
 
+void Scene::build_instances_lbvh(const std::vector<std::pair<uint32_t, uint32_t>>& mesh_ranges,
+                                 const std::vector<Placement>& placements) {
+    struct BlasInfo {
+        uint32_t node_offset;
+        Aabb bounds;
+    };
+    std::vector<BlasInfo> blas;
+    flat_nodes.clear();
+    for (const auto& r : mesh_ranges) {
+        uint32_t first = r.first, count = r.second;
+        std::vector<GpuTriangle> tris(triangles.begin() + first, triangles.begin() + first + count);
+        Bvh b = lbvh_build(tris, positions, 4).tree;
+        b.compact_primitives(tris);
+        std::copy(tris.begin(), tris.end(), triangles.begin() + first);
+        Aabb bounds;
+        for (const GpuTriangle& t : tris) bounds.grow(triangle_bounds(t, positions.data()));
+        uint32_t node_offset = (uint32_t)flat_nodes.size();
+        for (GpuBvhNode n : b.nodes) {
+            if (n.count == 0) n.left_first += node_offset;
+            else n.left_first += first;
+            flat_nodes.push_back(n);
+        }
+        blas.push_back(BlasInfo{node_offset, bounds});
+    }
+    std::vector<GpuInstance> inst;
+    std::vector<Aabb> world;
+    for (const Placement& p : placements) {
+        GpuInstance g = pack_instance(affine_inverse(p.object_to_world), blas[p.mesh].node_offset, p.material);
+        inst.push_back(g);
+        world.push_back(instance_world_bounds(g, blas[p.mesh].bounds));
+    }
+    Bvh tlas = lbvh_build_over_bounds(world, 4).tree;
+    tlas_root = (uint32_t)flat_nodes.size();
+    const uint32_t prim_base = (uint32_t)primitives.size();
+    for (GpuBvhNode n : tlas.nodes) {
+        if (n.count == 0) n.left_first += tlas_root;
+        else n.left_first += prim_base;
+        flat_nodes.push_back(n);
+    }
+    instances.clear();
+    for (uint32_t i : tlas.prim_indices) instances.push_back(inst[i]);
+    bvh = Bvh();
+}
+
 }  // namespace oracle

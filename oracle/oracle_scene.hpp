@@ -198,6 +198,11 @@ struct Scene {
     // TLAS over the instances' world bounds.
     void build_instances(const std::vector<std::pair<uint32_t, uint32_t>>& mesh_ranges,
                          const std::vector<Placement>& placements);
+    // The device-built variant (no reference counterpart): an LBVH per mesh
+    // range and an LBVH TLAS over the instances' world bounds, flattened the
+    // same way.
+    void build_instances_lbvh(const std::vector<std::pair<uint32_t, uint32_t>>& mesh_ranges,
+                              const std::vector<Placement>& placements);
     // InstanceSet::intersect (instance.rs:342-421) over the flattened arrays.
     bool intersect_instances(const Ray& ray, float tmin, float tmax, TraversalStats& st, TriHit& tri,
                              uint32_t& instance) const;

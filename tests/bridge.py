@@ -35,6 +35,18 @@ def scene_from_oracle(osc: "O.Scene", with_bvh=True) -> SceneDef:
 
 
 def oracle_from_scene(s: SceneDef, bvh="sah") -> "O.Scene":
+    """The oracle scene for a product SceneDef; a device-built instanced
+    scene (meshes + placements) gets the oracle's restatement of the device
+    BLAS/TLAS build."""
+    if s.meshes is not None:
+        osc = _oracle_arrays(s, "none")
+        o2w, mesh, material = s.placements
+        osc.build_instances_lbvh(s.meshes, o2w, mesh, material)
+        return osc
+    return _oracle_arrays(s, bvh)
+
+
+def _oracle_arrays(s: SceneDef, bvh) -> "O.Scene":
     env = None
     w, h = s.env_size
     if w:
