@@ -293,6 +293,14 @@ int32_t luc_guide_mixture(luc_ctx* ctx, const float* raw40, const float* in3, ui
  * writes an Accum-shaped image with samples = 1. Host arrays. */
 int32_t luc_denoise(luc_ctx* ctx, const GpuAccum* accum, uint32_t width, uint32_t height,
                     const luc_denoise_params* params, GpuAccum* out);
+/* The same on device buffers (GpuAccum arrays; out must not alias accum),
+ * queued on the context's stream without synchronising. With
+ * LUC_DENOISE_HALF_GUIDES the edge-stopping guides (normal, depth, albedo)
+ * are kept in FP16 (no reference counterpart): 10 bytes of guide per tap
+ * instead of 20, the colour stays FP32. */
+#define LUC_DENOISE_HALF_GUIDES 0x1u
+int32_t luc_denoise_dev(luc_ctx* ctx, const void* accum_dev, uint32_t width, uint32_t height,
+                        const luc_denoise_params* params, uint32_t flags, void* out_dev);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -128,4 +128,4 @@ luc::GuideTrain luc_guide_train_state(luc_ctx* c);
 int32_t luc_guide_prepare_frame(luc_ctx* c, uint64_t paths);
 // Implemented in denoise.cu.
 int32_t luc_denoise_device(luc_ctx* c, const GpuAccum* accum_dev, uint32_t w, uint32_t h,
-                           const luc_denoise_params* p, GpuAccum* out_dev);
+                           const luc_denoise_params* p, GpuAccum* out_dev, bool half_guides);

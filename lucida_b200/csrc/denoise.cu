@@ -15,17 +15,53 @@
 // A tap reads a float4 of colour+luminance, a float4 of guide and one float,
 // 36 bytes; a 1920x1080 frame's buffers (~72 MB) stay in the 126 MB L2, so a
 // pass costs HBM roughly one read and one write of the colour buffer.
+#include <cuda_fp16.h>
 #include "ctx.cuh"
 
 namespace luc {
+
+// Guide storage: FP32 (float4 normal+depth, float albedo luminance, float4
+// albedo) or, with kHalf, FP16 (8 + 2 + 8 bytes): a tap then reads 16 B of
+// colour plus 10 B of guides instead of 36 B.
+template <bool kHalf>
+struct GuideT;
+template <>
+struct GuideT<false> {
+    using G = float4;
+    using A = float;
+    using C = float4;
+    static __device__ __forceinline__ G pack(float4 v) { return v; }
+    static __device__ __forceinline__ float4 unpack(G v) { return v; }
+    static __device__ __forceinline__ A pack1(float v) { return v; }
+    static __device__ __forceinline__ float unpack1(A v) { return v; }
+};
+template <>
+struct GuideT<true> {
+    using G = uint2;  // four halves
+    using A = __half;
+    using C = uint2;
+    static __device__ __forceinline__ G pack(float4 v) {
+        __half2 a = __floats2half2_rn(v.x, v.y), b = __floats2half2_rn(v.z, v.w);
+        return make_uint2(*reinterpret_cast<uint32_t*>(&a), *reinterpret_cast<uint32_t*>(&b));
+    }
+    static __device__ __forceinline__ float4 unpack(G v) {
+        float2 a = __half22float2(*reinterpret_cast<__half2*>(&v.x)), b = __half22float2(*reinterpret_cast<__half2*>(&v.y));
+        return make_float4(a.x, a.y, b.x, b.y);
+    }
+    static __device__ __forceinline__ A pack1(float v) { return __float2half_rn(v); }
+    static __device__ __forceinline__ float unpack1(A v) { return __half2float(v); }
+};
 
 struct DnParams {
     uint32_t w, h, stride;
     float sigma_normal, sigma_depth, sigma_luminance, sigma_albedo;
 };
 
+template <bool kHalf>
 __global__ void k_dn_prepare(const GpuAccum* __restrict__ acc, uint32_t n, float4* __restrict__ color,
-                             float4* __restrict__ guide, float* __restrict__ alum, float4* __restrict__ albedo) {
+                             typename GuideT<kHalf>::G* __restrict__ guide, typename GuideT<kHalf>::A* __restrict__ alum,
+                             typename GuideT<kHalf>::C* __restrict__ albedo) {
+    using T = GuideT<kHalf>;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const GpuAccum a = acc[i];
         float inv = 1.0f / fmaxf(a.samples, 1.0f);
@@ -33,9 +69,9 @@ __global__ void k_dn_prepare(const GpuAccum* __restrict__ acc, uint32_t n, float
         V3 rad = ld3(a.radiance) * inv / alb;
         color[i] = make_float4(rad.x, rad.y, rad.z, luminance(rad));
         V3 nrm = ld3(a.normal) * inv;
-        guide[i] = make_float4(nrm.x, nrm.y, nrm.z, a.depth * inv);
-        alum[i] = luminance(alb);
-        albedo[i] = make_float4(alb.x, alb.y, alb.z, 0.0f);
+        guide[i] = T::pack(make_float4(nrm.x, nrm.y, nrm.z, a.depth * inv));
+        alum[i] = T::pack1(luminance(alb));
+        albedo[i] = T::pack(make_float4(alb.x, alb.y, alb.z, 0.0f));
     }
 }
 
@@ -61,16 +97,19 @@ __global__ void k_dn_measure(const float4* __restrict__ color, uint32_t w, uint3
 __constant__ float kB3[5] = {1.0f / 16.0f, 1.0f / 4.0f, 3.0f / 8.0f, 1.0f / 4.0f, 1.0f / 16.0f};
 
 // denoise.rs:171-217 / atrous.wgsl atrous_pass
+template <bool kHalf>
 __global__ void __launch_bounds__(256) k_dn_atrous(const float4* __restrict__ cin, float4* __restrict__ cout,
-                                                   const float4* __restrict__ guide, const float* __restrict__ alum,
+                                                   const typename GuideT<kHalf>::G* __restrict__ guide,
+                                                   const typename GuideT<kHalf>::A* __restrict__ alum,
                                                    const float* __restrict__ dev, DnParams p) {
+    using T = GuideT<kHalf>;
     uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= p.w || y >= p.h) return;
     const size_t ci = (size_t)y * p.w + x;
-    const float4 cg = __ldg(guide + ci);
+    const float4 cg = T::unpack(guide[ci]);
     const float4 cc = __ldg(cin + ci);
     const float cl = cc.w;
-    const float ca = fmaxf(__ldg(alum + ci), 1.0e-3f);
+    const float ca = fmaxf(T::unpack1(alum[ci]), 1.0e-3f);
     const float lum_scale = p.sigma_luminance * fmaxf(__ldg(dev + ci), 1.0e-4f);
     const float dscale = p.sigma_depth * fmaxf(fabsf(cg.w), 1.0e-3f);
     const float ascale = p.sigma_albedo * ca;
@@ -84,13 +123,13 @@ __global__ void __launch_bounds__(256) k_dn_atrous(const float4* __restrict__ ci
             int px = (int)x + (kx - 2) * s;
             if (px < 0 || px >= (int)p.w) continue;
             const size_t qi = (size_t)py * p.w + px;
-            const float4 qg = __ldg(guide + qi);
+            const float4 qg = T::unpack(guide[qi]);
             const float4 qc = __ldg(cin + qi);
             float nd = fmaxf(dot(V3{cg.x, cg.y, cg.z}, V3{qg.x, qg.y, qg.z}), 0.0f);
             float w_n = dpow(nd, p.sigma_normal);
             float w_d = dexp(-fabsf(cg.w - qg.w) / dscale);
             float w_l = dexp(-fabsf(cl - qc.w) / lum_scale);
-            float w_a = dexp(-fabsf(ca - __ldg(alum + qi)) / ascale);
+            float w_a = dexp(-fabsf(ca - T::unpack1(alum[qi])) / ascale);
             float wgt = kB3[kx] * kB3[ky] * w_n * w_d * w_l * w_a;
             sum = sum + V3{qc.x, qc.y, qc.z} * wgt;
             wsum = wsum + wgt;
@@ -104,10 +143,13 @@ __global__ void __launch_bounds__(256) k_dn_atrous(const float4* __restrict__ ci
     }
 }
 
-__global__ void k_dn_modulate(const float4* __restrict__ color, const float4* __restrict__ albedo,
-                              const float4* __restrict__ guide, uint32_t n, GpuAccum* __restrict__ out) {
+template <bool kHalf>
+__global__ void k_dn_modulate(const float4* __restrict__ color, const typename GuideT<kHalf>::C* __restrict__ albedo,
+                              const typename GuideT<kHalf>::G* __restrict__ guide, uint32_t n,
+                              GpuAccum* __restrict__ out) {
+    using T = GuideT<kHalf>;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float4 c = color[i], a = albedo[i], g = guide[i];
+        float4 c = color[i], a = T::unpack(albedo[i]), g = T::unpack(guide[i]);
         GpuAccum o;
         o.radiance[0] = c.x * a.x; o.radiance[1] = c.y * a.y; o.radiance[2] = c.z * a.z;
         o.samples = 1.0f;
@@ -125,33 +167,40 @@ __global__ void k_dn_modulate(const float4* __restrict__ color, const float4* __
 
 using namespace luc;
 
-int32_t luc_denoise_device(luc_ctx* c, const GpuAccum* accum, uint32_t w, uint32_t h, const luc_denoise_params* p,
+template <bool kHalf>
+static int32_t denoise_run(luc_ctx* c, const GpuAccum* accum, uint32_t w, uint32_t h, const luc_denoise_params* p,
                            GpuAccum* out) {
+    using T = GuideT<kHalf>;
     const size_t n = (size_t)w * h;
     cudaStream_t s = c->stream;
-    LUC_CUDA(c, c->dn_a.ensure(n * 16 * 2), "alloc denoise");  // colour ping + albedo
-    LUC_CUDA(c, c->dn_b.ensure(n * 16 * 2), "alloc denoise");  // colour pong + guide
-    LUC_CUDA(c, c->dn_dev.ensure(n * 4 * 2), "alloc denoise");  // deviation + albedo luminance
+    LUC_CUDA(c, c->dn_a.ensure(n * 16 * 2), "alloc denoise");  // colour ping + pong (FP32)
+    LUC_CUDA(c, c->dn_b.ensure(n * (sizeof(typename T::G) + sizeof(typename T::C))), "alloc denoise");  // guide, albedo
+    LUC_CUDA(c, c->dn_dev.ensure(n * (4 + sizeof(typename T::A)) + 16), "alloc denoise");  // deviation, albedo lum
     float4* ca = c->dn_a.as<float4>();
-    float4* albedo = ca + n;
-    float4* cb = c->dn_b.as<float4>();
-    float4* guide = cb + n;
+    float4* cb = ca + n;
+    typename T::G* guide = c->dn_b.as<typename T::G>();
+    typename T::C* albedo = reinterpret_cast<typename T::C*>(guide + n);
     float* dev = c->dn_dev.as<float>();
-    float* alum = dev + n;
+    typename T::A* alum = reinterpret_cast<typename T::A*>(dev + n);
     int grid1 = (int)std::min<size_t>((n + 255) / 256, (size_t)c->num_sms * 16);
     dim3 blk(16, 16), grid2((w + 15) / 16, (h + 15) / 16);
-    k_dn_prepare<<<grid1, 256, 0, s>>>(accum, (uint32_t)n, ca, guide, alum, albedo);
+    k_dn_prepare<kHalf><<<grid1, 256, 0, s>>>(accum, (uint32_t)n, ca, guide, alum, albedo);
     k_dn_measure<<<grid2, blk, 0, s>>>(ca, w, h, dev);
     DnParams dp{w, h, 1, p->sigma_normal, p->sigma_depth, p->sigma_luminance, p->sigma_albedo};
     float4 *cur = ca, *nxt = cb;
     for (uint32_t level = 0; level < p->iterations; ++level) {
         dp.stride = 1u << level;
-        k_dn_atrous<<<grid2, blk, 0, s>>>(cur, nxt, guide, alum, dev, dp);
+        k_dn_atrous<kHalf><<<grid2, blk, 0, s>>>(cur, nxt, guide, alum, dev, dp);
         std::swap(cur, nxt);
     }
-    k_dn_modulate<<<grid1, 256, 0, s>>>(cur, albedo, guide, (uint32_t)n, out);
+    k_dn_modulate<kHalf><<<grid1, 256, 0, s>>>(cur, albedo, guide, (uint32_t)n, out);
     LUC_CUDA(c, cudaGetLastError(), "denoise");
     return LUC_OK;
+}
+
+int32_t luc_denoise_device(luc_ctx* c, const GpuAccum* accum, uint32_t w, uint32_t h, const luc_denoise_params* p,
+                           GpuAccum* out, bool half_guides) {
+    return half_guides ? denoise_run<true>(c, accum, w, h, p, out) : denoise_run<false>(c, accum, w, h, p, out);
 }
 
 extern "C" int32_t luc_denoise(luc_ctx* c, const GpuAccum* accum, uint32_t w, uint32_t h,
@@ -165,9 +214,23 @@ extern "C" int32_t luc_denoise(luc_ctx* c, const GpuAccum* accum, uint32_t w, ui
     LUC_CUDA(c, c->dn_in.ensure(n * sizeof(GpuAccum)), "alloc denoise");
     LUC_CUDA(c, c->dn_out.ensure(n * sizeof(GpuAccum)), "alloc denoise");
     LUC_CUDA(c, cudaMemcpyAsync(c->dn_in.p, accum, n * sizeof(GpuAccum), cudaMemcpyHostToDevice, s), "upload");
-    int32_t rc = luc_denoise_device(c, c->dn_in.as<GpuAccum>(), w, h, p, c->dn_out.as<GpuAccum>());
+    int32_t rc = luc_denoise_device(c, c->dn_in.as<GpuAccum>(), w, h, p, c->dn_out.as<GpuAccum>(), false);
     if (rc) return rc;
     LUC_CUDA(c, cudaMemcpyAsync(out, c->dn_out.p, n * sizeof(GpuAccum), cudaMemcpyDeviceToHost, s), "readback");
     LUC_CUDA(c, cudaStreamSynchronize(s), "denoise");
     return LUC_OK;
+}
+
+// Device buffers in and out, on the context's stream (not synchronised);
+// flags bit 0 keeps the guides in FP16.
+extern "C" int32_t luc_denoise_dev(luc_ctx* c, const void* accum_dev, uint32_t w, uint32_t h,
+                                   const luc_denoise_params* p, uint32_t flags, void* out_dev) {
+    if (!c || !accum_dev || !out_dev || !p) return LUC_ERR_VALIDATION;
+    if (w == 0 || h == 0) return luc_fail(c, LUC_ERR_VALIDATION, "zero-sized image");
+    if (p->iterations > 16) return luc_fail(c, LUC_ERR_VALIDATION, "at most 16 a-trous iterations");
+    if (flags & ~LUC_DENOISE_HALF_GUIDES) return luc_fail(c, LUC_ERR_VALIDATION, "unknown denoise flag");
+    if (accum_dev == out_dev) return luc_fail(c, LUC_ERR_VALIDATION, "the output must not alias the accumulator");
+    cudaSetDevice(c->device);
+    return luc_denoise_device(c, (const GpuAccum*)accum_dev, w, h, p, (GpuAccum*)out_dev,
+                              (flags & LUC_DENOISE_HALF_GUIDES) != 0);
 }

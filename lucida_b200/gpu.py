@@ -137,7 +137,12 @@ class Gpu:
             pass
 
     def set_stream(self, stream_handle: int | None):
-        check(self._h, self._lib.luc_set_stream(self._h, C.c_void_p(stream_handle or 0)))
+        """Run on a caller's cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream).
+        None returns to the context's own stream; 0, the legacy default
+        stream's handle in torch, is passed as cudaStreamLegacy so the
+        library's work stays ordered with torch's default-stream work."""
+        handle = None if stream_handle is None else (stream_handle if stream_handle != 0 else 1)
+        check(self._h, self._lib.luc_set_stream(self._h, C.c_void_p(handle)))
 
     def upload(self, scene: SceneDef, force: bool = False):
         """Make `scene` resident. A SceneDef already resident is not sent

@@ -21,6 +21,7 @@ LUC_FLAG_NO_GUIDES = 0x100
 LUC_FLAG_PROFILE = 0x200
 LUC_FLAG_GUIDED = 0x400
 LUC_FLAG_REFERENCE_SHADOWS = 0x800
+LUC_DENOISE_HALF_GUIDES = 0x1
 
 
 class GpuError(RuntimeError):
@@ -97,6 +98,8 @@ _SIGS = {
     "luc_sort_u32_static_max": (C.c_uint32, []),
     "luc_denoise": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(DenoiseParams),
                                 C.c_void_p]),
+    "luc_denoise_dev": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(DenoiseParams),
+                                    C.c_uint32, C.c_void_p]),
     "luc_upload_meshes": (C.c_int32, [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_void_p, C.c_uint32]),
     "luc_set_instances": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
     "luc_read_scene": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),

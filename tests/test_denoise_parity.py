@@ -64,3 +64,35 @@ def test_accumulator_untouched_and_noise_reduced(gpu):
     err_noisy = np.median(np.abs(noisy - truth))
     err_dn = np.median(np.abs(out["radiance"] - truth))
     assert err_dn < err_noisy, (err_dn, err_noisy)
+
+
+@pytest.mark.parametrize("iterations,sn,sd,sl", [(5, 128.0, 1.0, 4.0), (4, 64.0, 0.08, 4.0)])
+def test_half_precision_guides(gpu, iterations, sn, sd, sl):
+    """luc_denoise_dev on device buffers: FP32 guides give exactly the host
+    entry point's image; FP16 guides stay within the reference's own
+    GPU-vs-CPU agreement bound (mean relative error < 4e-3) of the oracle."""
+    import ctypes as C
+    import torch
+    from lucida_b200.native import DenoiseParams as DP, LUC_DENOISE_HALF_GUIDES, check, lib
+    s = scenes.cornell_analytic()
+    w, h = 96, 80
+    acc = lb.render_accum(gpu, s, lb.RenderParams(width=w, height=h, samples=4, max_depth=6))
+    dp = lb.DenoiseParams(iterations, sn, sd, sl, 0.1)
+    host = lb.Denoiser(gpu).run(acc, dp).reshape(-1)
+    d_in = torch.from_numpy(np.ascontiguousarray(acc).view(np.uint8).reshape(-1).copy()).cuda()
+    d_out = torch.zeros_like(d_in)
+    p = DP(iterations, sn, sd, sl, 0.1)
+    outs = {}
+    for flags in (0, LUC_DENOISE_HALF_GUIDES):
+        torch.cuda.synchronize()
+        check(gpu.handle, lib().luc_denoise_dev(gpu.handle, C.c_void_p(d_in.data_ptr()), w, h, C.byref(p), flags,
+                                                C.c_void_p(d_out.data_ptr())))
+        torch.cuda.synchronize()
+        outs[flags] = d_out.cpu().numpy().view(L.ACCUM)
+    assert outs[0].tobytes() == host.tobytes()
+    film, alb, nrm, dep = _oracle_inputs(acc)
+    ref = O.denoise(film, alb, nrm, dep, w, h, iterations, sn, sd, sl, 0.1)
+    st = compare(outs[LUC_DENOISE_HALF_GUIDES]["radiance"], ref)
+    print("fp16 guides vs oracle", st)
+    assert st["mean_rel"] < 4e-3, st
+    assert d_in.cpu().numpy().tobytes() == np.ascontiguousarray(acc).view(np.uint8).reshape(-1).tobytes()
