@@ -244,6 +244,40 @@ int32_t luc_set_instances(luc_ctx* ctx, const float* object_to_world, const uint
  * to query it. */
 int32_t luc_read_scene(luc_ctx* ctx, uint32_t which, void* out, uint64_t capacity, uint64_t* bytes);
 
+/* ---- Batched multi-scene rendering (no reference counterpart) ----
+ * Renders many jobs (a resident scene, its uniforms, spp, bounces and a
+ * device accumulator each) through one shared path pool: the pool is filled
+ * in waves of whole samples taken from the jobs in order, paths of different
+ * scenes share the ray and hit queues and find their scene through their
+ * wave segment, and the whole batch is recorded as one CUDA graph. Each
+ * job's scene is the resident scene of its own context (luc_upload_scene on
+ * the same device; single-level scenes); the batch runs on `ctx`'s stream
+ * and pool. Accumulators are accumulated into, as luc_render does. */
+typedef struct luc_batch_job {
+    luc_ctx* scene;       /* context holding the scene */
+    GpuUniforms uniforms; /* camera, size, seed, sampler, sampling */
+    uint32_t spp, max_depth;
+    void* accum_dev;      /* width * height GpuAccum on the device */
+} luc_batch_job;
+/* Launch shape of the traversal stages: threads per block (64, 128, 256)
+ * and the queue entries a block claims per pull (32 = one warp at a time,
+ * else 1024, 4096 or 16384 per block). */
+typedef struct luc_batch_config {
+    uint32_t block, chunk;
+} luc_batch_config;
+int32_t luc_batch_configure(luc_ctx* ctx, const luc_batch_config* cfg);
+/* job_done_ms (num_jobs entries, may be null): device time from the batch's
+ * start until the wave that finished the job; stats may be null. */
+int32_t luc_render_batch(luc_ctx* ctx, const luc_batch_job* jobs, uint32_t num_jobs, double* job_done_ms,
+                         luc_render_stats* stats);
+/* Time every launch shape on the batch's first `waves` waves (rendering into
+ * scratch accumulators, the jobs' own are untouched), keep the fastest as
+ * the context's configuration and return it. tried (may be null) receives,
+ * per tried shape, {block, chunk, ms} as 3 doubles, in the order block in
+ * {64, 128, 256} x chunk in {32, 1024, 4096, 16384}. */
+int32_t luc_batch_autotune(luc_ctx* ctx, const luc_batch_job* jobs, uint32_t num_jobs, uint32_t waves,
+                           luc_batch_config* best, double* tried);
+
 /* ---- Learned path-guiding proposal (no reference counterpart) ----
  * Model: frequency-encoded position (12 frequencies per axis over the guide's
  * box), shading normal and outgoing direction (4 each), 120 features padded to

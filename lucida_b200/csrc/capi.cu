@@ -411,14 +411,16 @@ int32_t luc_upload_meshes(luc_ctx* c, const luc_scene_view* v, const uint32_t* m
     return upload_scene(c, v, &ms);
 }
 
-static int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth) {
+}  // extern "C"
+
+int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth) {
     RenderState& rs = c->rs;
     uint32_t ctrs = kCtrStride * (max_depth + 2);
     if (paths <= rs.capacity && ctrs <= rs.ctr_capacity) return LUC_OK;
     paths = std::max(paths, rs.capacity);
     ctrs = std::max(ctrs, rs.ctr_capacity);
     const size_t f4 = sizeof(float4);
-    size_t bytes = paths * (11 * f4 + 3 * sizeof(uint32_t)) + ctrs * sizeof(uint32_t) + 16 * 256;
+    size_t bytes = paths * (11 * f4 + 4 * sizeof(uint32_t)) + ctrs * sizeof(uint32_t) + 16 * 256;
     LUC_CUDA(c, c->pool.ensure(bytes), "allocate path pool");
     char* p = (char*)c->pool.p;
     auto take = [&](size_t n) {
@@ -441,6 +443,7 @@ static int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth) {
     ps.queue[0] = (uint32_t*)take(paths * 4);
     ps.queue[1] = (uint32_t*)take(paths * 4);
     ps.hinst = (uint32_t*)take(paths * 4);
+    ps.seg = (uint32_t*)take(paths * 4);
     ps.ctr = (uint32_t*)take(ctrs * 4);
     ps.stat = (unsigned long long*)take(8 * sizeof(unsigned long long));
     if ((size_t)(p - (char*)c->pool.p) > c->pool.bytes) return luc_fail(c, LUC_ERR_VALIDATION, "path pool carve");
@@ -448,6 +451,8 @@ static int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth) {
     rs.ctr_capacity = ctrs;
     return LUC_OK;
 }
+
+extern "C" {
 
 int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_depth, uint32_t flags,
                    GpuAccum* out_host, void* out_dev) {

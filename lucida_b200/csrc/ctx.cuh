@@ -58,7 +58,10 @@ struct luc_ctx {
     std::vector<GpuPrimitive> host_prims;
     uint32_t blas_nodes = 0, inst_capacity = 0, num_meshes = 0;
     bool needs_instances = false;
-    uint32_t total_nodes = 0, tlas_nodes = 0;  // nodes as uploaded or built; TLAS nodes of the last luc_set_instances
+    uint32_t total_nodes = 0, tlas_nodes = 0;
+    // Batched renders: launch shape, and the device tables of the last batch.
+    uint32_t batch_block = 128, batch_chunk = 32;
+    DevBuf b_scenes, b_jobs, b_segs, b_pixoff, b_scratch;  // nodes as uploaded or built; TLAS nodes of the last luc_set_instances
     luc::DevScene scene{};
     bool has_scene = false;
     uint32_t num_materials = 0;
@@ -126,6 +129,8 @@ int32_t luc_build_blases(luc_ctx* c, const uint32_t* first, const uint32_t* coun
 luc::GuideDev luc_guide_dev(const luc_ctx* c);
 luc::GuideTrain luc_guide_train_state(luc_ctx* c);
 int32_t luc_guide_prepare_frame(luc_ctx* c, uint64_t paths);
+// capi.cu: grow the path pool to `paths` paths and `max_depth` bounces.
+int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth);
 // Implemented in denoise.cu.
 int32_t luc_denoise_device(luc_ctx* c, const GpuAccum* accum_dev, uint32_t w, uint32_t h,
                            const luc_denoise_params* p, GpuAccum* out_dev, bool half_guides);

@@ -40,6 +40,7 @@ struct PathState {
     // bookkeeping words.
     float4* lobes;
     uint64_t lobe_stride;
+    uint32_t* seg;  // batched renders: the wave segment each path belongs to
     float4* rec;
     uint32_t* gmisc;
 };
@@ -107,6 +108,27 @@ struct RenderState {
 };
 
 void query_occupancy(RenderState& rs);
+// Batched multi-scene renders (luc_render_batch). A job is one render of
+// one resident scene; the pool is filled in waves, each a list of segments:
+// `nsamples` whole samples (every pixel) of one job, `count` = nsamples *
+// pixels paths starting at `first` in the wave. Stage kernels find a path's
+// scene and frame parameters through its segment.
+struct BatchJobDev {
+    FrameParams fp;  // per job: size, camera, sampler, sampling, max_depth, seed
+    uint32_t scene;
+    GpuAccum* accum;
+};
+struct BatchSegDev {
+    uint32_t first, count, job, sample_base, nsamples, scene;
+};
+struct BatchDev {
+    const DevScene* scenes;
+    const BatchJobDev* jobs;
+    const BatchSegDev* segs;  // this wave's segments
+    uint32_t num_segs;
+    uint32_t chunk;           // queue entries a CTA claims per pull (EXTEND / CONNECT)
+};
+
 // Guide training buffers (FP32 master weights, Adam moments, gradient) and
 // the packed copies the kernels read.
 struct GuideTrain {
@@ -119,6 +141,11 @@ struct GuideTrain {
 
 void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream,
                   StageTimer* timer, const GuideTrain* gt);
+// One wave of a batched render (wavefront.cu); `block` is the EXTEND /
+// CONNECT block size (64, 128 or 256).
+void record_wave(RenderState& rs, const BatchDev& bd, const uint32_t* pix_off, uint32_t num_paths,
+                 uint32_t total_pixels, uint32_t max_depth, int block, cudaStream_t s);
+int batch_blocks_per_sm(int block, bool connect);
 // guide.cu: per-depth inference and the post-batch training step.
 void launch_guide_infer(const RenderState& rs, const DevScene& sc, const FrameParams& fp, uint32_t depth,
                         cudaStream_t s);

@@ -41,74 +41,117 @@ __device__ __forceinline__ void flush_counts(unsigned long long* stat, uint32_t 
 __device__ __forceinline__ V3 xyz(float4 a) { return V3{a.x, a.y, a.z}; }
 
 // GENERATE (shaders/wavefront/generate.wgsl:35-88; camera.rs:373-405).
+// Camera ray and sampler state of path p: pixel `pixel`, sample `sample`.
+__device__ __forceinline__ void generate_one(PathState& ps, const FrameParams& fp, uint64_t p, uint32_t pixel,
+                                             uint32_t sample) {
+    uint32_t x = pixel % fp.width, y = pixel / fp.width;
+    Sampler smp = make_sampler(fp.sampler_kind, fp.frame_seed, pixel, sample);
+    float pu, pv, lu, lv;
+    smp.next_vec2(pu, pv);
+    smp.next_vec2(lu, lv);
+    float s = ((float)x + pu) / (float)fp.width;
+    float t = ((float)y + pv) / (float)fp.height;
+    V3 origin = fp.cam_origin;
+    V3 target = fp.cam_upper_left + s * fp.cam_horizontal + t * fp.cam_vertical;
+    V3 dir;
+    if (fp.lens_radius <= 0.0f) {
+        dir = normalize(target - origin);
+    } else {
+        float dx, dy;
+        concentric_disk(lu, lv, dx, dy);
+        dx = dx * fp.lens_radius;
+        dy = dy * fp.lens_radius;
+        V3 right = normalize(fp.cam_horizontal), down = normalize(fp.cam_vertical);
+        origin = origin + (right * dx + down * dy);
+        dir = normalize(target - origin);
+    }
+    store4(ps.o_pdf + p, origin, 0.0f);
+    store4(ps.dir + p, dir, 0.0f);
+    ps.thr[p] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(smp.state));
+    ps.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    store4(ps.prev + p, origin, 0.0f);
+    if (fp.guides) {
+        ps.galb[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        ps.gnrm[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
 __global__ void __launch_bounds__(256) k_generate(PathState ps, FrameParams fp) {
     const uint64_t n = fp.num_paths;
     const uint32_t sbase = *fp.sbase;
-    for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t pixel = (uint32_t)(p % fp.pixels);
-        uint32_t sample = sbase + (uint32_t)(p / fp.pixels);
-        uint32_t x = pixel % fp.width, y = pixel / fp.width;
-        Sampler smp = make_sampler(fp.sampler_kind, fp.frame_seed, pixel, sample);
-        float pu, pv, lu, lv;
-        smp.next_vec2(pu, pv);
-        smp.next_vec2(lu, lv);
-        float s = ((float)x + pu) / (float)fp.width;
-        float t = ((float)y + pv) / (float)fp.height;
-        V3 origin = fp.cam_origin;
-        V3 target = fp.cam_upper_left + s * fp.cam_horizontal + t * fp.cam_vertical;
-        V3 dir;
-        if (fp.lens_radius <= 0.0f) {
-            dir = normalize(target - origin);
-        } else {
-            float dx, dy;
-            concentric_disk(lu, lv, dx, dy);
-            dx = dx * fp.lens_radius;
-            dy = dy * fp.lens_radius;
-            V3 right = normalize(fp.cam_horizontal), down = normalize(fp.cam_vertical);
-            origin = origin + (right * dx + down * dy);
-            dir = normalize(target - origin);
-        }
-        store4(ps.o_pdf + p, origin, 0.0f);
-        store4(ps.dir + p, dir, 0.0f);
-        ps.thr[p] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(smp.state));
-        ps.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        store4(ps.prev + p, origin, 0.0f);
-        if (fp.guides) {
-            ps.galb[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            ps.gnrm[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
+    for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x)
+        generate_one(ps, fp, p, (uint32_t)(p % fp.pixels), sbase + (uint32_t)(p / fp.pixels));
+}
+
+// The last segment whose first path is <= p (segments sorted by `first`).
+__device__ __forceinline__ uint32_t find_segment(const BatchDev& bd, uint32_t p) {
+    uint32_t lo = 0, hi = bd.num_segs;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (bd.segs[mid].first <= p) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// GENERATE of a batched wave: every path learns its segment (job, sample).
+__global__ void __launch_bounds__(256) k_generate_batch(PathState ps, BatchDev bd, uint32_t num_paths) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < num_paths; p += gridDim.x * blockDim.x) {
+        const uint32_t s = find_segment(bd, p);
+        const BatchSegDev sg = bd.segs[s];
+        const FrameParams& fp = bd.jobs[sg.job].fp;
+        const uint32_t q = p - sg.first;
+        ps.seg[p] = s;
+        generate_one(ps, fp, p, q % fp.pixels, sg.sample_base + q / fp.pixels);
     }
 }
 
 // EXTEND (shaders/wavefront/extend.wgsl:35-68): closest hit per queued path.
 // Persistent ray pull: each warp claims 32 queue entries at a time from the
 // depth's cursor until the queue is drained, so fast warps keep taking work
-// instead of idling behind slow ones.
-template <bool kInst>
-__global__ void __launch_bounds__(128) k_extend(PathState ps, DevScene sc, FrameParams fp, uint32_t depth) {
+// instead of idling behind slow ones; with bd.chunk > 32 (batched renders,
+// chosen by the autotuner) a whole CTA claims `chunk` entries per pull.
+// kBatch: each ray's scene comes from its path's wave segment.
+template <bool kInst, bool kBatch, int kThreads>
+__global__ void __launch_bounds__(kThreads) k_extend(PathState ps, const __grid_constant__ DevScene sc_arg, FrameParams fp,
+                                                     BatchDev bd, uint32_t depth) {
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
     const uint32_t* queue = ps.queue[depth & 1];
     uint32_t* pull = ps.ctr + depth * kCtrStride + kCtrPullExtend;
     const uint32_t lane = threadIdx.x & 31u;
     TravCount tc;
     uint32_t rays = 0;
-    for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(pull, 32u);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= len) break;
-        const uint32_t i = base + lane;
-        if (i < len) {
-            uint32_t p = depth == 0 ? i : queue[i];
-            float4 o4 = ps.o_pdf[p], d4 = ps.dir[p];
-            float t, u, v;
-            uint32_t inst;
-            uint32_t id = closest_hit<kInst>(sc, xyz(o4), xyz(d4), t, u, v, inst, tc);
-            ps.hit[p] = make_float4(t, u, v, __uint_as_float(id));
-            if (kInst) ps.hinst[p] = inst;
-            ++rays;
+    auto trace = [&](uint32_t i) {
+        uint32_t p = depth == 0 ? i : queue[i];
+        float4 o4 = ps.o_pdf[p], d4 = ps.dir[p];
+        const DevScene& sc = kBatch ? bd.scenes[bd.segs[ps.seg[p]].scene] : sc_arg;
+        float t, u, v;
+        uint32_t inst;
+        uint32_t id = closest_hit<kInst>(sc, xyz(o4), xyz(d4), t, u, v, inst, tc);
+        ps.hit[p] = make_float4(t, u, v, __uint_as_float(id));
+        if (kInst) ps.hinst[p] = inst;
+        ++rays;
+    };
+    if (kBatch && bd.chunk > 32u) {
+        __shared__ uint32_t cta_base;
+        for (;;) {
+            if (threadIdx.x == 0) cta_base = atomicAdd(pull, bd.chunk);
+            __syncthreads();
+            const uint32_t cb = cta_base;
+            __syncthreads();
+            if (cb >= len) break;
+            const uint32_t end = min(cb + bd.chunk, len);
+            for (uint32_t i = cb + threadIdx.x; i < end; i += kThreads) trace(i);
         }
-        __syncwarp();
+    } else {
+        for (;;) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(pull, 32u);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (base >= len) break;
+            if (base + lane < len) trace(base + lane);
+            __syncwarp();
+        }
     }
     flush_counts(ps.stat, rays, tc);
 }
@@ -134,16 +177,20 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
 // the choice), with p = 0.5 p_bsdf + 0.5 p_guide as the path's sampling pdf in
 // both MIS sites (emission hit and NEE); plus training records for a
 // threshold-selected subset of those vertices.
-template <bool kGuided, bool kInst>
-__global__ void __launch_bounds__(128, 4) k_shade(PathState ps, DevScene sc, FrameParams fp, uint32_t depth) {
-    const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
+//
+// kBatch: the path's scene and frame parameters come from its wave segment
+// (luc_render_batch) instead of the kernel arguments.
+template <bool kGuided, bool kInst, bool kBatch = false>
+__global__ void __launch_bounds__(128, 4) k_shade(PathState ps, const __grid_constant__ DevScene sc_arg,
+                                                  const __grid_constant__ FrameParams fp_arg, BatchDev bd,
+                                                  uint32_t depth) {
+    const uint32_t len = depth == 0 ? (uint32_t)fp_arg.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
     const uint32_t rec_threshold = kGuided ? ps.gmisc[kGmThreshold] : 65536u;
-    const uint32_t sbase = *fp.sbase;
+    const uint32_t sbase_arg = kBatch ? 0u : *fp_arg.sbase;
     const uint32_t* queue = ps.queue[depth & 1];
     uint32_t* next_queue = ps.queue[(depth + 1) & 1];
     uint32_t* next_len = ps.ctr + (depth + 1) * kCtrStride + kCtrQueue;
     uint32_t* shadow_len = ps.ctr + depth * kCtrStride + kCtrShadow;
-    const bool last = depth + 1 >= fp.max_depth;
     const uint32_t stride = gridDim.x * blockDim.x;
     // Warp-uniform trip count so the ballots below see every lane.
     const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;
@@ -156,15 +203,22 @@ __global__ void __launch_bounds__(128, 4) k_shade(PathState ps, DevScene sc, Fra
         float sh_t = 0.0f;
         if (active) {
             p = depth == 0 ? i : queue[i];
+            const BatchSegDev* seg = kBatch ? bd.segs + ps.seg[p] : nullptr;
+            const BatchJobDev* job = kBatch ? bd.jobs + seg->job : nullptr;
+            const DevScene& sc = kBatch ? bd.scenes[job->scene] : sc_arg;
+            const FrameParams& fp = kBatch ? job->fp : fp_arg;
+            const uint32_t sbase = kBatch ? seg->sample_base : sbase_arg;
+            const uint32_t q = kBatch ? p - seg->first : p;  // path index within its own frame
+            const bool last = depth + 1 >= fp.max_depth;
             float4 o4 = ps.o_pdf[p], d4 = ps.dir[p], h4 = ps.hit[p], t4 = ps.thr[p], r4 = ps.rad[p];
             V3 dir = xyz(d4), thr = xyz(t4), rad = xyz(r4);
             float prev_pdf = o4.w;
             uint32_t id = __float_as_uint(h4.w);
-            uint32_t pixel = (uint32_t)(p % fp.pixels);
+            uint32_t pixel = (uint32_t)(q % fp.pixels);
             Sampler smp;
             smp.kind = fp.sampler_kind;
             smp.state = __float_as_uint(t4.w);
-            smp.index = sbase + (uint32_t)(p / fp.pixels);
+            smp.index = sbase + (uint32_t)(q / fp.pixels);
             smp.seed = sobol_pixel_seed(pixel, fp.frame_seed);
             bool rad_changed = false;
             if (kGuided) {
@@ -416,29 +470,44 @@ __global__ void __launch_bounds__(128, 4) k_shade(PathState ps, DevScene sc, Fra
 
 // CONNECT (shaders/wavefront/connect.wgsl:58-84): any-hit shadow rays, with
 // the same persistent ray pull as EXTEND.
-template <bool kInst>
-__global__ void __launch_bounds__(128) k_connect(PathState ps, DevScene sc, uint32_t depth) {
+template <bool kInst, bool kBatch, int kThreads>
+__global__ void __launch_bounds__(kThreads) k_connect(PathState ps, const __grid_constant__ DevScene sc_arg, BatchDev bd,
+                                                      uint32_t depth) {
     const uint32_t len = ps.ctr[depth * kCtrStride + kCtrShadow];
     uint32_t* pull = ps.ctr + depth * kCtrStride + kCtrPullConnect;
     const uint32_t lane = threadIdx.x & 31u;
     TravCount tc;
     uint32_t rays = 0;
-    for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(pull, 32u);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= len) break;
-        const uint32_t i = base + lane;
-        if (i < len) {
-            float4 o4 = ps.sh_o[i], d4 = ps.sh_d[i];
-            if (!occluded<kInst>(sc, xyz(o4), xyz(d4), o4.w, tc)) {
-                uint32_t p = __float_as_uint(d4.w);
-                float4 c4 = ps.sh_c[i], r4 = ps.rad[p];
-                ps.rad[p] = make_float4(r4.x + c4.x, r4.y + c4.y, r4.z + c4.z, 0.0f);
-            }
-            ++rays;
+    auto trace = [&](uint32_t i) {
+        float4 o4 = ps.sh_o[i], d4 = ps.sh_d[i];
+        uint32_t p = __float_as_uint(d4.w);
+        const DevScene& sc = kBatch ? bd.scenes[bd.segs[ps.seg[p]].scene] : sc_arg;
+        if (!occluded<kInst>(sc, xyz(o4), xyz(d4), o4.w, tc)) {
+            float4 c4 = ps.sh_c[i], r4 = ps.rad[p];
+            ps.rad[p] = make_float4(r4.x + c4.x, r4.y + c4.y, r4.z + c4.z, 0.0f);
         }
-        __syncwarp();
+        ++rays;
+    };
+    if (kBatch && bd.chunk > 32u) {
+        __shared__ uint32_t cta_base;
+        for (;;) {
+            if (threadIdx.x == 0) cta_base = atomicAdd(pull, bd.chunk);
+            __syncthreads();
+            const uint32_t cb = cta_base;
+            __syncthreads();
+            if (cb >= len) break;
+            const uint32_t end = min(cb + bd.chunk, len);
+            for (uint32_t i = cb + threadIdx.x; i < end; i += kThreads) trace(i);
+        }
+    } else {
+        for (;;) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(pull, 32u);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (base >= len) break;
+            if (base + lane < len) trace(base + lane);
+            __syncwarp();
+        }
     }
     flush_counts(ps.stat + 3, rays, tc);
 }
@@ -469,6 +538,46 @@ __global__ void __launch_bounds__(256) k_resolve(PathState ps, FrameParams fp, G
         a.depth = dep;
         a.samples = a.samples + (float)fp.batch_samples;
         accum[px] = a;
+    }
+}
+
+// RESOLVE of a batched wave: per (segment, pixel), the segment's samples in
+// sample order onto its job's accumulator. Threads walk the wave's pixels
+// segment after segment (pixel offsets are prefix sums over segments).
+__global__ void __launch_bounds__(256) k_resolve_batch(PathState ps, BatchDev bd, const uint32_t* __restrict__ pix_off,
+                                                       uint32_t total_pixels) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total_pixels; t += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = bd.num_segs;
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (pix_off[mid] <= t) lo = mid;
+            else hi = mid;
+        }
+        const BatchSegDev sg = bd.segs[lo];
+        const BatchJobDev& job = bd.jobs[sg.job];
+        const uint32_t px = t - pix_off[lo], pixels = job.fp.pixels;
+        GpuAccum a = job.accum[px];
+        V3 r = ld3(a.radiance), r2 = ld3(a.radiance_sq), al = ld3(a.albedo), nn = ld3(a.normal);
+        float dep = a.depth;
+        for (uint32_t j = 0; j < sg.nsamples; ++j) {
+            uint64_t p = (uint64_t)sg.first + px + (uint64_t)j * pixels;
+            V3 q = xyz(ps.rad[p]);
+            r = r + q;
+            r2 = r2 + q * q;
+            if (job.fp.guides) {
+                float4 g = ps.galb[p];
+                al = al + xyz(g);
+                dep = dep + g.w;
+                nn = nn + xyz(ps.gnrm[p]);
+            }
+        }
+        a.radiance[0] = r.x; a.radiance[1] = r.y; a.radiance[2] = r.z;
+        a.radiance_sq[0] = r2.x; a.radiance_sq[1] = r2.y; a.radiance_sq[2] = r2.z;
+        a.albedo[0] = al.x; a.albedo[1] = al.y; a.albedo[2] = al.z;
+        a.normal[0] = nn.x; a.normal[1] = nn.y; a.normal[2] = nn.z;
+        a.depth = dep;
+        a.samples = a.samples + (float)sg.nsamples;
+        job.accum[px] = a;
     }
 }
 
@@ -506,12 +615,12 @@ void query_occupancy(RenderState& rs) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, 128, 0);
         return b > 0 ? b : 8;
     };
-    rs.extend_blocks = occ((const void*)k_extend<false>);
-    rs.connect_blocks = occ((const void*)k_connect<false>);
+    rs.extend_blocks = occ((const void*)k_extend<false, false, 128>);
+    rs.connect_blocks = occ((const void*)k_connect<false, false, 128>);
     rs.shade_blocks = occ((const void*)k_shade<false, false>);
     rs.shade_blocks_guided = occ((const void*)k_shade<true, false>);
-    rs.extend_blocks_inst = occ((const void*)k_extend<true>);
-    rs.connect_blocks_inst = occ((const void*)k_connect<true>);
+    rs.extend_blocks_inst = occ((const void*)k_extend<true, false, 128>);
+    rs.connect_blocks_inst = occ((const void*)k_connect<true, false, 128>);
     rs.shade_blocks_inst = occ((const void*)k_shade<false, true>);
     rs.shade_blocks_guided_inst = occ((const void*)k_shade<true, true>);
 }
@@ -533,8 +642,8 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
     for (uint32_t d = 0; d < fp.max_depth; ++d) {
         if (timer) timer->mark(stream, StageTimer::kExtend);
         const bool inst = sc.num_instances > 0;
-        if (inst) k_extend<true><<<sms * rs.extend_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, d);
-        else k_extend<false><<<sms * rs.extend_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        if (inst) k_extend<true, false, 128><<<sms * rs.extend_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
+        else k_extend<false, false, 128><<<sms * rs.extend_blocks, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
         if (fp.guided && d + 1 < fp.max_depth) {
             if (timer) timer->mark(stream, StageTimer::kGuide);
             launch_guide_infer(rs, sc, fp, d, stream);
@@ -542,19 +651,19 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
         }
         if (timer) timer->mark(stream, StageTimer::kShade);
         if (fp.guided && inst)
-            k_shade<true, true><<<sms * rs.shade_blocks_guided_inst, 128, 0, stream>>>(rs.ps, sc, fp, d);
+            k_shade<true, true><<<sms * rs.shade_blocks_guided_inst, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
         else if (fp.guided)
-            k_shade<true, false><<<sms * rs.shade_blocks_guided, 128, 0, stream>>>(rs.ps, sc, fp, d);
+            k_shade<true, false><<<sms * rs.shade_blocks_guided, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
         else if (inst)
-            k_shade<false, true><<<sms * rs.shade_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, d);
+            k_shade<false, true><<<sms * rs.shade_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
         else
-            k_shade<false, false><<<sms * rs.shade_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
+            k_shade<false, false><<<sms * rs.shade_blocks, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
         rs.launches += 2;
         if (d + 1 < fp.max_depth && (fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) &&
             sc.light_strategies > 0) {
             if (timer) timer->mark(stream, StageTimer::kConnect);
-            if (inst) k_connect<true><<<sms * rs.connect_blocks_inst, 128, 0, stream>>>(rs.ps, sc, d);
-            else k_connect<false><<<sms * rs.connect_blocks, 128, 0, stream>>>(rs.ps, sc, d);
+            if (inst) k_connect<true, false, 128><<<sms * rs.connect_blocks_inst, 128, 0, stream>>>(rs.ps, sc, BatchDev{}, d);
+            else k_connect<false, false, 128><<<sms * rs.connect_blocks, 128, 0, stream>>>(rs.ps, sc, BatchDev{}, d);
             rs.launches++;
         }
     }
@@ -594,3 +703,54 @@ int32_t luc_build_tnodes_range(luc_ctx* c, uint32_t begin, uint32_t end) {
     LUC_CUDA(c, cudaGetLastError(), "traversal layout");
     return LUC_OK;
 }
+
+namespace luc {
+
+// One wave of a batched render (graph-capturable: fixed shapes, lengths on
+// the device). `block` selects the EXTEND / CONNECT instantiation.
+template <int B>
+static void wave_traverse(RenderState& rs, const BatchDev& bd, const FrameParams& fpw, uint32_t d, bool connect,
+                          int ext_blocks, int con_blocks, cudaStream_t s) {
+    const int sms = rs.num_sms;
+    if (!connect) k_extend<false, true, B><<<sms * ext_blocks, B, 0, s>>>(rs.ps, DevScene{}, fpw, bd, d);
+    else k_connect<false, true, B><<<sms * con_blocks, B, 0, s>>>(rs.ps, DevScene{}, bd, d);
+}
+
+int batch_blocks_per_sm(int block, bool connect) {
+    int b = 0;
+    const void* k = nullptr;
+    if (block == 64) k = connect ? (const void*)k_connect<false, true, 64> : (const void*)k_extend<false, true, 64>;
+    else if (block == 256) k = connect ? (const void*)k_connect<false, true, 256> : (const void*)k_extend<false, true, 256>;
+    else k = connect ? (const void*)k_connect<false, true, 128> : (const void*)k_extend<false, true, 128>;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, block, 0);
+    return b > 0 ? b : 1;
+}
+
+void record_wave(RenderState& rs, const BatchDev& bd, const uint32_t* pix_off, uint32_t num_paths,
+                 uint32_t total_pixels, uint32_t max_depth, int block, cudaStream_t s) {
+    const int sms = rs.num_sms;
+    cudaMemsetAsync(rs.ps.ctr, 0, kCtrStride * (max_depth + 2) * sizeof(uint32_t), s);
+    k_generate_batch<<<(int)std::min<uint64_t>((num_paths + 255) / 256, (uint64_t)sms * 16), 256, 0, s>>>(rs.ps, bd,
+                                                                                                      num_paths);
+    FrameParams fpw{};
+    fpw.num_paths = num_paths;
+    const int eb = batch_blocks_per_sm(block, false), cb = batch_blocks_per_sm(block, true);
+    for (uint32_t d = 0; d < max_depth; ++d) {
+        if (block == 64) wave_traverse<64>(rs, bd, fpw, d, false, eb, cb, s);
+        else if (block == 256) wave_traverse<256>(rs, bd, fpw, d, false, eb, cb, s);
+        else wave_traverse<128>(rs, bd, fpw, d, false, eb, cb, s);
+        k_shade<false, false, true><<<sms * rs.shade_blocks, 128, 0, s>>>(rs.ps, DevScene{}, fpw, bd, d);
+        rs.launches += 2;
+        if (d + 1 < max_depth) {
+            if (block == 64) wave_traverse<64>(rs, bd, fpw, d, true, eb, cb, s);
+            else if (block == 256) wave_traverse<256>(rs, bd, fpw, d, true, eb, cb, s);
+            else wave_traverse<128>(rs, bd, fpw, d, true, eb, cb, s);
+            rs.launches++;
+        }
+    }
+    k_resolve_batch<<<(int)std::min<uint64_t>((total_pixels + 255) / 256, (uint64_t)sms * 16), 256, 0, s>>>(
+        rs.ps, bd, pix_off, total_pixels);
+    rs.launches += 2;
+}
+
+}  // namespace luc

@@ -65,6 +65,15 @@ class RenderStats(C.Structure):
                 ("ms_train", C.c_double)]
 
 
+class BatchJob(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("uniforms", L.Uniforms), ("spp", C.c_uint32), ("max_depth", C.c_uint32),
+                ("accum_dev", C.c_void_p)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("block", C.c_uint32), ("chunk", C.c_uint32)]
+
+
 class GuideInfo(C.Structure):
     _fields_ = [("steps", C.c_uint32), ("last_records", C.c_uint32), ("last_loss", C.c_float),
                 ("threshold", C.c_uint32), ("num_params", C.c_uint32)]
@@ -100,6 +109,10 @@ _SIGS = {
                                 C.c_void_p]),
     "luc_denoise_dev": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(DenoiseParams),
                                     C.c_uint32, C.c_void_p]),
+    "luc_batch_configure": (C.c_int32, [C.c_void_p, C.POINTER(BatchConfig)]),
+    "luc_render_batch": (C.c_int32, [C.c_void_p, C.POINTER(BatchJob), C.c_uint32, C.c_void_p, C.POINTER(RenderStats)]),
+    "luc_batch_autotune": (C.c_int32, [C.c_void_p, C.POINTER(BatchJob), C.c_uint32, C.c_uint32,
+                                       C.POINTER(BatchConfig), C.c_void_p]),
     "luc_upload_meshes": (C.c_int32, [C.c_void_p, C.POINTER(SceneView), C.c_void_p, C.c_void_p, C.c_uint32]),
     "luc_set_instances": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
     "luc_read_scene": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),

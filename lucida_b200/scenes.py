@@ -179,7 +179,7 @@ def procedural_sky(width, height, sun_dir, sun_intensity, sun_radius_deg):
 
 # ----------------------------------------------------------------- config 2
 def displaced_spheres(count: int = 256, level: int = 4, seed: int = 2024, env_size=(1024, 512),
-                      amplitude: float = 0.05, radius_range=(0.45, 0.95)) -> SceneDef:
+                      amplitude: float = 0.05, radius_range=(0.45, 0.95), sky=None) -> SceneDef:
     rng = np.random.default_rng(seed)
     unit, faces = icosphere_unit(level)
     nv, nf = len(unit), len(faces)
@@ -211,7 +211,10 @@ def displaced_spheres(count: int = 256, level: int = 4, seed: int = 2024, env_si
     mats = np.array(mats, L.MATERIAL)
     prims = np.array([L.quad((-30, 0, -30), (0, 0, 60), (60, 0, 0), 0)], L.PRIMITIVE)
     w, h = env_size
-    px, cdf, total = procedural_sky(w, h, (-0.4, 0.55, -0.7), 1.0e4, 0.5) if w > 0 else (None, None, 0.0)
+    if sky is not None:  # a precomputed procedural_sky(...) triple, shared between scenes
+        px, cdf, total = sky
+    else:
+        px, cdf, total = procedural_sky(w, h, (-0.4, 0.55, -0.7), 1.0e4, 0.5) if w > 0 else (None, None, 0.0)
     return SceneDef(materials=mats, primitives=prims, lights=L.quad_lights(mats, prims), positions=positions,
                     vertex_attrs=attrs, triangles=tris, bvh_nodes=None,
                     camera=Camera(eye=(0.0, 7.0, 24.0), look_at=(0.0, 1.5, 0.0), vfov_deg=45.0),
@@ -336,3 +339,31 @@ def instanced_field(num_meshes: int = 16, tri_range=(50_000, 500_000), num_insta
                     env_pixels=px, env_cdf=cdf, env_total_weight=total,
                     meshes=np.array(meshes, np.uint32), placements=(o2w, mesh, material),
                     name=f"instanced-field-{num_meshes}x{num_instances}")
+
+
+BATCH_RESOLUTIONS = ((256, 256), (512, 512), (1024, 1024), (1920, 1080))
+BATCH_SPP = (4, 8, 16, 32, 64)
+
+
+def batch_workload(num_scenes: int = 64, tri_range=(10_000, 2_000_000), seed: int = 4096, level: int = 4,
+                   resolutions=BATCH_RESOLUTIONS, spp_choices=BATCH_SPP, depth_range=(4, 12), env_size=(1024, 512)):
+    """Uneven batch: `num_scenes` scenes of the displaced-spheres recipe whose
+    triangle counts are log-uniform in `tri_range` (whole level-`level`
+    icospheres), each with a resolution from `resolutions`, spp from
+    `spp_choices` and bounces uniform in `depth_range`, all seeded. Returns
+    [(SceneDef, width, height, spp, max_depth)]; the scenes share one sky."""
+    rng = np.random.default_rng(seed)
+    faces = 20 * 4 ** level
+    w, h = env_size
+    sky = procedural_sky(w, h, (-0.4, 0.55, -0.7), 1.0e4, 0.5) if w > 0 else (None, None, 0.0)
+    out = []
+    for i in range(num_scenes):
+        tris = float(np.exp(rng.uniform(np.log(tri_range[0]), np.log(tri_range[1]))))
+        count = max(1, int(round(tris / faces)))
+        res = resolutions[int(rng.integers(len(resolutions)))]
+        spp = int(spp_choices[int(rng.integers(len(spp_choices)))])
+        depth = int(rng.integers(depth_range[0], depth_range[1] + 1))
+        sc = displaced_spheres(count=count, level=level, seed=seed * 1000 + i, env_size=env_size, sky=sky)
+        sc.name = f"batch-{i}-{len(sc.triangles)}"
+        out.append((sc, res[0], res[1], spp, depth))
+    return out
