@@ -143,13 +143,24 @@ __global__ void k_hist4(const uint32_t* __restrict__ keys, uint32_t n, uint32_t*
     __shared__ uint32_t sh[4][256];
     for (int t = threadIdx.x; t < 1024; t += blockDim.x) (&sh[0][0])[t] = 0;
     __syncthreads();
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t k = keys[i];
+    auto count = [&](uint32_t k) {
         atomicAdd(&sh[0][k & 255u], 1u);
         atomicAdd(&sh[1][(k >> 8) & 255u], 1u);
         atomicAdd(&sh[2][(k >> 16) & 255u], 1u);
         atomicAdd(&sh[3][k >> 24], 1u);
+    };
+    // 16-byte loads where the array allows them (the scratch arrays are
+    // 256-byte aligned); the last n % 4 keys one at a time.
+    const uint32_t n4 = ((reinterpret_cast<uintptr_t>(keys) & 15u) == 0) ? n / 4 : 0;
+    const uint4* k4 = reinterpret_cast<const uint4*>(keys);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += gridDim.x * blockDim.x) {
+        uint4 v = k4[i];
+        count(v.x);
+        count(v.y);
+        count(v.z);
+        count(v.w);
     }
+    for (uint32_t i = 4 * n4 + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) count(keys[i]);
     __syncthreads();
     for (int t = threadIdx.x; t < 1024; t += blockDim.x) {
         uint32_t v = (&sh[0][0])[t];
@@ -174,14 +185,16 @@ __global__ void k_hist_scan(const uint32_t* __restrict__ hist, uint32_t* __restr
     }
 }
 
-__global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint32_t* __restrict__ kin,
+__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint32_t* __restrict__ kin,
                                                            const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
                                                            uint32_t* __restrict__ vout, uint32_t n, int shift,
                                                            const uint32_t* __restrict__ digit_offsets,
                                                            uint32_t* status, uint32_t* tile_counter, uint32_t* err) {
     __shared__ uint32_t s_tile;
     __shared__ uint32_t whist[kSortThreads / 32][256];
-    __shared__ uint32_t s_base[256];
+    __shared__ uint32_t s_base[256];   // global start of each digit's run from this tile
+    __shared__ uint32_t s_start[256];  // start of each digit's run within the tile
+    __shared__ uint32_t s_keys[kTile], s_vals[kTile];
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     for (uint32_t t = tid; t < (kSortThreads / 32) * 256; t += kSortThreads) (&whist[0][0])[t] = 0;
     if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
@@ -239,14 +252,39 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint32_t* __res
         atomicExch(status + (size_t)tile * 256 + tid, (excl + total) | kFlagInc);
     }
     s_base[tid] = digit_offsets[tid] + excl;
+    // Exclusive scan of the tile's digit totals: where each digit's run
+    // starts inside the tile (Hillis-Steele over 256 threads in s_start).
+    s_start[tid] = total;
     __syncthreads();
+    for (uint32_t off = 1; off < 256; off <<= 1) {
+        uint32_t t = tid >= off ? s_start[tid - off] : 0u;
+        __syncthreads();
+        s_start[tid] += t;
+        __syncthreads();
+    }
+    const uint32_t incl = s_start[tid];
+    __syncthreads();
+    s_start[tid] = incl - total;
+    __syncthreads();
+    // Sort the tile by digit in shared memory (stable: tile order within a
+    // digit), then write each digit's run out contiguously, so consecutive
+    // threads store to consecutive addresses.
 #pragma unroll
     for (int k = 0; k < kSortKpt; ++k) {
         if (rank[k] == kNone) continue;
         uint32_t digit = (key[k] >> shift) & 255u;
-        uint32_t dst = s_base[digit] + whist[warp][digit] + rank[k];
-        kout[dst] = key[k];
-        vout[dst] = val[k];
+        uint32_t local = s_start[digit] + whist[warp][digit] + rank[k];
+        s_keys[local] = key[k];
+        s_vals[local] = val[k];
+    }
+    __syncthreads();
+    const uint32_t count = min(kTile, n - tile * kTile);
+    for (uint32_t i = tid; i < count; i += kSortThreads) {
+        uint32_t kk = s_keys[i];
+        uint32_t digit = (kk >> shift) & 255u;
+        uint32_t dst = s_base[digit] + (i - s_start[digit]);
+        kout[dst] = kk;
+        vout[dst] = s_vals[i];
     }
 }
 

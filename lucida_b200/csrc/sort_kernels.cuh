@@ -17,7 +17,7 @@ __global__ void k_hist4(const uint32_t* __restrict__ keys, uint32_t n, uint32_t*
 __global__ void k_hist_scan(const uint32_t* __restrict__ hist, uint32_t* __restrict__ offsets);
 // One stable pass over digit (key >> shift) & 255; `status` (tiles x 256) and
 // `tile_counter` must be zero on entry; *err is set if a look-back wait gives up.
-__global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                            uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t n, int shift,
                            const uint32_t* __restrict__ digit_offsets, uint32_t* status, uint32_t* tile_counter,
                            uint32_t* err);
