@@ -142,7 +142,7 @@ int32_t luc_create(int32_t device, luc_ctx** out) {
     if (const char* g = std::getenv("LUC_NO_GRAPHS")) c->use_graphs = g[0] == '\0' || g[0] == '0';
     const std::vector<float>& et = energy_table_cached();
     if (upload(c->energy, et.data(), et.size(), c->stream) != cudaSuccess ||
-        cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        luc_init_sobol_tables(c->stream) != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) {
         cudaStreamDestroy(c->own_stream);
         delete c;
         return LUC_ERR_OUT_OF_MEMORY;

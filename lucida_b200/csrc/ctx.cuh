@@ -129,6 +129,8 @@ int32_t luc_build_blases(luc_ctx* c, const uint32_t* first, const uint32_t* coun
 luc::GuideDev luc_guide_dev(const luc_ctx* c);
 luc::GuideTrain luc_guide_train_state(luc_ctx* c);
 int32_t luc_guide_prepare_frame(luc_ctx* c, uint64_t paths);
+// wavefront.cu: fill the Sobol byte tables on the current device.
+cudaError_t luc_init_sobol_tables(cudaStream_t s);
 // capi.cu: grow the path pool to `paths` paths and `max_depth` bounces.
 int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth);
 // Implemented in denoise.cu.

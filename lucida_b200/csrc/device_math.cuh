@@ -117,7 +117,7 @@ LUC_HD float u32_to_unit(uint32_t v) { return (float)(v >> 8) * (1.0f / 16777216
 // Owen-scrambled Sobol (crates/core/src/sobol.rs:147-235). Dimension 0's
 // generator is the bit reversal; dimension 1's direction numbers follow
 // V[0] = 2^31, V[k] = V[k-1] ^ (V[k-1] >> 1).
-LUC_D uint32_t sobol_dim1(uint32_t index) {
+LUC_D uint32_t sobol_dim1_loop(uint32_t index) {
     uint32_t x = 0, v = 0x80000000u;
 #pragma unroll
     for (int k = 0; k < 32; ++k) {
@@ -125,6 +125,15 @@ LUC_D uint32_t sobol_dim1(uint32_t index) {
         v ^= v >> 1;
     }
     return x;
+}
+// The same product by bytes: g_sobol_dim1_bytes[256 * j + b] is the XOR of
+// the direction numbers V[8j + i] over the set bits i of b (4 KB, filled once
+// per device by luc_init_sobol_tables), so a draw costs four L1-resident
+// loads instead of a 32-step loop; the result is the same XOR sum.
+extern __device__ uint32_t g_sobol_dim1_bytes[1024];
+LUC_D uint32_t sobol_dim1(uint32_t index) {
+    return __ldg(g_sobol_dim1_bytes + (index & 255u)) ^ __ldg(g_sobol_dim1_bytes + 256 + ((index >> 8) & 255u)) ^
+           __ldg(g_sobol_dim1_bytes + 512 + ((index >> 16) & 255u)) ^ __ldg(g_sobol_dim1_bytes + 768 + (index >> 24));
 }
 LUC_HD uint32_t hash_u32(uint32_t x) {
     x ^= x >> 16;

@@ -754,3 +754,19 @@ void record_wave(RenderState& rs, const BatchDev& bd, const uint32_t* pix_off, u
 }
 
 }  // namespace luc
+
+namespace luc {
+// Sobol dimension-1 byte tables (see sobol_dim1 in device_math.cuh).
+__device__ uint32_t g_sobol_dim1_bytes[1024];
+
+__global__ void k_init_sobol_tables() {
+    const uint32_t t = threadIdx.x;  // 1024 threads: byte j = t / 256, value b = t % 256
+    const uint32_t j = t >> 8, b = t & 255u;
+    g_sobol_dim1_bytes[t] = sobol_dim1_loop(b << (8 * j));
+}
+}  // namespace luc
+
+cudaError_t luc_init_sobol_tables(cudaStream_t s) {
+    luc::k_init_sobol_tables<<<1, 1024, 0, s>>>();
+    return cudaGetLastError();
+}
