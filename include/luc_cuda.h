@@ -206,6 +206,15 @@ int32_t luc_sort_u32_dev(luc_ctx* ctx, void* keys_dev, void* vals_dev, uint32_t 
 int32_t luc_eval_bsdf(luc_ctx* ctx, const GpuMaterial* m, int32_t front, const float* wo3, const float* in3,
                       uint32_t n, int32_t mode, float* out_wi3, float* out_f3, float* out_pdf);
 int32_t luc_eval_env(luc_ctx* ctx, const float* in, uint32_t n, int32_t mode, float* dir3, float* rad3, float* pdf);
+/* Ray queries against the resident scene, n rays of 8 floats (origin xyz,
+ * t_max, direction xyz, unused), host arrays.
+ *   mode 0 = Scene::intersect (crates/core/src/scene.rs:452-527): out holds
+ *            n x (t, u, v, id as u32 bits), id = triangle (leaf order) or
+ *            analytic primitive | 0x80000000, 0xFFFFFFFF on a miss (t_max
+ *            is not used);
+ *   mode 1 = Scene::occluded (scene.rs:577-606) within (1e-4, t_max): out
+ *            holds n u32, 1 = occluded. */
+int32_t luc_intersect(luc_ctx* ctx, const float* rays8, uint32_t n, int32_t mode, void* out);
 
 /* Sort without allocating: the variant of luc_sort_u32_dev for callers that
  * cannot call cudaMalloc (a host that reserves all device memory up front, or
@@ -240,8 +249,11 @@ int32_t luc_set_instances(luc_ctx* ctx, const float* object_to_world, const uint
                           uint32_t num_instances);
 /* Copy the resident scene's arrays to the host: which = 0 BVH nodes (every
  * BLAS then the TLAS), 1 triangles (leaf order), 2 primitives (analytic, then
- * instance rows in TLAS-leaf order). *bytes receives the size; out may be null
- * to query it. */
+ * instance rows in TLAS-leaf order), 3 compressed 8-wide nodes (80 B each;
+ * 0 bytes when the scene traverses the binary tree), 4 the wide tree's
+ * triangle soup (48 B per triangle: p0 with the leaf-order index in p0.w as
+ * u32 bits, p1 - p0, p2 - p0). *bytes receives the size; out may be null to
+ * query it. */
 int32_t luc_read_scene(luc_ctx* ctx, uint32_t which, void* out, uint64_t capacity, uint64_t* bytes);
 
 /* ---- Batched multi-scene rendering (no reference counterpart) ----

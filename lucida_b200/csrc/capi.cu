@@ -140,6 +140,7 @@ int32_t luc_create(int32_t device, luc_ctx** out) {
     c->stream = c->own_stream;
     if (const char* b = std::getenv("LUC_PATH_BUDGET")) c->path_budget = std::strtoull(b, nullptr, 10);
     if (const char* g = std::getenv("LUC_NO_GRAPHS")) c->use_graphs = g[0] == '\0' || g[0] == '0';
+    if (const char* g = std::getenv("LUC_BINARY_BVH")) c->use_wide = g[0] == '\0' || g[0] == '0';
     const std::vector<float>& et = energy_table_cached();
     if (upload(c->energy, et.data(), et.size(), c->stream) != cudaSuccess ||
         luc_init_sobol_tables(c->stream) != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) {
@@ -157,7 +158,8 @@ void luc_destroy(luc_ctx* c) {
     cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->materials, &c->prims,    &c->lights,   &c->positions, &c->attrs,     &c->tris,
                       &c->nodes,     &c->env_px,   &c->env_cond, &c->env_marg,  &c->env_row_sin, &c->energy,
-                      &c->tnodes,    &c->soup,     &c->frame_word, &c->blas_roots,
+                      &c->tnodes,    &c->soup,     &c->frame_word, &c->blas_roots, &c->wnodes,  &c->wsoup,
+                      &c->wtasks,    &c->wctr,
                       &c->pool,      &c->accum_tmp, &c->lb_tris, &c->lb_pos,    &c->lb_boxes,  &c->lb_keys,
                       &c->lb_vals,   &c->lb_keys2, &c->lb_vals2, &c->lb_hist,   &c->lb_karras, &c->lb_parent,
                       &c->lb_nbounds, &c->lb_subtree, &c->lb_flags, &c->lb_nodes, &c->lb_rank, &c->lb_misc,
@@ -337,9 +339,14 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     LUC_CUDA(c, upload(c->env_cond, cond.data(), cond.size(), s), "upload env cdf");
     LUC_CUDA(c, upload(c->env_marg, marg.data(), marg.size(), s), "upload env marginal");
     LUC_CUDA(c, upload(c->env_row_sin, rsin.data(), rsin.size(), s), "upload env rows");
+    c->wide_nodes = 0;
     if (v->num_triangles && num_nodes) {
         int32_t rc2 = luc_build_traversal(c, num_nodes, v->num_triangles);
         if (rc2) return rc2;
+        if (c->use_wide && !ni && !meshes) {
+            rc2 = luc_build_wide(c, num_nodes, v->num_triangles);
+            if (rc2) return rc2;
+        }
     }
     LUC_CUDA(c, cudaStreamSynchronize(s), "scene upload");
 
@@ -363,6 +370,8 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     d.reference_shadows = false;
     d.tnodes = c->tnodes.as<float4>();
     d.soup = c->soup.as<float4>();
+    d.wnodes = c->wide_nodes ? c->wnodes.as<float4>() : nullptr;
+    d.wsoup = c->wide_nodes ? c->wsoup.as<float4>() : nullptr;
     d.root_first = 0;
     d.root_count = 0;
     if (d.num_nodes) {

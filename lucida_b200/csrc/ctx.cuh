@@ -48,6 +48,9 @@ struct luc_ctx {
     // Resident scene.
     DevBuf materials, prims, lights, positions, attrs, tris, nodes, env_px, env_cond, env_marg, env_row_sin, energy;
     DevBuf tnodes, soup;  // traversal layout derived from nodes / tris
+    DevBuf wnodes, wsoup, wtasks, wctr;  // compressed 8-wide tree (wide.cu)
+    uint32_t wide_nodes = 0;             // 0: the scene traverses the binary tree
+    bool use_wide = true;                // LUC_BINARY_BVH=1 turns the wide tree off
     DevBuf blas_roots;    // distinct BLAS roots of an instanced scene
     // Meshes uploaded for device-built instancing (luc_upload_meshes): per
     // mesh its BLAS root node and object-space bounds (6 floats), the BLAS
@@ -119,6 +122,9 @@ int32_t luc_gather_triangles(luc_ctx* c, const GpuTriangle* src, GpuTriangle* ds
 // Implemented in wavefront.cu: derive the traversal layout (child-pair
 // records, triangle soup) from the resident nodes and triangles.
 int32_t luc_build_traversal(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris);
+// wide.cu: collapse the binary tree into c->wnodes / c->wsoup (sets
+// c->wide_nodes; 0 when the tree is too deep for the level budget).
+int32_t luc_build_wide(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris);
 int32_t luc_build_tnodes_range(luc_ctx* c, uint32_t begin, uint32_t end);
 // Implemented in instances.cu: one LBVH per mesh range of the triangles in
 // lb_tris into c->nodes / c->tris (see luc_upload_meshes).

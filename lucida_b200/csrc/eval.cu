@@ -114,3 +114,43 @@ extern "C" int32_t luc_eval_env(luc_ctx* c, const float* in, uint32_t n, int32_t
                                   (float*)dout[2]);
                           });
 }
+
+// Ray queries against the resident scene: Scene::intersect (scene.rs:452-527)
+// for mode 0, Scene::occluded (scene.rs:577-606) for mode 1, through the same
+// traversal the integrator uses (wide tree, binary tree or instances).
+namespace luc {
+__global__ void k_intersect(const __grid_constant__ DevScene sc, const float* __restrict__ rays, uint32_t n,
+                           int32_t mode, float* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* r = rays + 8 * (size_t)i;
+    const V3 o{r[0], r[1], r[2]}, d{r[4], r[5], r[6]};
+    TravCount tc;
+    if (mode == 0) {
+        float t, u, v;
+        uint32_t inst;
+        const uint32_t id = sc.num_instances ? closest_hit<true>(sc, o, d, t, u, v, inst, tc)
+                                             : closest_hit<false>(sc, o, d, t, u, v, inst, tc);
+        reinterpret_cast<float4*>(out)[i] = make_float4(t, u, v, __uint_as_float(id));
+    } else {
+        const bool occ = sc.num_instances ? occluded<true>(sc, o, d, r[3], tc) : occluded<false>(sc, o, d, r[3], tc);
+        reinterpret_cast<uint32_t*>(out)[i] = occ ? 1u : 0u;
+    }
+}
+}  // namespace luc
+
+extern "C" int32_t luc_intersect(luc_ctx* c, const float* rays8, uint32_t n, int32_t mode, void* out) {
+    using namespace luc;
+    if (!c || (n && (!rays8 || !out))) return LUC_ERR_VALIDATION;
+    if (mode != 0 && mode != 1) return luc_fail(c, LUC_ERR_VALIDATION, "mode must be 0 (closest hit) or 1 (occluded)");
+    if (!c->has_scene) return luc_fail(c, LUC_ERR_VALIDATION, "no scene uploaded");
+    cudaSetDevice(c->device);
+    if (n == 0) return LUC_OK;
+    DevScene sc = c->scene;
+    return with_device_io(c, {{rays8, (size_t)n * 32}}, {{out, (size_t)n * (mode == 0 ? 16 : 4)}},
+                          [&](std::vector<void*>& din, std::vector<void*>& dout) {
+                              k_intersect<<<(n + 127) / 128, 128, 0, c->stream>>>(sc, (const float*)din[0], n, mode,
+                                                                                  (float*)dout[0]);
+                          });
+}
+

@@ -281,6 +281,8 @@ int32_t luc_set_instances(luc_ctx* c, const float* object_to_world, const uint32
     d.num_prims = np_;
     d.nodes = c->nodes.as<float4>();
     d.tnodes = c->tnodes.as<float4>();
+    d.wnodes = nullptr;  // two-level scenes traverse binary BLASes and TLAS
+    d.wsoup = nullptr;
     d.num_nodes = bn + 2 * c->inst_capacity;  // fixed while the capacity holds, so frame graphs keep replaying
     d.inst = reinterpret_cast<const GpuInstance*>(d.prims + np_);
     d.num_instances = n;
@@ -304,10 +306,14 @@ int32_t luc_read_scene(luc_ctx* c, uint32_t which, void* out, uint64_t capacity,
         case 0: src = c->nodes.p; n = (uint64_t)c->total_nodes * sizeof(GpuBvhNode); break;
         case 1: src = c->tris.p; n = (uint64_t)d.num_tris * sizeof(GpuTriangle); break;
         case 2: src = c->prims.p; n = ((uint64_t)d.num_prims + d.num_instances) * sizeof(GpuPrimitive); break;
-        default: return luc_fail(c, LUC_ERR_VALIDATION, "which: 0 nodes, 1 triangles, 2 primitives");
+        case 3: src = c->wnodes.p; n = d.wnodes ? (uint64_t)c->wide_nodes * 80 : 0; break;
+        case 4: src = c->wsoup.p; n = d.wnodes ? (uint64_t)d.num_tris * 48 : 0; break;
+        default:
+            return luc_fail(c, LUC_ERR_VALIDATION,
+                            "which: 0 nodes, 1 triangles, 2 primitives, 3 wide nodes, 4 wide triangle soup");
     }
     *bytes = n;
-    if (!out) return LUC_OK;
+    if (!out || n == 0) return LUC_OK;
     if (capacity < n) return luc_fail(c, LUC_ERR_VALIDATION, "output buffer too small");
     cudaSetDevice(c->device);
     LUC_CUDA(c, cudaMemcpyAsync(out, src, n, cudaMemcpyDeviceToHost, c->stream), "read scene");

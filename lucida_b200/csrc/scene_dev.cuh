@@ -20,6 +20,10 @@ struct DevScene {
     uint32_t num_nodes;
     const float4* tnodes;  // child-pair records, 4 float4 per internal node id
     const float4* soup;    // (p0, e1, e2) per triangle, leaf order
+    // Compressed 8-wide tree collapsed from `nodes` (wide.cu); null when the
+    // scene traverses the binary tree (instanced scenes, LUC_BINARY_BVH=1).
+    const float4* wnodes;  // 5 float4 per wide node, root = node 0
+    const float4* wsoup;   // (p0 | leaf-order index in p0.w, e1, e2) per triangle, wide-node order
     uint32_t root_first, root_count;  // the root when it is itself a leaf
     // Instancing (instance.rs): GpuInstance rows appended after the analytic
     // primitives, in TLAS-leaf order; the TLAS's first node in `nodes`; the
@@ -320,6 +324,133 @@ LUC_D bool bvh_any(const DevScene& s, TRef root, V3 o, V3 d, float tmin, float t
     }
 }
 
+// ---------------------------------------------------------------- wide tree
+// Node record (80 B, 5 x 16 B), built by wide.cu from the binary tree:
+//   [0] origin p (3 x f32), exponent bytes ex | ey << 8 | ez << 16, internal
+//       child mask << 24 (bit s: slot s holds an internal child);
+//   [1] first internal child (wide node index), first triangle (wide soup
+//       index), meta bytes of slots 0-3, of slots 4-7;
+//   [2] qlo.x of slots 0-7 (8 x u8), qlo.y; [3] qlo.z, qhi.x; [4] qhi.y, qhi.z.
+// Child box of slot s on axis a: [p + qlo * 2^(e-127), p + qhi * 2^(e-127)],
+// each plane at least one quantum outside the binary child's (padded) box.
+// A leaf slot's meta byte is count << 5 | offset: triangles first + offset ..
+// + count - 1 (count 1-4, at most 32 per node). Internal children are stored
+// contiguously in slot order. Slots are assigned by octant: slot s holds the
+// child lying towards corner s of the node (bit a set: the +a side). A ray
+// whose direction has sign bits oct (bit a set: negative along a) meets the
+// children roughly in ascending order of k = s ^ oct, the order in which the
+// hit bits are stored and visited.
+constexpr uint32_t kWideTri = 0x80000000u;  // group tag: triangle group
+constexpr int kWideStack = 64;
+constexpr int kWidePostpone = 8;  // fewer lanes than this with triangles: defer them
+
+LUC_D float wide_q(uint32_t word, uint32_t j) {  // byte j of word as an exact float
+    return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7440u | j)) - 8388608.0f;
+}
+
+// Slab tests of the 8 child boxes of wide node `node`. Returns the node group
+// (first child, internal mask << 8 | hit bits at positions slot ^ oct) and the
+// triangle group (first triangle | kWideTri, mask of hit triangles).
+LUC_D void wide_node(const float4* __restrict__ wn, uint32_t node, V3 o, V3 inv, uint32_t oct, float tmin,
+                     float tmax, uint2& ng, uint2& tg) {
+    const float4* q = wn + 5 * (size_t)node;
+    const float4 a = __ldg(q);
+    const uint4 b = __ldg(reinterpret_cast<const uint4*>(q + 1));
+    const uint4 c = __ldg(reinterpret_cast<const uint4*>(q + 2));
+    const uint4 d = __ldg(reinterpret_cast<const uint4*>(q + 3));
+    const uint4 e = __ldg(reinterpret_cast<const uint4*>(q + 4));
+    const uint32_t ew = __float_as_uint(a.w);
+    const float sx = __uint_as_float((ew & 0xFFu) << 23) * inv.x;
+    const float sy = __uint_as_float(((ew >> 8) & 0xFFu) << 23) * inv.y;
+    const float sz = __uint_as_float(((ew >> 16) & 0xFFu) << 23) * inv.z;
+    const float ox = (a.x - o.x) * inv.x, oy = (a.y - o.y) * inv.y, oz = (a.z - o.z) * inv.z;
+    const uint32_t imask = ew >> 24;
+    // Near plane: lo for a positive direction, hi for a negative one.
+    const bool nx = inv.x < 0.0f, ny = inv.y < 0.0f, nz = inv.z < 0.0f;
+    const uint32_t nx0 = nx ? d.z : c.x, nx1 = nx ? d.w : c.y, fx0 = nx ? c.x : d.z, fx1 = nx ? c.y : d.w;
+    const uint32_t ny0 = ny ? e.x : c.z, ny1 = ny ? e.y : c.w, fy0 = ny ? c.z : e.x, fy1 = ny ? c.w : e.y;
+    const uint32_t nz0 = nz ? e.z : d.x, nz1 = nz ? e.w : d.y, fz0 = nz ? d.x : e.z, fz1 = nz ? d.y : e.w;
+    uint32_t nh = 0, tm = 0;
+#pragma unroll
+    for (uint32_t s = 0; s < 8; ++s) {
+        const uint32_t j = s & 3u;
+        const bool hi = s >= 4;
+        const float tnx = __fmaf_rn(wide_q(hi ? nx1 : nx0, j), sx, ox), tfx = __fmaf_rn(wide_q(hi ? fx1 : fx0, j), sx, ox);
+        const float tny = __fmaf_rn(wide_q(hi ? ny1 : ny0, j), sy, oy), tfy = __fmaf_rn(wide_q(hi ? fy1 : fy0, j), sy, oy);
+        const float tnz = __fmaf_rn(wide_q(hi ? nz1 : nz0, j), sz, oz), tfz = __fmaf_rn(wide_q(hi ? fz1 : fz0, j), sz, oz);
+        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+        const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
+        if (tn <= tf) {
+            const uint32_t m = ((hi ? b.w : b.z) >> (8 * j)) & 0xFFu;
+            if (imask & (1u << s)) nh |= 1u << (s ^ oct);
+            else tm |= ((1u << (m >> 5)) - 1u) << (m & 31u);
+        }
+    }
+    ng = make_uint2(b.x, (imask << 8) | nh);
+    tg = make_uint2(b.y | kWideTri, tm);
+}
+
+// Closest hit (kAny = false) or any hit (kAny = true) through the wide tree.
+// The triangle test and its operands are those of the binary traversal
+// (hit_soup on the same (p0, e1, e2)), so the nearest hit is the same; only
+// which of two exactly tied triangles wins can differ. Groups: the current
+// node group descends into its nearest hit child, pushing the rest; triangle
+// groups are tested one triangle per step and deferred to the stack while
+// fewer than kWidePostpone lanes of the warp have one (Ylitie, Karras and
+// Laine 2017, compressed wide BVHs).
+template <bool kAny>
+LUC_D bool wide_trace(const DevScene& s, V3 o, V3 d, float tmin, float& tmax, float& bu, float& bv, uint32_t& btri,
+                      TravCount& tc) {
+    const V3 inv = safe_inv_dir(d);
+    const uint32_t oct = (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) | (inv.z < 0.0f ? 4u : 0u);
+    uint2 stack[kWideStack];
+    int sp = 0;
+    // Start from a virtual parent whose only child (slot 0, internal) is the
+    // root, so the root's own triangles go through the triangle phase too.
+    uint2 g = make_uint2(0u, (1u << 8) | (1u << oct)), t = make_uint2(0u, 0u);
+    bool found = false;
+    // Each node and triangle is visited at most once per ray in a tree; the
+    // guard only bounds the loop should the arrays ever not form one.
+    for (uint32_t guard = 0; guard < (1u << 24); ++guard) {
+        if (!(g.x & kWideTri) && (g.y & 0xFFu)) {
+            const uint32_t k = __ffs(g.y & 0xFFu) - 1u;
+            g.y &= ~(1u << k);
+            const uint32_t slot = k ^ oct;
+            const uint32_t child = g.x + __popc((g.y >> 8) & ((1u << slot) - 1u));
+            if ((g.y & 0xFFu) && sp < kWideStack) stack[sp++] = g;
+            wide_node(s.wnodes, child, o, inv, oct, tmin, tmax, g, t);
+            tc.nodes++;
+        } else if (g.x & kWideTri) {
+            t = g;
+            g = make_uint2(0u, 0u);
+        }
+        while (t.y) {
+            if (!kAny && (g.y & 0xFFu) && sp < kWideStack && __popc(__activemask()) < kWidePostpone) {
+                stack[sp++] = t;
+                break;
+            }
+            const uint32_t j = __ffs(t.y) - 1u;
+            t.y &= t.y - 1u;
+            const uint32_t k = (t.x & ~kWideTri) + j;
+            tc.tris++;
+            float th, uh, vh;
+            if (hit_soup(s.wsoup, k, o, d, tmin, tmax, th, uh, vh)) {
+                if (kAny) return true;
+                tmax = th;
+                bu = uh;
+                bv = vh;
+                btri = __float_as_uint(__ldg(s.wsoup + 3 * (size_t)k).w);
+                found = true;
+            }
+        }
+        if (!(g.y & 0xFFu)) {
+            if (sp == 0) break;
+            g = stack[--sp];
+        }
+    }
+    return found;
+}
+
 // ---------------------------------------------------------------- instancing
 // Root reference of the subtree at node i: (i, 0) if internal, else its leaf.
 LUC_D TRef node_ref(const DevScene& s, uint32_t i) {
@@ -461,6 +592,8 @@ LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, fl
     inst = 0u;
     if (kInst) {
         if (instances_closest(s, o, d, kTMin, best_t, bu, bv, tri, inst, tc)) id = tri;
+    } else if (s.wnodes) {
+        if (wide_trace<false>(s, o, d, kTMin, best_t, bu, bv, tri, tc)) id = tri;
     } else if (s.num_nodes > 0 && bvh_closest(s, TRef{s.root_count ? s.root_first : 0u, s.root_count}, o, d, kTMin,
                                               best_t, bu, bv, tri, tc)) {
         id = tri;
@@ -509,6 +642,11 @@ LUC_D bool occluded(const DevScene& s, V3 o, V3 d, float tmax, TravCount& tc) {
             if (hit_triangle(vtx(s, tr.i0), vtx(s, tr.i1), vtx(s, tr.i2), o, d, kTMin, tmax, th, uh, vh)) return true;
         }
         return false;
+    }
+    if (s.wnodes) {
+        float tm = tmax, bu, bv;
+        uint32_t bt;
+        return wide_trace<true>(s, o, d, kTMin, tm, bu, bv, bt, tc);
     }
     return bvh_any(s, TRef{s.root_count ? s.root_first : 0u, s.root_count}, o, d, kTMin, tmax, tc);
 }

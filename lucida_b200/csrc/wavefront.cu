@@ -22,7 +22,11 @@
 
 namespace luc {
 
-__device__ __forceinline__ void store4(float4* p, V3 v, float w) { *p = make_float4(v.x, v.y, v.z, w); }
+// Path-state records are touched once per stage and the pool is far larger
+// than L2: load and store them evict-first (ld/st.global.cs) so the BVH nodes
+// and the triangle soup the traversal re-reads stay L2-resident.
+__device__ __forceinline__ void store4(float4* p, V3 v, float w) { __stcs(p, make_float4(v.x, v.y, v.z, w)); }
+__device__ __forceinline__ float4 ld4(const float4* p) { return __ldcs(p); }
 
 // One atomic per warp: fold this thread's traversal counters into stat[k..k+2].
 __device__ __forceinline__ void flush_counts(unsigned long long* stat, uint32_t rays, const TravCount& tc) {
@@ -67,8 +71,8 @@ __device__ __forceinline__ void generate_one(PathState& ps, const FrameParams& f
     }
     store4(ps.o_pdf + p, origin, 0.0f);
     store4(ps.dir + p, dir, 0.0f);
-    ps.thr[p] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(smp.state));
-    ps.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    __stcs(ps.thr + p, make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(smp.state)));
+    __stcs(ps.rad + p, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
     store4(ps.prev + p, origin, 0.0f);
     if (fp.guides) {
         ps.galb[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -123,12 +127,12 @@ __global__ void __launch_bounds__(kThreads) k_extend(PathState ps, const __grid_
     uint32_t rays = 0;
     auto trace = [&](uint32_t i) {
         uint32_t p = depth == 0 ? i : queue[i];
-        float4 o4 = ps.o_pdf[p], d4 = ps.dir[p];
+        float4 o4 = ld4(ps.o_pdf + p), d4 = ld4(ps.dir + p);
         const DevScene& sc = kBatch ? bd.scenes[bd.segs[ps.seg[p]].scene] : sc_arg;
         float t, u, v;
         uint32_t inst;
         uint32_t id = closest_hit<kInst>(sc, xyz(o4), xyz(d4), t, u, v, inst, tc);
-        ps.hit[p] = make_float4(t, u, v, __uint_as_float(id));
+        __stcs(ps.hit + p, make_float4(t, u, v, __uint_as_float(id)));
         if (kInst) ps.hinst[p] = inst;
         ++rays;
     };
@@ -210,7 +214,8 @@ __global__ void __launch_bounds__(128, 4) k_shade(PathState ps, const __grid_con
             const uint32_t sbase = kBatch ? seg->sample_base : sbase_arg;
             const uint32_t q = kBatch ? p - seg->first : p;  // path index within its own frame
             const bool last = depth + 1 >= fp.max_depth;
-            float4 o4 = ps.o_pdf[p], d4 = ps.dir[p], h4 = ps.hit[p], t4 = ps.thr[p], r4 = ps.rad[p];
+            float4 o4 = ld4(ps.o_pdf + p), d4 = ld4(ps.dir + p), h4 = ld4(ps.hit + p), t4 = ld4(ps.thr + p),
+                   r4 = ld4(ps.rad + p);
             V3 dir = xyz(d4), thr = xyz(t4), rad = xyz(r4);
             float prev_pdf = o4.w;
             uint32_t id = __float_as_uint(h4.w);
@@ -402,7 +407,7 @@ __global__ void __launch_bounds__(128, 4) k_shade(PathState ps, const __grid_con
                                     V3 norg = offset_ray_origin(hit.position, wl.z < 0.0f ? -hit.gnormal : hit.gnormal);
                                     store4(ps.o_pdf + p, norg, pc);
                                     store4(ps.dir + p, wd, 0.0f);
-                                    ps.thr[p] = make_float4(thr.x, thr.y, thr.z, __uint_as_float(smp.state));
+                                    __stcs(ps.thr + p, make_float4(thr.x, thr.y, thr.z, __uint_as_float(smp.state)));
                                     uint32_t slot1 = 0u;
                                     if (gv && fp.rec_cap) {
                                         // Opportunistic warp aggregation of the two counters.
@@ -447,7 +452,7 @@ __global__ void __launch_bounds__(128, 4) k_shade(PathState ps, const __grid_con
                                 V3 norg = offset_ray_origin(hit.position, bs.wi.z < 0.0f ? -hit.gnormal : hit.gnormal);
                                 store4(ps.o_pdf + p, norg, bs.pdf);
                                 store4(ps.dir + p, ndir, 0.0f);
-                                ps.thr[p] = make_float4(thr.x, thr.y, thr.z, __uint_as_float(smp.state));
+                                __stcs(ps.thr + p, make_float4(thr.x, thr.y, thr.z, __uint_as_float(smp.state)));
                                 store4(ps.prev + p, hit.position, 0.0f);
                                 survive = true;
                             }
@@ -479,12 +484,12 @@ __global__ void __launch_bounds__(kThreads) k_connect(PathState ps, const __grid
     TravCount tc;
     uint32_t rays = 0;
     auto trace = [&](uint32_t i) {
-        float4 o4 = ps.sh_o[i], d4 = ps.sh_d[i];
+        float4 o4 = ld4(ps.sh_o + i), d4 = ld4(ps.sh_d + i);
         uint32_t p = __float_as_uint(d4.w);
         const DevScene& sc = kBatch ? bd.scenes[bd.segs[ps.seg[p]].scene] : sc_arg;
         if (!occluded<kInst>(sc, xyz(o4), xyz(d4), o4.w, tc)) {
-            float4 c4 = ps.sh_c[i], r4 = ps.rad[p];
-            ps.rad[p] = make_float4(r4.x + c4.x, r4.y + c4.y, r4.z + c4.z, 0.0f);
+            float4 c4 = ld4(ps.sh_c + i), r4 = ld4(ps.rad + p);
+            __stcs(ps.rad + p, make_float4(r4.x + c4.x, r4.y + c4.y, r4.z + c4.z, 0.0f));
         }
         ++rays;
     };

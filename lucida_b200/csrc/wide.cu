@@ -1,0 +1,352 @@
+// Compressed 8-wide BVH, collapsed on the device from the binary tree that
+// the traversal layout is derived from (the device LBVH, or a caller's tree).
+// No counterpart in Lucida, whose kernels walk the binary GpuBvhNode array
+// (bvh.rs:1045-1193); this is a re-layout of the same tree for the wide
+// traversal in scene_dev.cuh (node format documented there).
+//
+// Build, level by level (one launch per level of the wide tree, plus a
+// one-thread launch that advances the level range):
+//   * a task is a binary internal node, or a leaf chunk (a binary leaf with
+//     more than 4 triangles, 28 at a time); each task becomes one wide node;
+//   * an internal task opens children greedily, largest surface area first,
+//     until it has 8 children or none can be opened (a leaf with <= 4
+//     triangles stays a leaf slot, and a node holds at most 32 triangles);
+//   * children are placed in slots by octant (greedy assignment of children
+//     to the corner they lie towards), internal children get consecutive
+//     wide indices in slot order, leaf triangles consecutive soup slots;
+//   * quantization in double: origin two quanta below the node's box, one
+//     quantum of slack outside every child box, so quantized boxes contain the
+//     binary boxes (which carry the reference's magnitude-relative padding).
+// Node and soup slots are claimed with atomics, so the layout order depends
+// on scheduling; traversal results do not (slot order is deterministic and a
+// hit reports the triangle's leaf-order index stored in the soup).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "ctx.cuh"
+
+namespace luc {
+namespace {
+
+constexpr uint32_t kSmallLeaf = 4;   // leaves up to this size are leaf slots
+constexpr uint32_t kChunkTris = 28;  // triangles per leaf chunk node before chaining
+constexpr uint32_t kNodeTris = 32;   // triangle budget of one wide node
+constexpr uint32_t kKindInternal = 0, kKindChunk = 1;
+
+// ctr words
+constexpr int kWcBegin = 0, kWcEnd = 1, kWcAlloc = 2, kWcSoup = 3, kWcErr = 4, kWcWords = 8;
+constexpr uint32_t kErrTree = 1, kErrCapacity = 2;
+
+struct Child {
+    float lo[3], hi[3];
+    uint32_t node;   // binary node index (box source)
+    uint32_t first, count;
+    uint32_t kind;   // 0 internal binary node, 1 chunk (internal wide child), 2 leaf slot
+};
+
+__device__ __forceinline__ void node_box(const float4* nodes, uint32_t i, Child& c) {
+    float4 a = nodes[2 * (size_t)i], b = nodes[2 * (size_t)i + 1];
+    c.lo[0] = a.x; c.lo[1] = a.y; c.lo[2] = a.z;
+    c.hi[0] = b.x; c.hi[1] = b.y; c.hi[2] = b.z;
+}
+
+// Child record for binary node i (internal, small leaf or big leaf).
+__device__ __forceinline__ bool make_child(const float4* nodes, uint32_t num_nodes, uint32_t num_tris, uint32_t i,
+                                           Child& c) {
+    if (i >= num_nodes) return false;
+    node_box(nodes, i, c);
+    const uint32_t lf = __float_as_uint(nodes[2 * (size_t)i].w), cnt = __float_as_uint(nodes[2 * (size_t)i + 1].w);
+    c.node = i;
+    if (cnt == 0) {
+        c.kind = kKindInternal;
+        c.first = lf;
+        c.count = 0;
+        return lf + 1u < num_nodes && lf > i;  // children after their parent (preorder)
+    }
+    if ((uint64_t)lf + cnt > num_tris) return false;
+    c.first = lf;
+    c.count = cnt;
+    c.kind = cnt <= kSmallLeaf ? 2u : kKindChunk;
+    return true;
+}
+
+__device__ __forceinline__ float half_area(const Child& c) {
+    float dx = c.hi[0] - c.lo[0], dy = c.hi[1] - c.lo[1], dz = c.hi[2] - c.lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__global__ void k_wide_init(const float4* __restrict__ nodes, uint4* __restrict__ tasks, uint32_t* __restrict__ ctr) {
+    const uint32_t cnt = __float_as_uint(nodes[1].w), lf = __float_as_uint(nodes[0].w);
+    tasks[0] = cnt == 0 ? make_uint4(0u, lf, 0u, kKindInternal) : make_uint4(0u, lf, cnt, kKindChunk);
+    ctr[kWcBegin] = 0;
+    ctr[kWcEnd] = 1;
+    ctr[kWcAlloc] = 1;
+    ctr[kWcSoup] = 0;
+    ctr[kWcErr] = 0;
+}
+
+__global__ void k_wide_advance(uint32_t* __restrict__ ctr) {
+    ctr[kWcBegin] = ctr[kWcEnd];
+    ctr[kWcEnd] = ctr[kWcAlloc];
+}
+
+__global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ nodes, uint32_t num_nodes,
+                                                    const float4* __restrict__ soup, uint32_t num_tris,
+                                                    uint4* __restrict__ tasks, float4* __restrict__ wnodes,
+                                                    float4* __restrict__ wsoup, uint32_t cap,
+                                                    uint32_t* __restrict__ ctr) {
+    if (ctr[kWcErr]) return;  // a failed level ends the build
+    // Claims past the capacity failed (and flagged); never read beyond it.
+    const uint32_t begin = ctr[kWcBegin], end = min(ctr[kWcEnd], cap);
+    for (uint32_t w = begin + blockIdx.x * blockDim.x + threadIdx.x; w < end; w += gridDim.x * blockDim.x) {
+        const uint4 task = tasks[w];
+        Child ch[8];
+        uint32_t n = 0;
+        bool ok = true;
+        if (task.w == kKindInternal) {
+            ok = make_child(nodes, num_nodes, num_tris, task.y, ch[0]) &&
+                 make_child(nodes, num_nodes, num_tris, task.y + 1u, ch[1]);
+            n = 2;
+            uint32_t tris = (ch[0].kind == 2u ? ch[0].count : 0u) + (ch[1].kind == 2u ? ch[1].count : 0u);
+            // Open the largest internal child while the node has room.
+            while (ok && n < 8) {
+                int best = -1;
+                float best_a = -1.0f;
+                for (uint32_t k = 0; k < n; ++k) {
+                    if (ch[k].kind != kKindInternal) continue;
+                    float a = half_area(ch[k]);
+                    if (a > best_a) {
+                        // The grandchildren's small leaves must fit the triangle budget.
+                        Child l, r;
+                        if (!make_child(nodes, num_nodes, num_tris, ch[k].first, l) ||
+                            !make_child(nodes, num_nodes, num_tris, ch[k].first + 1u, r)) {
+                            ok = false;
+                            break;
+                        }
+                        uint32_t add = (l.kind == 2u ? l.count : 0u) + (r.kind == 2u ? r.count : 0u);
+                        if (tris + add > kNodeTris) continue;
+                        best = (int)k;
+                        best_a = a;
+                    }
+                }
+                if (!ok || best < 0) break;
+                Child l, r;
+                make_child(nodes, num_nodes, num_tris, ch[best].first, l);
+                make_child(nodes, num_nodes, num_tris, ch[best].first + 1u, r);
+                tris += (l.kind == 2u ? l.count : 0u) + (r.kind == 2u ? r.count : 0u);
+                ch[best] = l;
+                ch[n++] = r;
+            }
+        } else {
+            // Leaf chunk: up to 7 (or 8, for the last) slots of 4 triangles,
+            // every slot with the binary leaf's box; the rest chains on.
+            Child box;
+            node_box(nodes, task.x, box);
+            uint32_t first = task.y, rem = task.z;
+            const uint32_t here = rem <= kNodeTris ? rem : kChunkTris;
+            for (uint32_t k = 0; k < here; k += kSmallLeaf) {
+                ch[n] = box;
+                ch[n].node = task.x;
+                ch[n].first = first + k;
+                ch[n].count = min(kSmallLeaf, here - k);
+                ch[n].kind = 2u;
+                ++n;
+            }
+            if (rem > here) {
+                ch[n] = box;
+                ch[n].node = task.x;
+                ch[n].first = first + here;
+                ch[n].count = rem - here;
+                ch[n].kind = kKindChunk;
+                ++n;
+            }
+        }
+        if (!ok) {
+            atomicOr(ctr + kWcErr, kErrTree);
+            continue;
+        }
+        // Node box and octant slot assignment.
+        float lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = ch[0].lo[a];
+            hi[a] = ch[0].hi[a];
+            for (uint32_t k = 1; k < n; ++k) {
+                lo[a] = fminf(lo[a], ch[k].lo[a]);
+                hi[a] = fmaxf(hi[a], ch[k].hi[a]);
+            }
+        }
+        float cost[8][8];
+        for (uint32_t k = 0; k < n; ++k) {
+            float v[3];
+            for (int a = 0; a < 3; ++a) v[a] = (ch[k].lo[a] + ch[k].hi[a]) - (lo[a] + hi[a]);
+            for (uint32_t s = 0; s < 8; ++s)
+                cost[k][s] = -((s & 1u ? v[0] : -v[0]) + (s & 2u ? v[1] : -v[1]) + (s & 4u ? v[2] : -v[2]));
+        }
+        int slot_of[8];
+        uint32_t used_slots = 0, done = 0;
+        for (uint32_t r = 0; r < n; ++r) {
+            float bc = 3.4e38f;
+            int bk = -1, bs = -1;
+            for (uint32_t k = 0; k < n; ++k) {
+                if (done & (1u << k)) continue;
+                for (uint32_t s = 0; s < 8; ++s) {
+                    if (used_slots & (1u << s)) continue;
+                    if (cost[k][s] < bc || bk < 0) {
+                        bc = cost[k][s];
+                        bk = (int)k;
+                        bs = (int)s;
+                    }
+                }
+            }
+            slot_of[bk] = bs;
+            done |= 1u << bk;
+            used_slots |= 1u << bs;
+        }
+        int child_at[8];
+        for (int s = 0; s < 8; ++s) child_at[s] = -1;
+        for (uint32_t k = 0; k < n; ++k) child_at[slot_of[k]] = (int)k;
+        uint32_t imask = 0, ntri = 0;
+        for (int s = 0; s < 8; ++s) {
+            const int k = child_at[s];
+            if (k < 0) continue;
+            if (ch[k].kind == 2u) ntri += ch[k].count;
+            else imask |= 1u << s;
+        }
+        const uint32_t nint = __popc(imask);
+        const uint32_t cbase = nint ? atomicAdd(ctr + kWcAlloc, nint) : 0u;
+        const uint32_t tbase = ntri ? atomicAdd(ctr + kWcSoup, ntri) : 0u;
+        if ((nint && (uint64_t)cbase + nint > cap) || (uint64_t)tbase + ntri > num_tris) {
+            atomicOr(ctr + kWcErr, kErrCapacity);
+            continue;
+        }
+        // Quantization (double: exact for these magnitudes).
+        uint32_t ebits = 0;
+        float p[3];
+        double scale[3];
+        for (int a = 0; a < 3; ++a) {
+            const double ext = (double)hi[a] - (double)lo[a];
+            int ex = -126;
+            if (ext > 0.0) {
+                int e2;
+                frexp(ext / 250.0, &e2);  // ext / 250 < 2^e2
+                ex = max(-126, min(120, e2));
+            }
+            // No finer than 1/64 of the coordinates' ulp: the loop below then
+            // needs at most a few coarsening steps.
+            const double mag = fmax(fabs((double)lo[a]), fabs((double)hi[a]));
+            if (mag > 0.0) {
+                int em;
+                frexp(mag, &em);  // ulp(mag) = 2^(em - 24)
+                ex = max(ex, min(120, em - 24 - 6));
+            }
+            // Origin at least two quanta below the box, rounded down to float;
+            // coarsen the grid until the box's top plane fits in 253 quanta
+            // (the float origin can sit up to an ulp of the coordinates lower).
+            float pf = 0.0f;
+            for (;;) {
+                scale[a] = ldexp(1.0, ex);
+                const double pd = (double)lo[a] - 2.0 * scale[a];
+                pf = (float)pd;
+                if ((double)pf > pd) pf = nextafterf(pf, -3.4e38f);
+                if (ex >= 120 || ceil(((double)hi[a] - (double)pf) / scale[a]) + 1.0 <= 253.0) break;
+                ++ex;
+            }
+            p[a] = pf;
+            ebits |= (uint32_t)(ex + 127) << (8 * a);
+        }
+        ebits |= imask << 24;
+        uint32_t qlo[3][2] = {{0, 0}, {0, 0}, {0, 0}}, qhi[3][2] = {{0, 0}, {0, 0}, {0, 0}}, meta[2] = {0, 0};
+        uint32_t off = 0, rank = 0;
+        for (int s = 0; s < 8; ++s) {
+            const int k = child_at[s];
+            uint32_t l8[3], h8[3];
+            if (k < 0) {
+                for (int a = 0; a < 3; ++a) {
+                    l8[a] = 255u;  // empty: near plane beyond far plane, never hit
+                    h8[a] = 0u;
+                }
+            } else {
+                for (int a = 0; a < 3; ++a) {
+                    double ql = floor(((double)ch[k].lo[a] - (double)p[a]) / scale[a]) - 1.0;
+                    double qh = ceil(((double)ch[k].hi[a] - (double)p[a]) / scale[a]) + 1.0;
+                    l8[a] = (uint32_t)fmax(0.0, fmin(255.0, ql));
+                    h8[a] = (uint32_t)fmax(0.0, fmin(255.0, qh));
+                }
+                if (ch[k].kind == 2u) {
+                    meta[s >> 2] |= ((ch[k].count << 5) | off) << (8 * (s & 3));
+                    for (uint32_t i = 0; i < ch[k].count; ++i) {
+                        const size_t src = 3 * (size_t)(ch[k].first + i), dst = 3 * (size_t)(tbase + off + i);
+                        float4 q0 = soup[src];
+                        q0.w = __uint_as_float(ch[k].first + i);
+                        wsoup[dst] = q0;
+                        wsoup[dst + 1] = soup[src + 1];
+                        wsoup[dst + 2] = soup[src + 2];
+                    }
+                    off += ch[k].count;
+                } else {
+                    tasks[cbase + rank] = ch[k].kind == kKindInternal
+                                              ? make_uint4(ch[k].node, ch[k].first, 0u, kKindInternal)
+                                              : make_uint4(ch[k].node, ch[k].first, ch[k].count, kKindChunk);
+                    ++rank;
+                }
+            }
+            for (int a = 0; a < 3; ++a) {
+                qlo[a][s >> 2] |= l8[a] << (8 * (s & 3));
+                qhi[a][s >> 2] |= h8[a] << (8 * (s & 3));
+            }
+        }
+        float4* o = wnodes + 5 * (size_t)w;
+        o[0] = make_float4(p[0], p[1], p[2], __uint_as_float(ebits));
+        o[1] = make_float4(__uint_as_float(cbase), __uint_as_float(tbase), __uint_as_float(meta[0]),
+                           __uint_as_float(meta[1]));
+        o[2] = make_float4(__uint_as_float(qlo[0][0]), __uint_as_float(qlo[0][1]), __uint_as_float(qlo[1][0]),
+                           __uint_as_float(qlo[1][1]));
+        o[3] = make_float4(__uint_as_float(qlo[2][0]), __uint_as_float(qlo[2][1]), __uint_as_float(qhi[0][0]),
+                           __uint_as_float(qhi[0][1]));
+        o[4] = make_float4(__uint_as_float(qhi[1][0]), __uint_as_float(qhi[1][1]), __uint_as_float(qhi[2][0]),
+                           __uint_as_float(qhi[2][1]));
+    }
+}
+
+}  // namespace
+}  // namespace luc
+
+// Collapse the resident binary tree (c->nodes, c->soup in leaf order) into
+// c->wnodes / c->wsoup. Leaves c->wide_nodes = 0 (binary traversal) when the
+// tree is deeper than the level budget; fails on a malformed tree.
+int32_t luc_build_wide(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris) {
+    using namespace luc;
+    c->wide_nodes = 0;
+    if (!num_nodes || !num_tris) return LUC_OK;
+    const uint64_t cap = 2ull * num_nodes + num_tris / kChunkTris + 8;
+    if (cap > 0x7FFFFFFFull) return LUC_OK;
+    cudaStream_t s = c->stream;
+    LUC_CUDA(c, c->wnodes.ensure(cap * 80), "alloc wide nodes");
+    LUC_CUDA(c, c->wsoup.ensure((size_t)num_tris * 48), "alloc wide soup");
+    LUC_CUDA(c, c->wtasks.ensure(cap * 16), "alloc wide tasks");
+    LUC_CUDA(c, c->wctr.ensure(kWcWords * 4), "alloc wide counters");
+    uint32_t* ctr = c->wctr.as<uint32_t>();
+    k_wide_init<<<1, 1, 0, s>>>(c->nodes.as<float4>(), c->wtasks.as<uint4>(), ctr);
+    const int grid = c->num_sms * 8;
+    constexpr int kLevelsPerSync = 12, kMaxLevels = 240;
+    uint32_t h[kWcWords] = {};
+    for (int level = 0; level < kMaxLevels; level += kLevelsPerSync) {
+        for (int k = 0; k < kLevelsPerSync; ++k) {
+            k_wide_level<<<grid, 128, 0, s>>>(c->nodes.as<float4>(), num_nodes, c->soup.as<float4>(), num_tris,
+                                              c->wtasks.as<uint4>(), c->wnodes.as<float4>(), c->wsoup.as<float4>(),
+                                              (uint32_t)cap, ctr);
+            k_wide_advance<<<1, 1, 0, s>>>(ctr);
+        }
+        LUC_CUDA(c, cudaGetLastError(), "wide build");
+        LUC_CUDA(c, cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, s), "wide build counters");
+        LUC_CUDA(c, cudaStreamSynchronize(s), "wide build");
+        if (h[kWcErr] & kErrTree) return luc_fail(c, LUC_ERR_VALIDATION, "BVH: malformed tree (wide collapse)");
+        if (h[kWcErr]) return LUC_OK;  // capacity: keep the binary traversal
+        if (h[kWcBegin] == h[kWcEnd]) break;
+    }
+    if (h[kWcBegin] != h[kWcEnd] || h[kWcSoup] != num_tris) return LUC_OK;  // too deep: binary traversal
+    c->wide_nodes = h[kWcAlloc];
+    return LUC_OK;
+}

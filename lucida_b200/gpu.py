@@ -204,13 +204,33 @@ class Gpu:
 
     def read_scene(self, which: str) -> np.ndarray:
         """The resident scene's 'nodes', 'triangles' or 'primitives' (instance
-        rows after the analytic primitives)."""
-        code, dt = {"nodes": (0, L.BVH_NODE), "triangles": (1, L.TRIANGLE), "primitives": (2, L.PRIMITIVE)}[which]
+        rows after the analytic primitives); 'wide_nodes' (uint32 rows of 20
+        words) and 'wide_soup' (float32 rows of 12) of the compressed 8-wide
+        tree, empty when the scene traverses the binary tree."""
+        code, dt = {"nodes": (0, L.BVH_NODE), "triangles": (1, L.TRIANGLE), "primitives": (2, L.PRIMITIVE),
+                    "wide_nodes": (3, np.dtype((np.uint32, 20))), "wide_soup": (4, np.dtype((np.float32, 12)))}[which]
         n = C.c_uint64(0)
         check(self._h, self._lib.luc_read_scene(self._h, code, None, 0, C.byref(n)))
         out = np.zeros(n.value // dt.itemsize, dt)
         check(self._h, self._lib.luc_read_scene(self._h, code, ptr(out), out.nbytes, C.byref(n)))
         return out
+
+    def intersect(self, origins, directions, t_max=None):
+        """Closest hits of rays against the resident scene: (t, u, v, id)
+        with id uint32 (0xFFFFFFFF on a miss). With `t_max`, the occlusion
+        query within (1e-4, t_max) instead: a bool per ray."""
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(directions, np.float32).reshape(-1, 3)
+        rays = np.zeros((len(o), 8), np.float32)
+        rays[:, 0:3], rays[:, 4:7] = o, d
+        if t_max is None:
+            out = np.zeros((len(o), 4), np.float32)
+            check(self._h, self._lib.luc_intersect(self._h, ptr(rays), len(o), 0, ptr(out)))
+            return out[:, 0], out[:, 1], out[:, 2], out[:, 3].view(np.uint32)
+        rays[:, 3] = np.broadcast_to(np.asarray(t_max, np.float32), len(o))
+        occ = np.zeros(len(o), np.uint32)
+        check(self._h, self._lib.luc_intersect(self._h, ptr(rays), len(o), 1, ptr(occ)))
+        return occ.astype(bool)
 
     def stats(self) -> RenderStats:
         s = RenderStats()

@@ -102,6 +102,7 @@ _SIGS = {
                                   C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "luc_eval_env": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p, C.c_void_p,
                                  C.c_void_p]),
+    "luc_intersect": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p]),
     "luc_sort_u32_static": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_char_p,
                                         C.c_uint32]),
     "luc_sort_u32_static_max": (C.c_uint32, []),
