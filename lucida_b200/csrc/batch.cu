@@ -118,8 +118,10 @@ int32_t run_plan(luc_ctx* c, const luc_batch_job* jobs, uint32_t n, const Plan& 
     if (c->rs.shade_blocks == 0) query_occupancy(c->rs);
     std::vector<DevScene> scenes(n);
     std::vector<BatchJobDev> jd(n);
+    bool wide = true;
     for (uint32_t j = 0; j < n; ++j) {
         scenes[j] = jobs[j].scene->scene;
+        wide = wide && (scenes[j].wnodes || scenes[j].num_tris == 0);
         scenes[j].background = ld3(jobs[j].uniforms.background);
         scenes[j].reference_shadows = false;
         jd[j] = BatchJobDev{job_params(jobs[j]), j, (GpuAccum*)jobs[j].accum_dev};
@@ -140,7 +142,7 @@ int32_t run_plan(luc_ctx* c, const luc_batch_job* jobs, uint32_t n, const Plan& 
         BatchDev bd{c->b_scenes.as<DevScene>(), c->b_jobs.as<BatchJobDev>(), c->b_segs.as<BatchSegDev>() + x.seg_begin,
                     x.seg_count, chunk};
         record_wave(c->rs, bd, c->b_pixoff.as<uint32_t>() + x.seg_begin, x.num_paths, x.total_pixels, x.max_depth,
-                    (int)block, c->own_stream);
+                    (int)block, wide, c->own_stream);
         cudaEventRecordWithFlags(ev[w + 1], c->own_stream, cudaEventRecordExternal);
     }
     cudaError_t ce = cudaStreamEndCapture(c->own_stream, &graph);

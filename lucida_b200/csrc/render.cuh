@@ -104,6 +104,7 @@ struct RenderState {
     // Resident blocks per SM of each stage kernel (single-level / instanced).
     int extend_blocks = 0, connect_blocks = 0, shade_blocks = 0, shade_blocks_guided = 0;
     int extend_blocks_inst = 0, connect_blocks_inst = 0, shade_blocks_inst = 0, shade_blocks_guided_inst = 0;
+    int extend_blocks_bin = 0, connect_blocks_bin = 0;  // single-level scenes on the binary tree
     uint64_t launches = 0;
 };
 
@@ -143,9 +144,11 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
                   StageTimer* timer, const GuideTrain* gt);
 // One wave of a batched render (wavefront.cu); `block` is the EXTEND /
 // CONNECT block size (64, 128 or 256).
+// `wide`: every scene of the batch traverses a wide tree (or has no
+// triangles), so the wide-only traversal kernels serve them all.
 void record_wave(RenderState& rs, const BatchDev& bd, const uint32_t* pix_off, uint32_t num_paths,
-                 uint32_t total_pixels, uint32_t max_depth, int block, cudaStream_t s);
-int batch_blocks_per_sm(int block, bool connect);
+                 uint32_t total_pixels, uint32_t max_depth, int block, bool wide, cudaStream_t s);
+int batch_blocks_per_sm(int block, bool connect, bool wide);
 // guide.cu: per-depth inference and the post-batch training step.
 void launch_guide_infer(const RenderState& rs, const DevScene& sc, const FrameParams& fp, uint32_t depth,
                         cudaStream_t s);

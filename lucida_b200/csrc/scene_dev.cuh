@@ -342,7 +342,6 @@ LUC_D bool bvh_any(const DevScene& s, TRef root, V3 o, V3 d, float tmin, float t
 // hit bits are stored and visited.
 constexpr uint32_t kWideTri = 0x80000000u;  // group tag: triangle group
 constexpr int kWideStack = 64;
-constexpr int kWidePostpone = 8;  // fewer lanes than this with triangles: defer them
 
 LUC_D float wide_q(uint32_t word, uint32_t j) {  // byte j of word as an exact float
     return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7440u | j)) - 8388608.0f;
@@ -394,10 +393,10 @@ LUC_D void wide_node(const float4* __restrict__ wn, uint32_t node, V3 o, V3 inv,
 // The triangle test and its operands are those of the binary traversal
 // (hit_soup on the same (p0, e1, e2)), so the nearest hit is the same; only
 // which of two exactly tied triangles wins can differ. Groups: the current
-// node group descends into its nearest hit child, pushing the rest; triangle
-// groups are tested one triangle per step and deferred to the stack while
-// fewer than kWidePostpone lanes of the warp have one (Ylitie, Karras and
-// Laine 2017, compressed wide BVHs).
+// node group descends into its nearest hit child, pushing the rest; a node's
+// triangle group is tested right after the node, one triangle per step
+// (after Ylitie, Karras and Laine 2017, compressed wide BVHs; their deferral
+// of triangle groups while few lanes have one measured slower here).
 template <bool kAny>
 LUC_D bool wide_trace(const DevScene& s, V3 o, V3 d, float tmin, float& tmax, float& bu, float& bv, uint32_t& btri,
                       TravCount& tc) {
@@ -425,10 +424,6 @@ LUC_D bool wide_trace(const DevScene& s, V3 o, V3 d, float tmin, float& tmax, fl
             g = make_uint2(0u, 0u);
         }
         while (t.y) {
-            if (!kAny && (g.y & 0xFFu) && sp < kWideStack && __popc(__activemask()) < kWidePostpone) {
-                stack[sp++] = t;
-                break;
-            }
             const uint32_t j = __ffs(t.y) - 1u;
             t.y &= t.y - 1u;
             const uint32_t k = (t.x & ~kWideTri) + j;
@@ -570,8 +565,10 @@ LUC_D bool instances_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax, 
 // In an instanced scene the instances replace the single-level triangle path
 // (scene.rs:489-501) and `inst` receives the hit's instance (s.inst index).
 // kInst selects the instanced code at compile time, so kernels launched for
-// single-level scenes carry none of its registers.
-template <bool kInst>
+// single-level scenes carry none of its registers; likewise kWide for the
+// single-level tree: 1 wide tree only (scenes whose triangles have one), 0
+// binary tree only, 2 whichever the scene has.
+template <bool kInst, int kWide = 2>
 LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, float& v, uint32_t& inst,
                            TravCount& tc) {
     float best_t = kTMax;
@@ -592,7 +589,9 @@ LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, fl
     inst = 0u;
     if (kInst) {
         if (instances_closest(s, o, d, kTMin, best_t, bu, bv, tri, inst, tc)) id = tri;
-    } else if (s.wnodes) {
+    } else if (kWide == 1) {
+        if (s.wnodes && wide_trace<false>(s, o, d, kTMin, best_t, bu, bv, tri, tc)) id = tri;
+    } else if (kWide == 2 && s.wnodes) {
         if (wide_trace<false>(s, o, d, kTMin, best_t, bu, bv, tri, tc)) id = tri;
     } else if (s.num_nodes > 0 && bvh_closest(s, TRef{s.root_count ? s.root_first : 0u, s.root_count}, o, d, kTMin,
                                               best_t, bu, bv, tri, tc)) {
@@ -616,8 +615,8 @@ LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, fl
     return id;
 }
 
-// Scene::occluded (scene.rs:577-606).
-template <bool kInst>
+// Scene::occluded (scene.rs:577-606). kWide as for closest_hit.
+template <bool kInst, int kWide = 2>
 LUC_D bool occluded(const DevScene& s, V3 o, V3 d, float tmax, TravCount& tc) {
     for (uint32_t i = 0; i < s.num_prims; ++i) {
         const GpuPrimitive& p = s.prims[i];
@@ -635,7 +634,8 @@ LUC_D bool occluded(const DevScene& s, V3 o, V3 d, float tmax, TravCount& tc) {
             if (bvh_any(s, node_ref(s, s.blas_roots[b]), o, d, kTMin, tmax, tc)) return true;
         return false;
     }
-    if (s.num_nodes == 0) {
+    if (kWide == 1 && !s.wnodes) return false;  // no triangles
+    if (kWide != 1 && s.num_nodes == 0) {
         for (uint32_t k = 0; k < s.num_tris; ++k) {
             GpuTriangle tr = s.tris[k];
             float th, uh, vh;
@@ -643,7 +643,7 @@ LUC_D bool occluded(const DevScene& s, V3 o, V3 d, float tmax, TravCount& tc) {
         }
         return false;
     }
-    if (s.wnodes) {
+    if (kWide == 1 || (kWide == 2 && s.wnodes)) {
         float tm = tmax, bu, bv;
         uint32_t bt;
         return wide_trace<true>(s, o, d, kTMin, tm, bu, bv, bt, tc);

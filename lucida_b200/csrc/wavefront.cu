@@ -116,8 +116,12 @@ __global__ void __launch_bounds__(256) k_generate_batch(PathState ps, BatchDev b
 // instead of idling behind slow ones; with bd.chunk > 32 (batched renders,
 // chosen by the autotuner) a whole CTA claims `chunk` entries per pull.
 // kBatch: each ray's scene comes from its path's wave segment.
-template <bool kInst, bool kBatch, int kThreads>
-__global__ void __launch_bounds__(kThreads) k_extend(PathState ps, const __grid_constant__ DevScene sc_arg, FrameParams fp,
+// Wide-tree traversal runs at 32 warps per SM (64 registers): the loop is
+// latency-bound, and occupancy beat the registers the compiler would take.
+constexpr int wide_min_blocks(int threads) { return 1024 / threads; }
+
+template <bool kInst, bool kBatch, int kThreads, int kWide>
+__global__ void __launch_bounds__(kThreads, kWide == 1 ? wide_min_blocks(kThreads) : 1) k_extend(PathState ps, const __grid_constant__ DevScene sc_arg, FrameParams fp,
                                                      BatchDev bd, uint32_t depth) {
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
     const uint32_t* queue = ps.queue[depth & 1];
@@ -131,7 +135,7 @@ __global__ void __launch_bounds__(kThreads) k_extend(PathState ps, const __grid_
         const DevScene& sc = kBatch ? bd.scenes[bd.segs[ps.seg[p]].scene] : sc_arg;
         float t, u, v;
         uint32_t inst;
-        uint32_t id = closest_hit<kInst>(sc, xyz(o4), xyz(d4), t, u, v, inst, tc);
+        uint32_t id = closest_hit<kInst, kWide>(sc, xyz(o4), xyz(d4), t, u, v, inst, tc);
         __stcs(ps.hit + p, make_float4(t, u, v, __uint_as_float(id)));
         if (kInst) ps.hinst[p] = inst;
         ++rays;
@@ -475,8 +479,8 @@ __global__ void __launch_bounds__(128, 4) k_shade(PathState ps, const __grid_con
 
 // CONNECT (shaders/wavefront/connect.wgsl:58-84): any-hit shadow rays, with
 // the same persistent ray pull as EXTEND.
-template <bool kInst, bool kBatch, int kThreads>
-__global__ void __launch_bounds__(kThreads) k_connect(PathState ps, const __grid_constant__ DevScene sc_arg, BatchDev bd,
+template <bool kInst, bool kBatch, int kThreads, int kWide>
+__global__ void __launch_bounds__(kThreads, kWide == 1 ? wide_min_blocks(kThreads) : 1) k_connect(PathState ps, const __grid_constant__ DevScene sc_arg, BatchDev bd,
                                                       uint32_t depth) {
     const uint32_t len = ps.ctr[depth * kCtrStride + kCtrShadow];
     uint32_t* pull = ps.ctr + depth * kCtrStride + kCtrPullConnect;
@@ -487,7 +491,7 @@ __global__ void __launch_bounds__(kThreads) k_connect(PathState ps, const __grid
         float4 o4 = ld4(ps.sh_o + i), d4 = ld4(ps.sh_d + i);
         uint32_t p = __float_as_uint(d4.w);
         const DevScene& sc = kBatch ? bd.scenes[bd.segs[ps.seg[p]].scene] : sc_arg;
-        if (!occluded<kInst>(sc, xyz(o4), xyz(d4), o4.w, tc)) {
+        if (!occluded<kInst, kWide>(sc, xyz(o4), xyz(d4), o4.w, tc)) {
             float4 c4 = ld4(ps.sh_c + i), r4 = ld4(ps.rad + p);
             __stcs(ps.rad + p, make_float4(r4.x + c4.x, r4.y + c4.y, r4.z + c4.z, 0.0f));
         }
@@ -620,12 +624,14 @@ void query_occupancy(RenderState& rs) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, 128, 0);
         return b > 0 ? b : 8;
     };
-    rs.extend_blocks = occ((const void*)k_extend<false, false, 128>);
-    rs.connect_blocks = occ((const void*)k_connect<false, false, 128>);
+    rs.extend_blocks = occ((const void*)k_extend<false, false, 128, 1>);
+    rs.connect_blocks = occ((const void*)k_connect<false, false, 128, 1>);
+    rs.extend_blocks_bin = occ((const void*)k_extend<false, false, 128, 0>);
+    rs.connect_blocks_bin = occ((const void*)k_connect<false, false, 128, 0>);
     rs.shade_blocks = occ((const void*)k_shade<false, false>);
     rs.shade_blocks_guided = occ((const void*)k_shade<true, false>);
-    rs.extend_blocks_inst = occ((const void*)k_extend<true, false, 128>);
-    rs.connect_blocks_inst = occ((const void*)k_connect<true, false, 128>);
+    rs.extend_blocks_inst = occ((const void*)k_extend<true, false, 128, 0>);
+    rs.connect_blocks_inst = occ((const void*)k_connect<true, false, 128, 0>);
     rs.shade_blocks_inst = occ((const void*)k_shade<false, true>);
     rs.shade_blocks_guided_inst = occ((const void*)k_shade<true, true>);
 }
@@ -646,9 +652,13 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
     }
     for (uint32_t d = 0; d < fp.max_depth; ++d) {
         if (timer) timer->mark(stream, StageTimer::kExtend);
-        const bool inst = sc.num_instances > 0;
-        if (inst) k_extend<true, false, 128><<<sms * rs.extend_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
-        else k_extend<false, false, 128><<<sms * rs.extend_blocks, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
+        const bool inst = sc.num_instances > 0, wide = !inst && sc.wnodes;
+        if (inst)
+            k_extend<true, false, 128, 0><<<sms * rs.extend_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
+        else if (wide)
+            k_extend<false, false, 128, 1><<<sms * rs.extend_blocks, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
+        else
+            k_extend<false, false, 128, 0><<<sms * rs.extend_blocks_bin, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
         if (fp.guided && d + 1 < fp.max_depth) {
             if (timer) timer->mark(stream, StageTimer::kGuide);
             launch_guide_infer(rs, sc, fp, d, stream);
@@ -667,8 +677,12 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
         if (d + 1 < fp.max_depth && (fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) &&
             sc.light_strategies > 0) {
             if (timer) timer->mark(stream, StageTimer::kConnect);
-            if (inst) k_connect<true, false, 128><<<sms * rs.connect_blocks_inst, 128, 0, stream>>>(rs.ps, sc, BatchDev{}, d);
-            else k_connect<false, false, 128><<<sms * rs.connect_blocks, 128, 0, stream>>>(rs.ps, sc, BatchDev{}, d);
+            if (inst)
+                k_connect<true, false, 128, 0><<<sms * rs.connect_blocks_inst, 128, 0, stream>>>(rs.ps, sc, BatchDev{}, d);
+            else if (wide)
+                k_connect<false, false, 128, 1><<<sms * rs.connect_blocks, 128, 0, stream>>>(rs.ps, sc, BatchDev{}, d);
+            else
+                k_connect<false, false, 128, 0><<<sms * rs.connect_blocks_bin, 128, 0, stream>>>(rs.ps, sc, BatchDev{}, d);
             rs.launches++;
         }
     }
@@ -713,43 +727,54 @@ namespace luc {
 
 // One wave of a batched render (graph-capturable: fixed shapes, lengths on
 // the device). `block` selects the EXTEND / CONNECT instantiation.
-template <int B>
+template <int B, int W>
 static void wave_traverse(RenderState& rs, const BatchDev& bd, const FrameParams& fpw, uint32_t d, bool connect,
                           int ext_blocks, int con_blocks, cudaStream_t s) {
     const int sms = rs.num_sms;
-    if (!connect) k_extend<false, true, B><<<sms * ext_blocks, B, 0, s>>>(rs.ps, DevScene{}, fpw, bd, d);
-    else k_connect<false, true, B><<<sms * con_blocks, B, 0, s>>>(rs.ps, DevScene{}, bd, d);
+    if (!connect) k_extend<false, true, B, W><<<sms * ext_blocks, B, 0, s>>>(rs.ps, DevScene{}, fpw, bd, d);
+    else k_connect<false, true, B, W><<<sms * con_blocks, B, 0, s>>>(rs.ps, DevScene{}, bd, d);
+}
+template <int B>
+static void wave_traverse(RenderState& rs, const BatchDev& bd, const FrameParams& fpw, uint32_t d, bool connect,
+                          int ext_blocks, int con_blocks, bool wide, cudaStream_t s) {
+    if (wide) wave_traverse<B, 1>(rs, bd, fpw, d, connect, ext_blocks, con_blocks, s);
+    else wave_traverse<B, 0>(rs, bd, fpw, d, connect, ext_blocks, con_blocks, s);
 }
 
-int batch_blocks_per_sm(int block, bool connect) {
+template <int W>
+static const void* batch_kernel(int block, bool connect) {
+    if (block == 64) return connect ? (const void*)k_connect<false, true, 64, W> : (const void*)k_extend<false, true, 64, W>;
+    if (block == 256)
+        return connect ? (const void*)k_connect<false, true, 256, W> : (const void*)k_extend<false, true, 256, W>;
+    return connect ? (const void*)k_connect<false, true, 128, W> : (const void*)k_extend<false, true, 128, W>;
+}
+
+int batch_blocks_per_sm(int block, bool connect, bool wide) {
     int b = 0;
-    const void* k = nullptr;
-    if (block == 64) k = connect ? (const void*)k_connect<false, true, 64> : (const void*)k_extend<false, true, 64>;
-    else if (block == 256) k = connect ? (const void*)k_connect<false, true, 256> : (const void*)k_extend<false, true, 256>;
-    else k = connect ? (const void*)k_connect<false, true, 128> : (const void*)k_extend<false, true, 128>;
+    const void* k = wide ? batch_kernel<1>(block, connect) : batch_kernel<0>(block, connect);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, block, 0);
     return b > 0 ? b : 1;
 }
 
 void record_wave(RenderState& rs, const BatchDev& bd, const uint32_t* pix_off, uint32_t num_paths,
-                 uint32_t total_pixels, uint32_t max_depth, int block, cudaStream_t s) {
+                 uint32_t total_pixels, uint32_t max_depth, int block, bool wide, cudaStream_t s) {
     const int sms = rs.num_sms;
     cudaMemsetAsync(rs.ps.ctr, 0, kCtrStride * (max_depth + 2) * sizeof(uint32_t), s);
     k_generate_batch<<<(int)std::min<uint64_t>((num_paths + 255) / 256, (uint64_t)sms * 16), 256, 0, s>>>(rs.ps, bd,
                                                                                                       num_paths);
     FrameParams fpw{};
     fpw.num_paths = num_paths;
-    const int eb = batch_blocks_per_sm(block, false), cb = batch_blocks_per_sm(block, true);
+    const int eb = batch_blocks_per_sm(block, false, wide), cb = batch_blocks_per_sm(block, true, wide);
     for (uint32_t d = 0; d < max_depth; ++d) {
-        if (block == 64) wave_traverse<64>(rs, bd, fpw, d, false, eb, cb, s);
-        else if (block == 256) wave_traverse<256>(rs, bd, fpw, d, false, eb, cb, s);
-        else wave_traverse<128>(rs, bd, fpw, d, false, eb, cb, s);
+        if (block == 64) wave_traverse<64>(rs, bd, fpw, d, false, eb, cb, wide, s);
+        else if (block == 256) wave_traverse<256>(rs, bd, fpw, d, false, eb, cb, wide, s);
+        else wave_traverse<128>(rs, bd, fpw, d, false, eb, cb, wide, s);
         k_shade<false, false, true><<<sms * rs.shade_blocks, 128, 0, s>>>(rs.ps, DevScene{}, fpw, bd, d);
         rs.launches += 2;
         if (d + 1 < max_depth) {
-            if (block == 64) wave_traverse<64>(rs, bd, fpw, d, true, eb, cb, s);
-            else if (block == 256) wave_traverse<256>(rs, bd, fpw, d, true, eb, cb, s);
-            else wave_traverse<128>(rs, bd, fpw, d, true, eb, cb, s);
+            if (block == 64) wave_traverse<64>(rs, bd, fpw, d, true, eb, cb, wide, s);
+            else if (block == 256) wave_traverse<256>(rs, bd, fpw, d, true, eb, cb, wide, s);
+            else wave_traverse<128>(rs, bd, fpw, d, true, eb, cb, wide, s);
             rs.launches++;
         }
     }
