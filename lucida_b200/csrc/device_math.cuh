@@ -318,16 +318,20 @@ LUC_D float fresnel_dielectric(float ci, float eta) {
     float rpe = (c - eta * ct) / (c + eta * ct);
     return 0.5f * (rpa * rpa + rpe * rpe);
 }
+// The reference's powf(x, 0.5) is taken as the correctly rounded square root:
+// for a float x >= 0, sqrt(x) never lies within 2^-50 (relative) of a float
+// rounding midpoint, so a pow evaluated to double precision (error <= 2 ulp)
+// rounds to the same float as IEEE sqrtf.
 LUC_D V3 fresnel_conductor(float ci, V3 eta, V3 k) {
     float c = clampf(ci, 0.0f, 1.0f);
     float c2 = c * c, sin2 = 1.0f - c2;
     V3 eta2 = eta * eta, k2 = k * k;
     V3 t0 = eta2 - k2 - splat(sin2);
     V3 q = vmax(t0 * t0 + 4.0f * eta2 * k2, splat(0.0f));
-    V3 a2pb2 = V3{dpow(q.x, 0.5f), dpow(q.y, 0.5f), dpow(q.z, 0.5f)};
+    V3 a2pb2 = V3{sqrtf(q.x), sqrtf(q.y), sqrtf(q.z)};
     V3 t1 = a2pb2 + splat(c2);
     V3 qa = vmax(0.5f * (a2pb2 + t0), splat(0.0f));
-    V3 a = V3{dpow(qa.x, 0.5f), dpow(qa.y, 0.5f), dpow(qa.z, 0.5f)};
+    V3 a = V3{sqrtf(qa.x), sqrtf(qa.y), sqrtf(qa.z)};
     V3 t2 = 2.0f * c * a;
     V3 rs = (t1 - t2) / (t1 + t2);
     V3 t3 = c2 * a2pb2 + splat(sin2 * sin2);
@@ -383,24 +387,6 @@ LUC_D V3 surf_fresnel(const Surface& s, float c) {
 LUC_D V3 normal_reflectance(const Surface& s) {
     return s.conductor ? fresnel_conductor(1.0f, s.eta, s.k) : s.f0;
 }
-LUC_D V3 specular_albedo(const Surface& s, const float* table, float cos_o) {
-    float e = energy_lookup(table, s.roughness, fabsf(cos_o));
-    V3 f = surf_fresnel(s, fabsf(cos_o));
-    V3 fav = fresnel_average(normal_reflectance(s));
-    return vclamp01(f * e + fav * (1.0f - e));
-}
-LUC_D float specular_probability(const Surface& s, const float* table, float cos_o) {
-    if (s.transmission > 0.0f) {
-        float f = fresnel_dielectric(fabsf(cos_o), s.relative_ior);
-        if (f >= 1.0f) return 1.0f;
-        return clampf(f, 0.05f, 0.95f);
-    }
-    V3 sa = specular_albedo(s, table, cos_o);
-    float spec = luminance(sa);
-    float diff = luminance(s.diffuse_albedo * (splat(1.0f) - specular_albedo(s, table, cos_o)));
-    if (spec + diff <= 0.0f) return 1.0f;
-    return clampf(spec / (spec + diff), 0.1f, 0.9f);
-}
 LUC_D V3 reflection_fresnel(const Surface& s, float c) {
     if (s.transmission > 0.0f && !s.conductor) return splat(fresnel_dielectric(c, s.relative_ior));
     return surf_fresnel(s, c);
@@ -435,62 +421,89 @@ LUC_D float dielectric_pdf(float alpha, float eta, V3 wo, V3 wi) {
     float jac = fabsf(eta * eta * wih) / (denom * denom);
     return vndf_half_pdf(alpha, wo, h) * jac;
 }
-// surface::eval (bsdf.rs:1493-1540). Returns f.
-LUC_D V3 bsdf_eval(const Surface& s, const float* table, V3 wo, V3 wi) {
-    if (wo.z <= 0.0f) return splat(0.0f);
-    float alpha = rough_to_alpha(s.roughness);
+// What surface::eval, surface::pdf and surface::sample compute from wo alone
+// (valid for wo.z > 0), evaluated once per vertex and shared by every
+// direction evaluated there. Same operations as the per-call forms, so the
+// same values.
+struct SurfWo {
+    float alpha;      // rough_to_alpha(roughness)
+    float p_spec;     // specular_probability(wo.z)
+    float e;          // energy_lookup(roughness, wo.z)
+    V3 transmitted;   // 1 - specular_albedo(wo.z)
+    V3 fav;           // fresnel_average(normal_reflectance)
+};
+LUC_D SurfWo surf_wo(const Surface& s, const float* table, float cos_o) {
+    SurfWo w;
+    w.alpha = rough_to_alpha(s.roughness);
+    w.e = energy_lookup(table, s.roughness, fabsf(cos_o));
+    w.fav = fresnel_average(normal_reflectance(s));
+    const V3 sa = vclamp01(surf_fresnel(s, fabsf(cos_o)) * w.e + w.fav * (1.0f - w.e));  // specular_albedo
+    w.transmitted = splat(1.0f) - sa;
+    if (s.transmission > 0.0f) {
+        float f = fresnel_dielectric(fabsf(cos_o), s.relative_ior);
+        w.p_spec = f >= 1.0f ? 1.0f : clampf(f, 0.05f, 0.95f);
+    } else {
+        float spec = luminance(sa);
+        float diff = luminance(s.diffuse_albedo * w.transmitted);
+        w.p_spec = spec + diff <= 0.0f ? 1.0f : clampf(spec / (spec + diff), 0.1f, 0.9f);
+    }
+    return w;
+}
+// surface::eval (bsdf.rs:1493-1540) for wo.z > 0. Returns f.
+LUC_D V3 bsdf_eval_w(const Surface& s, const SurfWo& w, V3 wo, V3 wi) {
     if (wi.z < 0.0f) {
         if (s.transmission <= 0.0f) return splat(0.0f);
-        float t = dielectric_eval(alpha, s.relative_ior, wo, wi);
+        float t = dielectric_eval(w.alpha, s.relative_ior, wo, wi);
         return splat(t) * s.transmission * s.tint;
     }
     if (wi.z <= 0.0f) return splat(0.0f);
-    V3 transmitted = splat(1.0f) - specular_albedo(s, table, wo.z);
-    V3 f = s.diffuse_albedo * kInvPi * transmitted * (1.0f - s.transmission);
+    V3 f = s.diffuse_albedo * kInvPi * w.transmitted * (1.0f - s.transmission);
     V3 h = normalize_or(wo + wi, splat(0.0f));
     if (!(h == splat(0.0f))) {
-        float d = ggx_d(alpha, h.z);
-        float g2 = smith_g2(alpha, wo.z, wi.z);
+        float d = ggx_d(w.alpha, h.z);
+        float g2 = smith_g2(w.alpha, wo.z, wi.z);
         V3 fr = reflection_fresnel(s, fmaxf(dot(wo, h), 0.0f));
         V3 single = fr * (d * g2 / (4.0f * wo.z * wi.z));
         if (s.transmission > 0.0f) {
             f = f + single;
         } else {
-            float e = energy_lookup(table, s.roughness, wo.z);
-            V3 comp = splat(1.0f) + fresnel_average(normal_reflectance(s)) * ((1.0f - e) / e);
+            V3 comp = splat(1.0f) + w.fav * ((1.0f - w.e) / w.e);
             f = f + single * comp;
         }
     }
     return f;
 }
-// surface::pdf (bsdf.rs:1543-1562).
-LUC_D float bsdf_pdf(const Surface& s, const float* table, V3 wo, V3 wi) {
-    if (wo.z <= 0.0f) return 0.0f;
-    float p_spec = specular_probability(s, table, wo.z);
-    float alpha = rough_to_alpha(s.roughness);
-    float rest = 1.0f - p_spec;
+LUC_D V3 bsdf_eval(const Surface& s, const float* table, V3 wo, V3 wi) {
+    if (wo.z <= 0.0f) return splat(0.0f);
+    return bsdf_eval_w(s, surf_wo(s, table, wo.z), wo, wi);
+}
+// surface::pdf (bsdf.rs:1543-1562) for wo.z > 0.
+LUC_D float bsdf_pdf_w(const Surface& s, const SurfWo& w, V3 wo, V3 wi) {
+    float rest = 1.0f - w.p_spec;
     if (wi.z < 0.0f) {
         if (s.transmission <= 0.0f) return 0.0f;
-        return rest * s.transmission * dielectric_pdf(alpha, s.relative_ior, wo, wi);
+        return rest * s.transmission * dielectric_pdf(w.alpha, s.relative_ior, wo, wi);
     }
     if (wi.z <= 0.0f) return 0.0f;
     float spec = 0.0f;
     V3 h = normalize_or(wo + wi, splat(0.0f));
-    if (!(h == splat(0.0f))) spec = vndf_pdf(alpha, wo, h);
+    if (!(h == splat(0.0f))) spec = vndf_pdf(w.alpha, wo, h);
     float diff = wi.z * kInvPi;
-    return p_spec * spec + rest * (1.0f - s.transmission) * diff;
+    return w.p_spec * spec + rest * (1.0f - s.transmission) * diff;
+}
+LUC_D float bsdf_pdf(const Surface& s, const float* table, V3 wo, V3 wi) {
+    if (wo.z <= 0.0f) return 0.0f;
+    return bsdf_pdf_w(s, surf_wo(s, table, wo.z), wo, wi);
 }
 struct BsdfSample {
     V3 wi, weight;
     float pdf;
 };
-// The direction half of surface::sample (bsdf.rs:1571-1661): lobe choice by
-// u_lobe, then GGX reflection (VNDF), rough transmission or cosine-weighted
-// diffuse. False where surface::sample returns no sample.
-LUC_D bool bsdf_sample_dir(const Surface& s, const float* table, V3 wo, float u_lobe, float ux, float uy, V3& wi) {
-    if (wo.z <= 0.0f) return false;
-    float p_spec = specular_probability(s, table, wo.z);
-    float alpha = rough_to_alpha(s.roughness);
+// The direction half of surface::sample (bsdf.rs:1571-1661) for wo.z > 0:
+// lobe choice by u_lobe, then GGX reflection (VNDF), rough transmission or
+// cosine-weighted diffuse. False where surface::sample returns no sample.
+LUC_D bool bsdf_sample_dir_w(const Surface& s, const SurfWo& w, V3 wo, float u_lobe, float ux, float uy, V3& wi) {
+    const float p_spec = w.p_spec, alpha = w.alpha;
     if (u_lobe < p_spec) {
         V3 m = sample_vndf(wo, alpha, ux, uy);
         V3 r = reflect(wo, m);
@@ -514,14 +527,20 @@ LUC_D bool bsdf_sample_dir(const Surface& s, const float* table, V3 wo, float u_
     if (wi.z < 0.0f && s.transmission <= 0.0f) return false;
     return true;
 }
+LUC_D bool bsdf_sample_dir(const Surface& s, const float* table, V3 wo, float u_lobe, float ux, float uy, V3& wi) {
+    if (wo.z <= 0.0f) return false;
+    return bsdf_sample_dir_w(s, surf_wo(s, table, wo.z), wo, u_lobe, ux, uy, wi);
+}
 
 // surface::sample (bsdf.rs:1571-1661): direction, then f and the pdf there.
 LUC_D BsdfSample bsdf_sample(const Surface& s, const float* table, V3 wo, float u_lobe, float ux, float uy) {
     BsdfSample bad{V3{0.0f, 0.0f, 1.0f}, splat(0.0f), 0.0f};
+    if (wo.z <= 0.0f) return bad;
+    const SurfWo w = surf_wo(s, table, wo.z);
     V3 wi;
-    if (!bsdf_sample_dir(s, table, wo, u_lobe, ux, uy, wi)) return bad;
-    V3 f = bsdf_eval(s, table, wo, wi);
-    float pdf = bsdf_pdf(s, table, wo, wi);
+    if (!bsdf_sample_dir_w(s, w, wo, u_lobe, ux, uy, wi)) return bad;
+    V3 f = bsdf_eval_w(s, w, wo, wi);
+    float pdf = bsdf_pdf_w(s, w, wo, wi);
     if (pdf <= 0.0f) return bad;
     return BsdfSample{wi, f * (fabsf(wi.z) / pdf), pdf};
 }

@@ -302,7 +302,13 @@ __global__ void __launch_bounds__(128, 4) k_shade(PathState ps, const __grid_con
                                 surf.roughness >= kGuideMinRoughness;
                 const float4* lob = ps.lobes + i;  // this queue position's mixture (SoA planes)
                 if (wo.z > 0.0f) {
-                    // Next event estimation (integrator.rs:349-354, 418-532).
+                    // Everything surface::eval / pdf / sample take from wo alone.
+                    const SurfWo sw = surf_wo(surf, sc.energy, wo.z);
+                    // Next event estimation (integrator.rs:349-354, 418-532):
+                    // the light sample and its direction; f and pdf below.
+                    bool nee = false;
+                    V3 wiw{0, 0, 0}, lrad{0, 0, 0}, wi_n{0.0f, 0.0f, 1.0f};
+                    float dist = 0.0f, lpdf = 0.0f;
                     if ((fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) && !last &&
                         sc.light_strategies > 0) {
                         float u_sel = smp.next_f32();
@@ -311,8 +317,6 @@ __global__ void __launch_bounds__(128, 4) k_shade(PathState ps, const __grid_con
                         uint32_t nl = sc.num_lights, total = sc.light_strategies;
                         uint32_t pick = min(f2u(u_sel * (float)total), total - 1u);
                         bool ok = true;
-                        V3 wiw{0, 0, 0}, lrad{0, 0, 0};
-                        float dist = 0.0f, lpdf = 0.0f;
                         if (pick < nl) {
                             float u_light = ((float)pick + 0.5f) / (float)nl;
                             uint32_t idx = min(f2u(u_light * (float)nl), nl - 1u);
@@ -355,56 +359,71 @@ __global__ void __launch_bounds__(128, 4) k_shade(PathState ps, const __grid_con
                             }
                         }
                         if (ok && lpdf > 0.0f) {
-                            V3 wi = to_local(wiw, hit.normal);
-                            if (!(wi.z == 0.0f || (wi.z < 0.0f && surf.transmission <= 0.0f))) {
-                                V3 f = bsdf_eval(surf, sc.energy, wo, wi);
-                                if (max_elem(f) > 0.0f) {
-                                    float mis = 1.0f;
-                                    if (fp.sampling == LUC_SAMPLING_MIS) {
-                                        float pb = bsdf_pdf(surf, sc.energy, wo, wi);
-                                        if (gv) pb = 0.5f * pb + 0.5f * mixture_pdf_mem(lob, ps.lobe_stride, wiw);
-                                        mis = power_heuristic(lpdf, pb);
-                                    }
-                                    if (mis > 0.0f) {
-                                        sh_o = offset_ray_origin(hit.position, wi.z < 0.0f ? -hit.gnormal : hit.gnormal);
-                                        sh_d = wiw;
-                                        sh_t = dist * (1.0f - 1.0e-3f);
-                                        sh_c = thr * (f * fabsf(wi.z) * lrad * (mis / lpdf));
-                                        cast = true;
-                                    }
-                                }
-                            }
+                            wi_n = to_local(wiw, hit.normal);
+                            nee = !(wi_n.z == 0.0f || (wi_n.z < 0.0f && surf.transmission <= 0.0f));
                         }
                     }
-                    // BSDF sampling (integrator.rs:360-399). Skipped on the last
-                    // bounce, where its result would never be read.
-                    if (kGuided && !last) {
-                        // Guided frames: one code path for every vertex; the
-                        // choice dimension is drawn only where the guide applies.
-                        float u_choice = gv ? smp.next_f32() : 0.0f;
-                        float u_lobe = smp.next_f32();
+                    // BSDF sampling (integrator.rs:360-399): the direction. Skipped
+                    // on the last bounce, where its result would never be read.
+                    // Guided frames choose between the BSDF and the learned
+                    // mixture; the choice dimension is drawn only where the
+                    // guide applies.
+                    bool bsd = false;
+                    V3 wl{0.0f, 0.0f, 1.0f}, wd{0.0f, 0.0f, 1.0f};
+                    if (!last) {
+                        const float u_choice = kGuided && gv ? smp.next_f32() : 0.0f;
+                        const float u_lobe = smp.next_f32();
                         float ux, uy;
                         smp.next_vec2(ux, uy);
-                        // Only the direction depends on the choice; f and both
-                        // pdfs are then evaluated once, converged.
-                        V3 wl{0.0f, 0.0f, 1.0f}, wd{0.0f, 0.0f, 1.0f};
-                        bool ok;
                         if (!gv || u_choice < 0.5f) {
-                            ok = bsdf_sample_dir(surf, sc.energy, wo, u_lobe, ux, uy, wl);
+                            bsd = bsdf_sample_dir_w(surf, sw, wo, u_lobe, ux, uy, wl);
                             wd = to_world(wl, hit.normal);
                         } else {
                             wd = mixture_sample_mem(lob, ps.lobe_stride, u_lobe, ux, uy);
                             wl = to_local(wd, hit.normal);
-                            ok = !(wl.z == 0.0f || (wl.z < 0.0f && surf.transmission <= 0.0f));
+                            bsd = !(wl.z == 0.0f || (wl.z < 0.0f && surf.transmission <= 0.0f));
                         }
-                        V3 fc{0.0f, 0.0f, 0.0f};
-                        float pb = 0.0f;
-                        if (ok) {
-                            fc = bsdf_eval(surf, sc.energy, wo, wl) * fabsf(wl.z);
-                            pb = bsdf_pdf(surf, sc.energy, wo, wl);
+                    }
+                    // f and pdf at both directions through one copy of the
+                    // BSDF code (the loop is kept rolled on purpose: it halves
+                    // the kernel's instruction footprint).
+                    V3 f_n{0.0f, 0.0f, 0.0f}, f_b{0.0f, 0.0f, 0.0f};
+                    float p_n = 0.0f, p_b = 0.0f;
+#pragma unroll 1
+                    for (int k = 0; k < 2; ++k) {
+                        if (!(k == 0 ? nee : bsd)) continue;
+                        const V3 wi = k == 0 ? wi_n : wl;
+                        const V3 f = bsdf_eval_w(surf, sw, wo, wi);
+                        float pdf = 0.0f;
+                        if (k == 1 || (fp.sampling == LUC_SAMPLING_MIS && max_elem(f) > 0.0f))
+                            pdf = bsdf_pdf_w(surf, sw, wo, wi);
+                        if (k == 0) {
+                            f_n = f;
+                            p_n = pdf;
+                        } else {
+                            f_b = f;
+                            p_b = pdf;
                         }
+                    }
+                    if (nee && max_elem(f_n) > 0.0f) {
+                        float mis = 1.0f;
+                        if (fp.sampling == LUC_SAMPLING_MIS) {
+                            float pb = p_n;
+                            if (gv) pb = 0.5f * pb + 0.5f * mixture_pdf_mem(lob, ps.lobe_stride, wiw);
+                            mis = power_heuristic(lpdf, pb);
+                        }
+                        if (mis > 0.0f) {
+                            sh_o = offset_ray_origin(hit.position, wi_n.z < 0.0f ? -hit.gnormal : hit.gnormal);
+                            sh_d = wiw;
+                            sh_t = dist * (1.0f - 1.0e-3f);
+                            sh_c = thr * (f_n * fabsf(wi_n.z) * lrad * (mis / lpdf));
+                            cast = true;
+                        }
+                    }
+                    if (kGuided && !last) {
+                        const V3 fc = bsd ? f_b * fabsf(wl.z) : splat(0.0f);
                         if (max_elem(fc) > 0.0f) {
-                            const float pc = gv ? 0.5f * pb + 0.5f * mixture_pdf_mem(lob, ps.lobe_stride, wd) : pb;
+                            const float pc = gv ? 0.5f * p_b + 0.5f * mixture_pdf_mem(lob, ps.lobe_stride, wd) : p_b;
                             if (pc > 0.0f) {
                                 thr = thr * (fc / pc);
                                 if (max_elem(thr) > 0.0f) {
@@ -444,22 +463,16 @@ __global__ void __launch_bounds__(128, 4) k_shade(PathState ps, const __grid_con
                                 }
                             }
                         }
-                    } else if (!kGuided && !last) {
-                        float u_lobe = smp.next_f32();
-                        float ux, uy;
-                        smp.next_vec2(ux, uy);
-                        BsdfSample bs = bsdf_sample(surf, sc.energy, wo, u_lobe, ux, uy);
-                        if (bs.pdf > 0.0f) {
-                            thr = thr * bs.weight;
-                            if (max_elem(thr) > 0.0f) {
-                                V3 ndir = to_world(bs.wi, hit.normal);
-                                V3 norg = offset_ray_origin(hit.position, bs.wi.z < 0.0f ? -hit.gnormal : hit.gnormal);
-                                store4(ps.o_pdf + p, norg, bs.pdf);
-                                store4(ps.dir + p, ndir, 0.0f);
-                                __stcs(ps.thr + p, make_float4(thr.x, thr.y, thr.z, __uint_as_float(smp.state)));
-                                store4(ps.prev + p, hit.position, 0.0f);
-                                survive = true;
-                            }
+                    } else if (!kGuided && bsd && p_b > 0.0f) {
+                        // surface::sample's weight f |cos| / pdf.
+                        thr = thr * (f_b * (fabsf(wl.z) / p_b));
+                        if (max_elem(thr) > 0.0f) {
+                            V3 norg = offset_ray_origin(hit.position, wl.z < 0.0f ? -hit.gnormal : hit.gnormal);
+                            store4(ps.o_pdf + p, norg, p_b);
+                            store4(ps.dir + p, wd, 0.0f);
+                            __stcs(ps.thr + p, make_float4(thr.x, thr.y, thr.z, __uint_as_float(smp.state)));
+                            store4(ps.prev + p, hit.position, 0.0f);
+                            survive = true;
                         }
                     }
                 }
