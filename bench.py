@@ -39,7 +39,14 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 METRIC = "Mpaths/s at 8 bounces"
-NODE_BYTES, TRI_BYTES, RAY_IO_BYTES = 32, 64, 52  # algorithmic bytes per node visit / tri test / ray
+# Algorithmic bytes per node visit / triangle test / ray of EXTEND: a wide
+# node record (80 B) and a wide-soup triangle (48 B); the binary tree's
+# child-pair record (64 B for two children, 32 B per child tested) and soup
+# triangle (48 B). A ray reads its origin and direction (32 B) and queue
+# index (4 B) and writes its hit (16 B).
+WIDE_BYTES = (80, 48)
+BINARY_BYTES = (32, 48)
+RAY_IO_BYTES = 52
 
 
 def parse():
@@ -256,6 +263,7 @@ def main():
     gpu.set_stream(stream.cuda_stream)
     t0 = time.time()
     gpu.upload(scene)  # LBVH built on the device
+    wide = len(gpu.read_scene("wide_nodes")) > 0  # collapsed to the 8-wide tree unless LUC_BINARY_BVH=1
     torch.cuda.synchronize()
     upload_s = time.time() - t0
     acc = torch.zeros(P * 16, dtype=torch.float32, device="cuda")
@@ -325,14 +333,16 @@ def main():
     hbm, peak_kind = peaks()
     launches_extend = args.depth * args.steps
     ext_ms = stage["extend"] / launches_extend
-    bytes_per_launch = (counts["nodes_extend"] * NODE_BYTES + counts["tris_extend"] * TRI_BYTES +
+    node_b, tri_b = WIDE_BYTES if wide else BINARY_BYTES
+    bytes_per_launch = (counts["nodes_extend"] * node_b + counts["tris_extend"] * tri_b +
                         counts["rays_extend"] * RAY_IO_BYTES) / launches_extend
     achieved = bytes_per_launch / (ext_ms / 1e3) / 1e9
     roofline = {"kernel": "k_extend (closest-hit BVH traversal)", "bound": "hbm", "achieved": achieved,
                 "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_kind,
                 "traffic": None,
-                "model": f"node visits x {NODE_BYTES} B + triangle tests x {TRI_BYTES} B + rays x {RAY_IO_BYTES} B "
-                         "per launch (measured counters); most node bytes are L2 hits",
+                "model": f"{'wide' if wide else 'binary'} tree: node visits x {node_b} B + triangle tests x "
+                         f"{tri_b} B + rays x {RAY_IO_BYTES} B per launch (measured counters); most node bytes "
+                         "are L2 hits",
                 "ms_per_launch": ext_ms, "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
                 "per_ray": {"nodes": counts["nodes_extend"] / max(1, counts["rays_extend"]),
                             "tris": counts["tris_extend"] / max(1, counts["rays_extend"]),

@@ -188,8 +188,13 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
 //
 // kBatch: the path's scene and frame parameters come from its wave segment
 // (luc_render_batch) instead of the kernel arguments.
+//
+// 6 blocks of 128 per SM (80 registers, a few hundred bytes spilled): SHADE is
+// bound by the latency of its path-state, triangle and material loads, and
+// the extra warps hide more of it than the spills cost (measured against 4
+// blocks without spills).
 template <bool kGuided, bool kInst, bool kBatch = false>
-__global__ void __launch_bounds__(128, 4) k_shade(PathState ps, const __grid_constant__ DevScene sc_arg,
+__global__ void __launch_bounds__(128, 6) k_shade(PathState ps, const __grid_constant__ DevScene sc_arg,
                                                   const __grid_constant__ FrameParams fp_arg, BatchDev bd,
                                                   uint32_t depth) {
     const uint32_t len = depth == 0 ? (uint32_t)fp_arg.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
