@@ -47,6 +47,10 @@ METRIC = "Mpaths/s at 8 bounces"
 WIDE_BYTES = (80, 48)
 BINARY_BYTES = (32, 48)
 RAY_IO_BYTES = 52
+# DRAM bytes (read + write) per EXTEND ray on the wide tree, from an ncu
+# capture of every EXTEND launch of a 512x512x4-spp frame of the same scene
+# (500.1 MB over 2,862,333 rays); scaled by the rays of a launch.
+EXTEND_DRAM_BYTES_PER_RAY = 174.7
 
 
 def parse():
@@ -339,7 +343,9 @@ def main():
     achieved = bytes_per_launch / (ext_ms / 1e3) / 1e9
     roofline = {"kernel": "k_extend (closest-hit BVH traversal)", "bound": "hbm", "achieved": achieved,
                 "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_kind,
-                "traffic": None,
+                "traffic": EXTEND_DRAM_BYTES_PER_RAY * counts["rays_extend"] / launches_extend if wide else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per EXTEND ray on a 512x512x4-spp "
+                                  "frame of this scene, scaled by this launch size's rays",
                 "model": f"{'wide' if wide else 'binary'} tree: node visits x {node_b} B + triangle tests x "
                          f"{tri_b} B + rays x {RAY_IO_BYTES} B per launch (measured counters); most node bytes "
                          "are L2 hits",
