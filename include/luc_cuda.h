@@ -40,6 +40,10 @@ extern "C" {
 
 /* luc_render arch_flags (Architecture, crates/gpu/src/lib.rs:38-66). */
 #define LUC_ARCH_WAVEFRONT 0x0u
+/* One thread per pixel walks its samples and paths to the end in registers
+ * (Architecture::Megakernel): same accumulator as the wavefront. Not with
+ * LUC_FLAG_GUIDED. */
+#define LUC_ARCH_MEGAKERNEL 0x1u
 /* Skip the first-hit guide channels (albedo/normal/depth) of the
  * accumulator: they are needed only by the denoiser. */
 #define LUC_FLAG_NO_GUIDES 0x100u
@@ -58,6 +62,10 @@ extern "C" {
  * hierarchy. For parity with the reference; the default is the two-level
  * any-hit. No effect on scenes without instances. */
 #define LUC_FLAG_REFERENCE_SHADOWS 0x800u
+/* After the render, run the convergence meter (luc_convergence) over the
+ * accumulator; luc_get_stats reports it (render_with_measured,
+ * crates/gpu/src/lib.rs:86-97). */
+#define LUC_FLAG_MEASURE 0x1000u
 
 typedef struct luc_ctx luc_ctx;
 
@@ -135,6 +143,8 @@ typedef struct luc_render_stats {
     uint64_t nodes_extend, tris_extend; /* BVH node visits / triangle tests, closest hit */
     uint64_t nodes_shadow, tris_shadow; /* the same for shadow rays */
     double ms_guide, ms_train; /* guide inference and training (LUC_FLAG_GUIDED) */
+    double convergence;    /* LUC_FLAG_MEASURE: the convergence meter's figure; -1 otherwise or when no
+                              pixel is measurable */
 } luc_render_stats;
 
 /* Layout contract: returns LUC_LAYOUT_VERSION. */
@@ -215,6 +225,12 @@ int32_t luc_eval_env(luc_ctx* ctx, const float* in, uint32_t n, int32_t mode, fl
  *   mode 1 = Scene::occluded (scene.rs:577-606) within (1e-4, t_max): out
  *            holds n u32, 1 = occluded. */
 int32_t luc_intersect(luc_ctx* ctx, const float* rays8, uint32_t n, int32_t mode, void* out);
+/* Convergence meter (ConvergenceMeter, crates/gpu/src/stats.rs;
+ * shaders/stats/convergence.wgsl): over a device accumulator of `pixels`
+ * GpuAccum, the mean relative standard error of the pixel means, taken over
+ * pixels with >= 2 samples and mean luminance > 1e-3 (-1 if none). Assumes
+ * independent samples: with Sobol it over-reports. */
+int32_t luc_convergence(luc_ctx* ctx, const void* accum_dev, uint32_t pixels, float* out);
 
 /* Sort without allocating: the variant of luc_sort_u32_dev for callers that
  * cannot call cudaMalloc (a host that reserves all device memory up front, or

@@ -8,10 +8,11 @@ declared in include/luc_cuda.h (liblucida_cuda.so), with this package as the
 Python-side mirror of Lucida's `pt_gpu` API.
 """
 from .gpu import (Camera, DenoiseParams, Denoiser, Film, Gpu, GpuBuildOutput, GpuError, LbvhBuilder, RenderParams,
-                  SceneDef, accum_to_film, build_uniforms, render_accum, render_native_denoised, render_native_on,
-                  render_with)
+                  SceneDef, accum_to_film, build_uniforms, convergence, measure_convergence, render_accum,
+                  render_native_denoised, render_native_on, render_with, render_with_measured)
 from .guide import Guide, records_array
 
 __all__ = ["Camera", "DenoiseParams", "Denoiser", "Film", "Gpu", "GpuBuildOutput", "GpuError", "LbvhBuilder",
            "RenderParams", "SceneDef", "accum_to_film", "build_uniforms", "render_accum", "render_native_denoised",
-           "render_native_on", "render_with", "Guide", "records_array"]
+           "render_native_on", "render_with", "render_with_measured", "measure_convergence", "convergence", "Guide",
+           "records_array"]

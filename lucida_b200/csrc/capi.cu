@@ -159,7 +159,7 @@ void luc_destroy(luc_ctx* c) {
     DevBuf* bufs[] = {&c->materials, &c->prims,    &c->lights,   &c->positions, &c->attrs,     &c->tris,
                       &c->nodes,     &c->env_px,   &c->env_cond, &c->env_marg,  &c->env_row_sin, &c->energy,
                       &c->tnodes,    &c->soup,     &c->frame_word, &c->blas_roots, &c->wnodes,  &c->wsoup,
-                      &c->wtasks,    &c->wctr,
+                      &c->wtasks,    &c->wctr,     &c->conv_scratch,
                       &c->pool,      &c->accum_tmp, &c->lb_tris, &c->lb_pos,    &c->lb_boxes,  &c->lb_keys,
                       &c->lb_vals,   &c->lb_keys2, &c->lb_vals2, &c->lb_hist,   &c->lb_karras, &c->lb_parent,
                       &c->lb_nbounds, &c->lb_subtree, &c->lb_flags, &c->lb_nodes, &c->lb_rank, &c->lb_misc,
@@ -474,10 +474,15 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     if (max_depth == 0 || max_depth > 256) return luc_fail(c, LUC_ERR_VALIDATION, "max_depth must be in 1..=256");
     if ((out_host == nullptr) == (out_dev == nullptr))
         return luc_fail(c, LUC_ERR_VALIDATION, "exactly one of out_host / out_dev must be given");
-    if ((flags & 0xFFu) != LUC_ARCH_WAVEFRONT) return luc_fail(c, LUC_ERR_VALIDATION, "unknown architecture");
-    if (flags & ~(0xFFu | LUC_FLAG_NO_GUIDES | LUC_FLAG_PROFILE | LUC_FLAG_GUIDED | LUC_FLAG_REFERENCE_SHADOWS))
+    const uint32_t arch = flags & 0xFFu;
+    if (arch != LUC_ARCH_WAVEFRONT && arch != LUC_ARCH_MEGAKERNEL)
+        return luc_fail(c, LUC_ERR_VALIDATION, "unknown architecture");
+    if (flags & ~(0xFFu | LUC_FLAG_NO_GUIDES | LUC_FLAG_PROFILE | LUC_FLAG_GUIDED | LUC_FLAG_REFERENCE_SHADOWS |
+                  LUC_FLAG_MEASURE))
         return luc_fail(c, LUC_ERR_VALIDATION, "unknown render flag");
     const bool guided = (flags & LUC_FLAG_GUIDED) != 0;
+    const bool mega = arch == LUC_ARCH_MEGAKERNEL;
+    if (mega && guided) return luc_fail(c, LUC_ERR_VALIDATION, "the megakernel does not sample the learned guide");
     if (guided && !c->guide_ready)
         return luc_fail(c, LUC_ERR_VALIDATION, "LUC_FLAG_GUIDED needs luc_guide_init first");
     if (u->sampling_mode > 2 || u->sampler_kind > 1) return luc_fail(c, LUC_ERR_VALIDATION, "bad sampling mode");
@@ -492,7 +497,8 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
         LUC_CUDA(c, cudaMemsetAsync(accum, 0, pixels * sizeof(GpuAccum), s), "clear accumulator");
     }
     uint64_t per_batch = std::max<uint64_t>(1, std::min<uint64_t>(spp, c->path_budget / pixels));
-    int32_t rc = ensure_pool(c, per_batch * pixels, max_depth);
+    // The megakernel keeps paths in registers: only the counters are needed.
+    int32_t rc = ensure_pool(c, mega ? 1 : per_batch * pixels, max_depth);
     if (rc) return rc;
     if (guided) {
         rc = luc_guide_prepare_frame(c, c->rs.capacity);
@@ -539,7 +545,17 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     cudaMemsetAsync(c->rs.ps.stat, 0, 8 * sizeof(unsigned long long), s);
     cudaEventRecord(e0, s);
     const bool one_batch = per_batch >= spp;
-    if (one_batch && c->use_graphs) {
+    if (mega) {
+        // Every sample of every pixel in one launch, samples in order.
+        fp.sample_base = u->sample_offset;
+        LUC_CUDA(c, cudaMemcpyAsync(c->frame_word.p, &fp.sample_base, 4, cudaMemcpyHostToDevice, s),
+                 "upload sample base");
+        fp.batch_samples = spp;
+        fp.num_paths = (uint64_t)spp * pixels;
+        record_megakernel(c->rs, sc, fp, accum, s);
+        c->rs.launches++;
+        c->stats.paths += fp.num_paths;
+    } else if (one_batch && c->use_graphs) {
         // Single-batch frame: capture it once as a CUDA graph and replay it
         // while the frame parameters, scene, pool and accumulator repeat.
         // The sample offset reaches the kernels through the frame word, so
@@ -600,6 +616,14 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     cudaEventRecord(e1, s);
     cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) return luc_cuda_fail(c, le, "render launch");
+    float conv = -1.0f;
+    const bool measure = (flags & LUC_FLAG_MEASURE) != 0;
+    if (measure) {
+        rc = luc_record_convergence(c, accum, (uint32_t)pixels, s);
+        if (rc) return rc;
+        LUC_CUDA(c, cudaMemcpyAsync(&conv, c->conv_scratch.as<float2>() + 64, 4, cudaMemcpyDeviceToHost, s),
+                 "read convergence");
+    }
     if (out_host) {
         LUC_CUDA(c, cudaMemcpyAsync(out_host, accum, pixels * sizeof(GpuAccum), cudaMemcpyDeviceToHost, s),
                  "read back accumulator");
@@ -616,6 +640,7 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->stats.ms_total = ms;
+    c->stats.convergence = measure ? conv : -1.0;
     c->stats.launches = c->rs.launches;
     c->stats.rays_extend = counts[0];
     c->stats.nodes_extend = counts[1];

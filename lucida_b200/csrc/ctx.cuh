@@ -49,6 +49,7 @@ struct luc_ctx {
     DevBuf materials, prims, lights, positions, attrs, tris, nodes, env_px, env_cond, env_marg, env_row_sin, energy;
     DevBuf tnodes, soup;  // traversal layout derived from nodes / tris
     DevBuf wnodes, wsoup, wtasks, wctr;  // compressed 8-wide tree (wide.cu)
+    DevBuf conv_scratch;                 // convergence meter partials + result (stats.cu)
     uint32_t wide_nodes = 0;             // 0: the scene traverses the binary tree
     bool use_wide = true;                // LUC_BINARY_BVH=1 turns the wide tree off
     DevBuf blas_roots;    // distinct BLAS roots of an instanced scene
@@ -122,6 +123,9 @@ int32_t luc_gather_triangles(luc_ctx* c, const GpuTriangle* src, GpuTriangle* ds
 // Implemented in wavefront.cu: derive the traversal layout (child-pair
 // records, triangle soup) from the resident nodes and triangles.
 int32_t luc_build_traversal(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris);
+// stats.cu: record the convergence meter over a device accumulator on `s`;
+// the figure lands in c->conv_scratch after 64 float2 partials.
+int32_t luc_record_convergence(luc_ctx* c, const GpuAccum* accum, uint32_t pixels, cudaStream_t s);
 // wide.cu: collapse the binary tree into c->wnodes / c->wsoup (sets
 // c->wide_nodes; 0 when the tree is too deep for the level budget).
 int32_t luc_build_wide(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris);

@@ -19,6 +19,7 @@
 //   * RESOLVE sums a pixel's samples in sample order onto the accumulator,
 //     which makes batched and progressive renders bit-identical to one shot.
 #include "ctx.cuh"
+#include "shade.cuh"
 
 namespace luc {
 
@@ -48,27 +49,9 @@ __device__ __forceinline__ V3 xyz(float4 a) { return V3{a.x, a.y, a.z}; }
 // Camera ray and sampler state of path p: pixel `pixel`, sample `sample`.
 __device__ __forceinline__ void generate_one(PathState& ps, const FrameParams& fp, uint64_t p, uint32_t pixel,
                                              uint32_t sample) {
-    uint32_t x = pixel % fp.width, y = pixel / fp.width;
     Sampler smp = make_sampler(fp.sampler_kind, fp.frame_seed, pixel, sample);
-    float pu, pv, lu, lv;
-    smp.next_vec2(pu, pv);
-    smp.next_vec2(lu, lv);
-    float s = ((float)x + pu) / (float)fp.width;
-    float t = ((float)y + pv) / (float)fp.height;
-    V3 origin = fp.cam_origin;
-    V3 target = fp.cam_upper_left + s * fp.cam_horizontal + t * fp.cam_vertical;
-    V3 dir;
-    if (fp.lens_radius <= 0.0f) {
-        dir = normalize(target - origin);
-    } else {
-        float dx, dy;
-        concentric_disk(lu, lv, dx, dy);
-        dx = dx * fp.lens_radius;
-        dy = dy * fp.lens_radius;
-        V3 right = normalize(fp.cam_horizontal), down = normalize(fp.cam_vertical);
-        origin = origin + (right * dx + down * dy);
-        dir = normalize(target - origin);
-    }
+    V3 origin, dir;
+    camera_ray(fp, pixel, smp, origin, dir);
     store4(ps.o_pdf + p, origin, 0.0f);
     store4(ps.dir + p, dir, 0.0f);
     __stcs(ps.thr + p, make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(smp.state)));
@@ -177,6 +160,71 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
     return pred ? base + (uint32_t)__popc(mask & ((1u << lane) - 1u)) : 0xFFFFFFFFu;
 }
 
+// SHADE's sink for shade_vertex: the path pool. The path's next ray and the
+// first-hit guides are stored where they are computed; the shadow ray waits
+// in registers for the warp-aggregated append at the end of the step.
+// Guided frames also write the vertex's training record (a threshold-
+// selected subset of the candidates, warp-aggregated counters).
+template <bool kGuided>
+struct PoolSink {
+    const PathState& ps;
+    const Sampler& smp;
+    uint32_t p, depth, sbase, rec_threshold, rec_cap;
+    V3 dir_in;
+    bool survive = false, cast = false;
+    V3 sh_o{0, 0, 0}, sh_d{0, 0, 0}, sh_c{0, 0, 0};
+    float sh_t = 0.0f;
+    __device__ PoolSink(const PathState& ps_, uint32_t p_, uint32_t depth_, uint32_t sbase_, uint32_t thr_,
+                        uint32_t cap_, V3 dir_, const Sampler& smp_)
+        : ps(ps_), smp(smp_), p(p_), depth(depth_), sbase(sbase_), rec_threshold(thr_), rec_cap(cap_), dir_in(dir_) {}
+    __device__ __forceinline__ V3 prev() const { return xyz(ps.prev[p]); }
+    __device__ __forceinline__ void guides(V3 albedo, float t, V3 normal) {
+        store4(ps.galb + p, albedo, t);
+        store4(ps.gnrm + p, normal, 0.0f);
+    }
+    __device__ __forceinline__ void shadow(V3 o, V3 d, float t_max, V3 c) {
+        cast = true;
+        sh_o = o;
+        sh_d = d;
+        sh_t = t_max;
+        sh_c = c;
+    }
+    __device__ __forceinline__ void next(V3 norg, V3 ndir, float npdf, V3 thr, V3 hit_pos, V3 hit_nrm, bool record,
+                                         V3 rad) {
+        store4(ps.o_pdf + p, norg, npdf);
+        store4(ps.dir + p, ndir, 0.0f);
+        __stcs(ps.thr + p, make_float4(thr.x, thr.y, thr.z, __uint_as_float(smp.state)));
+        uint32_t slot1 = 0u;
+        if (kGuided && record) {
+            // Opportunistic warp aggregation of the two counters.
+            const uint32_t lane = threadIdx.x & 31u;
+            uint32_t am = __activemask();
+            uint32_t leader = __ffs(am) - 1u;
+            if (lane == leader) atomicAdd(ps.gmisc + kGmCandidates, (uint32_t)__popc(am));
+            uint32_t h = mix32(p * 0x9E3779B9u ^ (depth << 27) ^ (sbase * 0x85EBCA6Bu));
+            const bool want = (h & 0xFFFFu) < rec_threshold;
+            uint32_t wm = __ballot_sync(am, want);
+            if (want) {
+                uint32_t wl0 = __ffs(wm) - 1u, base = 0;
+                if (lane == wl0) base = atomicAdd(ps.gmisc + kGmRecords, (uint32_t)__popc(wm));
+                base = __shfl_sync(wm, base, wl0);
+                const uint32_t slot = base + (uint32_t)__popc(wm & ((1u << lane) - 1u));
+                if (slot < rec_cap) {
+                    float4* r = ps.rec + kGRecF4 * (size_t)slot;
+                    r[0] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, __uint_as_float(p));
+                    r[1] = make_float4(hit_nrm.x, hit_nrm.y, hit_nrm.z, thr.x);
+                    r[2] = make_float4(-dir_in.x, -dir_in.y, -dir_in.z, thr.y);
+                    r[3] = make_float4(ndir.x, ndir.y, ndir.z, thr.z);
+                    r[4] = make_float4(rad.x, rad.y, rad.z, npdf);
+                    slot1 = slot + 1u;
+                }
+            }
+        }
+        store4(ps.prev + p, hit_pos, __uint_as_float(slot1));
+        survive = true;
+    }
+};
+
 // SHADE (shaders/wavefront/shade.wgsl:119-348), one bounce of
 // integrator.rs:227-400 per queued path.
 //
@@ -222,19 +270,16 @@ __global__ void __launch_bounds__(128, 6) k_shade(PathState ps, const __grid_con
             const FrameParams& fp = kBatch ? job->fp : fp_arg;
             const uint32_t sbase = kBatch ? seg->sample_base : sbase_arg;
             const uint32_t q = kBatch ? p - seg->first : p;  // path index within its own frame
-            const bool last = depth + 1 >= fp.max_depth;
             float4 o4 = ld4(ps.o_pdf + p), d4 = ld4(ps.dir + p), h4 = ld4(ps.hit + p), t4 = ld4(ps.thr + p),
                    r4 = ld4(ps.rad + p);
-            V3 dir = xyz(d4), thr = xyz(t4), rad = xyz(r4);
-            float prev_pdf = o4.w;
-            uint32_t id = __float_as_uint(h4.w);
+            const V3 dir = xyz(d4);
+            V3 rad = xyz(r4);
             uint32_t pixel = (uint32_t)(q % fp.pixels);
             Sampler smp;
             smp.kind = fp.sampler_kind;
             smp.state = __float_as_uint(t4.w);
             smp.index = sbase + (uint32_t)(q / fp.pixels);
             smp.seed = sobol_pixel_seed(pixel, fp.frame_seed);
-            bool rad_changed = false;
             if (kGuided) {
                 // The record made at the previous vertex (slot + 1 in prev.w)
                 // starts its incident-radiance estimate here.
@@ -246,243 +291,18 @@ __global__ void __launch_bounds__(128, 6) k_shade(PathState ps, const __grid_con
                     rs[2] = rad.z;
                 }
             }
-            if (id == kMiss) {
-                // Escaped (integrator.rs:228-263).
-                if (sc.has_env) {
-                    V3 l = env_radiance(sc, dir);
-                    float weight;
-                    if (depth == 0 || fp.sampling == LUC_SAMPLING_BSDF) weight = 1.0f;
-                    else if (fp.sampling == LUC_SAMPLING_NEE) weight = 0.0f;
-                    else {
-                        uint32_t total = max(sc.light_strategies, 1u);
-                        weight = power_heuristic(prev_pdf, env_pdf(sc, dir) / (float)total);
-                    }
-                    if (weight > 0.0f) {
-                        rad = rad + thr * l * weight;
-                        rad_changed = true;
-                    }
-                } else {
-                    rad = rad + thr * sc.background;
-                    rad_changed = true;
-                }
-            } else {
-                V3 org = xyz(o4);
-                SurfaceHit hit = surface_hit_t<kInst>(sc, id, kInst ? ps.hinst[p] : 0u, h4.x, h4.y, h4.z, org, dir);
-                const GpuMaterial m = sc.materials[hit.material];
-                V3 emissive = ld3(m.emissive);
-                // Emission with MIS (integrator.rs:271-309).
-                if (hit.front && max_elem(emissive) > 0.0f) {
-                    float weight;
-                    if (depth == 0 || fp.sampling == LUC_SAMPLING_BSDF) weight = 1.0f;
-                    else if (fp.sampling == LUC_SAMPLING_NEE) weight = 0.0f;
-                    else {
-                        uint32_t n = sc.num_lights, total = sc.light_strategies;
-                        float pdf_light = 0.0f;
-                        V3 prev = xyz(ps.prev[p]);
-                        if (n != 0 && hit.light_area > 0.0f) {  // light.rs:241-263
-                            V3 tl = hit.position - prev;
-                            float d2 = dot(tl, tl);
-                            if (d2 > 0.0f) {
-                                V3 wi = tl / sqrtf(d2);
-                                float cl = dot(hit.gnormal, -wi);
-                                if (cl > 1.0e-6f) pdf_light = 1.0f / ((float)n * hit.light_area) * d2 / cl;
-                            }
-                        }
-                        pdf_light = pdf_light * ((float)n / (float)max(total, 1u));
-                        weight = power_heuristic(prev_pdf, pdf_light);
-                    }
-                    if (weight > 0.0f) {
-                        rad = rad + thr * emissive * weight;
-                        rad_changed = true;
-                    }
-                }
-                Surface surf = make_surface(m, hit.front);
-                if (depth == 0 && fp.guides) {
-                    V3 alb = vmax(surf.diffuse_albedo + surf.f0 + emissive, splat(1.0e-3f));
-                    store4(ps.galb + p, alb, h4.x);
-                    store4(ps.gnrm + p, hit.normal, 0.0f);
-                }
-                V3 wo = to_local(-dir, hit.normal);
-                const bool gv = kGuided && fp.guided && !last && surf.transmission <= 0.0f &&
-                                surf.roughness >= kGuideMinRoughness;
-                const float4* lob = ps.lobes + i;  // this queue position's mixture (SoA planes)
-                if (wo.z > 0.0f) {
-                    // Everything surface::eval / pdf / sample take from wo alone.
-                    const SurfWo sw = surf_wo(surf, sc.energy, wo.z);
-                    // Next event estimation (integrator.rs:349-354, 418-532):
-                    // the light sample and its direction; f and pdf below.
-                    bool nee = false;
-                    V3 wiw{0, 0, 0}, lrad{0, 0, 0}, wi_n{0.0f, 0.0f, 1.0f};
-                    float dist = 0.0f, lpdf = 0.0f;
-                    if ((fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) && !last &&
-                        sc.light_strategies > 0) {
-                        float u_sel = smp.next_f32();
-                        float ua, ub;
-                        smp.next_vec2(ua, ub);
-                        uint32_t nl = sc.num_lights, total = sc.light_strategies;
-                        uint32_t pick = min(f2u(u_sel * (float)total), total - 1u);
-                        bool ok = true;
-                        if (pick < nl) {
-                            float u_light = ((float)pick + 0.5f) / (float)nl;
-                            uint32_t idx = min(f2u(u_light * (float)nl), nl - 1u);
-                            const GpuLight L = sc.lights[idx];
-                            V3 lo = ld3(L.origin), eu = ld3(L.edge_u), ev = ld3(L.edge_v);
-                            V3 point;
-                            if (L.kind == LIGHT_KIND_TRIANGLE) {
-                                float su = sqrtf(ua);
-                                float b1 = 1.0f - su, b2 = ub * su;
-                                point = lo + b1 * eu + b2 * ev;
-                            } else {
-                                point = lo + ua * eu + ub * ev;
-                            }
-                            V3 tl = point - hit.position;
-                            float d2 = dot(tl, tl);
-                            if (d2 <= 0.0f) ok = false;
-                            else {
-                                dist = sqrtf(d2);
-                                wiw = tl / dist;
-                                float cl = dot(ld3(L.normal), -wiw);
-                                if (cl <= 1.0e-6f) ok = false;
-                                else {
-                                    float pa = 1.0f / ((float)nl * L.area);
-                                    float pw = pa * d2 / cl;
-                                    if (!isfinite(pw) || pw <= 0.0f) ok = false;
-                                    else {
-                                        lrad = ld3(sc.materials[L.material].emissive);
-                                        lpdf = pw * ((float)nl / (float)total);
-                                    }
-                                }
-                            }
-                        } else {
-                            EnvSample es = env_sample(sc, ua, ub);
-                            if (es.pdf <= 0.0f) ok = false;
-                            else {
-                                wiw = es.dir;
-                                lrad = es.rad;
-                                dist = __int_as_float(0x7f800000);
-                                lpdf = es.pdf / (float)total;
-                            }
-                        }
-                        if (ok && lpdf > 0.0f) {
-                            wi_n = to_local(wiw, hit.normal);
-                            nee = !(wi_n.z == 0.0f || (wi_n.z < 0.0f && surf.transmission <= 0.0f));
-                        }
-                    }
-                    // BSDF sampling (integrator.rs:360-399): the direction. Skipped
-                    // on the last bounce, where its result would never be read.
-                    // Guided frames choose between the BSDF and the learned
-                    // mixture; the choice dimension is drawn only where the
-                    // guide applies.
-                    bool bsd = false;
-                    V3 wl{0.0f, 0.0f, 1.0f}, wd{0.0f, 0.0f, 1.0f};
-                    if (!last) {
-                        const float u_choice = kGuided && gv ? smp.next_f32() : 0.0f;
-                        const float u_lobe = smp.next_f32();
-                        float ux, uy;
-                        smp.next_vec2(ux, uy);
-                        if (!gv || u_choice < 0.5f) {
-                            bsd = bsdf_sample_dir_w(surf, sw, wo, u_lobe, ux, uy, wl);
-                            wd = to_world(wl, hit.normal);
-                        } else {
-                            wd = mixture_sample_mem(lob, ps.lobe_stride, u_lobe, ux, uy);
-                            wl = to_local(wd, hit.normal);
-                            bsd = !(wl.z == 0.0f || (wl.z < 0.0f && surf.transmission <= 0.0f));
-                        }
-                    }
-                    // f and pdf at both directions through one copy of the
-                    // BSDF code (the loop is kept rolled on purpose: it halves
-                    // the kernel's instruction footprint).
-                    V3 f_n{0.0f, 0.0f, 0.0f}, f_b{0.0f, 0.0f, 0.0f};
-                    float p_n = 0.0f, p_b = 0.0f;
-#pragma unroll 1
-                    for (int k = 0; k < 2; ++k) {
-                        if (!(k == 0 ? nee : bsd)) continue;
-                        const V3 wi = k == 0 ? wi_n : wl;
-                        const V3 f = bsdf_eval_w(surf, sw, wo, wi);
-                        float pdf = 0.0f;
-                        if (k == 1 || (fp.sampling == LUC_SAMPLING_MIS && max_elem(f) > 0.0f))
-                            pdf = bsdf_pdf_w(surf, sw, wo, wi);
-                        if (k == 0) {
-                            f_n = f;
-                            p_n = pdf;
-                        } else {
-                            f_b = f;
-                            p_b = pdf;
-                        }
-                    }
-                    if (nee && max_elem(f_n) > 0.0f) {
-                        float mis = 1.0f;
-                        if (fp.sampling == LUC_SAMPLING_MIS) {
-                            float pb = p_n;
-                            if (gv) pb = 0.5f * pb + 0.5f * mixture_pdf_mem(lob, ps.lobe_stride, wiw);
-                            mis = power_heuristic(lpdf, pb);
-                        }
-                        if (mis > 0.0f) {
-                            sh_o = offset_ray_origin(hit.position, wi_n.z < 0.0f ? -hit.gnormal : hit.gnormal);
-                            sh_d = wiw;
-                            sh_t = dist * (1.0f - 1.0e-3f);
-                            sh_c = thr * (f_n * fabsf(wi_n.z) * lrad * (mis / lpdf));
-                            cast = true;
-                        }
-                    }
-                    if (kGuided && !last) {
-                        const V3 fc = bsd ? f_b * fabsf(wl.z) : splat(0.0f);
-                        if (max_elem(fc) > 0.0f) {
-                            const float pc = gv ? 0.5f * p_b + 0.5f * mixture_pdf_mem(lob, ps.lobe_stride, wd) : p_b;
-                            if (pc > 0.0f) {
-                                thr = thr * (fc / pc);
-                                if (max_elem(thr) > 0.0f) {
-                                    V3 norg = offset_ray_origin(hit.position, wl.z < 0.0f ? -hit.gnormal : hit.gnormal);
-                                    store4(ps.o_pdf + p, norg, pc);
-                                    store4(ps.dir + p, wd, 0.0f);
-                                    __stcs(ps.thr + p, make_float4(thr.x, thr.y, thr.z, __uint_as_float(smp.state)));
-                                    uint32_t slot1 = 0u;
-                                    if (gv && fp.rec_cap) {
-                                        // Opportunistic warp aggregation of the two counters.
-                                        const uint32_t lane = threadIdx.x & 31u;
-                                        uint32_t am = __activemask();
-                                        uint32_t leader = __ffs(am) - 1u;
-                                        if (lane == leader) atomicAdd(ps.gmisc + kGmCandidates, (uint32_t)__popc(am));
-                                        uint32_t h = mix32(p * 0x9E3779B9u ^ (depth << 27) ^ (sbase * 0x85EBCA6Bu));
-                                        const bool want = (h & 0xFFFFu) < rec_threshold;
-                                        uint32_t wm = __ballot_sync(am, want);
-                                        if (want) {
-                                            uint32_t wl0 = __ffs(wm) - 1u, base = 0;
-                                            if (lane == wl0) base = atomicAdd(ps.gmisc + kGmRecords, (uint32_t)__popc(wm));
-                                            base = __shfl_sync(wm, base, wl0);
-                                            const uint32_t slot = base + (uint32_t)__popc(wm & ((1u << lane) - 1u));
-                                            if (slot < fp.rec_cap) {
-                                                float4* r = ps.rec + kGRecF4 * (size_t)slot;
-                                                r[0] = make_float4(hit.position.x, hit.position.y, hit.position.z,
-                                                                   __uint_as_float(p));
-                                                r[1] = make_float4(hit.normal.x, hit.normal.y, hit.normal.z, thr.x);
-                                                r[2] = make_float4(-dir.x, -dir.y, -dir.z, thr.y);
-                                                r[3] = make_float4(wd.x, wd.y, wd.z, thr.z);
-                                                r[4] = make_float4(rad.x, rad.y, rad.z, pc);
-                                                slot1 = slot + 1u;
-                                            }
-                                        }
-                                    }
-                                    store4(ps.prev + p, hit.position, __uint_as_float(slot1));
-                                    survive = true;
-                                }
-                            }
-                        }
-                    } else if (!kGuided && bsd && p_b > 0.0f) {
-                        // surface::sample's weight f |cos| / pdf.
-                        thr = thr * (f_b * (fabsf(wl.z) / p_b));
-                        if (max_elem(thr) > 0.0f) {
-                            V3 norg = offset_ray_origin(hit.position, wl.z < 0.0f ? -hit.gnormal : hit.gnormal);
-                            store4(ps.o_pdf + p, norg, p_b);
-                            store4(ps.dir + p, wd, 0.0f);
-                            __stcs(ps.thr + p, make_float4(thr.x, thr.y, thr.z, __uint_as_float(smp.state)));
-                            store4(ps.prev + p, hit.position, 0.0f);
-                            survive = true;
-                        }
-                    }
-                }
+            PoolSink<kGuided> sink(ps, p, depth, sbase, rec_threshold, fp.rec_cap, dir, smp);
+            if (shade_vertex<kGuided, kInst>(sc, fp, depth, smp, xyz(o4), dir, xyz(t4), rad, o4.w, h4,
+                                             kInst ? ps.hinst[p] : 0u, ps.lobes + i, ps.lobe_stride, sink))
+                store4(ps.rad + p, rad, 0.0f);
+            survive = sink.survive;
+            if (sink.cast) {
+                cast = true;
+                sh_o = sink.sh_o;
+                sh_d = sink.sh_d;
+                sh_t = sink.sh_t;
+                sh_c = sink.sh_c;
             }
-            if (rad_changed) store4(ps.rad + p, rad, 0.0f);
         }
         uint32_t slot = warp_append(next_len, survive);
         if (survive) next_queue[slot] = p;

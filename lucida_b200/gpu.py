@@ -21,13 +21,13 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import layout as L
-from .native import (LUC_FLAG_GUIDED, LUC_FLAG_NO_GUIDES, LUC_FLAG_PROFILE, LUC_FLAG_REFERENCE_SHADOWS,
-                     DenoiseParams as _DP, GpuError, LbvhOut, RenderStats, SceneView, camera_uniforms, check, lib,
+from .native import (LUC_ARCH_MEGAKERNEL, LUC_ARCH_WAVEFRONT, LUC_FLAG_GUIDED, LUC_FLAG_MEASURE,
+                     LUC_FLAG_NO_GUIDES, LUC_FLAG_PROFILE, LUC_FLAG_REFERENCE_SHADOWS, DenoiseParams as _DP, GpuError, LbvhOut, RenderStats, SceneView, camera_uniforms, check, lib,
                      ptr)
 
 __all__ = ["Gpu", "SceneDef", "Camera", "RenderParams", "Film", "render_with", "render_native_on",
            "render_accum", "render_native_denoised", "LbvhBuilder", "GpuBuildOutput", "DenoiseParams",
-           "GpuError", "Denoiser"]
+           "GpuError", "Denoiser", "render_with_measured", "measure_convergence", "convergence"]
 
 
 @dataclass
@@ -263,17 +263,26 @@ def build_uniforms(scene: SceneDef, params: RenderParams) -> L.Uniforms:
     return u
 
 
+ARCHITECTURES = {"wavefront": LUC_ARCH_WAVEFRONT, "megakernel": LUC_ARCH_MEGAKERNEL}
+
+
 def render_accum(gpu: Gpu, scene: SceneDef, params: RenderParams, uniforms: L.Uniforms | None = None,
                  guides: bool = True, profile: bool = False, guided: bool = False,
-                 reference_shadows: bool = False) -> np.ndarray:
+                 reference_shadows: bool = False, architecture: str = "wavefront",
+                 measure: bool = False) -> np.ndarray:
     """Render and return the raw GpuAccum array, shape (height, width).
     guided=True samples with the context's learned guide (lucida_b200.guide),
-    which must have been initialised, and trains it after every batch."""
+    which must have been initialised, and trains it after every batch.
+    architecture: "wavefront" or "megakernel" (same accumulator). measure:
+    run the convergence meter afterwards (gpu.stats().convergence)."""
+    if architecture not in ARCHITECTURES:
+        raise GpuError(-4, f"unknown architecture {architecture!r}")
     gpu.upload(scene)
     u = uniforms if uniforms is not None else build_uniforms(scene, params)
     out = np.zeros(params.width * params.height, L.ACCUM)
-    flags = ((0 if guides else LUC_FLAG_NO_GUIDES) | (LUC_FLAG_PROFILE if profile else 0)
-             | (LUC_FLAG_GUIDED if guided else 0) | (LUC_FLAG_REFERENCE_SHADOWS if reference_shadows else 0))
+    flags = (ARCHITECTURES[architecture] | (0 if guides else LUC_FLAG_NO_GUIDES) | (LUC_FLAG_PROFILE if profile else 0)
+             | (LUC_FLAG_GUIDED if guided else 0) | (LUC_FLAG_REFERENCE_SHADOWS if reference_shadows else 0)
+             | (LUC_FLAG_MEASURE if measure else 0))
     check(gpu.handle, lib().luc_render(gpu.handle, C.byref(u), params.samples, params.max_depth, flags, ptr(out),
                                        None))
     return out.reshape(params.height, params.width)
@@ -286,10 +295,31 @@ def accum_to_film(acc: np.ndarray) -> Film:
 
 
 def render_with(gpu: Gpu, scene: SceneDef, params: RenderParams, arch: str = "wavefront") -> Film:
-    """pt_gpu::render_with (crates/gpu/src/lib.rs:69-79)."""
-    if arch != "wavefront":
-        raise GpuError(-4, f"architecture {arch!r} is not built; only the wavefront integrator is")
-    return accum_to_film(render_accum(gpu, scene, params))
+    """pt_gpu::render_with (crates/gpu/src/lib.rs:69-79): "wavefront" or
+    "megakernel"."""
+    return accum_to_film(render_accum(gpu, scene, params, architecture=arch))
+
+
+def render_with_measured(gpu: Gpu, scene: SceneDef, params: RenderParams, arch: str = "wavefront"):
+    """pt_gpu::render_with_measured (crates/gpu/src/lib.rs:86-97): the film
+    and the convergence meter's figure (-1 when nothing is measurable)."""
+    film = accum_to_film(render_accum(gpu, scene, params, architecture=arch, measure=True))
+    return film, float(gpu.stats().convergence)
+
+
+def measure_convergence(gpu: Gpu, scene: SceneDef, params: RenderParams) -> float:
+    """pt_gpu::measure_convergence (crates/gpu/src/lib.rs:419-426), which
+    renders with the megakernel."""
+    return render_with_measured(gpu, scene, params, "megakernel")[1]
+
+
+def convergence(gpu: Gpu, accum_dev, pixels: int) -> float:
+    """The convergence meter over a device accumulator (torch tensor or
+    address) of `pixels` GpuAccum (ConvergenceMeter::record + read)."""
+    out = C.c_float(0.0)
+    addr = accum_dev if isinstance(accum_dev, int) else accum_dev.data_ptr()
+    check(gpu.handle, lib().luc_convergence(gpu.handle, C.c_void_p(addr), int(pixels), C.byref(out)))
+    return float(out.value)
 
 
 def render_native_on(gpu: Gpu, scene: SceneDef, params: RenderParams) -> Film:

@@ -21,6 +21,9 @@ LUC_FLAG_NO_GUIDES = 0x100
 LUC_FLAG_PROFILE = 0x200
 LUC_FLAG_GUIDED = 0x400
 LUC_FLAG_REFERENCE_SHADOWS = 0x800
+LUC_FLAG_MEASURE = 0x1000
+LUC_ARCH_WAVEFRONT = 0x0
+LUC_ARCH_MEGAKERNEL = 0x1
 LUC_DENOISE_HALF_GUIDES = 0x1
 
 
@@ -62,7 +65,7 @@ class RenderStats(C.Structure):
                 ("launches", C.c_uint64), ("rays_extend", C.c_uint64), ("rays_shadow", C.c_uint64),
                 ("paths", C.c_uint64), ("nodes_extend", C.c_uint64), ("tris_extend", C.c_uint64),
                 ("nodes_shadow", C.c_uint64), ("tris_shadow", C.c_uint64), ("ms_guide", C.c_double),
-                ("ms_train", C.c_double)]
+                ("ms_train", C.c_double), ("convergence", C.c_double)]
 
 
 class BatchJob(C.Structure):
@@ -103,6 +106,7 @@ _SIGS = {
     "luc_eval_env": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p, C.c_void_p,
                                  C.c_void_p]),
     "luc_intersect": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p]),
+    "luc_convergence": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "luc_sort_u32_static": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_char_p,
                                         C.c_uint32]),
     "luc_sort_u32_static_max": (C.c_uint32, []),
