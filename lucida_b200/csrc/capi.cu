@@ -497,8 +497,7 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
         LUC_CUDA(c, cudaMemsetAsync(accum, 0, pixels * sizeof(GpuAccum), s), "clear accumulator");
     }
     uint64_t per_batch = std::max<uint64_t>(1, std::min<uint64_t>(spp, c->path_budget / pixels));
-    // The megakernel keeps paths in registers: only the counters are needed.
-    int32_t rc = ensure_pool(c, mega ? 1 : per_batch * pixels, max_depth);
+    int32_t rc = ensure_pool(c, per_batch * pixels, max_depth);
     if (rc) return rc;
     if (guided) {
         rc = luc_guide_prepare_frame(c, c->rs.capacity);
@@ -546,15 +545,20 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     cudaEventRecord(e0, s);
     const bool one_batch = per_batch >= spp;
     if (mega) {
-        // Every sample of every pixel in one launch, samples in order.
-        fp.sample_base = u->sample_offset;
-        LUC_CUDA(c, cudaMemcpyAsync(c->frame_word.p, &fp.sample_base, 4, cudaMemcpyHostToDevice, s),
-                 "upload sample base");
-        fp.batch_samples = spp;
-        fp.num_paths = (uint64_t)spp * pixels;
-        record_megakernel(c->rs, sc, fp, accum, s);
-        c->rs.launches++;
-        c->stats.paths += fp.num_paths;
+        // Batches of whole samples through the same pool as the wavefront:
+        // one launch walks every path of the batch, then RESOLVE.
+        for (uint32_t done = 0; done < spp;) {
+            uint32_t n = (uint32_t)std::min<uint64_t>(per_batch, spp - done);
+            fp.sample_base = u->sample_offset + done;
+            LUC_CUDA(c, cudaMemcpyAsync(c->frame_word.p, &fp.sample_base, 4, cudaMemcpyHostToDevice, s),
+                     "upload sample base");
+            fp.batch_samples = n;
+            fp.num_paths = (uint64_t)n * pixels;
+            record_megakernel(c->rs, sc, fp, accum, s);
+            c->rs.launches += 2;
+            done += n;
+            c->stats.paths += fp.num_paths;
+        }
     } else if (one_batch && c->use_graphs) {
         // Single-batch frame: capture it once as a CUDA graph and replay it
         // while the frame parameters, scene, pool and accumulator repeat.

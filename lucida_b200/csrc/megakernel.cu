@@ -1,16 +1,17 @@
 // Megakernel architecture (Architecture::Megakernel, crates/gpu/src/lib.rs:
-// 38-79; shaders/trace/megakernel.wgsl:61-266): one thread per pixel walks
-// its samples in order and each sample's path to the end, with the path in
-// registers: camera ray, then per bounce closest hit, shade_vertex (the same
-// function the wavefront's SHADE runs) and the shadow ray traced at once.
-// The radiance of a path is summed in the wavefront's order (emission at a
-// vertex, then that vertex's light sample, then the next vertex) and the
-// samples of a pixel are added onto the accumulator in sample order, as
-// RESOLVE does, so both architectures produce the same accumulator.
+// 38-79; shaders/trace/megakernel.wgsl:61-266): one thread per path (pixel,
+// sample) walks the path to its end with its state in registers: camera ray,
+// then per bounce closest hit, shade_vertex (the function the wavefront's
+// SHADE runs) and the shadow ray traced at once. The path's radiance is
+// summed in the wavefront's order (emission at a vertex, then that vertex's
+// light sample, then the next vertex) and lands in the pool's radiance and
+// guide fields, which RESOLVE adds per pixel in sample order: both
+// architectures produce the same accumulator, bit for bit.
 //
-// No queues and no path pool: the right choice when paths are short and the
-// scene trivial (the reference's README measures it faster there); for
-// divergent, traversal-heavy frames the wavefront wins.
+// No queues and no per-bounce state traffic: what a megakernel buys. On B200
+// the wavefront is faster on both benchmark scenes (divergent paths keep
+// whole warps waiting on their longest lane); the architecture is kept for
+// parity with the reference and as the convergence meter's renderer.
 #include "ctx.cuh"
 #include "shade.cuh"
 
@@ -52,73 +53,57 @@ struct RegSink {
 };
 
 template <bool kInst, int kWide>
-__global__ void __launch_bounds__(128) k_megakernel(const __grid_constant__ DevScene sc,
-                                                    const __grid_constant__ FrameParams fp,
-                                                    GpuAccum* __restrict__ accum, unsigned long long* stat) {
+__global__ void __launch_bounds__(128) k_megakernel(PathState ps, const __grid_constant__ DevScene sc,
+                                                    const __grid_constant__ FrameParams fp) {
     const uint32_t sbase = *fp.sbase;
     TravCount tce, tcs;
     uint32_t rays_e = 0, rays_s = 0;
-    for (uint32_t px = blockIdx.x * blockDim.x + threadIdx.x; px < fp.pixels; px += gridDim.x * blockDim.x) {
-        GpuAccum a = accum[px];
-        V3 r = ld3(a.radiance), r2 = ld3(a.radiance_sq), al = ld3(a.albedo), nn = ld3(a.normal);
-        float dep = a.depth;
-        for (uint32_t j = 0; j < fp.batch_samples; ++j) {
-            Sampler smp = make_sampler(fp.sampler_kind, fp.frame_seed, px, sbase + j);
-            V3 org, dir;
-            camera_ray(fp, px, smp, org, dir);
-            V3 thr{1.0f, 1.0f, 1.0f}, rad{0.0f, 0.0f, 0.0f}, prev = org;
-            float prev_pdf = 0.0f;
-            V3 g_alb{0.0f, 0.0f, 0.0f}, g_nrm{0.0f, 0.0f, 0.0f};
-            float g_dep = 0.0f;
-            for (uint32_t depth = 0; depth < fp.max_depth; ++depth) {
-                float t, u, v;
-                uint32_t inst;
-                const uint32_t id = closest_hit<kInst, kWide>(sc, org, dir, t, u, v, inst, tce);
-                ++rays_e;
-                RegSink sk;
-                sk.prev_v = prev;
-                shade_vertex<false, kInst>(sc, fp, depth, smp, org, dir, thr, rad, prev_pdf,
-                                           make_float4(t, u, v, __uint_as_float(id)), inst, nullptr, 0u, sk);
-                if (sk.guide_hit) {
-                    g_alb = sk.galb;
-                    g_dep = sk.gdepth;
-                    g_nrm = sk.gnrm;
-                }
-                if (sk.cast) {  // CONNECT (shaders/wavefront/connect.wgsl:58-84)
-                    ++rays_s;
-                    if (!occluded<kInst, kWide>(sc, sk.sh_o, sk.sh_d, sk.sh_t, tcs)) rad = rad + sk.sh_c;
-                }
-                if (!sk.survive) break;
-                org = sk.norg;
-                dir = sk.ndir;
-                prev_pdf = sk.npdf;
-                thr = sk.nthr;
-                prev = sk.hit_pos;
+    for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < fp.num_paths;
+         p += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t px = (uint32_t)(p % fp.pixels);
+        Sampler smp = make_sampler(fp.sampler_kind, fp.frame_seed, px, sbase + (uint32_t)(p / fp.pixels));
+        V3 org, dir;
+        camera_ray(fp, px, smp, org, dir);
+        V3 thr{1.0f, 1.0f, 1.0f}, rad{0.0f, 0.0f, 0.0f}, prev = org;
+        float prev_pdf = 0.0f;
+        RegSink first;  // first-hit guides
+        for (uint32_t depth = 0; depth < fp.max_depth; ++depth) {
+            float t, u, v;
+            uint32_t inst;
+            const uint32_t id = closest_hit<kInst, kWide>(sc, org, dir, t, u, v, inst, tce);
+            ++rays_e;
+            RegSink sk;
+            sk.prev_v = prev;
+            shade_vertex<false, kInst>(sc, fp, depth, smp, org, dir, thr, rad, prev_pdf,
+                                       make_float4(t, u, v, __uint_as_float(id)), inst, nullptr, 0u, sk);
+            if (sk.guide_hit) first = sk;
+            if (sk.cast) {  // CONNECT (shaders/wavefront/connect.wgsl:58-84)
+                ++rays_s;
+                if (!occluded<kInst, kWide>(sc, sk.sh_o, sk.sh_d, sk.sh_t, tcs)) rad = rad + sk.sh_c;
             }
-            // RESOLVE (shaders/wavefront/resolve.wgsl:14-48), one sample.
-            r = r + rad;
-            r2 = r2 + rad * rad;
-            if (fp.guides) {
-                al = al + g_alb;
-                dep = dep + g_dep;
-                nn = nn + g_nrm;
-            }
+            if (!sk.survive) break;
+            org = sk.norg;
+            dir = sk.ndir;
+            prev_pdf = sk.npdf;
+            thr = sk.nthr;
+            prev = sk.hit_pos;
         }
-        a.radiance[0] = r.x; a.radiance[1] = r.y; a.radiance[2] = r.z;
-        a.radiance_sq[0] = r2.x; a.radiance_sq[1] = r2.y; a.radiance_sq[2] = r2.z;
-        a.albedo[0] = al.x; a.albedo[1] = al.y; a.albedo[2] = al.z;
-        a.normal[0] = nn.x; a.normal[1] = nn.y; a.normal[2] = nn.z;
-        a.depth = dep;
-        a.samples = a.samples + (float)fp.batch_samples;
-        accum[px] = a;
+        __stcs(ps.rad + p, make_float4(rad.x, rad.y, rad.z, 0.0f));
+        if (fp.guides) {
+            ps.galb[p] = first.guide_hit ? make_float4(first.galb.x, first.galb.y, first.galb.z, first.gdepth)
+                                         : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            ps.gnrm[p] = first.guide_hit ? make_float4(first.gnrm.x, first.gnrm.y, first.gnrm.z, 0.0f)
+                                         : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
     }
-    // One atomic per warp per counter.
+    // One atomic per warp per counter (every lane reaches here: the loop
+    // above has no early exit).
     unsigned long long v[6] = {rays_e, tce.nodes, tce.tris, rays_s, tcs.nodes, tcs.tris};
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
         unsigned long long x = v[k];
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xFFFFFFFFu, x, o);
-        if ((threadIdx.x & 31u) == 0) atomicAdd(stat + k, x);
+        if ((threadIdx.x & 31u) == 0) atomicAdd(ps.stat + k, x);
     }
 }
 
@@ -131,23 +116,21 @@ int blocks_per_sm() {
 
 }  // namespace
 
-// One launch: every pixel, fp.batch_samples samples from *fp.sbase on.
+// One batch: every path in one launch, then RESOLVE.
 void record_megakernel(const RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum,
                        cudaStream_t s) {
-    const uint64_t want = (fp.pixels + 127) / 128;
+    const uint64_t want = (fp.num_paths + 127) / 128;
     if (sc.num_instances) {
         static const int b = blocks_per_sm<true, 0>();
-        k_megakernel<true, 0><<<(int)std::min<uint64_t>(want, (uint64_t)rs.num_sms * b), 128, 0, s>>>(sc, fp, accum,
-                                                                                                      rs.ps.stat);
+        k_megakernel<true, 0><<<(int)std::min<uint64_t>(want, (uint64_t)rs.num_sms * b), 128, 0, s>>>(rs.ps, sc, fp);
     } else if (sc.wnodes) {
         static const int b = blocks_per_sm<false, 1>();
-        k_megakernel<false, 1><<<(int)std::min<uint64_t>(want, (uint64_t)rs.num_sms * b), 128, 0, s>>>(sc, fp, accum,
-                                                                                                       rs.ps.stat);
+        k_megakernel<false, 1><<<(int)std::min<uint64_t>(want, (uint64_t)rs.num_sms * b), 128, 0, s>>>(rs.ps, sc, fp);
     } else {
         static const int b = blocks_per_sm<false, 0>();
-        k_megakernel<false, 0><<<(int)std::min<uint64_t>(want, (uint64_t)rs.num_sms * b), 128, 0, s>>>(sc, fp, accum,
-                                                                                                       rs.ps.stat);
+        k_megakernel<false, 0><<<(int)std::min<uint64_t>(want, (uint64_t)rs.num_sms * b), 128, 0, s>>>(rs.ps, sc, fp);
     }
+    launch_resolve(rs, fp, accum, s);
 }
 
 }  // namespace luc

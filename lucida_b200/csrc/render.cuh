@@ -142,10 +142,12 @@ struct GuideTrain {
 
 void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream,
                   StageTimer* timer, const GuideTrain* gt);
-// megakernel.cu: one launch of the megakernel architecture over every pixel
-// (fp.batch_samples samples each, from *fp.sbase), accumulating like RESOLVE.
+// megakernel.cu: one batch of the megakernel architecture (every path of
+// fp.num_paths from start to end in one launch, then RESOLVE).
 void record_megakernel(const RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum,
                        cudaStream_t s);
+// wavefront.cu: RESOLVE of one batch from the pool's radiance and guides.
+void launch_resolve(const RenderState& rs, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream);
 // One wave of a batched render (wavefront.cu); `block` is the EXTEND /
 // CONNECT block size (64, 128 or 256).
 // `wide`: every scene of the batch traverses a wide tree (or has no

@@ -237,12 +237,12 @@ struct PoolSink {
 // kBatch: the path's scene and frame parameters come from its wave segment
 // (luc_render_batch) instead of the kernel arguments.
 //
-// 6 blocks of 128 per SM (80 registers, a few hundred bytes spilled): SHADE is
+// 7 blocks of 128 per SM (72 registers, a few hundred bytes spilled): SHADE is
 // bound by the latency of its path-state, triangle and material loads, and
-// the extra warps hide more of it than the spills cost (measured against 4
-// blocks without spills).
+// the extra warps hide more of it than the spills cost (measured against 4,
+// 5 and 6 blocks).
 template <bool kGuided, bool kInst, bool kBatch = false>
-__global__ void __launch_bounds__(128, 6) k_shade(PathState ps, const __grid_constant__ DevScene sc_arg,
+__global__ void __launch_bounds__(128, 7) k_shade(PathState ps, const __grid_constant__ DevScene sc_arg,
                                                   const __grid_constant__ FrameParams fp_arg, BatchDev bd,
                                                   uint32_t depth) {
     const uint32_t len = depth == 0 ? (uint32_t)fp_arg.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
@@ -533,6 +533,11 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
         rs.launches += 4;
     }
     if (timer) timer->mark(stream, StageTimer::kEnd);
+}
+
+// RESOLVE of one batch (the megakernel's paths end in the same pool fields).
+void launch_resolve(const RenderState& rs, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream) {
+    k_resolve<<<rs.num_sms * 8, 256, 0, stream>>>(rs.ps, fp, accum);
 }
 
 }  // namespace luc

@@ -42,7 +42,7 @@ def test_megakernel_equals_wavefront(gpu, name, mode):
         assert w.tobytes() == m.tobytes(), (name, mode, sampler)
         assert (sw.rays_extend, sw.rays_shadow, sw.nodes_extend, sw.tris_extend, sw.nodes_shadow) == \
                (sm.rays_extend, sm.rays_shadow, sm.nodes_extend, sm.tris_extend, sm.nodes_shadow)
-        assert sm.paths == sw.paths == 64 * 48 * 6 and sm.launches == 1
+        assert sm.paths == sw.paths == 64 * 48 * 6 and sm.launches == 2  # one walk + RESOLVE
 
 
 def test_megakernel_on_triangle_workload_and_instances(gpu):
