@@ -17,41 +17,15 @@ import base64
 import hashlib
 import json
 import os
-import re
 import sys
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", ".."))
+from lucida_b200.packed import parse_manifest  # noqa: E402
 
 SECTIONS = ["materials", "primitives", "lights", "positions", "vertexAttrs", "triangles", "bvhNodes",
             "envRadiance", "envCdf"]
 ELEM = {"materials": 80, "primitives": 64, "lights": 64, "positions": 16, "vertexAttrs": 32,
         "triangles": 16, "bvhNodes": 32, "envRadiance": 16, "envCdf": 4}
-
-
-def parse_manifest(text):
-    scenes = {}
-    for block in re.split(r"\n  \{\n", text)[1:]:
-        name = re.search(r'name: "([^"]+)"', block).group(1)
-        rec = {"asset": re.search(r'asset: "([^"]+)"', block).group(1),
-               "byteLength": int(re.search(r"byteLength: (\d+)", block).group(1)),
-               "remote": "remote: null" not in block}
-        rec["sections"] = {}
-        for s in SECTIONS:
-            m = re.search(r"%s: \{ byteOffset: (\d+), count: (\d+) \}" % s, block)
-            rec["sections"][s] = (int(m.group(1)), int(m.group(2)))
-        inst = re.search(r"instancing: \{ count: (\d+), analyticPrimitives: (\d+), tlasRoot: (\d+) \}", block)
-        rec["instancing"] = [int(inst.group(i)) for i in (1, 2, 3)]
-        env = re.search(r"env: \{ width: (\d+), height: (\d+), totalWeight: ([-0-9.e+]+) \}", block)
-        rec["env"] = [int(env.group(1)), int(env.group(2)), float(env.group(3))]
-        bg = re.search(r"background: \[([^\]]*)\]", block).group(1)
-        rec["background"] = [float(x) for x in bg.split(",")]
-        cam = re.search(r"camera: \{ eye: \[([^\]]*)\], lookAt: \[([^\]]*)\], up: \[([^\]]*)\], "
-                        r"vfovDeg: ([-0-9.e]+), aperture: ([-0-9.e]+), focusDistance: ([-0-9.e]+) \}", block)
-        rec["camera"] = {"eye": [float(x) for x in cam.group(1).split(",")],
-                         "look_at": [float(x) for x in cam.group(2).split(",")],
-                         "up": [float(x) for x in cam.group(3).split(",")],
-                         "vfov_deg": float(cam.group(4)), "aperture": float(cam.group(5)),
-                         "focus_distance": float(cam.group(6))}
-        scenes[name] = rec
-    return scenes
 
 
 def main(root):

@@ -142,6 +142,49 @@ def test_progressive_equals_one_shot(gpu):
     assert np.all(prog["samples"] == 8)
 
 
+@pytest.mark.parametrize("depth", [1, 2, 4, 8, 16])
+def test_agreement_across_path_lengths(gpu, depth):
+    """cpu_gpu_agreement.rs:93-117: cornell-box at max_depth 1, 2, 4, 8, 16."""
+    acc, ref = _render_both(gpu, O.Scene.builtin("cornell-box"), 48, 48, 8, depth)
+    _check(acc, ref, f"depth {depth}")
+
+
+def test_deep_dielectric_paths(gpu):
+    """cpu_gpu_agreement.rs:521-569: glass-box at max_depth 24."""
+    acc, ref = _render_both(gpu, O.Scene.builtin("glass-box"), 64, 48, 8, 24)
+    _check(acc, ref, "glass-box d24")
+
+
+def test_empty_primitive_arrays(gpu):
+    """cpu_gpu_agreement.rs:174-198: cornell-box without its analytic
+    primitives (lights and all) renders and agrees with the oracle."""
+    osc = O.Scene.builtin("cornell-box")
+    s = scene_from_oracle(osc)
+    empty = lb.SceneDef(materials=s.materials, primitives=s.primitives[:0], lights=s.lights[:0],
+                        positions=s.positions, vertex_attrs=s.vertex_attrs, triangles=s.triangles,
+                        camera=s.camera, background=s.background)
+    bare = O.Scene.from_arrays(s.materials.view(O.MATERIAL), s.primitives[:0].view(O.PRIMITIVE), s.positions,
+                               s.vertex_attrs.view(O.VERTEX_ATTR), s.triangles.view(O.TRIANGLE),
+                               lights=s.lights[:0].view(O.LIGHT), background=s.background,
+                               camera=dict(eye=s.camera.eye, look_at=s.camera.look_at, vfov_deg=s.camera.vfov_deg,
+                                           up=s.camera.up, aperture=s.camera.aperture,
+                                           focus_distance=s.camera.focus_distance), bvh="sah")
+    acc, ref = _render_both(gpu, bare, 48, 48, 8, 3, scene=empty)
+    assert np.array_equal(acc["radiance"], ref[:, 0:3].reshape(acc["radiance"].shape))
+
+
+def test_furnace_spheres_invisible(gpu):
+    """cpu_gpu_agreement.rs:347-375: in the white furnace the energy-
+    conserving metal spheres vanish: mean radiance 1 within 3e-3 at 24
+    bounces (the reference's 160x80, 512 spp)."""
+    s = scene_from_oracle(O.Scene.builtin("furnace-test"))
+    f = lb.render_with(gpu, s, lb.RenderParams(width=160, height=80, samples=512, max_depth=24))
+    assert np.all(np.isfinite(f.data))
+    mean = float(f.data[..., 0].astype(np.float64).mean())
+    print("furnace mean", mean, "worst", float(np.abs(f.data[..., 0] - 1.0).max()))
+    assert abs(mean - 1.0) < 3e-3
+
+
 def test_depth_sweep_energy_monotone(gpu):
     """integrator.rs:803-833: raising the bounce limit only adds energy."""
     s = scenes.cornell_analytic()
