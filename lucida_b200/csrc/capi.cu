@@ -159,7 +159,7 @@ void luc_destroy(luc_ctx* c) {
     DevBuf* bufs[] = {&c->materials, &c->prims,    &c->lights,   &c->positions, &c->attrs,     &c->tris,
                       &c->nodes,     &c->env_px,   &c->env_cond, &c->env_marg,  &c->env_row_sin, &c->energy,
                       &c->tnodes,    &c->soup,     &c->frame_word, &c->blas_roots, &c->wnodes,  &c->wsoup,
-                      &c->wtasks,    &c->wctr,     &c->conv_scratch,
+                      &c->wtasks,    &c->wctr,     &c->conv_scratch, &c->wroots, &c->blas_wide,
                       &c->pool,      &c->accum_tmp, &c->lb_tris, &c->lb_pos,    &c->lb_boxes,  &c->lb_keys,
                       &c->lb_vals,   &c->lb_keys2, &c->lb_vals2, &c->lb_hist,   &c->lb_karras, &c->lb_parent,
                       &c->lb_nbounds, &c->lb_subtree, &c->lb_flags, &c->lb_nodes, &c->lb_rank, &c->lb_misc,
@@ -346,6 +346,12 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
         if (c->use_wide && !ni && !meshes) {
             rc2 = luc_build_wide(c, num_nodes, v->num_triangles);
             if (rc2) return rc2;
+        } else if (c->use_wide) {
+            // Two-level scenes: one wide tree per BLAS (the TLAS stays binary,
+            // rebuilt per frame); instances reach theirs through blas_wide.
+            const std::vector<uint32_t>& br = meshes ? c->host_mesh_root : roots;
+            rc2 = luc_build_wide_roots(c, br.data(), (uint32_t)br.size(), true, num_nodes, v->num_triangles);
+            if (rc2) return rc2;
         }
     }
     LUC_CUDA(c, cudaStreamSynchronize(s), "scene upload");
@@ -372,6 +378,7 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     d.soup = c->soup.as<float4>();
     d.wnodes = c->wide_nodes ? c->wnodes.as<float4>() : nullptr;
     d.wsoup = c->wide_nodes ? c->wsoup.as<float4>() : nullptr;
+    d.blas_wide = c->wide_nodes && (ni || meshes) ? c->blas_wide.as<uint32_t>() : nullptr;
     d.root_first = 0;
     d.root_count = 0;
     if (d.num_nodes) {

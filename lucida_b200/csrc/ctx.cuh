@@ -49,6 +49,7 @@ struct luc_ctx {
     DevBuf materials, prims, lights, positions, attrs, tris, nodes, env_px, env_cond, env_marg, env_row_sin, energy;
     DevBuf tnodes, soup;  // traversal layout derived from nodes / tris
     DevBuf wnodes, wsoup, wtasks, wctr;  // compressed 8-wide tree (wide.cu)
+    DevBuf wroots, blas_wide;            // its roots; BLAS binary root -> wide root (two-level scenes)
     DevBuf conv_scratch;                 // convergence meter partials + result (stats.cu)
     uint32_t wide_nodes = 0;             // 0: the scene traverses the binary tree
     bool use_wide = true;                // LUC_BINARY_BVH=1 turns the wide tree off
@@ -129,6 +130,10 @@ int32_t luc_record_convergence(luc_ctx* c, const GpuAccum* accum, uint32_t pixel
 // wide.cu: collapse the binary tree into c->wnodes / c->wsoup (sets
 // c->wide_nodes; 0 when the tree is too deep for the level budget).
 int32_t luc_build_wide(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris);
+// The same over several roots (one wide tree each, wide node k = roots[k]'s
+// tree); with `map`, fills c->blas_wide (binary root -> wide root).
+int32_t luc_build_wide_roots(luc_ctx* c, const uint32_t* roots, uint32_t nroots, bool map, uint32_t num_nodes,
+                             uint32_t num_tris);
 int32_t luc_build_tnodes_range(luc_ctx* c, uint32_t begin, uint32_t end);
 // Implemented in instances.cu: one LBVH per mesh range of the triangles in
 // lb_tris into c->nodes / c->tris (see luc_upload_meshes).

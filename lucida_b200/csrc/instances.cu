@@ -281,8 +281,10 @@ int32_t luc_set_instances(luc_ctx* c, const float* object_to_world, const uint32
     d.num_prims = np_;
     d.nodes = c->nodes.as<float4>();
     d.tnodes = c->tnodes.as<float4>();
-    d.wnodes = nullptr;  // two-level scenes traverse binary BLASes and TLAS
-    d.wsoup = nullptr;
+    // The BLASes' wide trees (built at upload) stay; the TLAS is binary.
+    d.wnodes = c->wide_nodes ? c->wnodes.as<float4>() : nullptr;
+    d.wsoup = c->wide_nodes ? c->wsoup.as<float4>() : nullptr;
+    d.blas_wide = c->wide_nodes ? c->blas_wide.as<uint32_t>() : nullptr;
     d.num_nodes = bn + 2 * c->inst_capacity;  // fixed while the capacity holds, so frame graphs keep replaying
     d.inst = reinterpret_cast<const GpuInstance*>(d.prims + np_);
     d.num_instances = n;

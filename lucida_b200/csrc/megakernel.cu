@@ -120,7 +120,10 @@ int blocks_per_sm() {
 void record_megakernel(const RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum,
                        cudaStream_t s) {
     const uint64_t want = (fp.num_paths + 127) / 128;
-    if (sc.num_instances) {
+    if (sc.num_instances && sc.blas_wide) {
+        static const int b = blocks_per_sm<true, 1>();
+        k_megakernel<true, 1><<<(int)std::min<uint64_t>(want, (uint64_t)rs.num_sms * b), 128, 0, s>>>(rs.ps, sc, fp);
+    } else if (sc.num_instances) {
         static const int b = blocks_per_sm<true, 0>();
         k_megakernel<true, 0><<<(int)std::min<uint64_t>(want, (uint64_t)rs.num_sms * b), 128, 0, s>>>(rs.ps, sc, fp);
     } else if (sc.wnodes) {

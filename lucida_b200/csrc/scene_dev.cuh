@@ -24,6 +24,9 @@ struct DevScene {
     // scene traverses the binary tree (instanced scenes, LUC_BINARY_BVH=1).
     const float4* wnodes;  // 5 float4 per wide node, root = node 0
     const float4* wsoup;   // (p0 | leaf-order index in p0.w, e1, e2) per triangle, wide-node order
+    // Two-level scenes: the wide trees are the BLASes'; blas_wide maps a BLAS's
+    // binary root (an instance row's blas_root) to its wide root.
+    const uint32_t* blas_wide;
     uint32_t root_first, root_count;  // the root when it is itself a leaf
     // Instancing (instance.rs): GpuInstance rows appended after the analytic
     // primitives, in TLAS-leaf order; the TLAS's first node in `nodes`; the
@@ -398,15 +401,15 @@ LUC_D void wide_node(const float4* __restrict__ wn, uint32_t node, V3 o, V3 inv,
 // (after Ylitie, Karras and Laine 2017, compressed wide BVHs; their deferral
 // of triangle groups while few lanes have one measured slower here).
 template <bool kAny>
-LUC_D bool wide_trace(const DevScene& s, V3 o, V3 d, float tmin, float& tmax, float& bu, float& bv, uint32_t& btri,
-                      TravCount& tc) {
+LUC_D bool wide_trace(const DevScene& s, uint32_t root, V3 o, V3 d, float tmin, float& tmax, float& bu, float& bv,
+                      uint32_t& btri, TravCount& tc) {
     const V3 inv = safe_inv_dir(d);
     const uint32_t oct = (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) | (inv.z < 0.0f ? 4u : 0u);
     uint2 stack[kWideStack];
     int sp = 0;
     // Start from a virtual parent whose only child (slot 0, internal) is the
     // root, so the root's own triangles go through the triangle phase too.
-    uint2 g = make_uint2(0u, (1u << 8) | (1u << oct)), t = make_uint2(0u, 0u);
+    uint2 g = make_uint2(root, (1u << 8) | (1u << oct)), t = make_uint2(0u, 0u);
     bool found = false;
     // Each node and triangle is visited at most once per ray in a tree; the
     // guard only bounds the loop should the arrays ever not form one.
@@ -479,6 +482,8 @@ LUC_D V3 inst_normal(const GpuInstance& g, V3 n) {
 // rows), and at each instance walk its BLAS with the ray in object space and
 // the closest t so far — the transform keeps t, so one t_max serves both
 // levels. The returned triangle index is absolute; `instance` indexes s.inst.
+// kWide: the BLASes are walked through their wide trees (s.blas_wide).
+template <int kWide>
 LUC_D bool instances_closest(const DevScene& s, V3 o, V3 d, float tmin, float& closest, float& bu, float& bv,
                              uint32_t& btri, uint32_t& binst, TravCount& tc) {
     const V3 inv = safe_inv_dir(d);
@@ -510,8 +515,11 @@ LUC_D bool instances_closest(const DevScene& s, V3 o, V3 d, float tmin, float& c
             for (uint32_t ii = cur.a; ii < cur.a + cur.cnt; ++ii) {
                 const uint32_t k = ii - s.num_prims;
                 const GpuInstance g = s.inst[k];
-                if (bvh_closest(s, node_ref(s, g.blas_root), inst_point(g, o), inst_vector(g, d), tmin, closest, bu, bv,
-                                btri, tc)) {
+                const bool h = kWide ? wide_trace<false>(s, __ldg(s.blas_wide + g.blas_root), inst_point(g, o),
+                                                         inst_vector(g, d), tmin, closest, bu, bv, btri, tc)
+                                     : bvh_closest(s, node_ref(s, g.blas_root), inst_point(g, o), inst_vector(g, d),
+                                                   tmin, closest, bu, bv, btri, tc);
+                if (h) {
                     binst = k;
                     found = true;
                 }
@@ -524,6 +532,7 @@ LUC_D bool instances_closest(const DevScene& s, V3 o, V3 d, float tmin, float& c
 }
 
 // Any hit through the two levels (the default for shadow rays).
+template <int kWide>
 LUC_D bool instances_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax, TravCount& tc) {
     const V3 inv = safe_inv_dir(d);
     const V3 oi = V3{o.x * inv.x, o.y * inv.y, o.z * inv.z};
@@ -551,7 +560,11 @@ LUC_D bool instances_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax, 
         } else {
             for (uint32_t ii = cur.a; ii < cur.a + cur.cnt; ++ii) {
                 const GpuInstance g = s.inst[ii - s.num_prims];
-                if (bvh_any(s, node_ref(s, g.blas_root), inst_point(g, o), inst_vector(g, d), tmin, tmax, tc))
+                float tm = tmax, bu, bv;
+                uint32_t bt;
+                if (kWide ? wide_trace<true>(s, __ldg(s.blas_wide + g.blas_root), inst_point(g, o), inst_vector(g, d),
+                                             tmin, tm, bu, bv, bt, tc)
+                          : bvh_any(s, node_ref(s, g.blas_root), inst_point(g, o), inst_vector(g, d), tmin, tmax, tc))
                     return true;
             }
         }
@@ -588,11 +601,14 @@ LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, fl
     uint32_t tri;
     inst = 0u;
     if (kInst) {
-        if (instances_closest(s, o, d, kTMin, best_t, bu, bv, tri, inst, tc)) id = tri;
+        const bool h = kWide == 1 || (kWide == 2 && s.blas_wide)
+                           ? instances_closest<1>(s, o, d, kTMin, best_t, bu, bv, tri, inst, tc)
+                           : instances_closest<0>(s, o, d, kTMin, best_t, bu, bv, tri, inst, tc);
+        if (h) id = tri;
     } else if (kWide == 1) {
-        if (s.wnodes && wide_trace<false>(s, o, d, kTMin, best_t, bu, bv, tri, tc)) id = tri;
+        if (s.wnodes && wide_trace<false>(s, 0u, o, d, kTMin, best_t, bu, bv, tri, tc)) id = tri;
     } else if (kWide == 2 && s.wnodes) {
-        if (wide_trace<false>(s, o, d, kTMin, best_t, bu, bv, tri, tc)) id = tri;
+        if (wide_trace<false>(s, 0u, o, d, kTMin, best_t, bu, bv, tri, tc)) id = tri;
     } else if (s.num_nodes > 0 && bvh_closest(s, TRef{s.root_count ? s.root_first : 0u, s.root_count}, o, d, kTMin,
                                               best_t, bu, bv, tri, tc)) {
         id = tri;
@@ -627,11 +643,18 @@ LUC_D bool occluded(const DevScene& s, V3 o, V3 d, float tmax, TravCount& tc) {
         if (h) return true;
     }
     if (kInst) {
-        if (!s.reference_shadows) return instances_any(s, o, d, kTMin, tmax, tc);
+        const bool wide = kWide == 1 || (kWide == 2 && s.blas_wide);
+        if (!s.reference_shadows) return wide ? instances_any<1>(s, o, d, kTMin, tmax, tc)
+                                              : instances_any<0>(s, o, d, kTMin, tmax, tc);
         // The reference's shadow rays (scene.rs:577-606) test every mesh's
         // triangles untransformed, in object space.
-        for (uint32_t b = 0; b < s.num_blas; ++b)
-            if (bvh_any(s, node_ref(s, s.blas_roots[b]), o, d, kTMin, tmax, tc)) return true;
+        for (uint32_t b = 0; b < s.num_blas; ++b) {
+            float tm = tmax, bu, bv;
+            uint32_t bt;
+            if (wide ? wide_trace<true>(s, __ldg(s.blas_wide + s.blas_roots[b]), o, d, kTMin, tm, bu, bv, bt, tc)
+                     : bvh_any(s, node_ref(s, s.blas_roots[b]), o, d, kTMin, tmax, tc))
+                return true;
+        }
         return false;
     }
     if (kWide == 1 && !s.wnodes) return false;  // no triangles
@@ -646,7 +669,7 @@ LUC_D bool occluded(const DevScene& s, V3 o, V3 d, float tmax, TravCount& tc) {
     if (kWide == 1 || (kWide == 2 && s.wnodes)) {
         float tm = tmax, bu, bv;
         uint32_t bt;
-        return wide_trace<true>(s, o, d, kTMin, tm, bu, bv, bt, tc);
+        return wide_trace<true>(s, 0u, o, d, kTMin, tm, bu, bv, bt, tc);
     }
     return bvh_any(s, TRef{s.root_count ? s.root_first : 0u, s.root_count}, o, d, kTMin, tmax, tc);
 }

@@ -77,14 +77,28 @@ __device__ __forceinline__ float half_area(const Child& c) {
     return dx * dy + dy * dz + dz * dx;
 }
 
-__global__ void k_wide_init(const float4* __restrict__ nodes, uint4* __restrict__ tasks, uint32_t* __restrict__ ctr) {
-    const uint32_t cnt = __float_as_uint(nodes[1].w), lf = __float_as_uint(nodes[0].w);
-    tasks[0] = cnt == 0 ? make_uint4(0u, lf, 0u, kKindInternal) : make_uint4(0u, lf, cnt, kKindChunk);
-    ctr[kWcBegin] = 0;
-    ctr[kWcEnd] = 1;
-    ctr[kWcAlloc] = 1;
-    ctr[kWcSoup] = 0;
-    ctr[kWcErr] = 0;
+// Task k = binary root roots[k] (wide node k); map[roots[k]] = k when given.
+__global__ void k_wide_init(const float4* __restrict__ nodes, uint32_t num_nodes, const uint32_t* __restrict__ roots,
+                            uint32_t nroots, uint4* __restrict__ tasks, uint32_t* __restrict__ map,
+                            uint32_t* __restrict__ ctr) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0) {
+        ctr[kWcBegin] = 0;
+        ctr[kWcEnd] = nroots;
+        ctr[kWcAlloc] = nroots;
+        ctr[kWcSoup] = 0;
+        ctr[kWcErr] = 0;
+    }
+    if (k >= nroots) return;
+    const uint32_t r = roots[k];
+    if (r >= num_nodes) {
+        atomicOr(ctr + kWcErr, kErrTree);
+        tasks[k] = make_uint4(0u, 0u, 0u, kKindChunk);  // empty chunk: no reads
+        return;
+    }
+    const uint32_t cnt = __float_as_uint(nodes[2 * (size_t)r + 1].w), lf = __float_as_uint(nodes[2 * (size_t)r].w);
+    tasks[k] = cnt == 0 ? make_uint4(r, lf, 0u, kKindInternal) : make_uint4(r, lf, cnt, kKindChunk);
+    if (map) map[r] = k;
 }
 
 __global__ void k_wide_advance(uint32_t* __restrict__ ctr) {
@@ -314,21 +328,34 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
 }  // namespace luc
 
 // Collapse the resident binary tree (c->nodes, c->soup in leaf order) into
-// c->wnodes / c->wsoup. Leaves c->wide_nodes = 0 (binary traversal) when the
-// tree is deeper than the level budget; fails on a malformed tree.
-int32_t luc_build_wide(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris) {
+// c->wnodes / c->wsoup: one wide tree per root in `roots` (host array; wide
+// node k is the root of the tree of roots[k]), whose trees must together
+// cover every triangle. With `map`, c->blas_wide[roots[k]] = k (two-level
+// scenes reach a BLAS's wide tree from its binary root). Leaves
+// c->wide_nodes = 0 (binary traversal) when a tree is deeper than the level
+// budget or the trees miss triangles; fails on a malformed tree.
+int32_t luc_build_wide_roots(luc_ctx* c, const uint32_t* roots, uint32_t nroots, bool map, uint32_t num_nodes,
+                             uint32_t num_tris) {
     using namespace luc;
     c->wide_nodes = 0;
-    if (!num_nodes || !num_tris) return LUC_OK;
-    const uint64_t cap = 2ull * num_nodes + num_tris / kChunkTris + 8;
+    if (!num_nodes || !num_tris || !nroots) return LUC_OK;
+    const uint64_t cap = 2ull * num_nodes + num_tris / kChunkTris + nroots + 8;
     if (cap > 0x7FFFFFFFull) return LUC_OK;
     cudaStream_t s = c->stream;
     LUC_CUDA(c, c->wnodes.ensure(cap * 80), "alloc wide nodes");
     LUC_CUDA(c, c->wsoup.ensure((size_t)num_tris * 48), "alloc wide soup");
     LUC_CUDA(c, c->wtasks.ensure(cap * 16), "alloc wide tasks");
     LUC_CUDA(c, c->wctr.ensure(kWcWords * 4), "alloc wide counters");
+    LUC_CUDA(c, upload(c->wroots, roots, nroots, s), "upload wide roots");
+    uint32_t* wmap = nullptr;
+    if (map) {
+        LUC_CUDA(c, c->blas_wide.ensure((size_t)num_nodes * 4), "alloc wide root map");
+        LUC_CUDA(c, cudaMemsetAsync(c->blas_wide.p, 0xFF, (size_t)num_nodes * 4, s), "clear wide root map");
+        wmap = c->blas_wide.as<uint32_t>();
+    }
     uint32_t* ctr = c->wctr.as<uint32_t>();
-    k_wide_init<<<1, 1, 0, s>>>(c->nodes.as<float4>(), c->wtasks.as<uint4>(), ctr);
+    k_wide_init<<<(nroots + 127) / 128, 128, 0, s>>>(c->nodes.as<float4>(), num_nodes, c->wroots.as<uint32_t>(),
+                                                      nroots, c->wtasks.as<uint4>(), wmap, ctr);
     const int grid = c->num_sms * 8;
     constexpr int kLevelsPerSync = 12, kMaxLevels = 240;
     uint32_t h[kWcWords] = {};
@@ -349,4 +376,9 @@ int32_t luc_build_wide(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris) {
     if (h[kWcBegin] != h[kWcEnd] || h[kWcSoup] != num_tris) return LUC_OK;  // too deep: binary traversal
     c->wide_nodes = h[kWcAlloc];
     return LUC_OK;
+}
+
+int32_t luc_build_wide(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris) {
+    const uint32_t root = 0;
+    return luc_build_wide_roots(c, &root, 1, false, num_nodes, num_tris);
 }
