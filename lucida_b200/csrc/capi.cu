@@ -1,5 +1,6 @@
 // The C ABI of liblucida_cuda.so (include/luc_cuda.h): context, scene
 // residency, and the render(scene, camera, spp, bounces) entry point.
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -159,7 +160,7 @@ void luc_destroy(luc_ctx* c) {
     DevBuf* bufs[] = {&c->materials, &c->prims,    &c->lights,   &c->positions, &c->attrs,     &c->tris,
                       &c->nodes,     &c->env_px,   &c->env_cond, &c->env_marg,  &c->env_row_sin, &c->energy,
                       &c->tnodes,    &c->soup,     &c->frame_word, &c->blas_roots, &c->wnodes,  &c->wsoup,
-                      &c->wtasks,    &c->wctr,     &c->conv_scratch, &c->wroots, &c->blas_wide,
+                      &c->wtasks,    &c->wctr,     &c->conv_scratch, &c->wroots, &c->blas_wide, &c->upload_scratch,
                       &c->pool,      &c->accum_tmp, &c->lb_tris, &c->lb_pos,    &c->lb_boxes,  &c->lb_keys,
                       &c->lb_vals,   &c->lb_keys2, &c->lb_vals2, &c->lb_hist,   &c->lb_karras, &c->lb_parent,
                       &c->lb_nbounds, &c->lb_subtree, &c->lb_flags, &c->lb_nodes, &c->lb_rank, &c->lb_misc,
@@ -191,6 +192,72 @@ struct MeshSpec {
     uint32_t n;
 };
 
+namespace {
+
+// Triangle validation on the device: the smallest index of a triangle whose
+// vertex or material index is out of range (0xFFFFFFFF: none).
+__global__ void k_validate_tris(const GpuTriangle* __restrict__ t, uint32_t n, uint32_t nv, uint32_t nm,
+                                uint32_t* __restrict__ first_bad) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const GpuTriangle g = t[i];
+        if (g.i0 >= nv || g.i1 >= nv || g.i2 >= nv || g.material >= nm) atomicMin(first_bad, i);
+    }
+}
+
+// Vertex bounds on the device (the guide's default position box): min / max
+// per axis as order-preserving integer keys (NaN skipped, -0 taken as +0).
+__device__ __forceinline__ int float_key(float f) {
+    const int b = __float_as_int(f == 0.0f ? 0.0f : f);
+    return b >= 0 ? b : b ^ 0x7FFFFFFF;
+}
+__global__ void k_vertex_bounds(const float4* __restrict__ pos, uint32_t n, int* __restrict__ keys) {
+    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 p = pos[i];
+        const float q[3] = {p.x, p.y, p.z};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (q[a] != q[a]) continue;
+            const int k = float_key(q[a]);
+            lo[a] = min(lo[a], k);
+            hi[a] = max(hi[a], k);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[a] = min(lo[a], __shfl_down_sync(0xFFFFFFFFu, lo[a], o));
+            hi[a] = max(hi[a], __shfl_down_sync(0xFFFFFFFFu, hi[a], o));
+        }
+        if ((threadIdx.x & 31u) == 0) {
+            atomicMin(keys + a, lo[a]);
+            atomicMax(keys + 3 + a, hi[a]);
+        }
+    }
+}
+float key_float(int k) {
+    const int b = k >= 0 ? k : k ^ 0x7FFFFFFF;
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+}
+
+int32_t validate_tris_dev(luc_ctx* c, const GpuTriangle* t, uint32_t n, uint32_t nv, uint32_t nm) {
+    if (n == 0) return LUC_OK;
+    LUC_CUDA(c, c->upload_scratch.ensure(64), "alloc upload scratch");
+    uint32_t* bad = c->upload_scratch.as<uint32_t>();
+    LUC_CUDA(c, cudaMemsetAsync(bad, 0xFF, 4, c->stream), "clear validation word");
+    k_validate_tris<<<(int)std::min<uint64_t>((n + 255) / 256, (uint64_t)c->num_sms * 8), 256, 0, c->stream>>>(
+        t, n, nv, nm, bad);
+    uint32_t h = 0;
+    LUC_CUDA(c, cudaMemcpyAsync(&h, bad, 4, cudaMemcpyDeviceToHost, c->stream), "read validation word");
+    LUC_CUDA(c, cudaStreamSynchronize(c->stream), "validate triangles");
+    if (h != 0xFFFFFFFFu) return luc_fail(c, LUC_ERR_VALIDATION, "triangle " + std::to_string(h) + " indexes out of range");
+    return LUC_OK;
+}
+
+}  // namespace
+
 static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec* meshes) {
     if (!c || !v) return LUC_ERR_VALIDATION;
     cudaSetDevice(c->device);
@@ -219,12 +286,8 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     for (uint32_t i = 0; i < v->num_lights; ++i)
         if (v->lights[i].material >= v->num_materials)
             return luc_fail(c, LUC_ERR_VALIDATION, "light " + std::to_string(i) + " has a bad material");
-    for (uint32_t i = 0; i < v->num_triangles; ++i) {
-        const GpuTriangle& t = v->triangles[i];
-        if (t.i0 >= v->num_vertices || t.i1 >= v->num_vertices || t.i2 >= v->num_vertices ||
-            t.material >= v->num_materials)
-            return luc_fail(c, LUC_ERR_VALIDATION, "triangle " + std::to_string(i) + " indexes out of range");
-    }
+    // Triangle indices are validated on the device, right after their upload
+    // and before any kernel dereferences them (validate_tris_dev).
     for (uint32_t i = 0; i < v->num_bvh_nodes; ++i) {
         const GpuBvhNode& n = v->bvh_nodes[i];
         const bool tlas = ni && i >= v->tlas_root;
@@ -240,10 +303,12 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     if (v->env_width && (!v->env_pixels || !v->env_cdf || v->env_height == 0 ||
                          v->env_cdf_width < std::max(v->env_width, v->env_height) + 1))
         return luc_fail(c, LUC_ERR_VALIDATION, "environment map without pixels or a packed CDF");
-    // Scene bounds (the guide's default position box): vertices, spheres,
-    // quad corners.
+    // Scene bounds (the guide's default position box): vertices (reduced on
+    // the device after their upload, merged in at the end), spheres, quad
+    // corners.
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    const bool vertex_bounds = v->num_vertices && v->num_triangles && !ni;
     {
-        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
         auto grow = [&](float x, float y, float z) {
             const float q[3] = {x, y, z};
             for (int a = 0; a < 3; ++a) {
@@ -251,8 +316,6 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
                 hi[a] = std::max(hi[a], q[a]);
             }
         };
-        for (uint32_t i = 0; i < v->num_vertices && v->num_triangles && !ni; ++i)
-            grow(v->positions[4 * i], v->positions[4 * i + 1], v->positions[4 * i + 2]);
         if (ni && v->num_triangles) {  // instanced: the TLAS root's box (world space)
             const GpuBvhNode& r = v->bvh_nodes[v->tlas_root];
             grow(r.bounds_min[0], r.bounds_min[1], r.bounds_min[2]);
@@ -272,10 +335,6 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
                 grow(o[0] + p.radius, o[1] + p.radius, o[2] + p.radius);
             }
         }
-        for (int a = 0; a < 3; ++a) {
-            c->scene_lo[a] = lo[a] <= hi[a] ? lo[a] : 0.0f;
-            c->scene_hi[a] = lo[a] <= hi[a] ? hi[a] : 1.0f;
-        }
     }
     cudaStream_t s = c->stream;
     c->has_scene = false;
@@ -289,12 +348,24 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     LUC_CUDA(c, upload(c->lights, v->lights, v->num_lights, s), "upload lights");
     LUC_CUDA(c, upload(c->positions, v->positions, 4 * (size_t)v->num_vertices, s), "upload positions");
     LUC_CUDA(c, upload(c->attrs, v->vertex_attrs, v->num_vertices, s), "upload vertex attrs");
+    int bkeys[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
+    if (vertex_bounds) {
+        LUC_CUDA(c, c->upload_scratch.ensure(64), "alloc upload scratch");
+        int* keys = c->upload_scratch.as<int>() + 4;
+        LUC_CUDA(c, cudaMemcpyAsync(keys, bkeys, sizeof(bkeys), cudaMemcpyHostToDevice, s), "init bounds");
+        k_vertex_bounds<<<(int)std::min<uint64_t>((v->num_vertices + 255) / 256, (uint64_t)c->num_sms * 4), 256, 0,
+                          s>>>(c->positions.as<float4>(), v->num_vertices, keys);
+        LUC_CUDA(c, cudaMemcpyAsync(bkeys, keys, sizeof(bkeys), cudaMemcpyDeviceToHost, s), "read bounds");
+    }
     uint32_t num_nodes = v->num_bvh_nodes;
     c->num_meshes = 0;
     c->needs_instances = false;
     if (meshes) {
         // One BLAS per mesh now; the TLAS comes with luc_set_instances.
         LUC_CUDA(c, upload(c->lb_tris, v->triangles, v->num_triangles, s), "upload triangles");
+        if (int32_t rv = validate_tris_dev(c, c->lb_tris.as<GpuTriangle>(), v->num_triangles, v->num_vertices,
+                                           v->num_materials))
+            return rv;
         int32_t rc = luc_build_blases(c, meshes->first, meshes->count, meshes->n, v->num_triangles, &num_nodes);
         if (rc) return rc;
         c->num_meshes = meshes->n;
@@ -306,6 +377,9 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
         // No caller tree: build an LBVH on the device and reorder our copy of
         // the triangles into leaf order (Bvh::compact_primitives).
         LUC_CUDA(c, upload(c->lb_tris, v->triangles, v->num_triangles, s), "upload triangles");
+        if (int32_t rv = validate_tris_dev(c, c->lb_tris.as<GpuTriangle>(), v->num_triangles, v->num_vertices,
+                                           v->num_materials))
+            return rv;
         int32_t rc = luc_triangle_boxes_device(c, c->lb_tris.as<GpuTriangle>(), c->positions.as<float4>(),
                                                v->num_triangles);
         if (rc) return rc;
@@ -320,6 +394,9 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
                                     cudaMemcpyDeviceToDevice, s), "copy nodes");
     } else {
         LUC_CUDA(c, upload(c->tris, v->triangles, v->num_triangles, s), "upload triangles");
+        if (int32_t rv = validate_tris_dev(c, c->tris.as<GpuTriangle>(), v->num_triangles, v->num_vertices,
+                                           v->num_materials))
+            return rv;
         LUC_CUDA(c, upload(c->nodes, v->bvh_nodes, v->num_bvh_nodes, s), "upload bvh nodes");
     }
     // Environment: pixels, the packed CDF split into conditional rows and
@@ -355,6 +432,15 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
         }
     }
     LUC_CUDA(c, cudaStreamSynchronize(s), "scene upload");
+    if (vertex_bounds)
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], key_float(bkeys[a]));
+            hi[a] = std::max(hi[a], key_float(bkeys[3 + a]));
+        }
+    for (int a = 0; a < 3; ++a) {
+        c->scene_lo[a] = lo[a] <= hi[a] ? lo[a] : 0.0f;
+        c->scene_hi[a] = lo[a] <= hi[a] ? hi[a] : 1.0f;
+    }
 
     DevScene& d = c->scene;
     d.materials = c->materials.as<GpuMaterial>();
@@ -402,7 +488,6 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     c->num_materials = v->num_materials;
     c->total_nodes = num_nodes;
     c->has_scene = true;
-    c->scene_version++;
     return LUC_OK;
 }
 
@@ -578,7 +663,10 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
         fp.num_paths = (uint64_t)spp * pixels;
         uint32_t lr_bits = 0;
         std::memcpy(&lr_bits, &gt.lr, 4);
-        const uint64_t extra[10] = {(uint64_t)(uintptr_t)accum,        c->scene_version,
+        // The scene enters the key through the DevScene bytes (pointers,
+        // counts, roots): the kernels read the arrays at run time, so a
+        // re-upload into the same buffers replays the graph unchanged.
+        const uint64_t extra[10] = {(uint64_t)(uintptr_t)accum,        0u,
                                     (uint64_t)(uintptr_t)c->rs.ps.o_pdf, (uint64_t)(tp != nullptr),
                                     (uint64_t)(uintptr_t)c->rs.ps.lobes, (uint64_t)(uintptr_t)c->rs.ps.rec,
                                     (uint64_t)(uintptr_t)c->rs.ps.gmisc, (uint64_t)(uintptr_t)gt.params,

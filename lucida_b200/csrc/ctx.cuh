@@ -38,7 +38,6 @@ struct FrameGraph {
 
 struct luc_ctx {
     int device = 0;
-    uint64_t scene_version = 0;
     FrameGraph graph;
     bool use_graphs = true;
     cudaStream_t own_stream = nullptr;
@@ -51,6 +50,7 @@ struct luc_ctx {
     DevBuf wnodes, wsoup, wtasks, wctr;  // compressed 8-wide tree (wide.cu)
     DevBuf wroots, blas_wide;            // its roots; BLAS binary root -> wide root (two-level scenes)
     DevBuf conv_scratch;                 // convergence meter partials + result (stats.cu)
+    DevBuf upload_scratch;               // upload: validation word, vertex-bound keys
     uint32_t wide_nodes = 0;             // 0: the scene traverses the binary tree
     bool use_wide = true;                // LUC_BINARY_BVH=1 turns the wide tree off
     DevBuf blas_roots;    // distinct BLAS roots of an instanced scene

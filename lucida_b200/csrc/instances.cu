@@ -215,20 +215,16 @@ int32_t luc_set_instances(luc_ctx* c, const float* object_to_world, const uint32
     cudaStream_t s = c->stream;
     const uint32_t np_ = (uint32_t)c->host_prims.size();
     const uint32_t bn = c->blas_nodes;
-    bool moved = false;
     if (n > c->inst_capacity) {
         // Room for the instance rows after the analytic primitives and for the
         // largest TLAS (2n - 1 nodes) after the BLASes; BLAS contents kept.
-        void* old_nodes = c->nodes.p;
-        void* old_prims = c->prims.p;
         LUC_CUDA(c, grow_keep(c, c->nodes, ((size_t)bn + 2 * n) * sizeof(GpuBvhNode), (size_t)bn * sizeof(GpuBvhNode)),
                  "grow nodes");
         LUC_CUDA(c, grow_keep(c, c->tnodes, ((size_t)bn + 2 * n) * 64, (size_t)bn * 64), "grow traversal nodes");
         LUC_CUDA(c, c->prims.ensure(((size_t)np_ + n) * sizeof(GpuPrimitive)), "grow primitives");
         LUC_CUDA(c, cudaMemcpyAsync(c->prims.p, c->host_prims.data(), (size_t)np_ * sizeof(GpuPrimitive),
                                     cudaMemcpyHostToDevice, s), "upload primitives");
-        c->inst_capacity = n;
-        moved = old_nodes != c->nodes.p || old_prims != c->prims.p;
+        c->inst_capacity = n;  // moved arrays change the DevScene bytes, which key the frame graph
     }
     LUC_CUDA(c, c->inst_in.ensure((size_t)n * 56), "alloc instance input");
     float* d_o2w = c->inst_in.as<float>();
@@ -294,7 +290,6 @@ int32_t luc_set_instances(luc_ctx* c, const float* object_to_world, const uint32
     c->tlas_nodes = tn;
     c->total_nodes = bn + tn;
     c->needs_instances = false;
-    if (moved) c->scene_version++;
     return LUC_OK;
 }
 
