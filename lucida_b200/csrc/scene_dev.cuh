@@ -332,29 +332,46 @@ LUC_D bool bvh_any(const DevScene& s, TRef root, V3 o, V3 d, float tmin, float t
 //   [0] origin p (3 x f32), exponent bytes ex | ey << 8 | ez << 16, internal
 //       child mask << 24 (bit s: slot s holds an internal child);
 //   [1] first internal child (wide node index), first triangle (wide soup
-//       index), meta bytes of slots 0-3, of slots 4-7;
+//       index), triangle count mask (nibble s: the low `count` bits set for
+//       a leaf slot s of 1-4 triangles), unused;
 //   [2] qlo.x of slots 0-7 (8 x u8), qlo.y; [3] qlo.z, qhi.x; [4] qhi.y, qhi.z.
 // Child box of slot s on axis a: [p + qlo * 2^(e-127), p + qhi * 2^(e-127)],
 // each plane at least one quantum outside the binary child's (padded) box.
-// A leaf slot's meta byte is count << 5 | offset: triangles first + offset ..
-// + count - 1 (count 1-4, at most 32 per node). Internal children are stored
-// contiguously in slot order. Slots are assigned by octant: slot s holds the
-// child lying towards corner s of the node (bit a set: the +a side). A ray
-// whose direction has sign bits oct (bit a set: negative along a) meets the
-// children roughly in ascending order of k = s ^ oct, the order in which the
-// hit bits are stored and visited.
-constexpr uint32_t kWideTri = 0x80000000u;  // group tag: triangle group
+// Internal children are stored contiguously in slot order; so are the leaf
+// slots' triangles, so bit b of the count mask is triangle
+// first + popc(count mask below b). Slots are assigned by octant: slot s
+// holds the child lying towards corner s of the node (bit a set: the +a
+// side). A ray whose direction has sign bits oct (bit a set: negative along
+// a) meets the children roughly in ascending order of k = s ^ oct, the order
+// in which the hit bits are stored and visited.
 constexpr int kWideStack = 64;
 
-LUC_D float wide_q(uint32_t word, uint32_t j) {  // byte j of word as an exact float
+// Byte j of word as an exact float (2^23 + byte, minus 2^23): one PRMT and
+// one FADD per plane.
+LUC_D float wide_q(uint32_t word, uint32_t j) {
     return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7440u | j)) - 8388608.0f;
 }
 
+// Bit s of an 8-bit mask to nibble s (0x1 in each set slot's nibble).
+LUC_D uint32_t spread_nibbles(uint32_t x) {
+    x = (x | (x << 12)) & 0x000F000Fu;
+    x = (x | (x << 6)) & 0x03030303u;
+    return (x | (x << 3)) & 0x11111111u;
+}
+// Bit i of an 8-bit mask to bit i ^ oct (branch-free: oct differs per lane).
+LUC_D uint32_t xor_permute8(uint32_t x, uint32_t oct) {
+    const uint32_t m1 = 0u - (oct & 1u), m2 = 0u - ((oct >> 1) & 1u), m4 = 0u - ((oct >> 2) & 1u);
+    x ^= (x ^ (((x & 0x55u) << 1) | ((x >> 1) & 0x55u))) & m1;
+    x ^= (x ^ (((x & 0x33u) << 2) | ((x >> 2) & 0x33u))) & m2;
+    x ^= (x ^ (((x & 0x0Fu) << 4) | ((x >> 4) & 0x0Fu))) & m4;
+    return x;
+}
+
 // Slab tests of the 8 child boxes of wide node `node`. Returns the node group
-// (first child, internal mask << 8 | hit bits at positions slot ^ oct) and the
-// triangle group (first triangle | kWideTri, mask of hit triangles).
+// (first child, internal mask << 8 | hit bits at positions slot ^ oct) and
+// the triangle group (first triangle, mask of hit triangle bits, count mask).
 LUC_D void wide_node(const float4* __restrict__ wn, uint32_t node, V3 o, V3 inv, uint32_t oct, float tmin,
-                     float tmax, uint2& ng, uint2& tg) {
+                     float tmax, uint2& ng, uint3& tg) {
     const float4* q = wn + 5 * (size_t)node;
     const float4 a = __ldg(q);
     const uint4 b = __ldg(reinterpret_cast<const uint4*>(q + 1));
@@ -372,7 +389,7 @@ LUC_D void wide_node(const float4* __restrict__ wn, uint32_t node, V3 o, V3 inv,
     const uint32_t nx0 = nx ? d.z : c.x, nx1 = nx ? d.w : c.y, fx0 = nx ? c.x : d.z, fx1 = nx ? c.y : d.w;
     const uint32_t ny0 = ny ? e.x : c.z, ny1 = ny ? e.y : c.w, fy0 = ny ? c.z : e.x, fy1 = ny ? c.w : e.y;
     const uint32_t nz0 = nz ? e.z : d.x, nz1 = nz ? e.w : d.y, fz0 = nz ? d.x : e.z, fz1 = nz ? d.y : e.w;
-    uint32_t nh = 0, tm = 0;
+    uint32_t hm = 0;  // hit slots, slot order
 #pragma unroll
     for (uint32_t s = 0; s < 8; ++s) {
         const uint32_t j = s & 3u;
@@ -382,24 +399,22 @@ LUC_D void wide_node(const float4* __restrict__ wn, uint32_t node, V3 o, V3 inv,
         const float tnz = __fmaf_rn(wide_q(hi ? nz1 : nz0, j), sz, oz), tfz = __fmaf_rn(wide_q(hi ? fz1 : fz0, j), sz, oz);
         const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
         const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
-        if (tn <= tf) {
-            const uint32_t m = ((hi ? b.w : b.z) >> (8 * j)) & 0xFFu;
-            if (imask & (1u << s)) nh |= 1u << (s ^ oct);
-            else tm |= ((1u << (m >> 5)) - 1u) << (m & 31u);
-        }
+        hm |= (tn <= tf ? 1u : 0u) << s;
     }
-    ng = make_uint2(b.x, (imask << 8) | nh);
-    tg = make_uint2(b.y | kWideTri, tm);
+    // Leaf slots: their nibbles of the count mask; empty slots have none.
+    ng = make_uint2(b.x, (imask << 8) | xor_permute8(hm & imask, oct));
+    tg = make_uint3(b.y, (spread_nibbles(hm & ~imask) * 0xFu) & b.z, b.z);
 }
 
-// Closest hit (kAny = false) or any hit (kAny = true) through the wide tree.
-// The triangle test and its operands are those of the binary traversal
-// (hit_soup on the same (p0, e1, e2)), so the nearest hit is the same; only
-// which of two exactly tied triangles wins can differ. Groups: the current
-// node group descends into its nearest hit child, pushing the rest; a node's
-// triangle group is tested right after the node, one triangle per step
-// (after Ylitie, Karras and Laine 2017, compressed wide BVHs; their deferral
-// of triangle groups while few lanes have one measured slower here).
+// Closest hit (kAny = false) or any hit (kAny = true) through the wide tree
+// whose root is wide node `root`. The triangle test and its operands are
+// those of the binary traversal (hit_soup on the same (p0, e1, e2)), so the
+// nearest hit is the same; only which of two exactly tied triangles wins can
+// differ. The current node group descends into its nearest hit child,
+// pushing the rest; a node's triangle group is tested right after the node,
+// one triangle per step (after Ylitie, Karras and Laine 2017, compressed
+// wide BVHs; their deferral of triangle groups while few lanes have one
+// measured slower here).
 template <bool kAny>
 LUC_D bool wide_trace(const DevScene& s, uint32_t root, V3 o, V3 d, float tmin, float& tmax, float& bu, float& bv,
                       uint32_t& btri, TravCount& tc) {
@@ -408,37 +423,35 @@ LUC_D bool wide_trace(const DevScene& s, uint32_t root, V3 o, V3 d, float tmin, 
     uint2 stack[kWideStack];
     int sp = 0;
     // Start from a virtual parent whose only child (slot 0, internal) is the
-    // root, so the root's own triangles go through the triangle phase too.
-    uint2 g = make_uint2(root, (1u << 8) | (1u << oct)), t = make_uint2(0u, 0u);
+    // root.
+    uint2 g = make_uint2(root, (1u << 8) | (1u << oct));
     bool found = false;
     // Each node and triangle is visited at most once per ray in a tree; the
     // guard only bounds the loop should the arrays ever not form one.
     for (uint32_t guard = 0; guard < (1u << 24); ++guard) {
-        if (!(g.x & kWideTri) && (g.y & 0xFFu)) {
+        if (g.y & 0xFFu) {
             const uint32_t k = __ffs(g.y & 0xFFu) - 1u;
             g.y &= ~(1u << k);
             const uint32_t slot = k ^ oct;
             const uint32_t child = g.x + __popc((g.y >> 8) & ((1u << slot) - 1u));
             if ((g.y & 0xFFu) && sp < kWideStack) stack[sp++] = g;
+            uint3 t;
             wide_node(s.wnodes, child, o, inv, oct, tmin, tmax, g, t);
             tc.nodes++;
-        } else if (g.x & kWideTri) {
-            t = g;
-            g = make_uint2(0u, 0u);
-        }
-        while (t.y) {
-            const uint32_t j = __ffs(t.y) - 1u;
-            t.y &= t.y - 1u;
-            const uint32_t k = (t.x & ~kWideTri) + j;
-            tc.tris++;
-            float th, uh, vh;
-            if (hit_soup(s.wsoup, k, o, d, tmin, tmax, th, uh, vh)) {
-                if (kAny) return true;
-                tmax = th;
-                bu = uh;
-                bv = vh;
-                btri = __float_as_uint(__ldg(s.wsoup + 3 * (size_t)k).w);
-                found = true;
+            while (t.y) {
+                const uint32_t bit = __ffs(t.y) - 1u;
+                t.y &= t.y - 1u;
+                const uint32_t k = t.x + __popc(t.z & ((1u << bit) - 1u));
+                tc.tris++;
+                float th, uh, vh;
+                if (hit_soup(s.wsoup, k, o, d, tmin, tmax, th, uh, vh)) {
+                    if (kAny) return true;
+                    tmax = th;
+                    bu = uh;
+                    bv = vh;
+                    btri = __float_as_uint(__ldg(s.wsoup + 3 * (size_t)k).w);
+                    found = true;
+                }
             }
         }
         if (!(g.y & 0xFFu)) {

@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
             ebits |= (uint32_t)(ex + 127) << (8 * a);
         }
         ebits |= imask << 24;
-        uint32_t qlo[3][2] = {{0, 0}, {0, 0}, {0, 0}}, qhi[3][2] = {{0, 0}, {0, 0}, {0, 0}}, meta[2] = {0, 0};
+        uint32_t qlo[3][2] = {{0, 0}, {0, 0}, {0, 0}}, qhi[3][2] = {{0, 0}, {0, 0}, {0, 0}}, cntmask = 0;
         uint32_t off = 0, rank = 0;
         for (int s = 0; s < 8; ++s) {
             const int k = child_at[s];
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
                     h8[a] = (uint32_t)fmax(0.0, fmin(255.0, qh));
                 }
                 if (ch[k].kind == 2u) {
-                    meta[s >> 2] |= ((ch[k].count << 5) | off) << (8 * (s & 3));
+                    cntmask |= ((1u << ch[k].count) - 1u) << (4 * s);  // nibble s: the slot's triangles
                     for (uint32_t i = 0; i < ch[k].count; ++i) {
                         const size_t src = 3 * (size_t)(ch[k].first + i), dst = 3 * (size_t)(tbase + off + i);
                         float4 q0 = soup[src];
@@ -313,8 +313,7 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
         }
         float4* o = wnodes + 5 * (size_t)w;
         o[0] = make_float4(p[0], p[1], p[2], __uint_as_float(ebits));
-        o[1] = make_float4(__uint_as_float(cbase), __uint_as_float(tbase), __uint_as_float(meta[0]),
-                           __uint_as_float(meta[1]));
+        o[1] = make_float4(__uint_as_float(cbase), __uint_as_float(tbase), __uint_as_float(cntmask), 0.0f);
         o[2] = make_float4(__uint_as_float(qlo[0][0]), __uint_as_float(qlo[0][1]), __uint_as_float(qlo[1][0]),
                            __uint_as_float(qlo[1][1]));
         o[3] = make_float4(__uint_as_float(qlo[2][0]), __uint_as_float(qlo[2][1]), __uint_as_float(qhi[0][0]),

@@ -63,8 +63,7 @@ def _decode(w):
     qhi = np.stack([bytes8(14), bytes8(16), bytes8(18)], 1)
     lo = p[:, :, None] + qlo * scale[:, :, None]
     hi = p[:, :, None] + qhi * scale[:, :, None]
-    meta = w[:, 6:8].copy().view(np.uint8).reshape(-1, 8).astype(np.uint32)
-    return dict(cbase=w[:, 4], tbase=w[:, 5], imask=imask, meta=meta, lo=lo, hi=hi)
+    return dict(cbase=w[:, 4], tbase=w[:, 5], imask=imask, cntmask=w[:, 6], lo=lo, hi=hi)
 
 
 def _check_structure(g, tris_leaf_order, pos):
@@ -99,10 +98,12 @@ def _check_structure(g, tris_leaf_order, pos):
                 clo, chi = visit(int(d["cbase"][k]) + rank)
                 rank += 1
             else:
-                m = int(d["meta"][k, s])
-                cnt, off = m >> 5, m & 31
+                cm = int(d["cntmask"][k])
+                nib = (cm >> (4 * s)) & 0xF
+                cnt, off = bin(nib).count("1"), bin(cm & ((1 << (4 * s)) - 1)).count("1")
                 if cnt == 0:
                     continue
+                assert nib == (1 << cnt) - 1  # a slot's triangles are its nibble's low bits
                 first = int(d["tbase"][k]) + off
                 seen_tris[first:first + cnt] += 1
                 clo = tlo[first:first + cnt].min(0)
