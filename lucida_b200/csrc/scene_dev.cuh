@@ -415,19 +415,94 @@ LUC_D void wide_node(const float4* __restrict__ wn, uint32_t node, V3 o, V3 inv,
 // one triangle per step (after Ylitie, Karras and Laine 2017, compressed
 // wide BVHs; their deferral of triangle groups while few lanes have one
 // measured slower here).
+// A resumable walk of one ray through a wide tree: begin() then step()
+// until it reports the end. Used whole by wide_trace and one node at a time
+// by kernels that refill finished lanes with new rays (k_extend_dyn): both
+// visit the same nodes and triangles in the same order.
+struct WideWalk {
+    V3 o, d, inv;
+    uint32_t oct, btri;
+    float tmax, bu, bv;
+    bool found;
+    uint2 g;
+    int sp;
+    uint32_t steps;
+    uint2 stack[kWideStack];
+
+    LUC_D void begin(uint32_t root, V3 o_, V3 d_, float tmax_) {
+        o = o_;
+        d = d_;
+        inv = safe_inv_dir(d_);
+        oct = (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) | (inv.z < 0.0f ? 4u : 0u);
+        tmax = tmax_;
+        bu = bv = 0.0f;
+        btri = 0u;
+        found = false;
+        // A virtual parent whose only child (slot 0, internal) is the root.
+        g = make_uint2(root, (1u << 8) | (1u << oct));
+        sp = 0;
+        steps = 0;
+    }
+    // One node visit and its triangles. True when the walk is over: the
+    // stack is empty, or (kAny) a hit was found. Each node and triangle is
+    // visited at most once per ray in a tree; the step limit only bounds the
+    // walk should the arrays ever not form one.
+    template <bool kAny>
+    LUC_D bool step(const DevScene& s, float tmin, TravCount& tc) {
+        if (g.y & 0xFFu) {
+            const uint32_t k = __ffs(g.y & 0xFFu) - 1u;
+            g.y &= ~(1u << k);
+            const uint32_t slot = k ^ oct;
+            const uint32_t child = g.x + __popc((g.y >> 8) & ((1u << slot) - 1u));
+            if ((g.y & 0xFFu) && sp < kWideStack) stack[sp++] = g;
+            uint3 t;
+            wide_node(s.wnodes, child, o, inv, oct, tmin, tmax, g, t);
+            tc.nodes++;
+            while (t.y) {
+                const uint32_t bit = __ffs(t.y) - 1u;
+                t.y &= t.y - 1u;
+                const uint32_t kt = t.x + __popc(t.z & ((1u << bit) - 1u));
+                tc.tris++;
+                float th, uh, vh;
+                if (hit_soup(s.wsoup, kt, o, d, tmin, tmax, th, uh, vh)) {
+                    found = true;
+                    if (kAny) return true;
+                    tmax = th;
+                    bu = uh;
+                    bv = vh;
+                    btri = __float_as_uint(__ldg(s.wsoup + 3 * (size_t)kt).w);
+                }
+            }
+        }
+        if (!(g.y & 0xFFu)) {
+            if (sp == 0) return true;
+            g = stack[--sp];
+        }
+        return ++steps >= (1u << 24);
+    }
+};
+
+// Closest hit (kAny = false) or any hit (kAny = true) through the wide tree
+// whose root is wide node `root`. The triangle test and its operands are
+// those of the binary traversal (hit_soup on the same (p0, e1, e2)), so the
+// nearest hit is the same; only which of two exactly tied triangles wins can
+// differ. The current node group descends into its nearest hit child,
+// pushing the rest; a node's triangle group is tested right after the node,
+// one triangle per step (after Ylitie, Karras and Laine 2017, compressed
+// wide BVHs; their deferral of triangle groups while few lanes have one
+// measured slower here).
 template <bool kAny>
 LUC_D bool wide_trace(const DevScene& s, uint32_t root, V3 o, V3 d, float tmin, float& tmax, float& bu, float& bv,
                       uint32_t& btri, TravCount& tc) {
+    // WideWalk's steps as one loop (kept separate: the compiler schedules
+    // the uninterrupted loop better; the megakernel-vs-wavefront bit-exact
+    // tests hold the two to the same visiting order).
     const V3 inv = safe_inv_dir(d);
     const uint32_t oct = (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) | (inv.z < 0.0f ? 4u : 0u);
     uint2 stack[kWideStack];
     int sp = 0;
-    // Start from a virtual parent whose only child (slot 0, internal) is the
-    // root.
     uint2 g = make_uint2(root, (1u << 8) | (1u << oct));
     bool found = false;
-    // Each node and triangle is visited at most once per ray in a tree; the
-    // guard only bounds the loop should the arrays ever not form one.
     for (uint32_t guard = 0; guard < (1u << 24); ++guard) {
         if (g.y & 0xFFu) {
             const uint32_t k = __ffs(g.y & 0xFFu) - 1u;
@@ -441,15 +516,15 @@ LUC_D bool wide_trace(const DevScene& s, uint32_t root, V3 o, V3 d, float tmin, 
             while (t.y) {
                 const uint32_t bit = __ffs(t.y) - 1u;
                 t.y &= t.y - 1u;
-                const uint32_t k = t.x + __popc(t.z & ((1u << bit) - 1u));
+                const uint32_t kt = t.x + __popc(t.z & ((1u << bit) - 1u));
                 tc.tris++;
                 float th, uh, vh;
-                if (hit_soup(s.wsoup, k, o, d, tmin, tmax, th, uh, vh)) {
+                if (hit_soup(s.wsoup, kt, o, d, tmin, tmax, th, uh, vh)) {
                     if (kAny) return true;
                     tmax = th;
                     bu = uh;
                     bv = vh;
-                    btri = __float_as_uint(__ldg(s.wsoup + 3 * (size_t)k).w);
+                    btri = __float_as_uint(__ldg(s.wsoup + 3 * (size_t)kt).w);
                     found = true;
                 }
             }
@@ -594,11 +669,9 @@ LUC_D bool instances_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax, 
 // single-level scenes carry none of its registers; likewise kWide for the
 // single-level tree: 1 wide tree only (scenes whose triangles have one), 0
 // binary tree only, 2 whichever the scene has.
-template <bool kInst, int kWide = 2>
-LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, float& v, uint32_t& inst,
-                           TravCount& tc) {
-    float best_t = kTMax;
-    uint32_t id = kMiss;
+// The analytic-primitive half of Scene::intersect: brute force, nearest t
+// below best_t (kTMax to start); id = primitive | kAnalytic on a hit.
+LUC_D void analytic_closest(const DevScene& s, V3 o, V3 d, float& best_t, uint32_t& id) {
     for (uint32_t i = 0; i < s.num_prims; ++i) {
         const GpuPrimitive& p = s.prims[i];
         float th;
@@ -610,6 +683,14 @@ LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, fl
             id = i | kAnalytic;
         }
     }
+}
+
+template <bool kInst, int kWide = 2>
+LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, float& v, uint32_t& inst,
+                           TravCount& tc) {
+    float best_t = kTMax;
+    uint32_t id = kMiss;
+    analytic_closest(s, o, d, best_t, id);
     float bu = 0.0f, bv = 0.0f;
     uint32_t tri;
     inst = 0u;

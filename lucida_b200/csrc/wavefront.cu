@@ -102,6 +102,9 @@ __global__ void __launch_bounds__(256) k_generate_batch(PathState ps, BatchDev b
 // Wide-tree traversal runs at 32 warps per SM (64 registers): the loop is
 // latency-bound, and occupancy beat the registers the compiler would take.
 constexpr int wide_min_blocks(int threads) { return 1024 / threads; }
+// k_extend_dyn refills a warp's finished lanes once this many are idle
+// (measured best against 1, 16 and 32).
+constexpr int kExtendRefill = 8;
 
 template <bool kInst, bool kBatch, int kThreads, int kWide>
 __global__ void __launch_bounds__(kThreads, kWide == 1 ? wide_min_blocks(kThreads) : 1) k_extend(PathState ps, const __grid_constant__ DevScene sc_arg, FrameParams fp,
@@ -142,6 +145,60 @@ __global__ void __launch_bounds__(kThreads, kWide == 1 ? wide_min_blocks(kThread
             if (base >= len) break;
             if (base + lane < len) trace(base + lane);
             __syncwarp();
+        }
+    }
+    flush_counts(ps.stat, rays, tc);
+}
+
+// EXTEND on the wide tree of a single-level scene, with dynamic ray fetch
+// (Aila and Laine 2009; Aila, Laine and Karras 2012): each warp walks 32
+// rays one node at a time and, whenever at least kRefill lanes have finished,
+// refills them with the next rays of the queue (one atomic per refill), so
+// lanes do not idle until the warp's longest ray ends. Each ray's walk is
+// wide_trace's (WideWalk), so the hits are the same.
+template <int kThreads, int kRefill>
+__global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_extend_dyn(PathState ps,
+                                                                                    const __grid_constant__ DevScene sc,
+                                                                                    FrameParams fp, uint32_t depth) {
+    const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
+    const uint32_t* queue = ps.queue[depth & 1];
+    uint32_t* pull = ps.ctr + depth * kCtrStride + kCtrPullExtend;
+    const uint32_t lane = threadIdx.x & 31u, below = (1u << lane) - 1u;
+    TravCount tc;
+    uint32_t rays = 0, p = 0, pid = kMiss;
+    bool live = false, exhausted = false;
+    WideWalk w;
+    for (;;) {
+        const uint32_t need = __ballot_sync(0xFFFFFFFFu, !live);
+        if (!exhausted && __popc(need) >= kRefill) {
+            const uint32_t leader = __ffs(need) - 1u, n = __popc(need);
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(pull, n);
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            exhausted = base + n >= len;
+            if (!live) {
+                const uint32_t i = base + __popc(need & below);
+                if (i < len) {
+                    p = depth == 0 ? i : queue[i];
+                    const V3 o = xyz(ld4(ps.o_pdf + p)), d = xyz(ld4(ps.dir + p));
+                    float best_t = kTMax;
+                    pid = kMiss;
+                    analytic_closest(sc, o, d, best_t, pid);  // Scene::intersect: primitives first
+                    w.begin(0u, o, d, best_t);
+                    live = true;
+                }
+            }
+        }
+        if (__ballot_sync(0xFFFFFFFFu, live) == 0) {
+            if (exhausted) break;
+            continue;
+        }
+        // One node per refill check (measured best against 4, 8 and 16).
+        if (live && w.step<false>(sc, kTMin, tc)) {
+            __stcs(ps.hit + p, make_float4(w.tmax, w.found ? w.bu : 0.0f, w.found ? w.bv : 0.0f,
+                                           __uint_as_float(w.found ? w.btri : pid)));
+            ++rays;
+            live = false;
         }
     }
     flush_counts(ps.stat, rays, tc);
@@ -462,7 +519,7 @@ void query_occupancy(RenderState& rs) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, 128, 0);
         return b > 0 ? b : 8;
     };
-    rs.extend_blocks = occ((const void*)k_extend<false, false, 128, 1>);
+    rs.extend_blocks = occ((const void*)k_extend_dyn<128, kExtendRefill>);
     rs.connect_blocks = occ((const void*)k_connect<false, false, 128, 1>);
     rs.extend_blocks_bin = occ((const void*)k_extend<false, false, 128, 0>);
     rs.connect_blocks_bin = occ((const void*)k_connect<false, false, 128, 0>);
@@ -499,7 +556,7 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
             k_extend<true, false, 128, 0><<<sms * rs.extend_blocks_inst_bin, 128, 0, stream>>>(rs.ps, sc, fp,
                                                                                                BatchDev{}, d);
         else if (wide)
-            k_extend<false, false, 128, 1><<<sms * rs.extend_blocks, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
+            k_extend_dyn<128, kExtendRefill><<<sms * rs.extend_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
         else
             k_extend<false, false, 128, 0><<<sms * rs.extend_blocks_bin, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
         if (fp.guided && d + 1 < fp.max_depth) {
