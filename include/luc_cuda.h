@@ -321,6 +321,7 @@ typedef struct luc_guide_info {
     float last_loss;       /* loss of the last step */
     uint32_t threshold;    /* current recording fraction, out of 65536 */
     uint32_t num_params;   /* 19176 */
+    uint32_t tc_error;     /* nonzero: a tensor-core kernel's bounded wait ran out (inference results invalid) */
 } luc_guide_info;
 
 /* Initialise the guide: params (num_params floats) or, when null, a seeded
@@ -336,6 +337,9 @@ int32_t luc_guide_get_params(luc_ctx* ctx, float* out);
 int32_t luc_guide_stats(luc_ctx* ctx, luc_guide_info* out);
 /* Raw network outputs (40 floats per row) for rows of 9 floats: position,
  * shading normal, outgoing direction. Host arrays. */
+/* luc_guide_forward through a chosen implementation: path 0 the tcgen05
+ * tensor-core kernel (what luc_guide_forward runs), 1 the mma.sync kernel. */
+int32_t luc_guide_forward_ex(luc_ctx* ctx, const float* in9, uint32_t n, int32_t path, float* out40);
 int32_t luc_guide_forward(luc_ctx* ctx, const float* in9, uint32_t n, float* out40);
 /* Host training records, 20 floats each: position, F, normal, -, outgoing
  * direction, -, sampled direction, -, 4 unused. steps == 0: the gradient of

@@ -124,6 +124,15 @@ int32_t luc_gather_triangles(luc_ctx* c, const GpuTriangle* src, GpuTriangle* ds
 // Implemented in wavefront.cu: derive the traversal layout (child-pair
 // records, triangle soup) from the resident nodes and triangles.
 int32_t luc_build_traversal(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris);
+// guide_tc.cu: the guide MLP forward on tcgen05 (n rows of 9 inputs -> 40
+// raw outputs); *err becomes nonzero if a bounded wait ran out.
+cudaError_t launch_guide_forward_tc(const float* in9, uint32_t n, const luc::GuideDev& g, float* out40, uint32_t* err,
+                                    int num_sms, cudaStream_t s);
+// guide_tc.cu: per-bounce guide inference on tcgen05 (the render's path);
+// guide_tc_setup opts its kernels into their shared memory (before capture).
+void launch_guide_infer_tc(const luc::RenderState& rs, const luc::DevScene& sc, const luc::FrameParams& fp,
+                           uint32_t depth, cudaStream_t s);
+cudaError_t guide_tc_setup();
 // stats.cu: record the convergence meter over a device accumulator on `s`;
 // the figure lands in c->conv_scratch after 64 float2 partials.
 int32_t luc_record_convergence(luc_ctx* c, const GpuAccum* accum, uint32_t pixels, cudaStream_t s);

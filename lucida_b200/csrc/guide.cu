@@ -731,6 +731,7 @@ static cudaError_t guide_kernel_setup(int device) {
         e = cudaFuncSetAttribute(k_guide_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InferSmem));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem));
+    if (e == cudaSuccess) e = guide_tc_setup();
     if (e != cudaSuccess) return e;
     int b = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_guide_infer, kInferWarps * 32, sizeof(InferSmem));
@@ -739,9 +740,15 @@ static cudaError_t guide_kernel_setup(int device) {
     return cudaSuccess;
 }
 
+// Per bounce: the guide's mixtures for the queued paths. The register-
+// chained mma.sync kernel: measured 1.5 ms per 1-spp 1024^2 guided frame
+// against 2.1 ms for the tcgen05 tile kernel (guide_tc.cu), whose four
+// dependent layers per 128-row tile each wait on a CTA-wide barrier and an
+// MMA round trip through TMEM. LUC_GUIDE_TC=1 selects that one per context.
 void launch_guide_infer(const RenderState& rs, const DevScene& sc, const FrameParams& fp, uint32_t depth,
                         cudaStream_t s) {
-    k_guide_infer<<<rs.num_sms * g_infer_blocks, kInferWarps * 32, sizeof(InferSmem), s>>>(rs.ps, sc, fp, depth);
+    if (rs.guide_tc) launch_guide_infer_tc(rs, sc, fp, depth, s);
+    else k_guide_infer<<<rs.num_sms * g_infer_blocks, kInferWarps * 32, sizeof(InferSmem), s>>>(rs.ps, sc, fp, depth);
 }
 
 void launch_guide_train(const RenderState& rs, const FrameParams& fp, const GuideTrain& gt, cudaStream_t s) {
@@ -888,11 +895,13 @@ int32_t luc_guide_stats(luc_ctx* c, luc_guide_info* out) {
     std::memcpy(&out->last_loss, &misc[kGmLastLoss], 4);
     out->threshold = misc[kGmThreshold];
     out->num_params = kGParams;
+    out->tc_error = misc[kGmTcError];
     return LUC_OK;
 }
 
-int32_t luc_guide_forward(luc_ctx* c, const float* in9, uint32_t n, float* out40) {
+int32_t luc_guide_forward_ex(luc_ctx* c, const float* in9, uint32_t n, int32_t path, float* out40) {
     if (!c || (n && (!in9 || !out40))) return LUC_ERR_VALIDATION;
+    if (path != 0 && path != 1) return luc_fail(c, LUC_ERR_VALIDATION, "path: 0 tcgen05, 1 mma.sync");
     if (int32_t rc = require_guide(c)) return rc;
     if (n == 0) return LUC_OK;
     cudaSetDevice(c->device);
@@ -901,12 +910,25 @@ int32_t luc_guide_forward(luc_ctx* c, const float* in9, uint32_t n, float* out40
     float* din = c->g_io.as<float>();
     float* dout = din + (size_t)n * 9;
     LUC_CUDA(c, cudaMemcpyAsync(din, in9, (size_t)n * 9 * sizeof(float), cudaMemcpyHostToDevice, s), "upload");
-    int grid = (int)std::min<uint64_t>((n + 16 * kInferWarps - 1) / (16 * kInferWarps), (uint64_t)c->num_sms * 2);
-    k_guide_forward<<<grid, kInferWarps * 32, sizeof(InferSmem), s>>>(din, n, luc_guide_dev(c), dout);
-    LUC_CUDA(c, cudaGetLastError(), "guide forward");
+    uint32_t* err = c->g_misc.as<uint32_t>() + kGmTcError;
+    if (path == 0) {
+        LUC_CUDA(c, cudaMemsetAsync(err, 0, 4, s), "clear error word");
+        LUC_CUDA(c, launch_guide_forward_tc(din, n, luc_guide_dev(c), dout, err, c->num_sms, s), "guide forward");
+    } else {
+        int grid = (int)std::min<uint64_t>((n + 16 * kInferWarps - 1) / (16 * kInferWarps), (uint64_t)c->num_sms * 2);
+        k_guide_forward<<<grid, kInferWarps * 32, sizeof(InferSmem), s>>>(din, n, luc_guide_dev(c), dout);
+        LUC_CUDA(c, cudaGetLastError(), "guide forward");
+    }
+    uint32_t h_err = 0;
     LUC_CUDA(c, cudaMemcpyAsync(out40, dout, (size_t)n * kGOut * sizeof(float), cudaMemcpyDeviceToHost, s), "readback");
+    LUC_CUDA(c, cudaMemcpyAsync(&h_err, err, 4, cudaMemcpyDeviceToHost, s), "read error word");
     LUC_CUDA(c, cudaStreamSynchronize(s), "guide forward");
+    if (path == 0 && h_err) return luc_fail(c, LUC_ERR_LAUNCH, "guide forward: a tensor-core wait ran out");
     return LUC_OK;
+}
+
+int32_t luc_guide_forward(luc_ctx* c, const float* in9, uint32_t n, float* out40) {
+    return luc_guide_forward_ex(c, in9, n, 0, out40);
 }
 
 int32_t luc_guide_train_records(luc_ctx* c, const float* records, uint32_t n, uint32_t steps, float* grad_out,

@@ -35,6 +35,7 @@ constexpr int kGmCandidates = 4;  // guided, surviving vertices this batch
 constexpr int kGmThreshold = 5;   // recording threshold, 16-bit fraction
 constexpr int kGmLastLoss = 6;    // loss of the last step (f32)
 constexpr int kGmLastRecords = 7; // records used by the last step
+constexpr int kGmTcError = 8;     // a tensor-core kernel's bounded wait ran out (nonzero)
 constexpr int kGmWords = 16;
 
 // Training record, 5 float4 per guided vertex:

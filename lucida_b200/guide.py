@@ -60,11 +60,13 @@ class Guide:
         check(self.gpu.handle, lib().luc_guide_stats(self.gpu.handle, C.byref(s)))
         return s
 
-    def forward(self, x, n, wo) -> np.ndarray:
-        """Raw outputs (N, 40) for positions, shading normals and outgoing directions."""
+    def forward(self, x, n, wo, path: str = "tcgen05") -> np.ndarray:
+        """Raw outputs (N, 40) for positions, shading normals and outgoing
+        directions, through the tcgen05 tensor-core kernel or the mma.sync one."""
         a = np.ascontiguousarray(np.concatenate([np.asarray(v, np.float32).reshape(-1, 3) for v in (x, n, wo)], 1))
         out = np.zeros((len(a), 40), np.float32)
-        check(self.gpu.handle, lib().luc_guide_forward(self.gpu.handle, ptr(a), len(a), ptr(out)))
+        code = {"tcgen05": 0, "mma.sync": 1}[path]
+        check(self.gpu.handle, lib().luc_guide_forward_ex(self.gpu.handle, ptr(a), len(a), code, ptr(out)))
         return out
 
     def gradient(self, records: np.ndarray):

@@ -79,7 +79,7 @@ class BatchConfig(C.Structure):
 
 class GuideInfo(C.Structure):
     _fields_ = [("steps", C.c_uint32), ("last_records", C.c_uint32), ("last_loss", C.c_float),
-                ("threshold", C.c_uint32), ("num_params", C.c_uint32)]
+                ("threshold", C.c_uint32), ("num_params", C.c_uint32), ("tc_error", C.c_uint32)]
 
 
 # Every entry point include/luc_cuda.h declares, with its ctypes signature.
@@ -126,6 +126,7 @@ _SIGS = {
     "luc_guide_get_params": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "luc_guide_stats": (C.c_int32, [C.c_void_p, C.POINTER(GuideInfo)]),
     "luc_guide_forward": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "luc_guide_forward_ex": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p]),
     "luc_guide_train_records": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                             C.c_void_p]),
     "luc_guide_mixture": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p,

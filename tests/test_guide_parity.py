@@ -71,6 +71,22 @@ def test_forward_matches_the_bf16_oracle(gpu):
     print("forward: max/mean err (of max |out|):", err.max() / scale, err.mean() / scale)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 127, 128, 129, 40_000])
+def test_tcgen05_forward_matches_mma_sync(gpu, n):
+    """The tcgen05 (TMEM) forward against the mma.sync one: the same BF16
+    operands and activations, FP32 accumulation in a different order."""
+    from lucida_b200 import Guide
+    guide = Guide(gpu, params=_params(3), lo=LO, hi=HI)
+    x, nrm, wo = _inputs(n, 5)
+    a = guide.forward(x, nrm, wo, path="tcgen05")
+    b = guide.forward(x, nrm, wo, path="mma.sync")
+    scale = max(np.abs(b).max(), 1e-6)
+    err = np.abs(a - b)
+    print(n, "tcgen05 vs mma.sync max/mean err (of max |out|):", err.max() / scale, err.mean() / scale)
+    assert np.all(np.isfinite(a)) and err.max() < 2e-2 * scale and err.mean() < 2e-4 * scale
+
+
 def _records(n, seed):
     rng = np.random.default_rng(seed)
     x, nrm, wo = _inputs(n, seed + 1)
@@ -200,15 +216,31 @@ def _block_means(gpu, scene, spp, depth, guided, sampling, calls, seed):
     return np.array(out)
 
 
+@pytest.fixture(scope="module")
+def gpu_tc():
+    """A context whose renders run the guide inference on the tcgen05 kernel."""
+    import os
+    import lucida_b200 as lb
+    os.environ["LUC_GUIDE_TC"] = "1"
+    try:
+        g = lb.Gpu(0)
+    finally:
+        del os.environ["LUC_GUIDE_TC"]
+    yield g
+    g.close()
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("sampling", ["mis", "nee", "bsdf"])
-def test_guided_render_is_unbiased(gpu, sampling):
+@pytest.mark.parametrize("inference", ["mma.sync", "tcgen05"])
+def test_guided_render_is_unbiased(gpu, gpu_tc, sampling, inference):
     """Cornell box, 64 x 64: 64 guided batches of 8 spp (an untrained guide
     that takes one Adam step per batch) against 16 plain batches of 64 spp.
     Block means must agree within their standard errors (estimated from the
     spread across batches): |z| < 5 for each of the 64 blocks, mean |z| < 1.5,
     and the image means within 1%."""
     from lucida_b200 import Guide, scenes
+    gpu = gpu_tc if inference == "tcgen05" else gpu
     scene = scenes.cornell_analytic()
     gpu.upload(scene, force=True)
     guide = Guide(gpu, seed=3)
@@ -216,6 +248,7 @@ def test_guided_render_is_unbiased(gpu, sampling):
     g = _block_means(gpu, scene, 8, 6, True, sampling, 64, 0x5EED1234)
     st = guide.stats()
     assert st.steps == 64 and st.last_records > 0
+    assert st.tc_error == 0  # every tensor-core inference tile completed
     r = _block_means(gpu, scene, 64, 6, False, sampling, 16, 0xC0FFEE)
     mg, mr = g.mean(0), r.mean(0)
     se = np.sqrt(g.var(0, ddof=1) / len(g) + r.var(0, ddof=1) / len(r))
