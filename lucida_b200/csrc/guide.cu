@@ -740,11 +740,10 @@ static cudaError_t guide_kernel_setup(int device) {
     return cudaSuccess;
 }
 
-// Per bounce: the guide's mixtures for the queued paths. The register-
-// chained mma.sync kernel: measured 1.5 ms per 1-spp 1024^2 guided frame
-// against 2.1 ms for the tcgen05 tile kernel (guide_tc.cu), whose four
-// dependent layers per 128-row tile each wait on a CTA-wide barrier and an
-// MMA round trip through TMEM. LUC_GUIDE_TC=1 selects that one per context.
+// Per bounce: the guide's mixtures for the queued paths, by default on the
+// tcgen05 team kernel (guide_tc.cu: 1.14 ms per 1-spp 1024^2 guided frame);
+// LUC_GUIDE_TC=0 selects the register-chained mma.sync kernel (1.45 ms)
+// per context. Both give the same mixtures bit for bit.
 void launch_guide_infer(const RenderState& rs, const DevScene& sc, const FrameParams& fp, uint32_t depth,
                         cudaStream_t s) {
     if (rs.guide_tc) launch_guide_infer_tc(rs, sc, fp, depth, s);

@@ -4,20 +4,23 @@
 // encoding as the mma.sync forward in guide.cu (BF16 operands, FP32
 // accumulation, bias + ReLU in FP32, BF16 activations between layers).
 //
-// One CTA of 128 threads owns 128-row tiles, one row per thread:
-//   * the thread writes its row's 128 features (64 sin/cos pairs) into the
-//     A tile in shared memory, BF16, in the canonical K-major no-swizzle
-//     layout: 8 x 16-byte core matrices, 8-element K chunks LBO apart, 8-row
-//     groups 128 B apart;
+// Eight teams per CTA (one CTA per SM), each a 128-row pipeline: four warps,
+// one thread per row (its TMEM lane), a named barrier, an mbarrier, 64 TMEM
+// columns and a 16 KB operand region:
+//   * the thread writes its row's features (BF16, 64 sin/cos pairs) into the
+//     region in the canonical K-major no-swizzle layout — 8 x 16-byte core
+//     matrices, 8-element K chunks LBO apart, 8-row groups 128 B apart — in
+//     two K halves, the first layer accumulating over both;
 //   * one thread issues the layer's MMAs (M = 128, N = 64 or 48, K = 16
 //     each) against the weights (B, same layout, loaded once per CTA) into
-//     TMEM columns 0..63, and commits them to an mbarrier;
-//   * every thread waits (bounded), reads its row of the accumulator from
-//     TMEM (warp w reads lanes 32w..32w+31), adds the bias, applies ReLU and
-//     writes the BF16 activations as the next layer's A tile;
+//     the team's TMEM columns and commits them to the team's mbarrier;
+//   * every thread waits (bounded), reads its row of the accumulator
+//     (tcgen05.ld, 16 columns at a time), adds the bias, applies ReLU and
+//     writes the BF16 activations back into the region as the next A tile;
 //   * the last layer's 48 outputs (40 used) go to the caller's functor.
-// A wait that runs out of iterations sets the CTA's error word (reported in
-// *err), all threads leave the tile loop together and the TMEM is freed.
+// Eight tiles in flight per SM hide one another's MMA round trips. A wait
+// that runs out of iterations sets the error word (*err); the team votes, so
+// all its threads leave the tile loop together, and the TMEM is freed.
 #include <cuda_bf16.h>
 
 #include "ctx.cuh"
@@ -27,32 +30,12 @@ namespace luc {
 namespace tcg {
 
 constexpr int kM = 128;
-constexpr int kParts = 4, kThreads = kM * kParts;  // four threads per row
 constexpr uint32_t kLboA = kM * 16;            // A tiles: 128 rows per 8-element K chunk
 constexpr uint32_t kLboH = kGHid * 16;         // B tiles of 64 output units
 constexpr uint32_t kLboO = kGOutPad * 16;      // B tile of the 48 (40 used) output units
 constexpr uint32_t kSbo = 128;                 // 8 rows of 16 B
 constexpr uint32_t kTmemCols = 64;
 constexpr uint32_t kWaitLimit = 1u << 22;
-
-struct Smem {
-    // The features (A of the first layer) and, once that layer has run, the
-    // tile's raw outputs (bias added) share the first 32 KB.
-    union {
-        uint8_t x[(kGIn / 8) * kLboA];    // features, 32 KB
-        float o[kM][kGOutPad];           // 24 KB
-    };
-    uint8_t h[(kGHid / 8) * kLboA];   // hidden activations, 16 KB
-    uint8_t w1[(kGIn / 8) * kLboH];   // 16 KB
-    uint8_t w2[(kGHid / 8) * kLboH];  // 8 KB
-    uint8_t w3[(kGHid / 8) * kLboH];  // 8 KB
-    uint8_t w4[(kGHid / 8) * kLboO];  // 6 KB
-    float b[kGBias];
-    float in[kM][9];          // the tile's inputs (computed once per row)
-    uint8_t valid[kM];
-    unsigned long long mbar;
-    uint32_t tmem;
-};
 
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -97,22 +80,6 @@ __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::be
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// 32 consecutive FP32 columns of this thread's TMEM lane.
-__device__ __forceinline__ void ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-        "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
-}
-
 // 16 consecutive FP32 columns of this thread's TMEM lane.
 __device__ __forceinline__ void ld16(uint32_t taddr, float (&v)[16]) {
     uint32_t r[16];
@@ -139,30 +106,35 @@ __device__ __forceinline__ uint4* chunk(uint8_t* tile, int c, int r) {
     return reinterpret_cast<uint4*>(tile + c * kLboA + (r >> 3) * kSbo + (r & 7) * 16);
 }
 
-// Weights (row = output unit, K contiguous, BF16) into the B layout.
-__device__ void load_weights(Smem& S, const uint16_t* __restrict__ wbf, const float* __restrict__ bias) {
-    auto load = [&](uint8_t* dst, const uint16_t* src, int n, int k, uint32_t lbo) {
-        const int chunks = n * (k / 8);
-        for (int i = threadIdx.x; i < chunks; i += blockDim.x) {
-            const int row = i / (k / 8), c = i % (k / 8);
-            const uint4 v = *reinterpret_cast<const uint4*>(src + row * k + c * 8);
-            *reinterpret_cast<uint4*>(dst + c * lbo + (row >> 3) * kSbo + (row & 7) * 16) = v;
-        }
-    };
-    load(S.w1, wbf, kGHid, kGIn, kLboH);
-    load(S.w2, wbf + kGHid * kGIn, kGHid, kGHid, kLboH);
-    load(S.w3, wbf + kGHid * kGIn + kGHid * kGHid, kGHid, kGHid, kLboH);
-    load(S.w4, wbf + kGHid * kGIn + 2 * kGHid * kGHid, kGOutPad, kGHid, kLboO);
-    for (int i = threadIdx.x; i < kGBias; i += blockDim.x) S.b[i] = bias[i];
+// ---------------------------------------------------------------- teams
+// Eight teams per CTA, each a complete 128-row pipeline of its own: four
+// warps (one per TMEM lane quadrant, one thread per row), a 16 KB operand
+// region (the first layer's features in two K halves, then the hidden
+// activations), 64 TMEM columns, an mbarrier and a named barrier. The
+// weights are shared. Eight tiles are in flight per SM, so one team's
+// features and epilogues overlap the others' MMA round trips.
+constexpr int kTeams = 8, kTeamThreads = kM, kTeamCta = kTeams * kTeamThreads;
+constexpr uint32_t kRegion = (kGHid / 8) * kLboA;  // 16 KB: 128 rows x 64 BF16
+
+struct TeamSmem {
+    uint8_t a[kTeams][kRegion];
+    uint8_t w1[(kGIn / 8) * kLboH], w2[(kGHid / 8) * kLboH], w3[(kGHid / 8) * kLboH], w4[(kGHid / 8) * kLboO];
+    float b[kGBias];
+    unsigned long long mbar[kTeams];
+    uint32_t tmem;
+};
+
+__device__ __forceinline__ void team_sync(int team) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + team), "r"(kTeamThreads) : "memory");
 }
 
-// The 128 features of one row (position: 12 frequencies per axis of the
-// box-normalised point; normal and outgoing direction: 4 each; sin/cos
-// pairs, zero padding from 120) into row r of the feature tile.
-__device__ __forceinline__ void write_features(Smem& S, int r, int part, const float (&in)[9], const GuideDev& g) {
+// Feature pairs [32 h, 32 h + 32) of a row (the K half h of the first
+// layer) as 8 chunks of the team's region.
+__device__ __forceinline__ void write_feature_half(uint8_t* region, int r, int h, const float (&in)[9],
+                                                   const GuideDev& g) {
 #pragma unroll
-    for (int cc = 0; cc < kGIn / 8 / kParts; ++cc) {
-        const int c = part * (kGIn / 8 / kParts) + cc;
+    for (int cc = 0; cc < 8; ++cc) {
+        const int c = 8 * h + cc;
         uint32_t w[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -184,46 +156,38 @@ __device__ __forceinline__ void write_features(Smem& S, int r, int part, const f
             sincosf(arg, &sn, &cs);
             w[j] = pack2(sn, cs);
         }
-        *chunk(S.x, c, r) = make_uint4(w[0], w[1], w[2], w[3]);
+        *chunk(region, cc, r) = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 
-// bias + ReLU of this thread's 16 accumulator columns (16 part .. + 15)
-// into row r of the hidden tile.
-__device__ __forceinline__ void write_hidden(Smem& S, int r, int part, const float (&v)[16],
-                                             const float* __restrict__ b) {
-#pragma unroll
-    for (int cc = 0; cc < 2; ++cc) {
-        uint32_t w[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int k = 8 * cc + 2 * j, n = 16 * part + k;
-            w[j] = pack2(fmaxf(v[k] + b[n], 0.0f), fmaxf(v[k + 1] + b[n + 1], 0.0f));
-        }
-        *chunk(S.h, 2 * part + cc, r) = make_uint4(w[0], w[1], w[2], w[3]);
-    }
-}
-
-// The tile loop. load(row, in) fills a row's 9 inputs (false: no row to
-// evaluate); store(row, out) receives the 48 raw outputs (bias added) of
-// every valid row. Thread (warp w, lane l) serves row 32 (w % 4) + l — the
-// TMEM lane quadrant warp w may read — as part w / 4 of four: the part-0
-// thread loads the inputs and later decodes; each part computes 16 feature
-// pairs and reads 16 accumulator columns.
 template <typename Load, typename Store>
-__device__ void forward_tiles(uint32_t n, const GuideDev& g, uint32_t* err, Load load, Store store) {
+__device__ void forward_teams(uint32_t n, const GuideDev& g, uint32_t* err, Load load, Store store) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    Smem& S = *reinterpret_cast<Smem*>(smem_raw);
-    const int t = threadIdx.x, warp = t >> 5, part = warp >> 2;
-    const int r = 32 * (warp & 3) + (t & 31);
-    load_weights(S, g.wbf, g.bias);
-    if (t == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%1], %0;" ::"r"(1u), "r"(saddr(&S.mbar)) : "memory");
+    TeamSmem& S = *reinterpret_cast<TeamSmem*>(smem_raw);
+    const int t = threadIdx.x, warp = t >> 5, team = warp >> 2, tt = t & (kTeamThreads - 1);
+    const int r = 32 * (warp & 3) + (t & 31);  // this thread's row = its TMEM lane
+    {
+        auto load_w = [&](uint8_t* dst, const uint16_t* src, int nn, int k, uint32_t lbo) {
+            const int chunks = nn * (k / 8);
+            for (int i = t; i < chunks; i += blockDim.x) {
+                const int row = i / (k / 8), c = i % (k / 8);
+                *reinterpret_cast<uint4*>(dst + c * lbo + (row >> 3) * kSbo + (row & 7) * 16) =
+                    *reinterpret_cast<const uint4*>(src + row * k + c * 8);
+            }
+        };
+        load_w(S.w1, g.wbf, kGHid, kGIn, kLboH);
+        load_w(S.w2, g.wbf + kGHid * kGIn, kGHid, kGHid, kLboH);
+        load_w(S.w3, g.wbf + kGHid * kGIn + kGHid * kGHid, kGHid, kGHid, kLboH);
+        load_w(S.w4, g.wbf + kGHid * kGIn + 2 * kGHid * kGHid, kGOutPad, kGHid, kLboO);
+        for (int i = t; i < kGBias; i += blockDim.x) S.b[i] = g.bias[i];
+    }
+    if (t < kTeams) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%1], %0;" ::"r"(1u), "r"(saddr(&S.mbar[t])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&S.tmem)),
-                     "r"(kTmemCols)
+                     "r"(kTeams * kTmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -231,88 +195,110 @@ __device__ void forward_tiles(uint32_t n, const GuideDev& g, uint32_t* err, Load
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tmem = S.tmem, mbar = saddr(&S.mbar);
-    const uint32_t lane_addr = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + 16 * part;
+    const uint32_t tcol = S.tmem + kTmemCols * team;  // this team's accumulator columns
+    const uint32_t lane_addr = tcol + ((uint32_t)(32 * (warp & 3)) << 16);
+    const uint32_t mbar = saddr(&S.mbar[team]);
+    uint8_t* region = S.a[team];
     uint32_t phase = 0;
     bool failed = false;
-    // One layer: MMAs over K (k16 steps), commit, bounded wait; every thread
-    // learns whether the CTA's wait completed.
-    auto layer = [&](const uint8_t* a, uint32_t lba, const uint8_t* w, uint32_t lbw, int ksteps, int nout) {
+    // MMAs over ksteps k16 steps from the region against w (first: whether D
+    // starts fresh), commit, bounded wait; the whole team learns the outcome.
+    auto mma_step = [&](const uint8_t* w, uint32_t lbw, int ksteps, int nout, bool fresh) {
         fence_async_smem();
         fence_before();
-        __syncthreads();
+        team_sync(team);
         fence_after();
-        if (t == 0) {
+        if (tt == 0) {
             for (int ks = 0; ks < ksteps; ++ks)
-                mma(tmem, desc(saddr(a) + 2 * ks * lba, lba), desc(saddr(w) + 2 * ks * lbw, lbw), idesc(nout),
-                    ks > 0 ? 1u : 0u);
+                mma(tcol, desc(saddr(region) + 2 * ks * kLboA, kLboA), desc(saddr(w) + 2 * ks * lbw, lbw), idesc(nout),
+                    (fresh && ks == 0) ? 0u : 1u);
             commit(mbar);
         }
         const bool ok = wait_phase(mbar, phase);
         phase ^= 1u;
         fence_after();
-        return __syncthreads_and(ok) != 0;
+        // The team votes on the outcome (threads time out independently),
+        // so all of them leave the tile loop together or none does.
+        uint32_t any_fail;
+        asm volatile(
+            "{\n\t.reg .pred q, p;\n\t"
+            "setp.ne.u32 q, %1, 0;\n\t"
+            "bar.red.or.pred p, %2, %3, q;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(any_fail)
+            : "r"(ok ? 0u : 1u), "r"(1 + team), "r"(kTeamThreads)
+            : "memory");
+        return any_fail == 0u;
     };
-    for (uint32_t base = blockIdx.x * kM; base < n; base += gridDim.x * kM) {
+    // bias + ReLU of 64 accumulator columns (16 at a time) into the region.
+    auto epilogue = [&](const float* b) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float v[16];
+            ld16(lane_addr + 16 * q, v);
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                uint32_t w[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int k = 8 * cc + 2 * j, nn = 16 * q + k;
+                    w[j] = pack2(fmaxf(v[k] + b[nn], 0.0f), fmaxf(v[k + 1] + b[nn + 1], 0.0f));
+                }
+                *chunk(region, 2 * q + cc, r) = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+        }
+    };
+    const uint32_t stride = gridDim.x * kTeams * kM;
+    for (uint32_t base = (blockIdx.x * kTeams + team) * kM; base < n; base += stride) {
         const uint32_t row = base + r;
-        if (part == 0) {
-            float in[9] = {0, 0, 0, 0, 0, 1, 0, 0, 1};
-            const bool valid = row < n && load(row, in);
+        float in[9] = {0, 0, 0, 0, 0, 1, 0, 0, 1};
+        const bool valid = row < n && load(row, in);
+        write_feature_half(region, r, 0, in, g);
+        bool ok = mma_step(S.w1, kLboH, 4, kGHid, true);
+        if (ok) {
+            write_feature_half(region, r, 1, in, g);
+            ok = mma_step(S.w1 + 8 * kLboH, kLboH, 4, kGHid, false);
+        }
+        if (ok) {
+            epilogue(S.b);
+            ok = mma_step(S.w2, kLboH, 4, kGHid, true);
+        }
+        if (ok) {
+            epilogue(S.b + kGHid);
+            ok = mma_step(S.w3, kLboH, 4, kGHid, true);
+        }
+        if (ok) {
+            epilogue(S.b + 2 * kGHid);
+            ok = mma_step(S.w4, kLboO, 4, kGOutPad, true);
+        }
+        if (!ok) {
+            failed = true;
+            break;
+        }
+        float o[kGOutPad];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) S.in[r][k] = in[k];
-            S.valid[r] = valid ? 1 : 0;
-        }
-        __syncthreads();
-        {
-            float in[9];
+        for (int q = 0; q < 3; ++q) {
+            float v[16];
+            ld16(lane_addr + 16 * q, v);
 #pragma unroll
-            for (int k = 0; k < 9; ++k) in[k] = S.in[r][k];
-            write_features(S, r, part, in, g);
+            for (int k = 0; k < 16; ++k) o[16 * q + k] = v[k] + S.b[3 * kGHid + 16 * q + k];
         }
-        float v[16];
-        if (!layer(S.x, kLboA, S.w1, kLboH, kGIn / 16, kGHid)) {
-            failed = true;
-            break;
-        }
-        ld16(lane_addr, v);
-        write_hidden(S, r, part, v, S.b);
-        if (!layer(S.h, kLboA, S.w2, kLboH, kGHid / 16, kGHid)) {
-            failed = true;
-            break;
-        }
-        ld16(lane_addr, v);
-        write_hidden(S, r, part, v, S.b + kGHid);
-        if (!layer(S.h, kLboA, S.w3, kLboH, kGHid / 16, kGHid)) {
-            failed = true;
-            break;
-        }
-        ld16(lane_addr, v);
-        write_hidden(S, r, part, v, S.b + 2 * kGHid);
-        if (!layer(S.h, kLboA, S.w4, kLboO, kGHid / 16, kGOutPad)) {
-            failed = true;
-            break;
-        }
-        ld16(lane_addr, v);  // part 3 reads columns 48..63, which the last layer does not write
-        if (part < kGOutPad / 16) {
-#pragma unroll
-            for (int k = 0; k < 16; ++k) S.o[r][16 * part + k] = v[k] + S.b[3 * kGHid + 16 * part + k];
-        }
+        if (valid) store(row, o);
         fence_before();
-        __syncthreads();
-        if (part == 0 && S.valid[r]) store(row, S.o[r]);
     }
-    if (failed && t == 0) atomicOr(err, 1u);
+    if (failed && tt == 0) atomicOr(err, 1u);
     fence_before();
     __syncthreads();
     fence_after();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(S.tmem), "r"(kTeams * kTmemCols)
+                     : "memory");
 }
 
 // Raw outputs (bias added) of n rows of 9 inputs: the test-facing forward.
-__global__ void __launch_bounds__(kThreads, 2) k_forward_tc(const float* __restrict__ in9, uint32_t n, GuideDev g,
+__global__ void __launch_bounds__(kTeamCta, 1) k_forward_tc(const float* __restrict__ in9, uint32_t n, GuideDev g,
                                                    float* __restrict__ out40, uint32_t* err) {
-    forward_tiles(
+    forward_teams(
         n, g, err,
         [&](uint32_t row, float (&in)[9]) {
 #pragma unroll
@@ -330,11 +316,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_forward_tc(const float* __restr
 // Inputs are the hit point, the shading normal and the outgoing direction.
 // The decode is the per-row form of the two-lane decode it replaces, in the
 // same operation order (the softmax sum is the two half-sums added).
-__global__ void __launch_bounds__(kThreads, 2) k_infer_tc(PathState ps, const __grid_constant__ DevScene sc,
+__global__ void __launch_bounds__(kTeamCta, 1) k_infer_tc(PathState ps, const __grid_constant__ DevScene sc,
                                                  const __grid_constant__ FrameParams fp, uint32_t depth) {
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
     const uint32_t* queue = ps.queue[depth & 1];
-    forward_tiles(
+    forward_teams(
         len, fp.guide, ps.gmisc + kGmTcError,
         [&](uint32_t i, float (&in)[9]) {
             const uint32_t q = depth == 0 ? i : queue[i];
@@ -389,18 +375,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_infer_tc(PathState ps, const __
 cudaError_t guide_tc_setup() {
     using namespace luc;
     cudaError_t e = cudaFuncSetAttribute(tcg::k_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(tcg::Smem));
+                                         (int)sizeof(tcg::TeamSmem));
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(tcg::k_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(tcg::Smem));
+        e = cudaFuncSetAttribute(tcg::k_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(tcg::TeamSmem));
     return e;
 }
 
 void launch_guide_infer_tc(const luc::RenderState& rs, const luc::DevScene& sc, const luc::FrameParams& fp,
                            uint32_t depth, cudaStream_t s) {
     using namespace luc;
-    // Persistent tiles: two CTAs fit an SM (shared memory), each holding 64
-    // TMEM columns.
-    tcg::k_infer_tc<<<rs.num_sms * 2, tcg::kThreads, sizeof(tcg::Smem), s>>>(rs.ps, sc, fp, depth);
+    // Persistent: one CTA of eight teams per SM (all 512 TMEM columns).
+    tcg::k_infer_tc<<<rs.num_sms, tcg::kTeamCta, sizeof(tcg::TeamSmem), s>>>(rs.ps, sc, fp, depth);
 }
 
 // Launch the tensor-core forward over n rows of 9 inputs (device arrays).
@@ -409,7 +395,8 @@ cudaError_t launch_guide_forward_tc(const float* in9, uint32_t n, const luc::Gui
     using namespace luc;
     static const cudaError_t attr = guide_tc_setup();
     if (attr != cudaSuccess) return attr;
-    const int grid = (int)std::min<uint64_t>((n + tcg::kM - 1) / tcg::kM, (uint64_t)num_sms * 2);
-    tcg::k_forward_tc<<<grid, tcg::kThreads, sizeof(tcg::Smem), s>>>(in9, n, g, out40, err);
+    const uint64_t per_cta = (uint64_t)tcg::kTeams * tcg::kM;
+    const int grid = (int)std::min<uint64_t>((n + per_cta - 1) / per_cta, (uint64_t)num_sms);
+    tcg::k_forward_tc<<<grid, tcg::kTeamCta, sizeof(tcg::TeamSmem), s>>>(in9, n, g, out40, err);
     return cudaGetLastError();
 }

@@ -106,7 +106,7 @@ struct RenderState {
     int extend_blocks_inst = 0, connect_blocks_inst = 0, shade_blocks_inst = 0, shade_blocks_guided_inst = 0;
     int extend_blocks_bin = 0, connect_blocks_bin = 0;  // single-level scenes on the binary tree
     int extend_blocks_inst_bin = 0, connect_blocks_inst_bin = 0;  // two-level scenes on binary BLASes
-    bool guide_tc = false;  // guide inference on the tcgen05 tile kernel (LUC_GUIDE_TC=1)
+    bool guide_tc = true;  // guide inference on tcgen05 (LUC_GUIDE_TC=0: the mma.sync kernel)
     uint64_t launches = 0;
 };
 

@@ -217,11 +217,12 @@ def _block_means(gpu, scene, spp, depth, guided, sampling, calls, seed):
 
 
 @pytest.fixture(scope="module")
-def gpu_tc():
-    """A context whose renders run the guide inference on the tcgen05 kernel."""
+def gpu_mma():
+    """A context whose renders run the guide inference on the mma.sync
+    kernel (the default is tcgen05)."""
     import os
     import lucida_b200 as lb
-    os.environ["LUC_GUIDE_TC"] = "1"
+    os.environ["LUC_GUIDE_TC"] = "0"
     try:
         g = lb.Gpu(0)
     finally:
@@ -233,14 +234,14 @@ def gpu_tc():
 @pytest.mark.gpu
 @pytest.mark.parametrize("sampling", ["mis", "nee", "bsdf"])
 @pytest.mark.parametrize("inference", ["mma.sync", "tcgen05"])
-def test_guided_render_is_unbiased(gpu, gpu_tc, sampling, inference):
+def test_guided_render_is_unbiased(gpu, gpu_mma, sampling, inference):
     """Cornell box, 64 x 64: 64 guided batches of 8 spp (an untrained guide
     that takes one Adam step per batch) against 16 plain batches of 64 spp.
     Block means must agree within their standard errors (estimated from the
     spread across batches): |z| < 5 for each of the 64 blocks, mean |z| < 1.5,
     and the image means within 1%."""
     from lucida_b200 import Guide, scenes
-    gpu = gpu_tc if inference == "tcgen05" else gpu
+    gpu = gpu_mma if inference == "mma.sync" else gpu
     scene = scenes.cornell_analytic()
     gpu.upload(scene, force=True)
     guide = Guide(gpu, seed=3)
