@@ -294,12 +294,13 @@ struct PoolSink {
 // kBatch: the path's scene and frame parameters come from its wave segment
 // (luc_render_batch) instead of the kernel arguments.
 //
-// 7 blocks of 128 per SM (72 registers, a few hundred bytes spilled): SHADE is
-// bound by the latency of its path-state, triangle and material loads, and
+// 8 blocks of 128 per SM (64 registers, about 700 bytes spilled to L1): SHADE
+// is bound by the latency of its path-state, triangle and material loads, and
 // the extra warps hide more of it than the spills cost (measured against 4,
-// 5 and 6 blocks).
+// 5, 6 and 7 blocks; 7 -> 8 took the displaced-sphere frame's SHADE from
+// 16.0 to 15.5 ms).
 template <bool kGuided, bool kInst, bool kBatch = false>
-__global__ void __launch_bounds__(128, 7) k_shade(PathState ps, const __grid_constant__ DevScene sc_arg,
+__global__ void __launch_bounds__(128, 8) k_shade(PathState ps, const __grid_constant__ DevScene sc_arg,
                                                   const __grid_constant__ FrameParams fp_arg, BatchDev bd,
                                                   uint32_t depth) {
     const uint32_t len = depth == 0 ? (uint32_t)fp_arg.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];

@@ -232,6 +232,15 @@ class Gpu:
         check(self._h, self._lib.luc_intersect(self._h, ptr(rays), len(o), 1, ptr(occ)))
         return occ.astype(bool)
 
+    def env_sample(self, u2):
+        """EnvMap::sample (envmap.rs:235-275) of the resident scene's
+        environment at each (u, v) pair: (direction, radiance, pdf)."""
+        u = np.ascontiguousarray(u2, np.float32).reshape(-1, 2)
+        n = len(u)
+        d, r, p = np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32), np.zeros(n, np.float32)
+        check(self._h, self._lib.luc_eval_env(self._h, ptr(u), n, 0, ptr(d), ptr(r), ptr(p)))
+        return d, r, p
+
     def stats(self) -> RenderStats:
         s = RenderStats()
         check(self._h, self._lib.luc_get_stats(self._h, C.byref(s)))
