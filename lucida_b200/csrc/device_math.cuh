@@ -181,9 +181,13 @@ struct Sampler {
             y = u32_to_unit(pcg_next(state));
             return;
         }
+        // Dimensions 2g and 2g+1 (even-aligned) share the group seed and the
+        // scrambled index: sobol_sample for both, with those computed once.
         state = (state + 1u) & ~1u;
-        x = sobol_sample(index, state, seed);
-        y = sobol_sample(index, state + 1u, seed);
+        const uint32_t gseed = hash_u32(seed ^ ((state >> 1) * 0x9e3779b9u));
+        const uint32_t shuffled = owen_scramble(index, gseed);
+        x = u32_to_unit(owen_scramble(__brev(shuffled), hash_u32(gseed + 1u)));
+        y = u32_to_unit(owen_scramble(sobol_dim1(shuffled), hash_u32(gseed + 2u)));
         state += 2u;
     }
 };

@@ -30,20 +30,8 @@ __global__ void k_tri_bounds(const GpuTriangle* __restrict__ tris, const float4*
                              float* __restrict__ boxes) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         GpuTriangle t = tris[i];
-        float4 a = pos[t.i0], b = pos[t.i1], c = pos[t.i2];
-        float lo[3] = {fminf(fminf(INFINITY, a.x), b.x), fminf(fminf(INFINITY, a.y), b.y),
-                       fminf(fminf(INFINITY, a.z), b.z)};
-        float hi[3] = {fmaxf(fmaxf(-INFINITY, a.x), b.x), fmaxf(fmaxf(-INFINITY, a.y), b.y),
-                       fmaxf(fmaxf(-INFINITY, a.z), b.z)};
-        lo[0] = fminf(lo[0], c.x); lo[1] = fminf(lo[1], c.y); lo[2] = fminf(lo[2], c.z);
-        hi[0] = fmaxf(hi[0], c.x); hi[1] = fmaxf(hi[1], c.y); hi[2] = fmaxf(hi[2], c.z);
-        // Aabb::pad: 1e-6 * (1 + max(|lo|, |hi|)) per axis.
-        for (int k = 0; k < 3; ++k) {
-            float scale = 1.0f + fmaxf(fabsf(lo[k]), fabsf(hi[k]));
-            float p = 1.0e-6f * scale;
-            lo[k] = lo[k] - p;
-            hi[k] = hi[k] + p;
-        }
+        float lo[3], hi[3];
+        padded_tri_box(pos[t.i0], pos[t.i1], pos[t.i2], lo, hi);
         float* o = boxes + 6 * (size_t)i;
         o[0] = lo[0]; o[1] = lo[1]; o[2] = lo[2]; o[3] = hi[0]; o[4] = hi[1]; o[5] = hi[2];
     }

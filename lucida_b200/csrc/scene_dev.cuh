@@ -84,6 +84,17 @@ LUC_D float env_pdf_texel(const DevScene& s, uint32_t i, uint32_t j) {
     float pdf_uv = weight / s.env_total * (float)(s.env_w * s.env_h);
     return pdf_uv / (2.0f * kPi * kPi * st);
 }
+// Radiance and pdf of the texel a direction falls in (one direction-to-texel
+// mapping serves both): EnvMap::radiance and EnvMap::pdf, envmap.rs:188-232.
+LUC_D V3 env_radiance_pdf(const DevScene& s, V3 d, float& pdf) {
+    float u, v;
+    env_uv(d, u, v);
+    uint32_t i, j;
+    env_texel(s, u, v, i, j);
+    pdf = env_pdf_texel(s, i, j);
+    float4 p = __ldg(s.env_px + (size_t)j * s.env_w + i);
+    return V3{p.x, p.y, p.z};
+}
 LUC_D float env_pdf(const DevScene& s, V3 d) {  // envmap.rs:211-232
     float u, v;
     env_uv(d, u, v);
@@ -137,6 +148,23 @@ LUC_D EnvSample env_sample(const DevScene& s, float ux, float uy) {  // envmap.r
 }
 
 // ---------------------------------------------------------------- geometry
+// A triangle's bounds padded as Aabb::pad does (bvh.rs:100-111): per axis
+// 1e-6 * (1 + max(|lo|, |hi|)) outwards. Every box of the binary tree is a
+// union of these.
+LUC_D void padded_tri_box(float4 a, float4 b, float4 c, float lo[3], float hi[3]) {
+    lo[0] = fminf(fminf(fminf(INFINITY, a.x), b.x), c.x);
+    lo[1] = fminf(fminf(fminf(INFINITY, a.y), b.y), c.y);
+    lo[2] = fminf(fminf(fminf(INFINITY, a.z), b.z), c.z);
+    hi[0] = fmaxf(fmaxf(fmaxf(-INFINITY, a.x), b.x), c.x);
+    hi[1] = fmaxf(fmaxf(fmaxf(-INFINITY, a.y), b.y), c.y);
+    hi[2] = fmaxf(fmaxf(fmaxf(-INFINITY, a.z), b.z), c.z);
+    for (int k = 0; k < 3; ++k) {
+        const float scale = 1.0f + fmaxf(fabsf(lo[k]), fabsf(hi[k]));
+        const float p = 1.0e-6f * scale;
+        lo[k] = lo[k] - p;
+        hi[k] = hi[k] + p;
+    }
+}
 LUC_D V3 vtx(const DevScene& s, uint32_t i) {
     float4 p = __ldg(s.positions + i);
     return V3{p.x, p.y, p.z};

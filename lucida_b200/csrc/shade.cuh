@@ -59,13 +59,14 @@ LUC_D bool shade_vertex(const DevScene& sc, const FrameParams& fp, uint32_t dept
     if (id == kMiss) {
         // Escaped (integrator.rs:228-263).
         if (sc.has_env) {
-            V3 l = env_radiance(sc, dir);
+            float epdf;
+            V3 l = env_radiance_pdf(sc, dir, epdf);
             float weight;
             if (depth == 0 || fp.sampling == LUC_SAMPLING_BSDF) weight = 1.0f;
             else if (fp.sampling == LUC_SAMPLING_NEE) weight = 0.0f;
             else {
                 uint32_t total = max(sc.light_strategies, 1u);
-                weight = power_heuristic(prev_pdf, env_pdf(sc, dir) / (float)total);
+                weight = power_heuristic(prev_pdf, epdf / (float)total);
             }
             if (weight > 0.0f) {
                 rad = rad + thr * l * weight;

@@ -11,6 +11,8 @@
 //   * an internal task opens children greedily, largest surface area first,
 //     until it has 8 children or none can be opened (a leaf with <= 4
 //     triangles stays a leaf slot, and a node holds at most 32 triangles);
+//     slots still free then take halves of its largest leaf slots, each
+//     with the box of its own triangles;
 //   * children are placed in slots by octant (greedy assignment of children
 //     to the corner they lie towards), internal children get consecutive
 //     wide indices in slot order, leaf triangles consecutive soup slots;
@@ -72,6 +74,25 @@ __device__ __forceinline__ bool make_child(const float4* nodes, uint32_t num_nod
     return true;
 }
 
+// The box of triangles [c.first, c.first + c.count) (leaf order): the union
+// of their padded bounds, as the binary tree's own leaf boxes are made.
+__device__ __forceinline__ void range_box(const GpuTriangle* __restrict__ tris, const float4* __restrict__ pos,
+                                          Child& c) {
+    for (int a = 0; a < 3; ++a) {
+        c.lo[a] = INFINITY;
+        c.hi[a] = -INFINITY;
+    }
+    for (uint32_t i = c.first; i < c.first + c.count; ++i) {
+        const GpuTriangle t = tris[i];
+        float lo[3], hi[3];
+        padded_tri_box(pos[t.i0], pos[t.i1], pos[t.i2], lo, hi);
+        for (int a = 0; a < 3; ++a) {
+            c.lo[a] = fminf(c.lo[a], lo[a]);
+            c.hi[a] = fmaxf(c.hi[a], hi[a]);
+        }
+    }
+}
+
 __device__ __forceinline__ float half_area(const Child& c) {
     float dx = c.hi[0] - c.lo[0], dy = c.hi[1] - c.lo[1], dz = c.hi[2] - c.lo[2];
     return dx * dy + dy * dz + dz * dx;
@@ -108,7 +129,8 @@ __global__ void k_wide_advance(uint32_t* __restrict__ ctr) {
 
 __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ nodes, uint32_t num_nodes,
                                                     const float4* __restrict__ soup, uint32_t num_tris,
-                                                    uint4* __restrict__ tasks, float4* __restrict__ wnodes,
+                                                    const GpuTriangle* __restrict__ tri_idx,
+                                                    const float4* __restrict__ tri_pos, uint4* __restrict__ tasks, float4* __restrict__ wnodes,
                                                     float4* __restrict__ wsoup, uint32_t cap,
                                                     uint32_t* __restrict__ ctr) {
     if (ctr[kWcErr]) return;  // a failed level ends the build
@@ -153,6 +175,31 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
                 ch[best] = l;
                 ch[n++] = r;
             }
+            // Slots still free: split leaf slots, largest first, into the two
+            // halves of their triangle range, each with its own box, so a ray
+            // that reaches them tests fewer triangles (the binary tree's
+            // leaves hold up to 4 triangles under one box).
+            while (ok && n < 8) {
+                int best = -1;
+                float best_a = -1.0f;
+                for (uint32_t k = 0; k < n; ++k) {
+                    if (ch[k].kind != 2u || ch[k].count < 2u) continue;
+                    const float a = half_area(ch[k]);
+                    if (a > best_a) {
+                        best = (int)k;
+                        best_a = a;
+                    }
+                }
+                if (best < 0) break;
+                Child l = ch[best], r = ch[best];
+                l.count = (ch[best].count + 1u) / 2u;
+                r.first = l.first + l.count;
+                r.count = ch[best].count - l.count;
+                range_box(tri_idx, tri_pos, l);
+                range_box(tri_idx, tri_pos, r);
+                ch[best] = l;
+                ch[n++] = r;
+            }
         } else {
             // Leaf chunk: up to 7 (or 8, for the last) slots of 4 triangles,
             // every slot with the binary leaf's box; the rest chains on.
@@ -161,11 +208,11 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
             uint32_t first = task.y, rem = task.z;
             const uint32_t here = rem <= kNodeTris ? rem : kChunkTris;
             for (uint32_t k = 0; k < here; k += kSmallLeaf) {
-                ch[n] = box;
                 ch[n].node = task.x;
                 ch[n].first = first + k;
                 ch[n].count = min(kSmallLeaf, here - k);
                 ch[n].kind = 2u;
+                range_box(tri_idx, tri_pos, ch[n]);  // each slot's own triangles
                 ++n;
             }
             if (rem > here) {
@@ -361,6 +408,7 @@ int32_t luc_build_wide_roots(luc_ctx* c, const uint32_t* roots, uint32_t nroots,
     for (int level = 0; level < kMaxLevels; level += kLevelsPerSync) {
         for (int k = 0; k < kLevelsPerSync; ++k) {
             k_wide_level<<<grid, 128, 0, s>>>(c->nodes.as<float4>(), num_nodes, c->soup.as<float4>(), num_tris,
+                                              c->tris.as<GpuTriangle>(), c->positions.as<float4>(),
                                               c->wtasks.as<uint4>(), c->wnodes.as<float4>(), c->wsoup.as<float4>(),
                                               (uint32_t)cap, ctr);
             k_wide_advance<<<1, 1, 0, s>>>(ctr);
