@@ -11,8 +11,9 @@
 //   * an internal task opens children greedily, largest surface area first,
 //     until it has 8 children or none can be opened (a leaf with <= 4
 //     triangles stays a leaf slot, and a node holds at most 32 triangles);
-//     slots still free then take halves of its largest leaf slots, each
-//     with the box of its own triangles;
+//     leaf slots of 2+ triangles compete for the free slots by area too,
+//     splitting into the two subsets of least area x triangles, each under
+//     the box of its own triangles;
 //   * children are placed in slots by octant (greedy assignment of children
 //     to the corner they lie towards), internal children get consecutive
 //     wide indices in slot order, leaf triangles consecutive soup slots;
@@ -35,6 +36,11 @@ namespace {
 constexpr uint32_t kSmallLeaf = 4;   // leaves up to this size are leaf slots
 constexpr uint32_t kChunkTris = 28;  // triangles per leaf chunk node before chaining
 constexpr uint32_t kNodeTris = 32;   // triangle budget of one wide node
+// Priority of splitting a leaf slot against opening an internal child of the
+// same area: the displaced-sphere frame ran 324 / 335 / 341 / 341 / 340
+// Mpaths/s at weights 1 / 2 / 4 / 8 / 16 (3.96 triangle tests and 14.2 node
+// visits per closest-hit ray at 4).
+constexpr float kLeafSplitWeight = 4.0f;
 constexpr uint32_t kKindInternal = 0, kKindChunk = 1;
 
 // ctr words
@@ -46,6 +52,7 @@ struct Child {
     uint32_t node;   // binary node index (box source)
     uint32_t first, count;
     uint32_t kind;   // 0 internal binary node, 1 chunk (internal wide child), 2 leaf slot
+    uint32_t sub;    // leaf slot: its triangles, bit i = triangle first + i (count = popc)
 };
 
 __device__ __forceinline__ void node_box(const float4* nodes, uint32_t i, Child& c) {
@@ -71,26 +78,71 @@ __device__ __forceinline__ bool make_child(const float4* nodes, uint32_t num_nod
     c.first = lf;
     c.count = cnt;
     c.kind = cnt <= kSmallLeaf ? 2u : kKindChunk;
+    c.sub = cnt <= kSmallLeaf ? (1u << cnt) - 1u : 0u;
     return true;
 }
 
-// The box of triangles [c.first, c.first + c.count) (leaf order): the union
-// of their padded bounds, as the binary tree's own leaf boxes are made.
-__device__ __forceinline__ void range_box(const GpuTriangle* __restrict__ tris, const float4* __restrict__ pos,
-                                          Child& c) {
+// Leaf slots hold up to 4 triangles of one binary leaf (a subset `sub` of
+// [first, first + 4), leaf order), under the union of their padded bounds,
+// as the binary tree's own leaf boxes are made.
+__device__ __forceinline__ float box_half_area(const float lo[3], const float hi[3]) {
+    const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+struct LeafBoxes {
+    float lo[kSmallLeaf][3], hi[kSmallLeaf][3];
+};
+__device__ __forceinline__ void leaf_boxes(const GpuTriangle* __restrict__ tris, const float4* __restrict__ pos,
+                                           const Child& c, LeafBoxes& b) {
+    for (uint32_t i = 0; i < kSmallLeaf; ++i)
+        if (c.sub >> i & 1u) {
+            const GpuTriangle t = tris[c.first + i];
+            padded_tri_box(pos[t.i0], pos[t.i1], pos[t.i2], b.lo[i], b.hi[i]);
+        }
+}
+__device__ __forceinline__ void subset_box(const LeafBoxes& b, uint32_t sub, float lo[3], float hi[3]) {
     for (int a = 0; a < 3; ++a) {
-        c.lo[a] = INFINITY;
-        c.hi[a] = -INFINITY;
+        lo[a] = INFINITY;
+        hi[a] = -INFINITY;
     }
-    for (uint32_t i = c.first; i < c.first + c.count; ++i) {
-        const GpuTriangle t = tris[i];
+    for (uint32_t i = 0; i < kSmallLeaf; ++i)
+        if (sub >> i & 1u)
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = fminf(lo[a], b.lo[i][a]);
+                hi[a] = fmaxf(hi[a], b.hi[i][a]);
+            }
+}
+// Split leaf slot c (2 or more triangles) into the two subsets with the
+// least surface-area cost (area x triangles, summed); l and r get their
+// boxes.
+__device__ __forceinline__ void split_leaf(const GpuTriangle* __restrict__ tris, const float4* __restrict__ pos,
+                                           const Child& c, Child& l, Child& r) {
+    LeafBoxes b;
+    leaf_boxes(tris, pos, c, b);
+    const uint32_t low = c.sub & (0u - c.sub);
+    float best = INFINITY;
+    uint32_t best_s = low;
+    // Subsets holding the lowest triangle, short of all of them.
+    for (uint32_t sset = c.sub; sset; sset = (sset - 1u) & c.sub) {
+        if (!(sset & low) || sset == c.sub) continue;
         float lo[3], hi[3];
-        padded_tri_box(pos[t.i0], pos[t.i1], pos[t.i2], lo, hi);
-        for (int a = 0; a < 3; ++a) {
-            c.lo[a] = fminf(c.lo[a], lo[a]);
-            c.hi[a] = fmaxf(c.hi[a], hi[a]);
+        subset_box(b, sset, lo, hi);
+        float cost = box_half_area(lo, hi) * (float)__popc(sset);
+        subset_box(b, c.sub ^ sset, lo, hi);
+        cost += box_half_area(lo, hi) * (float)__popc(c.sub ^ sset);
+        if (cost < best) {
+            best = cost;
+            best_s = sset;
         }
     }
+    l = c;
+    r = c;
+    l.sub = best_s;
+    r.sub = c.sub ^ best_s;
+    l.count = __popc(l.sub);
+    r.count = __popc(r.sub);
+    subset_box(b, l.sub, l.lo, l.hi);
+    subset_box(b, r.sub, r.lo, r.hi);
 }
 
 __device__ __forceinline__ float half_area(const Child& c) {
@@ -146,11 +198,23 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
                  make_child(nodes, num_nodes, num_tris, task.y + 1u, ch[1]);
             n = 2;
             uint32_t tris = (ch[0].kind == 2u ? ch[0].count : 0u) + (ch[1].kind == 2u ? ch[1].count : 0u);
-            // Open the largest internal child while the node has room.
+            // Open the largest child while the node has room: an internal
+            // child into its two children, a leaf slot of 2+ triangles into
+            // two slots of fewer triangles under their own boxes (the binary
+            // tree's leaves hold up to 4 triangles under one box); leaf
+            // areas count kLeafSplitWeight times.
             while (ok && n < 8) {
                 int best = -1;
                 float best_a = -1.0f;
                 for (uint32_t k = 0; k < n; ++k) {
+                    if (ch[k].kind == 2u) {
+                        const float a = ch[k].count >= 2u ? half_area(ch[k]) * kLeafSplitWeight : -1.0f;
+                        if (a > best_a) {
+                            best = (int)k;
+                            best_a = a;
+                        }
+                        continue;
+                    }
                     if (ch[k].kind != kKindInternal) continue;
                     float a = half_area(ch[k]);
                     if (a > best_a) {
@@ -168,35 +232,17 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
                     }
                 }
                 if (!ok || best < 0) break;
+                if (ch[best].kind == 2u) {
+                    Child l, r;
+                    split_leaf(tri_idx, tri_pos, ch[best], l, r);
+                    ch[best] = l;
+                    ch[n++] = r;
+                    continue;
+                }
                 Child l, r;
                 make_child(nodes, num_nodes, num_tris, ch[best].first, l);
                 make_child(nodes, num_nodes, num_tris, ch[best].first + 1u, r);
                 tris += (l.kind == 2u ? l.count : 0u) + (r.kind == 2u ? r.count : 0u);
-                ch[best] = l;
-                ch[n++] = r;
-            }
-            // Slots still free: split leaf slots, largest first, into the two
-            // halves of their triangle range, each with its own box, so a ray
-            // that reaches them tests fewer triangles (the binary tree's
-            // leaves hold up to 4 triangles under one box).
-            while (ok && n < 8) {
-                int best = -1;
-                float best_a = -1.0f;
-                for (uint32_t k = 0; k < n; ++k) {
-                    if (ch[k].kind != 2u || ch[k].count < 2u) continue;
-                    const float a = half_area(ch[k]);
-                    if (a > best_a) {
-                        best = (int)k;
-                        best_a = a;
-                    }
-                }
-                if (best < 0) break;
-                Child l = ch[best], r = ch[best];
-                l.count = (ch[best].count + 1u) / 2u;
-                r.first = l.first + l.count;
-                r.count = ch[best].count - l.count;
-                range_box(tri_idx, tri_pos, l);
-                range_box(tri_idx, tri_pos, r);
                 ch[best] = l;
                 ch[n++] = r;
             }
@@ -212,7 +258,10 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
                 ch[n].first = first + k;
                 ch[n].count = min(kSmallLeaf, here - k);
                 ch[n].kind = 2u;
-                range_box(tri_idx, tri_pos, ch[n]);  // each slot's own triangles
+                ch[n].sub = (1u << ch[n].count) - 1u;
+                LeafBoxes lb;  // each slot under its own triangles' box
+                leaf_boxes(tri_idx, tri_pos, ch[n], lb);
+                subset_box(lb, ch[n].sub, ch[n].lo, ch[n].hi);
                 ++n;
             }
             if (rem > here) {
@@ -337,10 +386,12 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
                 }
                 if (ch[k].kind == 2u) {
                     cntmask |= ((1u << ch[k].count) - 1u) << (4 * s);  // nibble s: the slot's triangles
-                    for (uint32_t i = 0; i < ch[k].count; ++i) {
-                        const size_t src = 3 * (size_t)(ch[k].first + i), dst = 3 * (size_t)(tbase + off + i);
+                    uint32_t i = 0;
+                    for (uint32_t bits = ch[k].sub; bits; bits &= bits - 1u, ++i) {
+                        const uint32_t t = ch[k].first + (uint32_t)(__ffs(bits) - 1);
+                        const size_t src = 3 * (size_t)t, dst = 3 * (size_t)(tbase + off + i);
                         float4 q0 = soup[src];
-                        q0.w = __uint_as_float(ch[k].first + i);
+                        q0.w = __uint_as_float(t);
                         wsoup[dst] = q0;
                         wsoup[dst + 1] = soup[src + 1];
                         wsoup[dst + 2] = soup[src + 2];
