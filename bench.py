@@ -49,8 +49,8 @@ BINARY_BYTES = (32, 48)
 RAY_IO_BYTES = 52
 # DRAM bytes (read + write) per EXTEND ray on the wide tree, from an ncu
 # capture of every EXTEND launch of a 512x512x4-spp frame of the same scene
-# (500.1 MB over 2,862,333 rays); scaled by the rays of a launch.
-EXTEND_DRAM_BYTES_PER_RAY = 174.7
+# (514.4 MB over 2,862,333 rays); scaled by the rays of a launch.
+EXTEND_DRAM_BYTES_PER_RAY = 179.7
 
 
 def parse():
