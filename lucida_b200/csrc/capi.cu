@@ -171,6 +171,9 @@ void luc_destroy(luc_ctx* c) {
     for (DevBuf* b : bufs) b->release();
     if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
     c->graph.timer.release();
+    if (c->side_stream) cudaStreamDestroy(c->side_stream);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -600,7 +603,18 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
         c->rs.ps.rec = c->g_rec.as<float4>();
         c->rs.ps.gmisc = c->g_misc.as<uint32_t>();
     }
-    const GuideTrain gt = guided ? luc_guide_train_state(c) : GuideTrain{};
+    GuideTrain gt = guided ? luc_guide_train_state(c) : GuideTrain{};
+    // A guided, trained, single-batch graph frame leaves its gradient step
+    // to the start of the next guided frame, where it runs beside GENERATE
+    // and the first EXTEND (which read neither the records nor the guide);
+    // every other render, and every guide call, runs a pending step first.
+    const bool one_batch = per_batch >= spp;
+    const bool defer = guided && gt.train && c->guide_rec_cap && one_batch && c->use_graphs && !mega &&
+                       !(flags & LUC_FLAG_PROFILE);
+    if (!defer || !c->guide_pending)
+        if (int32_t rc2 = luc_guide_flush(c)) return rc2;
+    const bool pending = defer && c->guide_pending;
+    gt.defer = defer;
 
     LUC_CUDA(c, c->frame_word.ensure(256), "allocate frame word");
     FrameParams fp{};
@@ -636,7 +650,6 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     cudaEventCreate(&e1);
     cudaMemsetAsync(c->rs.ps.stat, 0, 8 * sizeof(unsigned long long), s);
     cudaEventRecord(e0, s);
-    const bool one_batch = per_batch >= spp;
     if (mega) {
         // Batches of whole samples through the same pool as the wavefront:
         // one launch walks every path of the batch, then RESOLVE.
@@ -667,7 +680,7 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
         // The scene enters the key through the DevScene bytes (pointers,
         // counts, roots): the kernels read the arrays at run time, so a
         // re-upload into the same buffers replays the graph unchanged.
-        const uint64_t extra[10] = {(uint64_t)(uintptr_t)accum,        0u,
+        const uint64_t extra[10] = {(uint64_t)(uintptr_t)accum,        (uint64_t)pending | (uint64_t)defer << 1,
                                     (uint64_t)(uintptr_t)c->rs.ps.o_pdf, (uint64_t)(tp != nullptr),
                                     (uint64_t)(uintptr_t)c->rs.ps.lobes, (uint64_t)(uintptr_t)c->rs.ps.rec,
                                     (uint64_t)(uintptr_t)c->rs.ps.gmisc, (uint64_t)(uintptr_t)gt.params,
@@ -683,8 +696,28 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
             g.timer.release();
             cudaGraph_t graph = nullptr;
             uint64_t before = c->rs.launches;
+            if (pending && !c->side_stream) {
+                // Highest priority: the step's blocks are placed ahead of
+                // the EXTEND blocks that would otherwise fill every SM.
+                int lo_prio = 0, hi_prio = 0;
+                cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+                LUC_CUDA(c, cudaStreamCreateWithPriority(&c->side_stream, cudaStreamNonBlocking, hi_prio),
+                         "create side stream");
+                LUC_CUDA(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming), "create event");
+                LUC_CUDA(c, cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming), "create event");
+            }
             LUC_CUDA(c, cudaStreamBeginCapture(c->own_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-            record_batch(c->rs, sc, fp, accum, c->own_stream, tp ? &g.timer : nullptr, &gt);
+            GuideTrain gcap = gt;
+            if (pending) {
+                // Fork: the previous frame's step on the side stream.
+                cudaEventRecord(c->ev_fork, c->own_stream);
+                cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0);
+                launch_guide_step(c->rs, c->guide_pending_cap, luc_guide_dev(c), gt, c->side_stream);
+                cudaEventRecord(c->ev_join, c->side_stream);
+                gcap.join = c->ev_join;
+                c->rs.launches += 3;
+            }
+            record_batch(c->rs, sc, fp, accum, c->own_stream, tp ? &g.timer : nullptr, &gcap);
             LUC_CUDA(c, cudaStreamEndCapture(c->own_stream, &graph), "end capture");
             cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
             cudaGraphDestroy(graph);
@@ -700,6 +733,10 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
         LUC_CUDA(c, cudaGraphLaunch(g.exec, s), "launch frame graph");
         c->rs.launches += g.launches;
         c->stats.paths += fp.num_paths;
+        if (defer) {
+            c->guide_pending = true;
+            c->guide_pending_cap = fp.rec_cap;
+        }
     } else {
         for (uint32_t done = 0; done < spp;) {
             uint32_t n = (uint32_t)std::min<uint64_t>(per_batch, spp - done);

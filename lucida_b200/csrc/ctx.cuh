@@ -85,6 +85,12 @@ struct luc_ctx {
     DevBuf g_params, g_m, g_v, g_grad, g_wbf, g_bias, g_misc, g_lobes, g_rec, g_io;
     bool guide_ready = false, guide_train = true;
     uint32_t guide_rec_cap = 1u << 18;
+    // The last guided frame's gradient step, not yet run (its records' cap),
+    // and the stream and events that run it beside the next frame's start.
+    bool guide_pending = false;
+    uint32_t guide_pending_cap = 0;
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     float guide_lr = 1.0e-2f;
     float guide_lo[3] = {0, 0, 0}, guide_hi[3] = {1, 1, 1};
     // Bounds of the uploaded scene (vertices and analytic primitives).
@@ -153,6 +159,7 @@ int32_t luc_build_blases(luc_ctx* c, const uint32_t* first, const uint32_t* coun
 luc::GuideDev luc_guide_dev(const luc_ctx* c);
 luc::GuideTrain luc_guide_train_state(luc_ctx* c);
 int32_t luc_guide_prepare_frame(luc_ctx* c, uint64_t paths);
+int32_t luc_guide_flush(luc_ctx* c);
 // wavefront.cu: fill the Sobol byte tables on the current device.
 cudaError_t luc_init_sobol_tables(cudaStream_t s);
 // capi.cu: grow the path pool to `paths` paths and `max_depth` bounces.

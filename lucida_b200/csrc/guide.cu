@@ -750,14 +750,21 @@ void launch_guide_infer(const RenderState& rs, const DevScene& sc, const FramePa
     else k_guide_infer<<<rs.num_sms * g_infer_blocks, kInferWarps * 32, sizeof(InferSmem), s>>>(rs.ps, sc, fp, depth);
 }
 
-void launch_guide_train(const RenderState& rs, const FrameParams& fp, const GuideTrain& gt, cudaStream_t s) {
-    cudaMemsetAsync(gt.grad, 0, kGParams * sizeof(float), s);
+void launch_guide_finalize(const RenderState& rs, const FrameParams& fp, cudaStream_t s) {
     cudaMemsetAsync(rs.ps.gmisc + kGmWeightSum, 0, 2 * sizeof(uint32_t), s);  // weight sum, loss
     k_guide_finalize<<<rs.num_sms * 4, 256, 0, s>>>(rs.ps, fp.rec_cap);
-    k_guide_train<<<rs.num_sms, kGuideThreads, sizeof(TrainSmem), s>>>(rs.ps.rec, fp.rec_cap, rs.ps.gmisc, fp.guide,
-                                                                         gt.grad);
+}
+
+void launch_guide_step(const RenderState& rs, uint32_t cap, const GuideDev& g, const GuideTrain& gt, cudaStream_t s) {
+    cudaMemsetAsync(gt.grad, 0, kGParams * sizeof(float), s);
+    k_guide_train<<<rs.num_sms, kGuideThreads, sizeof(TrainSmem), s>>>(rs.ps.rec, cap, rs.ps.gmisc, g, gt.grad);
     k_guide_adam<<<(kGParams + 255) / 256, 256, 0, s>>>(gt.params, gt.m, gt.v, gt.grad, rs.ps.gmisc, gt.lr);
-    k_guide_pack<<<(kGBf16 + 255) / 256, 256, 0, s>>>(gt.params, gt.wbf, gt.bias, rs.ps.gmisc, fp.rec_cap, 1u);
+    k_guide_pack<<<(kGBf16 + 255) / 256, 256, 0, s>>>(gt.params, gt.wbf, gt.bias, rs.ps.gmisc, cap, 1u);
+}
+
+void launch_guide_train(const RenderState& rs, const FrameParams& fp, const GuideTrain& gt, cudaStream_t s) {
+    launch_guide_finalize(rs, fp, s);
+    launch_guide_step(rs, fp.rec_cap, fp.guide, gt, s);
 }
 
 }  // namespace luc
@@ -792,6 +799,17 @@ GuideTrain luc_guide_train_state(luc_ctx* c) {
     gt.lr = c->guide_lr;
     gt.train = c->guide_train;
     return gt;
+}
+
+// A gradient step left pending by a guided frame (GuideTrain::defer) runs
+// now, on the context's stream, before anything reads or changes the guide.
+int32_t luc_guide_flush(luc_ctx* c) {
+    if (!c->guide_pending) return LUC_OK;
+    c->guide_pending = false;
+    cudaSetDevice(c->device);
+    launch_guide_step(c->rs, c->guide_pending_cap, luc_guide_dev(c), luc_guide_train_state(c), c->stream);
+    LUC_CUDA(c, cudaGetLastError(), "guide step");
+    return LUC_OK;
 }
 
 int32_t luc_guide_prepare_frame(luc_ctx* c, uint64_t paths) {
@@ -839,6 +857,7 @@ int32_t luc_guide_init(luc_ctx* c, const float* params, uint64_t seed, const flo
     for (float x : p)
         if (!std::isfinite(x)) return luc_fail(c, LUC_ERR_VALIDATION, "guide parameters must be finite");
     cudaStream_t s = c->stream;
+    c->guide_pending = false;  // a step of the guide being replaced
     LUC_CUDA(c, c->g_params.ensure(kGParams * sizeof(float)), "allocate guide");
     LUC_CUDA(c, c->g_m.ensure(kGParams * sizeof(float)), "allocate guide");
     LUC_CUDA(c, c->g_v.ensure(kGParams * sizeof(float)), "allocate guide");
@@ -866,6 +885,7 @@ int32_t luc_guide_configure(luc_ctx* c, uint32_t train, uint32_t records_per_ste
     if (records_per_step == 0 || records_per_step > (1u << 24))
         return luc_fail(c, LUC_ERR_VALIDATION, "records_per_step must be in 1..=2^24");
     if (!(lr > 0.0f) || !std::isfinite(lr)) return luc_fail(c, LUC_ERR_VALIDATION, "lr must be positive and finite");
+    if (int32_t rc = luc_guide_flush(c)) return rc;  // with the settings it was recorded under
     c->guide_train = train != 0;
     c->guide_rec_cap = records_per_step;
     c->guide_lr = lr;
@@ -875,6 +895,7 @@ int32_t luc_guide_configure(luc_ctx* c, uint32_t train, uint32_t records_per_ste
 int32_t luc_guide_get_params(luc_ctx* c, float* out) {
     if (!c || !out) return LUC_ERR_VALIDATION;
     if (int32_t rc = require_guide(c)) return rc;
+    if (int32_t rc = luc_guide_flush(c)) return rc;
     cudaSetDevice(c->device);
     LUC_CUDA(c, cudaMemcpyAsync(out, c->g_params.p, kGParams * sizeof(float), cudaMemcpyDeviceToHost, c->stream),
              "read guide");
@@ -885,6 +906,7 @@ int32_t luc_guide_get_params(luc_ctx* c, float* out) {
 int32_t luc_guide_stats(luc_ctx* c, luc_guide_info* out) {
     if (!c || !out) return LUC_ERR_VALIDATION;
     if (int32_t rc = require_guide(c)) return rc;
+    if (int32_t rc = luc_guide_flush(c)) return rc;
     cudaSetDevice(c->device);
     uint32_t misc[kGmWords];
     LUC_CUDA(c, cudaMemcpyAsync(misc, c->g_misc.p, sizeof(misc), cudaMemcpyDeviceToHost, c->stream), "read guide");
@@ -902,6 +924,7 @@ int32_t luc_guide_forward_ex(luc_ctx* c, const float* in9, uint32_t n, int32_t p
     if (!c || (n && (!in9 || !out40))) return LUC_ERR_VALIDATION;
     if (path != 0 && path != 1) return luc_fail(c, LUC_ERR_VALIDATION, "path: 0 tcgen05, 1 mma.sync");
     if (int32_t rc = require_guide(c)) return rc;
+    if (int32_t rc = luc_guide_flush(c)) return rc;
     if (n == 0) return LUC_OK;
     cudaSetDevice(c->device);
     cudaStream_t s = c->stream;
@@ -934,6 +957,7 @@ int32_t luc_guide_train_records(luc_ctx* c, const float* records, uint32_t n, ui
                                 float* loss_out) {
     if (!c || (n && !records)) return LUC_ERR_VALIDATION;
     if (int32_t rc = require_guide(c)) return rc;
+    if (int32_t rc = luc_guide_flush(c)) return rc;
     if (n == 0) return luc_fail(c, LUC_ERR_VALIDATION, "no records");
     cudaSetDevice(c->device);
     cudaStream_t s = c->stream;

@@ -140,6 +140,12 @@ struct GuideTrain {
     float* bias;
     float lr;
     bool train;
+    // defer: the batch ends after k_guide_finalize; its gradient step runs
+    // at the start of the next guided frame, beside GENERATE and the first
+    // EXTEND. join: the event such a step records; the frame waits for it
+    // after its first EXTEND (before any guide inference or SHADE).
+    bool defer = false;
+    cudaEvent_t join = nullptr;
 };
 
 void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream,
@@ -161,5 +167,9 @@ int batch_blocks_per_sm(int block, bool connect, bool wide);
 void launch_guide_infer(const RenderState& rs, const DevScene& sc, const FrameParams& fp, uint32_t depth,
                         cudaStream_t s);
 void launch_guide_train(const RenderState& rs, const FrameParams& fp, const GuideTrain& gt, cudaStream_t s);
+// The two halves of launch_guide_train: record weights (needs the batch's
+// path pool) and the gradient step on them (records and guide state only).
+void launch_guide_finalize(const RenderState& rs, const FrameParams& fp, cudaStream_t s);
+void launch_guide_step(const RenderState& rs, uint32_t cap, const GuideDev& g, const GuideTrain& gt, cudaStream_t s);
 
 }  // namespace luc

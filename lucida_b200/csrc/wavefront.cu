@@ -560,6 +560,7 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
             k_extend_dyn<128, kExtendRefill><<<sms * rs.extend_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
         else
             k_extend<false, false, 128, 0><<<sms * rs.extend_blocks_bin, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
+        if (d == 0 && gt && gt->join) cudaStreamWaitEvent(stream, gt->join, 0);  // the previous frame's step
         if (fp.guided && d + 1 < fp.max_depth) {
             if (timer) timer->mark(stream, StageTimer::kGuide);
             launch_guide_infer(rs, sc, fp, d, stream);
@@ -590,13 +591,19 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
             rs.launches++;
         }
     }
+    if (fp.max_depth == 0 && gt && gt->join) cudaStreamWaitEvent(stream, gt->join, 0);
     if (timer) timer->mark(stream, StageTimer::kResolve);
     k_resolve<<<sms * 8, 256, 0, stream>>>(rs.ps, fp, accum);
     rs.launches++;
     if (fp.guided && fp.rec_cap && gt && gt->train) {
         if (timer) timer->mark(stream, StageTimer::kTrain);
-        launch_guide_train(rs, fp, *gt, stream);
-        rs.launches += 4;
+        if (gt->defer) {
+            launch_guide_finalize(rs, fp, stream);
+            rs.launches += 1;
+        } else {
+            launch_guide_train(rs, fp, *gt, stream);
+            rs.launches += 4;
+        }
     }
     if (timer) timer->mark(stream, StageTimer::kEnd);
 }
