@@ -174,6 +174,8 @@ void luc_destroy(luc_ctx* c) {
     if (c->side_stream) cudaStreamDestroy(c->side_stream);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->ev_ready) cudaEventDestroy(c->ev_ready);
+    if (c->ev_done) cudaEventDestroy(c->ev_done);
     cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -696,7 +698,10 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
             g.timer.release();
             cudaGraph_t graph = nullptr;
             uint64_t before = c->rs.launches;
-            if (pending && !c->side_stream) {
+            // Unprofiled frames run each CONNECT on the side stream, beside
+            // the next EXTEND (stage timers need the stages in sequence).
+            const bool overlap = tp == nullptr;
+            if ((pending || overlap) && !c->side_stream) {
                 // Highest priority: the step's blocks are placed ahead of
                 // the EXTEND blocks that would otherwise fill every SM.
                 int lo_prio = 0, hi_prio = 0;
@@ -705,7 +710,10 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
                          "create side stream");
                 LUC_CUDA(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming), "create event");
                 LUC_CUDA(c, cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming), "create event");
+                LUC_CUDA(c, cudaEventCreateWithFlags(&c->ev_ready, cudaEventDisableTiming), "create event");
+                LUC_CUDA(c, cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming), "create event");
             }
+            const ConnectOverlap ov{c->side_stream, c->ev_ready, c->ev_done};
             LUC_CUDA(c, cudaStreamBeginCapture(c->own_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
             GuideTrain gcap = gt;
             if (pending) {
@@ -717,7 +725,7 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
                 gcap.join = c->ev_join;
                 c->rs.launches += 3;
             }
-            record_batch(c->rs, sc, fp, accum, c->own_stream, tp ? &g.timer : nullptr, &gcap);
+            record_batch(c->rs, sc, fp, accum, c->own_stream, tp ? &g.timer : nullptr, &gcap, overlap ? &ov : nullptr);
             LUC_CUDA(c, cudaStreamEndCapture(c->own_stream, &graph), "end capture");
             cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
             cudaGraphDestroy(graph);

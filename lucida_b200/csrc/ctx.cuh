@@ -91,6 +91,7 @@ struct luc_ctx {
     uint32_t guide_pending_cap = 0;
     cudaStream_t side_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_ready = nullptr, ev_done = nullptr;  // CONNECT beside the next EXTEND
     float guide_lr = 1.0e-2f;
     float guide_lo[3] = {0, 0, 0}, guide_hi[3] = {1, 1, 1};
     // Bounds of the uploaded scene (vertices and analytic primitives).

@@ -148,8 +148,16 @@ struct GuideTrain {
     cudaEvent_t join = nullptr;
 };
 
+// CONNECT on a second stream: CONNECT(d) runs beside EXTEND(d+1) and its
+// guide inference; the frame waits for it before SHADE(d+1), which rewrites
+// the shadow-ray buffers and the path radiance CONNECT adds to, and before
+// RESOLVE.
+struct ConnectOverlap {
+    cudaStream_t side;
+    cudaEvent_t ready, done;
+};
 void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream,
-                  StageTimer* timer, const GuideTrain* gt);
+                  StageTimer* timer, const GuideTrain* gt, const ConnectOverlap* ov = nullptr);
 // megakernel.cu: one batch of the megakernel architecture (every path of
 // fp.num_paths from start to end in one launch, then RESOLVE).
 void record_megakernel(const RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum,

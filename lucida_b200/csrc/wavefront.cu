@@ -537,9 +537,14 @@ void query_occupancy(RenderState& rs) {
 // Host side: record one batch of the frame on `stream` (graph-capturable:
 // fixed launch shapes, device-resident lengths).
 void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream,
-                  StageTimer* timer, const GuideTrain* gt) {
+                  StageTimer* timer, const GuideTrain* gt, const ConnectOverlap* ov) {
     const int sms = rs.num_sms;
     const uint32_t stride_ctr = kCtrStride * (fp.max_depth + 2);
+    bool connect_out = false;  // a CONNECT on ov->side not yet waited for
+    auto join_connect = [&]() {
+        if (connect_out) cudaStreamWaitEvent(stream, ov->done, 0);
+        connect_out = false;
+    };
     cudaMemsetAsync(rs.ps.ctr, 0, stride_ctr * sizeof(uint32_t), stream);
     if (timer) timer->mark(stream, StageTimer::kGenerate);
     {
@@ -566,6 +571,7 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
             launch_guide_infer(rs, sc, fp, d, stream);
             rs.launches++;
         }
+        join_connect();
         if (timer) timer->mark(stream, StageTimer::kShade);
         if (fp.guided && inst)
             k_shade<true, true><<<sms * rs.shade_blocks_guided_inst, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
@@ -579,19 +585,30 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
         if (d + 1 < fp.max_depth && (fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) &&
             sc.light_strategies > 0) {
             if (timer) timer->mark(stream, StageTimer::kConnect);
+            cudaStream_t cs = stream;
+            if (ov) {
+                cudaEventRecord(ov->ready, stream);
+                cudaStreamWaitEvent(ov->side, ov->ready, 0);
+                cs = ov->side;
+            }
             // Two-level shadow rays walk the binary BLASes: measured faster
             // than the wide ones for any-hit (C5: 133 against 153 ms / frame).
             if (inst)
-                k_connect<true, false, 128, 0><<<sms * rs.connect_blocks_inst_bin, 128, 0, stream>>>(rs.ps, sc,
-                                                                                                     BatchDev{}, d);
+                k_connect<true, false, 128, 0><<<sms * rs.connect_blocks_inst_bin, 128, 0, cs>>>(rs.ps, sc,
+                                                                                                 BatchDev{}, d);
             else if (wide)
-                k_connect<false, false, 128, 1><<<sms * rs.connect_blocks, 128, 0, stream>>>(rs.ps, sc, BatchDev{}, d);
+                k_connect<false, false, 128, 1><<<sms * rs.connect_blocks, 128, 0, cs>>>(rs.ps, sc, BatchDev{}, d);
             else
-                k_connect<false, false, 128, 0><<<sms * rs.connect_blocks_bin, 128, 0, stream>>>(rs.ps, sc, BatchDev{}, d);
+                k_connect<false, false, 128, 0><<<sms * rs.connect_blocks_bin, 128, 0, cs>>>(rs.ps, sc, BatchDev{}, d);
             rs.launches++;
+            if (ov) {
+                cudaEventRecord(ov->done, ov->side);
+                connect_out = true;
+            }
         }
     }
     if (fp.max_depth == 0 && gt && gt->join) cudaStreamWaitEvent(stream, gt->join, 0);
+    join_connect();
     if (timer) timer->mark(stream, StageTimer::kResolve);
     k_resolve<<<sms * 8, 256, 0, stream>>>(rs.ps, fp, accum);
     rs.launches++;
