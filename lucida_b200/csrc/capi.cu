@@ -167,7 +167,8 @@ void luc_destroy(luc_ctx* c) {
                       &c->lb_nbounds, &c->lb_subtree, &c->lb_flags, &c->lb_nodes, &c->lb_rank, &c->lb_misc,
                       &c->lb_icount, &c->lb_look, &c->lb_codes, &c->dn_in,  &c->dn_out,    &c->dn_a,      &c->dn_b,
                       &c->dn_dev,    &c->g_params, &c->g_m,     &c->g_v,       &c->g_grad,    &c->g_wbf,
-                      &c->g_bias,    &c->g_misc,   &c->g_lobes, &c->g_rec,     &c->g_io};
+                      &c->g_bias,    &c->g_misc,   &c->g_lobes, &c->g_rec,     &c->g_io,
+                      &c->g_part};
     for (DevBuf* b : bufs) b->release();
     if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
     c->graph.timer.release();

@@ -82,7 +82,7 @@ struct luc_ctx {
     DevBuf dn_in, dn_out, dn_a, dn_b, dn_dev;
     // Learned guide: FP32 master, Adam moments, gradient, packed weights,
     // bookkeeping words, per-path mixtures, training records, host-call io.
-    DevBuf g_params, g_m, g_v, g_grad, g_wbf, g_bias, g_misc, g_lobes, g_rec, g_io;
+    DevBuf g_params, g_m, g_v, g_grad, g_wbf, g_bias, g_misc, g_lobes, g_rec, g_io, g_part;
     bool guide_ready = false, guide_train = true;
     uint32_t guide_rec_cap = 1u << 18;
     // The last guided frame's gradient step, not yet run (its records' cap),

@@ -332,17 +332,27 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(PathState ps, 
 }
 
 // ---------------------------------------------------------------- training
+// Under 113 KB, so two CTAs (8 warps) share an SM: the weight gradients
+// accumulate in each CTA's slice of a global buffer (kPartFloats per CTA,
+// L2-resident; each warp owns its rows, so plain read-modify-write), and the
+// raw outputs share the input-gradient planes (outputs are dead once the
+// loss epilogue has turned them into dy).
 struct TrainSmem {
     NetSmem net;
-    float dw1[kGHid * kGIn], dw2[kGHid * kGHid], dw3[kGHid * kGHid], dw4[kGOutPad * kGHid];
     float db[kGBias];
     uint16_t x[kTileRows * kSIn];
     uint16_t h[3][kTileRows * kSHid];
     uint16_t dy[kTileRows * kSOut];
-    uint16_t dh[2][kTileRows * kSHid];
-    float o[kTileRows * kGOutPad];
+    union {
+        uint16_t dh[2][kTileRows * kSHid];
+        float o[kTileRows * kGOutPad];
+    };
     float loss;
 };
+static_assert(sizeof(TrainSmem) <= 113 * 1024, "two training CTAs per SM");
+// Per-CTA weight-gradient slice: dW1 | dW2 | dW3 | dW4 (kGOutPad rows).
+constexpr int kPartW1 = 0, kPartW2 = kGHid * kGIn, kPartW3 = kPartW2 + kGHid * kGHid,
+              kPartW4 = kPartW3 + kGHid * kGHid, kPartFloats = kPartW4 + kGOutPad * kGHid;
 
 // dW[m][n] += sum_r G[r][m] H[r][n] over the tile's 64 rows for the 16 output
 // rows m0..m0+15. G is [64][SG] (m contiguous), H is [64][SH]; both operands
@@ -458,22 +468,21 @@ __device__ __forceinline__ float row_loss_grad(const float* __restrict__ o, V3 d
 // One gradient evaluation over the records (count gmisc[kGmRecords], capped
 // at `cap`; normaliser 1 / gmisc[kGmWeightSum]) added into grad (FP32, master
 // layout), and the loss into gmisc[kGmLoss].
-__global__ void __launch_bounds__(kGuideThreads) k_guide_train(const float4* __restrict__ rec, uint32_t cap,
-                                                                uint32_t* __restrict__ gmisc, GuideDev g,
-                                                                float* __restrict__ grad) {
+__global__ void __launch_bounds__(kGuideThreads, 2) k_guide_train(const float4* __restrict__ rec, uint32_t cap,
+                                                                   uint32_t* __restrict__ gmisc, GuideDev g,
+                                                                   float* __restrict__ grad, float* __restrict__ part) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
     const uint32_t n = min(gmisc[kGmRecords], cap);
     const float wsum = u2f(gmisc[kGmWeightSum]);
     const float invS = wsum > 0.0f ? 1.0f / wsum : 0.0f;
+    // This CTA's gradient slice starts at zero, tiles or not (k_guide_fold
+    // sums every slice).
+    float* P = part + (size_t)blockIdx.x * kPartFloats;
+    for (int i = threadIdx.x; i < kPartFloats / 4; i += blockDim.x)
+        reinterpret_cast<float4*>(P)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (blockIdx.x * kTileRows >= n) return;
     load_net(S.net, g.wbf, g.bias);
-    for (int i = threadIdx.x; i < kGHid * kGIn; i += blockDim.x) S.dw1[i] = 0.f;
-    for (int i = threadIdx.x; i < kGHid * kGHid; i += blockDim.x) {
-        S.dw2[i] = 0.f;
-        S.dw3[i] = 0.f;
-    }
-    for (int i = threadIdx.x; i < kGOutPad * kGHid; i += blockDim.x) S.dw4[i] = 0.f;
     for (int i = threadIdx.x; i < kGBias; i += blockDim.x) S.db[i] = 0.f;
     if (threadIdx.x == 0) S.loss = 0.f;
     __syncthreads();
@@ -529,33 +538,25 @@ __global__ void __launch_bounds__(kGuideThreads) k_guide_train(const float4* __r
         }
         __syncthreads();
         // Layer 4: dW4 (48 rows: warps 0..2, 16 each) and dH3.
-        if (warp < 3) acc_weight_grad<kGHid, kSHid, kSOut>(S.dy, S.h[2], S.dw4, warp * 16, lane);
+        if (warp < 3) acc_weight_grad<kGHid, kSHid, kSOut>(S.dy, S.h[2], P + kPartW4, warp * 16, lane);
         input_grad<kGOutPad, kSOut>(S.dy, S.net.w4, S.h[2], S.dh[0], S.db + 2 * kGHid, r0, lane);
         __syncthreads();
-        acc_weight_grad<kGHid, kSHid, kSHid>(S.dh[0], S.h[1], S.dw3, warp * 16, lane);
+        acc_weight_grad<kGHid, kSHid, kSHid>(S.dh[0], S.h[1], P + kPartW3, warp * 16, lane);
         input_grad<kGHid, kSHid>(S.dh[0], S.net.w3, S.h[1], S.dh[1], S.db + kGHid, r0, lane);
         __syncthreads();
-        acc_weight_grad<kGHid, kSHid, kSHid>(S.dh[1], S.h[0], S.dw2, warp * 16, lane);
+        acc_weight_grad<kGHid, kSHid, kSHid>(S.dh[1], S.h[0], P + kPartW2, warp * 16, lane);
         input_grad<kGHid, kSHid>(S.dh[1], S.net.w2, S.h[0], S.dh[0], S.db, r0, lane);
         __syncthreads();
-        acc_weight_grad<kGIn, kSIn, kSHid>(S.dh[0], S.x, S.dw1, warp * 16, lane);
+        acc_weight_grad<kGIn, kSIn, kSHid>(S.dh[0], S.x, P + kPartW1, warp * 16, lane);
         __syncthreads();
     }
-    // Fold this CTA's gradients into the global FP32 gradient.
-    float* gW1 = grad;
-    float* gb1 = gW1 + kGHid * kGIn;
-    float* gW2 = gb1 + kGHid;
-    float* gb2 = gW2 + kGHid * kGHid;
-    float* gW3 = gb2 + kGHid;
-    float* gb3 = gW3 + kGHid * kGHid;
-    float* gW4 = gb3 + kGHid;
-    float* gb4 = gW4 + kGOut * kGHid;
-    for (int i = threadIdx.x; i < kGHid * kGIn; i += blockDim.x) atomicAdd(gW1 + i, S.dw1[i]);
-    for (int i = threadIdx.x; i < kGHid * kGHid; i += blockDim.x) {
-        atomicAdd(gW2 + i, S.dw2[i]);
-        atomicAdd(gW3 + i, S.dw3[i]);
-    }
-    for (int i = threadIdx.x; i < kGOut * kGHid; i += blockDim.x) atomicAdd(gW4 + i, S.dw4[i]);
+    // Bias gradients and loss into the global FP32 gradient (layout W1 b1 W2
+    // b2 W3 b3 W4 b4); the weight gradients stay in this CTA's slice for
+    // k_guide_fold.
+    float* gb1 = grad + kGHid * kGIn;
+    float* gb2 = gb1 + kGHid + kGHid * kGHid;
+    float* gb3 = gb2 + kGHid + kGHid * kGHid;
+    float* gb4 = gb3 + kGHid + kGOut * kGHid;
     for (int i = threadIdx.x; i < kGHid; i += blockDim.x) {
         atomicAdd(gb1 + i, S.db[i]);
         atomicAdd(gb2 + i, S.db[kGHid + i]);
@@ -563,6 +564,40 @@ __global__ void __launch_bounds__(kGuideThreads) k_guide_train(const float4* __r
     }
     for (int i = threadIdx.x; i < kGOut; i += blockDim.x) atomicAdd(gb4 + i, S.db[3 * kGHid + i]);
     if (threadIdx.x == 0) atomicAdd(reinterpret_cast<float*>(gmisc + kGmLoss), S.loss);
+}
+
+// Sum of the CTAs' weight-gradient slices into the FP32 gradient (added to
+// what the training kernel put there: the bias gradients). One thread per
+// weight, slices in CTA order: the sum is deterministic.
+__global__ void k_guide_fold(const float* __restrict__ part, uint32_t nparts, float* __restrict__ grad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kPartFloats) return;
+    int dst;
+    if (i < kPartW2) dst = i;                                        // W1
+    else if (i < kPartW3) dst = kGHid * kGIn + kGHid + (i - kPartW2);  // W2
+    else if (i < kPartW4) dst = kGHid * kGIn + 2 * kGHid + kGHid * kGHid + (i - kPartW3);  // W3
+    else if (i - kPartW4 < kGOut * kGHid)
+        dst = kGHid * kGIn + 3 * kGHid + 2 * kGHid * kGHid + (i - kPartW4);  // W4 (padding rows dropped)
+    else return;
+    float s = 0.f;
+    for (uint32_t c = 0; c < nparts; ++c) s += part[(size_t)c * kPartFloats + i];
+    grad[dst] += s;
+}
+
+// The training kernel's grid: one CTA per 64-row tile, at most two per SM.
+uint32_t guide_train_grid(uint32_t cap, int num_sms) {
+    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((cap + kTileRows - 1) / kTileRows, 2ull * num_sms));
+}
+size_t guide_part_bytes(int num_sms) { return (size_t)2 * num_sms * kPartFloats * sizeof(float); }
+
+// One gradient evaluation over records rec[0, min(count, cap)) into grad
+// (zeroed here) and the loss word.
+void launch_guide_gradient(const float4* rec, uint32_t cap, uint32_t* gmisc, const GuideDev& g, float* grad,
+                           float* part, int num_sms, cudaStream_t s) {
+    const uint32_t grid = guide_train_grid(cap, num_sms);
+    cudaMemsetAsync(grad, 0, kGParams * sizeof(float), s);
+    k_guide_train<<<grid, kGuideThreads, sizeof(TrainSmem), s>>>(rec, cap, gmisc, g, grad, part);
+    k_guide_fold<<<(kPartFloats + 255) / 256, 256, 0, s>>>(part, grid, grad);
 }
 
 // Records of a rendered batch: F = luminance of the radiance that arrived
@@ -731,6 +766,9 @@ static cudaError_t guide_kernel_setup(int device) {
         e = cudaFuncSetAttribute(k_guide_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InferSmem));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrainSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_guide_train, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
     if (e == cudaSuccess) e = guide_tc_setup();
     if (e != cudaSuccess) return e;
     int b = 0;
@@ -756,8 +794,7 @@ void launch_guide_finalize(const RenderState& rs, const FrameParams& fp, cudaStr
 }
 
 void launch_guide_step(const RenderState& rs, uint32_t cap, const GuideDev& g, const GuideTrain& gt, cudaStream_t s) {
-    cudaMemsetAsync(gt.grad, 0, kGParams * sizeof(float), s);
-    k_guide_train<<<rs.num_sms, kGuideThreads, sizeof(TrainSmem), s>>>(rs.ps.rec, cap, rs.ps.gmisc, g, gt.grad);
+    launch_guide_gradient(rs.ps.rec, cap, rs.ps.gmisc, g, gt.grad, gt.part, rs.num_sms, s);
     k_guide_adam<<<(kGParams + 255) / 256, 256, 0, s>>>(gt.params, gt.m, gt.v, gt.grad, rs.ps.gmisc, gt.lr);
     k_guide_pack<<<(kGBf16 + 255) / 256, 256, 0, s>>>(gt.params, gt.wbf, gt.bias, rs.ps.gmisc, cap, 1u);
 }
@@ -796,6 +833,7 @@ GuideTrain luc_guide_train_state(luc_ctx* c) {
     gt.grad = c->g_grad.as<float>();
     gt.wbf = c->g_wbf.as<uint16_t>();
     gt.bias = c->g_bias.as<float>();
+    gt.part = c->g_part.as<float>();
     gt.lr = c->guide_lr;
     gt.train = c->guide_train;
     return gt;
@@ -818,6 +856,7 @@ int32_t luc_guide_prepare_frame(luc_ctx* c, uint64_t paths) {
     LUC_CUDA(c, c->g_lobes.ensure(paths * kGLobeF4 * sizeof(float4)), "allocate guide lobes");
     LUC_CUDA(c, c->g_rec.ensure((size_t)std::max<uint32_t>(c->guide_rec_cap, 1) * kGRecF4 * sizeof(float4)),
              "allocate guide records");
+    LUC_CUDA(c, c->g_part.ensure(guide_part_bytes(c->num_sms)), "allocate guide gradient slices");
     return LUC_OK;
 }
 
@@ -967,15 +1006,14 @@ int32_t luc_guide_train_records(luc_ctx* c, const float* records, uint32_t n, ui
              "upload records");
     uint32_t* gm = c->g_misc.as<uint32_t>();
     const uint32_t rounds = steps == 0 ? 1 : steps;
-    const int grid = (int)std::min<uint64_t>((n + kTileRows - 1) / kTileRows, (uint64_t)c->num_sms);
+    LUC_CUDA(c, c->g_part.ensure(guide_part_bytes(c->num_sms)), "allocate guide gradient slices");
     const uint32_t count = n;
     for (uint32_t it = 0; it < rounds; ++it) {
         LUC_CUDA(c, cudaMemcpyAsync(gm + kGmRecords, &count, sizeof(count), cudaMemcpyHostToDevice, s), "upload count");
         LUC_CUDA(c, cudaMemsetAsync(gm + kGmWeightSum, 0, 2 * sizeof(uint32_t), s), "clear sums");
-        LUC_CUDA(c, cudaMemsetAsync(c->g_grad.p, 0, kGParams * sizeof(float), s), "clear gradient");
         k_guide_weight_sum<<<c->num_sms * 2, 256, 0, s>>>(rec, n, gm);
-        k_guide_train<<<grid, kGuideThreads, sizeof(TrainSmem), s>>>(rec, n, gm, luc_guide_dev(c),
-                                                                     c->g_grad.as<float>());
+        launch_guide_gradient(rec, n, gm, luc_guide_dev(c), c->g_grad.as<float>(), c->g_part.as<float>(),
+                              c->num_sms, s);
         if (steps > 0) {
             k_guide_adam<<<(kGParams + 255) / 256, 256, 0, s>>>(c->g_params.as<float>(), c->g_m.as<float>(),
                                                                 c->g_v.as<float>(), c->g_grad.as<float>(), gm,

@@ -138,6 +138,7 @@ struct GuideTrain {
     float *params, *m, *v, *grad;
     uint16_t* wbf;
     float* bias;
+    float* part;  // per-CTA weight-gradient slices of the training kernel
     float lr;
     bool train;
     // defer: the batch ends after k_guide_finalize; its gradient step runs
