@@ -45,11 +45,13 @@ LUC_D void camera_ray(const FrameParams& fp, uint32_t pixel, Sampler& smp, V3& o
 //   void shadow(V3 o, V3 d, float t_max, V3 contribution)   NEE shadow ray
 //   void next(V3 origin, V3 dir, float pdf, V3 thr, V3 hit_position,
 //             V3 hit_normal, bool record, V3 rad)     the path continues
+// kNoLights: the scene has no emitter list (num_lights == 0; the caller
+// checks), so the light-sampling code is compiled out of the vertex.
 // `h4` is the closest-hit record (t, u, v, id bits) and `inst` its instance;
 // `rad` is updated in place (the return value says whether it changed);
 // `lob` / `lobe_stride` locate the path's guide mixture (guided frames). The
 // sampler advances in place.
-template <bool kGuided, bool kInst, typename Sink>
+template <bool kGuided, bool kInst, bool kNoLights = false, typename Sink>
 LUC_D bool shade_vertex(const DevScene& sc, const FrameParams& fp, uint32_t depth, Sampler& smp, V3 org, V3 dir,
                         V3 thr, V3& rad, float prev_pdf, float4 h4, uint32_t inst, const float4* lob,
                         uint32_t lobe_stride, Sink& sink) {
@@ -87,7 +89,7 @@ LUC_D bool shade_vertex(const DevScene& sc, const FrameParams& fp, uint32_t dept
         if (depth == 0 || fp.sampling == LUC_SAMPLING_BSDF) weight = 1.0f;
         else if (fp.sampling == LUC_SAMPLING_NEE) weight = 0.0f;
         else {
-            uint32_t n = sc.num_lights, total = sc.light_strategies;
+            uint32_t n = kNoLights ? 0u : sc.num_lights, total = sc.light_strategies;
             float pdf_light = 0.0f;
             if (n != 0 && hit.light_area > 0.0f) {  // light.rs:241-263
                 const V3 prev = sink.prev();
@@ -124,7 +126,7 @@ LUC_D bool shade_vertex(const DevScene& sc, const FrameParams& fp, uint32_t dept
         float u_sel = smp.next_f32();
         float ua, ub;
         smp.next_vec2(ua, ub);
-        uint32_t nl = sc.num_lights, total = sc.light_strategies;
+        uint32_t nl = kNoLights ? 0u : sc.num_lights, total = sc.light_strategies;
         uint32_t pick = min(f2u(u_sel * (float)total), total - 1u);
         bool ok = true;
         if (pick < nl) {

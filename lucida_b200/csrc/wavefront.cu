@@ -299,7 +299,11 @@ struct PoolSink {
 // the extra warps hide more of it than the spills cost (measured against 4,
 // 5, 6 and 7 blocks; 7 -> 8 took the displaced-sphere frame's SHADE from
 // 16.0 to 15.5 ms).
-template <bool kGuided, bool kInst, bool kBatch = false>
+// kSobol / kNoLights (launched only when fp.sampler_kind is Sobol / the
+// scene has no emitter list): the other sampler's and the light-sampling code
+// are compiled out, which shrinks the kernel whose top stall is instruction
+// fetch (15.6 -> 14.7 ms per displaced-sphere frame with both).
+template <bool kGuided, bool kInst, bool kBatch = false, bool kSobol = false, bool kNoLights = false>
 __global__ void __launch_bounds__(128, 8) k_shade(PathState ps, const __grid_constant__ DevScene sc_arg,
                                                   const __grid_constant__ FrameParams fp_arg, BatchDev bd,
                                                   uint32_t depth) {
@@ -334,7 +338,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(PathState ps, const __grid_con
             V3 rad = xyz(r4);
             uint32_t pixel = (uint32_t)(q % fp.pixels);
             Sampler smp;
-            smp.kind = fp.sampler_kind;
+            smp.kind = kSobol ? LUC_SAMPLER_SOBOL : fp.sampler_kind;
             smp.state = __float_as_uint(t4.w);
             smp.index = sbase + (uint32_t)(q / fp.pixels);
             smp.seed = sobol_pixel_seed(pixel, fp.frame_seed);
@@ -350,7 +354,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(PathState ps, const __grid_con
                 }
             }
             PoolSink<kGuided> sink(ps, p, depth, sbase, rec_threshold, fp.rec_cap, dir, smp);
-            if (shade_vertex<kGuided, kInst>(sc, fp, depth, smp, xyz(o4), dir, xyz(t4), rad, o4.w, h4,
+            if (shade_vertex<kGuided, kInst, kNoLights>(sc, fp, depth, smp, xyz(o4), dir, xyz(t4), rad, o4.w, h4,
                                              kInst ? ps.hinst[p] : 0u, ps.lobes + i, ps.lobe_stride, sink))
                 store4(ps.rad + p, rad, 0.0f);
             survive = sink.survive;
@@ -534,6 +538,22 @@ void query_occupancy(RenderState& rs) {
     rs.shade_blocks_guided_inst = occ((const void*)k_shade<true, true>);
 }
 
+// SHADE of one bounce, specialised on the frame's sampler and on whether the
+// scene has an emitter list.
+template <bool kGuided, bool kInst>
+void launch_shade(const RenderState& rs, int grid, const DevScene& sc, const FrameParams& fp, uint32_t d,
+                  cudaStream_t s) {
+    const bool sobol = fp.sampler_kind == LUC_SAMPLER_SOBOL, no_lights = sc.num_lights == 0;
+    if (sobol && no_lights)
+        k_shade<kGuided, kInst, false, true, true><<<grid, 128, 0, s>>>(rs.ps, sc, fp, BatchDev{}, d);
+    else if (sobol)
+        k_shade<kGuided, kInst, false, true, false><<<grid, 128, 0, s>>>(rs.ps, sc, fp, BatchDev{}, d);
+    else if (no_lights)
+        k_shade<kGuided, kInst, false, false, true><<<grid, 128, 0, s>>>(rs.ps, sc, fp, BatchDev{}, d);
+    else
+        k_shade<kGuided, kInst><<<grid, 128, 0, s>>>(rs.ps, sc, fp, BatchDev{}, d);
+}
+
 // Host side: record one batch of the frame on `stream` (graph-capturable:
 // fixed launch shapes, device-resident lengths).
 void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, GpuAccum* accum, cudaStream_t stream,
@@ -574,13 +594,13 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
         join_connect();
         if (timer) timer->mark(stream, StageTimer::kShade);
         if (fp.guided && inst)
-            k_shade<true, true><<<sms * rs.shade_blocks_guided_inst, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
+            launch_shade<true, true>(rs, sms * rs.shade_blocks_guided_inst, sc, fp, d, stream);
         else if (fp.guided)
-            k_shade<true, false><<<sms * rs.shade_blocks_guided, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
+            launch_shade<true, false>(rs, sms * rs.shade_blocks_guided, sc, fp, d, stream);
         else if (inst)
-            k_shade<false, true><<<sms * rs.shade_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
+            launch_shade<false, true>(rs, sms * rs.shade_blocks_inst, sc, fp, d, stream);
         else
-            k_shade<false, false><<<sms * rs.shade_blocks, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
+            launch_shade<false, false>(rs, sms * rs.shade_blocks, sc, fp, d, stream);
         rs.launches += 2;
         if (d + 1 < fp.max_depth && (fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) &&
             sc.light_strategies > 0) {
