@@ -45,27 +45,29 @@ LUC_D void camera_ray(const FrameParams& fp, uint32_t pixel, Sampler& smp, V3& o
 //   void shadow(V3 o, V3 d, float t_max, V3 contribution)   NEE shadow ray
 //   void next(V3 origin, V3 dir, float pdf, V3 thr, V3 hit_position,
 //             V3 hit_normal, bool record, V3 rad)     the path continues
-// kNoLights: the scene has no emitter list (num_lights == 0; the caller
-// checks), so the light-sampling code is compiled out of the vertex.
+// kSkyMis: MIS sampling in a scene lit only by its environment map (no
+// emitter list; the caller checks), with the code of the other cases
+// compiled out of the vertex.
 // `h4` is the closest-hit record (t, u, v, id bits) and `inst` its instance;
 // `rad` is updated in place (the return value says whether it changed);
 // `lob` / `lobe_stride` locate the path's guide mixture (guided frames). The
 // sampler advances in place.
-template <bool kGuided, bool kInst, bool kNoLights = false, typename Sink>
+template <bool kGuided, bool kInst, bool kSkyMis = false, typename Sink>
 LUC_D bool shade_vertex(const DevScene& sc, const FrameParams& fp, uint32_t depth, Sampler& smp, V3 org, V3 dir,
                         V3 thr, V3& rad, float prev_pdf, float4 h4, uint32_t inst, const float4* lob,
                         uint32_t lobe_stride, Sink& sink) {
     const bool last = depth + 1 >= fp.max_depth;
+    const uint32_t sampling = kSkyMis ? LUC_SAMPLING_MIS : fp.sampling;
     const uint32_t id = __float_as_uint(h4.w);
     bool rad_changed = false;
     if (id == kMiss) {
         // Escaped (integrator.rs:228-263).
-        if (sc.has_env) {
+        if (kSkyMis || sc.has_env) {
             float epdf;
             V3 l = env_radiance_pdf(sc, dir, epdf);
             float weight;
-            if (depth == 0 || fp.sampling == LUC_SAMPLING_BSDF) weight = 1.0f;
-            else if (fp.sampling == LUC_SAMPLING_NEE) weight = 0.0f;
+            if (depth == 0 || sampling == LUC_SAMPLING_BSDF) weight = 1.0f;
+            else if (sampling == LUC_SAMPLING_NEE) weight = 0.0f;
             else {
                 uint32_t total = max(sc.light_strategies, 1u);
                 weight = power_heuristic(prev_pdf, epdf / (float)total);
@@ -86,10 +88,10 @@ LUC_D bool shade_vertex(const DevScene& sc, const FrameParams& fp, uint32_t dept
     // Emission with MIS (integrator.rs:271-309).
     if (hit.front && max_elem(emissive) > 0.0f) {
         float weight;
-        if (depth == 0 || fp.sampling == LUC_SAMPLING_BSDF) weight = 1.0f;
-        else if (fp.sampling == LUC_SAMPLING_NEE) weight = 0.0f;
+        if (depth == 0 || sampling == LUC_SAMPLING_BSDF) weight = 1.0f;
+        else if (sampling == LUC_SAMPLING_NEE) weight = 0.0f;
         else {
-            uint32_t n = kNoLights ? 0u : sc.num_lights, total = sc.light_strategies;
+            uint32_t n = kSkyMis ? 0u : sc.num_lights, total = sc.light_strategies;
             float pdf_light = 0.0f;
             if (n != 0 && hit.light_area > 0.0f) {  // light.rs:241-263
                 const V3 prev = sink.prev();
@@ -122,11 +124,11 @@ LUC_D bool shade_vertex(const DevScene& sc, const FrameParams& fp, uint32_t dept
     bool nee = false;
     V3 wiw{0, 0, 0}, lrad{0, 0, 0}, wi_n{0.0f, 0.0f, 1.0f};
     float dist = 0.0f, lpdf = 0.0f;
-    if ((fp.sampling == LUC_SAMPLING_NEE || fp.sampling == LUC_SAMPLING_MIS) && !last && sc.light_strategies > 0) {
+    if ((sampling == LUC_SAMPLING_NEE || sampling == LUC_SAMPLING_MIS) && !last && sc.light_strategies > 0) {
         float u_sel = smp.next_f32();
         float ua, ub;
         smp.next_vec2(ua, ub);
-        uint32_t nl = kNoLights ? 0u : sc.num_lights, total = sc.light_strategies;
+        uint32_t nl = kSkyMis ? 0u : sc.num_lights, total = sc.light_strategies;
         uint32_t pick = min(f2u(u_sel * (float)total), total - 1u);
         bool ok = true;
         if (pick < nl) {
@@ -205,7 +207,7 @@ LUC_D bool shade_vertex(const DevScene& sc, const FrameParams& fp, uint32_t dept
         const V3 wi = k == 0 ? wi_n : wl;
         const V3 f = bsdf_eval_w(surf, sw, wo, wi);
         float pdf = 0.0f;
-        if (k == 1 || (fp.sampling == LUC_SAMPLING_MIS && max_elem(f) > 0.0f)) pdf = bsdf_pdf_w(surf, sw, wo, wi);
+        if (k == 1 || (sampling == LUC_SAMPLING_MIS && max_elem(f) > 0.0f)) pdf = bsdf_pdf_w(surf, sw, wo, wi);
         if (k == 0) {
             f_n = f;
             p_n = pdf;
@@ -216,7 +218,7 @@ LUC_D bool shade_vertex(const DevScene& sc, const FrameParams& fp, uint32_t dept
     }
     if (nee && max_elem(f_n) > 0.0f) {
         float mis = 1.0f;
-        if (fp.sampling == LUC_SAMPLING_MIS) {
+        if (sampling == LUC_SAMPLING_MIS) {
             float pb = p_n;
             if (gv) pb = 0.5f * pb + 0.5f * mixture_pdf_mem(lob, lobe_stride, wiw);
             mis = power_heuristic(lpdf, pb);

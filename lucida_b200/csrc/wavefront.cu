@@ -299,11 +299,12 @@ struct PoolSink {
 // the extra warps hide more of it than the spills cost (measured against 4,
 // 5, 6 and 7 blocks; 7 -> 8 took the displaced-sphere frame's SHADE from
 // 16.0 to 15.5 ms).
-// kSobol / kNoLights (launched only when fp.sampler_kind is Sobol / the
-// scene has no emitter list): the other sampler's and the light-sampling code
-// are compiled out, which shrinks the kernel whose top stall is instruction
-// fetch (15.6 -> 14.7 ms per displaced-sphere frame with both).
-template <bool kGuided, bool kInst, bool kBatch = false, bool kSobol = false, bool kNoLights = false>
+// kSobol (launched only for Sobol frames) and kSkyMis (MIS frames of scenes
+// lit only by an environment map): the code of the other cases is compiled
+// out of the kernel whose top stall is instruction fetch (displaced-sphere
+// frame: SHADE 15.6 ms generic, 14.7 with kSobol and no light sampling,
+// 14.4 with MIS and the environment fixed too).
+template <bool kGuided, bool kInst, bool kBatch = false, bool kSobol = false, bool kSkyMis = false>
 __global__ void __launch_bounds__(128, 8) k_shade(PathState ps, const __grid_constant__ DevScene sc_arg,
                                                   const __grid_constant__ FrameParams fp_arg, BatchDev bd,
                                                   uint32_t depth) {
@@ -354,7 +355,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(PathState ps, const __grid_con
                 }
             }
             PoolSink<kGuided> sink(ps, p, depth, sbase, rec_threshold, fp.rec_cap, dir, smp);
-            if (shade_vertex<kGuided, kInst, kNoLights>(sc, fp, depth, smp, xyz(o4), dir, xyz(t4), rad, o4.w, h4,
+            if (shade_vertex<kGuided, kInst, kSkyMis>(sc, fp, depth, smp, xyz(o4), dir, xyz(t4), rad, o4.w, h4,
                                              kInst ? ps.hinst[p] : 0u, ps.lobes + i, ps.lobe_stride, sink))
                 store4(ps.rad + p, rad, 0.0f);
             survive = sink.survive;
@@ -538,18 +539,17 @@ void query_occupancy(RenderState& rs) {
     rs.shade_blocks_guided_inst = occ((const void*)k_shade<true, true>);
 }
 
-// SHADE of one bounce, specialised on the frame's sampler and on whether the
-// scene has an emitter list.
+// SHADE of one bounce, specialised on the frame's sampler and on MIS frames
+// of scenes lit only by their environment map.
 template <bool kGuided, bool kInst>
 void launch_shade(const RenderState& rs, int grid, const DevScene& sc, const FrameParams& fp, uint32_t d,
                   cudaStream_t s) {
-    const bool sobol = fp.sampler_kind == LUC_SAMPLER_SOBOL, no_lights = sc.num_lights == 0;
-    if (sobol && no_lights)
+    const bool sobol = fp.sampler_kind == LUC_SAMPLER_SOBOL;
+    const bool sky_mis = fp.sampling == LUC_SAMPLING_MIS && sc.num_lights == 0 && sc.has_env;
+    if (sobol && sky_mis)
         k_shade<kGuided, kInst, false, true, true><<<grid, 128, 0, s>>>(rs.ps, sc, fp, BatchDev{}, d);
     else if (sobol)
         k_shade<kGuided, kInst, false, true, false><<<grid, 128, 0, s>>>(rs.ps, sc, fp, BatchDev{}, d);
-    else if (no_lights)
-        k_shade<kGuided, kInst, false, false, true><<<grid, 128, 0, s>>>(rs.ps, sc, fp, BatchDev{}, d);
     else
         k_shade<kGuided, kInst><<<grid, 128, 0, s>>>(rs.ps, sc, fp, BatchDev{}, d);
 }
