@@ -408,20 +408,21 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     }
     // Environment: pixels, the packed CDF split into conditional rows and
     // the marginal, and the per-row sin(theta) the pdf divides by.
-    std::vector<float> cond, marg, rsin;
+    // The rows are copied straight out of the caller's packed array (pitch
+    // env_cdf_width floats): no host staging.
+    std::vector<float> rsin;
+    LUC_CUDA(c, upload(c->env_px, v->env_pixels, 4 * (size_t)v->env_width * v->env_height, s), "upload env");
     if (v->env_width) {
-        uint32_t w = v->env_width, h = v->env_height, cw = v->env_cdf_width;
-        cond.resize((size_t)(w + 1) * h);
-        for (uint32_t j = 0; j < h; ++j)
-            std::memcpy(&cond[(size_t)j * (w + 1)], v->env_cdf + (size_t)j * cw, (w + 1) * sizeof(float));
-        marg.assign(v->env_cdf + (size_t)h * cw, v->env_cdf + (size_t)h * cw + h + 1);
+        const uint32_t w = v->env_width, h = v->env_height, cw = v->env_cdf_width;
+        LUC_CUDA(c, c->env_cond.ensure((size_t)(w + 1) * h * sizeof(float)), "alloc env cdf");
+        LUC_CUDA(c, cudaMemcpy2DAsync(c->env_cond.p, (w + 1) * sizeof(float), v->env_cdf, (size_t)cw * sizeof(float),
+                                      (w + 1) * sizeof(float), h, cudaMemcpyHostToDevice, s),
+                 "upload env cdf");
+        LUC_CUDA(c, upload(c->env_marg, v->env_cdf + (size_t)h * cw, (size_t)h + 1, s), "upload env marginal");
         rsin.resize(h);
         const float PI = 3.14159265358979323846f;
         for (uint32_t j = 0; j < h; ++j) rsin[j] = std::sin(((float)j + 0.5f) / (float)h * PI);
     }
-    LUC_CUDA(c, upload(c->env_px, v->env_pixels, 4 * (size_t)v->env_width * v->env_height, s), "upload env");
-    LUC_CUDA(c, upload(c->env_cond, cond.data(), cond.size(), s), "upload env cdf");
-    LUC_CUDA(c, upload(c->env_marg, marg.data(), marg.size(), s), "upload env marginal");
     LUC_CUDA(c, upload(c->env_row_sin, rsin.data(), rsin.size(), s), "upload env rows");
     c->wide_nodes = 0;
     if (v->num_triangles && num_nodes) {
