@@ -177,6 +177,8 @@ void luc_destroy(luc_ctx* c) {
     if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->ev_ready) cudaEventDestroy(c->ev_ready);
     if (c->ev_done) cudaEventDestroy(c->ev_done);
+    if (c->ev_up0) cudaEventDestroy(c->ev_up0);
+    if (c->ev_up1) cudaEventDestroy(c->ev_up1);
     cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -265,6 +267,20 @@ int32_t validate_tris_dev(luc_ctx* c, const GpuTriangle* t, uint32_t n, uint32_t
 
 }  // namespace
 
+// The context's second stream (highest priority: a frame's deferred guide
+// step must get its blocks ahead of the EXTEND blocks that would otherwise
+// fill every SM) and the events that order work across the two streams.
+static int32_t ensure_side_stream(luc_ctx* c) {
+    if (!c->side_stream) {
+        int lo_prio = 0, hi_prio = 0;
+        cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+        LUC_CUDA(c, cudaStreamCreateWithPriority(&c->side_stream, cudaStreamNonBlocking, hi_prio), "create side stream");
+    }
+    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_join, &c->ev_ready, &c->ev_done, &c->ev_up0, &c->ev_up1})
+        if (!*e) LUC_CUDA(c, cudaEventCreateWithFlags(e, cudaEventDisableTiming), "create event");
+    return LUC_OK;
+}
+
 static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec* meshes) {
     if (!c || !v) return LUC_ERR_VALIDATION;
     cudaSetDevice(c->device);
@@ -345,6 +361,18 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     }
     cudaStream_t s = c->stream;
     c->has_scene = false;
+    // Vertex attributes and the environment go up on the side stream, beside
+    // the BVH build (nothing in it reads them), once the context's earlier
+    // work is done with the buffers. Every return waits for those copies: the
+    // caller may free its arrays once the upload returns.
+    if (int32_t rc = ensure_side_stream(c)) return rc;
+    const cudaStream_t side = c->side_stream;
+    struct SideWait {
+        cudaStream_t st;
+        ~SideWait() { cudaStreamSynchronize(st); }
+    } side_wait{side};
+    LUC_CUDA(c, cudaEventRecord(c->ev_up0, s), "order uploads");
+    LUC_CUDA(c, cudaStreamWaitEvent(side, c->ev_up0, 0), "order uploads");
     LUC_CUDA(c, upload(c->materials, v->materials, v->num_materials, s), "upload materials");
     LUC_CUDA(c, upload(c->prims, v->primitives, (size_t)np_ + ni, s), "upload primitives");
     std::vector<uint32_t> roots;
@@ -354,7 +382,7 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     LUC_CUDA(c, upload(c->blas_roots, roots.data(), roots.size(), s), "upload blas roots");
     LUC_CUDA(c, upload(c->lights, v->lights, v->num_lights, s), "upload lights");
     LUC_CUDA(c, upload(c->positions, v->positions, 4 * (size_t)v->num_vertices, s), "upload positions");
-    LUC_CUDA(c, upload(c->attrs, v->vertex_attrs, v->num_vertices, s), "upload vertex attrs");
+    LUC_CUDA(c, upload(c->attrs, v->vertex_attrs, v->num_vertices, side), "upload vertex attrs");
     int bkeys[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
     if (vertex_bounds) {
         LUC_CUDA(c, c->upload_scratch.ensure(64), "alloc upload scratch");
@@ -411,19 +439,19 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     // The rows are copied straight out of the caller's packed array (pitch
     // env_cdf_width floats): no host staging.
     std::vector<float> rsin;
-    LUC_CUDA(c, upload(c->env_px, v->env_pixels, 4 * (size_t)v->env_width * v->env_height, s), "upload env");
+    LUC_CUDA(c, upload(c->env_px, v->env_pixels, 4 * (size_t)v->env_width * v->env_height, side), "upload env");
     if (v->env_width) {
         const uint32_t w = v->env_width, h = v->env_height, cw = v->env_cdf_width;
         LUC_CUDA(c, c->env_cond.ensure((size_t)(w + 1) * h * sizeof(float)), "alloc env cdf");
         LUC_CUDA(c, cudaMemcpy2DAsync(c->env_cond.p, (w + 1) * sizeof(float), v->env_cdf, (size_t)cw * sizeof(float),
-                                      (w + 1) * sizeof(float), h, cudaMemcpyHostToDevice, s),
+                                      (w + 1) * sizeof(float), h, cudaMemcpyHostToDevice, side),
                  "upload env cdf");
-        LUC_CUDA(c, upload(c->env_marg, v->env_cdf + (size_t)h * cw, (size_t)h + 1, s), "upload env marginal");
+        LUC_CUDA(c, upload(c->env_marg, v->env_cdf + (size_t)h * cw, (size_t)h + 1, side), "upload env marginal");
         rsin.resize(h);
         const float PI = 3.14159265358979323846f;
         for (uint32_t j = 0; j < h; ++j) rsin[j] = std::sin(((float)j + 0.5f) / (float)h * PI);
     }
-    LUC_CUDA(c, upload(c->env_row_sin, rsin.data(), rsin.size(), s), "upload env rows");
+    LUC_CUDA(c, upload(c->env_row_sin, rsin.data(), rsin.size(), side), "upload env rows");
     c->wide_nodes = 0;
     if (v->num_triangles && num_nodes) {
         int32_t rc2 = luc_build_traversal(c, num_nodes, v->num_triangles);
@@ -439,6 +467,8 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
             if (rc2) return rc2;
         }
     }
+    LUC_CUDA(c, cudaEventRecord(c->ev_up1, side), "join uploads");
+    LUC_CUDA(c, cudaStreamWaitEvent(s, c->ev_up1, 0), "join uploads");
     LUC_CUDA(c, cudaStreamSynchronize(s), "scene upload");
     if (vertex_bounds)
         for (int a = 0; a < 3; ++a) {
@@ -703,18 +733,8 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
             // Unprofiled frames run each CONNECT on the side stream, beside
             // the next EXTEND (stage timers need the stages in sequence).
             const bool overlap = tp == nullptr;
-            if ((pending || overlap) && !c->side_stream) {
-                // Highest priority: the step's blocks are placed ahead of
-                // the EXTEND blocks that would otherwise fill every SM.
-                int lo_prio = 0, hi_prio = 0;
-                cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
-                LUC_CUDA(c, cudaStreamCreateWithPriority(&c->side_stream, cudaStreamNonBlocking, hi_prio),
-                         "create side stream");
-                LUC_CUDA(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming), "create event");
-                LUC_CUDA(c, cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming), "create event");
-                LUC_CUDA(c, cudaEventCreateWithFlags(&c->ev_ready, cudaEventDisableTiming), "create event");
-                LUC_CUDA(c, cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming), "create event");
-            }
+            if (pending || overlap)
+                if (int32_t rc2 = ensure_side_stream(c)) return rc2;
             const ConnectOverlap ov{c->side_stream, c->ev_ready, c->ev_done};
             LUC_CUDA(c, cudaStreamBeginCapture(c->own_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
             GuideTrain gcap = gt;

@@ -92,6 +92,7 @@ struct luc_ctx {
     cudaStream_t side_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_ready = nullptr, ev_done = nullptr;  // CONNECT beside the next EXTEND
+    cudaEvent_t ev_up0 = nullptr, ev_up1 = nullptr;     // uploads beside the BVH build
     float guide_lr = 1.0e-2f;
     float guide_lo[3] = {0, 0, 0}, guide_hi[3] = {1, 1, 1};
     // Bounds of the uploaded scene (vertices and analytic primitives).
