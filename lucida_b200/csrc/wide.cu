@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
         // Quantization (double: exact for these magnitudes).
         uint32_t ebits = 0;
         float p[3];
-        double scale[3];
+        double scale[3], inv_scale[3];
         for (int a = 0; a < 3; ++a) {
             const double ext = (double)hi[a] - (double)lo[a];
             int ex = -126;
@@ -363,10 +363,11 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
             float pf = 0.0f;
             for (;;) {
                 scale[a] = ldexp(1.0, ex);
+                inv_scale[a] = ldexp(1.0, -ex);  // x / 2^ex == x * 2^-ex exactly: no double divisions
                 const double pd = (double)lo[a] - 2.0 * scale[a];
                 pf = (float)pd;
                 if ((double)pf > pd) pf = nextafterf(pf, -3.4e38f);
-                if (ex >= 120 || ceil(((double)hi[a] - (double)pf) / scale[a]) + 1.0 <= 253.0) break;
+                if (ex >= 120 || ceil(((double)hi[a] - (double)pf) * inv_scale[a]) + 1.0 <= 253.0) break;
                 ++ex;
             }
             p[a] = pf;
@@ -385,8 +386,8 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
                 }
             } else {
                 for (int a = 0; a < 3; ++a) {
-                    double ql = floor(((double)ch[k].lo[a] - (double)p[a]) / scale[a]) - 1.0;
-                    double qh = ceil(((double)ch[k].hi[a] - (double)p[a]) / scale[a]) + 1.0;
+                    double ql = floor(((double)ch[k].lo[a] - (double)p[a]) * inv_scale[a]) - 1.0;
+                    double qh = ceil(((double)ch[k].hi[a] - (double)p[a]) * inv_scale[a]) + 1.0;
                     l8[a] = (uint32_t)fmax(0.0, fmin(255.0, ql));
                     h8[a] = (uint32_t)fmax(0.0, fmin(255.0, qh));
                 }
