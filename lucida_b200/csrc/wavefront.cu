@@ -106,8 +106,10 @@ constexpr int wide_min_blocks(int threads) { return 1024 / threads; }
 // (measured best against 1, 16 and 32).
 constexpr int kExtendRefill = 8;
 
+// Two-level closest-hit walks (kInst) at 28 warps per SM (72 registers): the
+// instanced frame's EXTEND took 602 ms at 32 warps (spilling) and 574 at 28.
 template <bool kInst, bool kBatch, int kThreads, int kWide>
-__global__ void __launch_bounds__(kThreads, kWide == 1 ? wide_min_blocks(kThreads) : 1) k_extend(PathState ps, const __grid_constant__ DevScene sc_arg, FrameParams fp,
+__global__ void __launch_bounds__(kThreads, kWide == 1 ? (kInst ? 7 * 128 / kThreads : wide_min_blocks(kThreads)) : 1) k_extend(PathState ps, const __grid_constant__ DevScene sc_arg, FrameParams fp,
                                                      BatchDev bd, uint32_t depth) {
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
     const uint32_t* queue = ps.queue[depth & 1];
