@@ -381,9 +381,11 @@ __global__ void __launch_bounds__(128, 8) k_shade(PathState ps, const __grid_con
 }
 
 // CONNECT (shaders/wavefront/connect.wgsl:58-84): any-hit shadow rays, with
-// the same persistent ray pull as EXTEND.
+// the same persistent ray pull as EXTEND. Two-level any-hit walks (kInst,
+// binary BLASes) run at 32 warps per SM too: the instanced frame's CONNECT
+// took 133 ms unbounded (82 registers, 24 warps), 110 at 28 warps, 103 at 32.
 template <bool kInst, bool kBatch, int kThreads, int kWide>
-__global__ void __launch_bounds__(kThreads, kWide == 1 ? wide_min_blocks(kThreads) : 1) k_connect(PathState ps, const __grid_constant__ DevScene sc_arg, BatchDev bd,
+__global__ void __launch_bounds__(kThreads, kWide == 1 || kInst ? wide_min_blocks(kThreads) : 1) k_connect(PathState ps, const __grid_constant__ DevScene sc_arg, BatchDev bd,
                                                       uint32_t depth) {
     const uint32_t len = ps.ctr[depth * kCtrStride + kCtrShadow];
     uint32_t* pull = ps.ctr + depth * kCtrStride + kCtrPullConnect;
