@@ -14,6 +14,8 @@ the library's stream, which is torch's current stream), L2 flushed with a
 public API with host buffers: every step uploads the scene from pinned host
 memory (and rebuilds the LBVH), renders, and reads the 64 MiB accumulator
 back into pinned host memory, exactly what pt_gpu::render_with does per call.
+The roofline's per-stage times come from profiled repeats of the timed frames
+(stage events, stages in sequence), run after the timed region.
 
 Multi-GPU (--gpus N under torchrun): each rank renders the same frame with a
 disjoint sample range (sample_offset = rank * spp) — independent replicas, no
