@@ -53,7 +53,10 @@ struct RegSink {
 };
 
 template <bool kInst, int kWide>
-__global__ void __launch_bounds__(128) k_megakernel(PathState ps, const __grid_constant__ DevScene sc,
+// 4 blocks of 128 per SM (128 registers): the analytic Cornell box ran 420
+// Mpaths/s at the compiler's 148-159 registers (3 blocks), 487 at 4 blocks,
+// 437 at 6, 421 at 8.
+__global__ void __launch_bounds__(128, 4) k_megakernel(PathState ps, const __grid_constant__ DevScene sc,
                                                     const __grid_constant__ FrameParams fp) {
     const uint32_t sbase = *fp.sbase;
     TravCount tce, tcs;
