@@ -240,8 +240,9 @@ int32_t luc_convergence(luc_ctx* ctx, const void* accum_dev, uint32_t pixels, fl
  * cudaStream_t of the current device; null = the legacy default stream) and
  * returns when the sort is done. Scratch is a file-scope device array (about
  * 8.3 MiB, held on every GPU that loads the library until exit), shared by
- * every call: calls that overlap on the GPU race. The first call on a device
- * resolves the array's address, so make it before any stream capture.
+ * every call: calls that overlap on the GPU race. Each call looks up the
+ * array's device address in the current context, and it is synchronous: it
+ * waits on `stream` for the sort and reads back its status before returning.
  * Larger n returns LUC_ERR_VALIDATION; messages go to err_msg (may be null). */
 int32_t luc_sort_u32_static(void* keys_dev, void* vals_dev, uint32_t n, void* stream, char* err_msg,
                             uint32_t err_len);

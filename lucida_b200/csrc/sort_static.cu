@@ -12,7 +12,6 @@
 // allocating routine.
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include "ctx.cuh"
 #include "sort_kernels.cuh"
 
@@ -32,16 +31,14 @@ static __device__ __align__(256) uint32_t g_scratch_vals[kStaticMaxKeys];
 static __device__ __align__(256) uint32_t g_scratch_status[kStaticMaxTiles * 256];
 static __device__ __align__(256) uint32_t g_scratch_hist[kHistWords];
 
-// Device addresses of the arrays, per device. In host code the array names
-// are host-side stand-ins, never device addresses, so kernels only ever get
-// the addresses cudaGetSymbolAddress returns.
+// Device addresses of the arrays in the current context. In host code the
+// array names are host-side stand-ins, never device addresses, so kernels
+// only ever get the addresses cudaGetSymbolAddress returns. They are looked
+// up on every call (cheap once the module is loaded), so no address outlives
+// the context it was taken in.
 struct ScratchAddr {
     uint32_t *keys = nullptr, *vals = nullptr, *status = nullptr, *hist = nullptr;
-    bool ready = false;
 };
-constexpr int kMaxDevices = 64;
-ScratchAddr g_addr[kMaxDevices];
-std::mutex g_addr_mu;
 
 void set_err(char* msg, uint32_t len, const char* text) {
     if (msg && len) {
@@ -50,26 +47,30 @@ void set_err(char* msg, uint32_t len, const char* text) {
     }
 }
 
-// Resolve the arrays' device addresses on the current device, once.
-int32_t scratch_for_device(int dev, ScratchAddr& out, char* msg, uint32_t len) {
-    std::lock_guard<std::mutex> lock(g_addr_mu);
-    ScratchAddr& a = g_addr[dev];
-    if (!a.ready) {
-        cudaError_t e;
-        if ((e = cudaGetSymbolAddress((void**)&a.keys, g_scratch_keys)) != cudaSuccess ||
-            (e = cudaGetSymbolAddress((void**)&a.vals, g_scratch_vals)) != cudaSuccess ||
-            (e = cudaGetSymbolAddress((void**)&a.status, g_scratch_status)) != cudaSuccess ||
-            (e = cudaGetSymbolAddress((void**)&a.hist, g_scratch_hist)) != cudaSuccess) {
-            char buf[256];
-            std::snprintf(buf, sizeof(buf), "luc_sort_u32_static: cudaGetSymbolAddress failed: %s",
-                          cudaGetErrorString(e));
-            set_err(msg, len, buf);
-            return LUC_ERR_LAUNCH;
-        }
-        a.ready = true;
+int32_t scratch_addresses(ScratchAddr& a, char* msg, uint32_t len) {
+    cudaError_t e;
+    if ((e = cudaGetSymbolAddress((void**)&a.keys, g_scratch_keys)) != cudaSuccess ||
+        (e = cudaGetSymbolAddress((void**)&a.vals, g_scratch_vals)) != cudaSuccess ||
+        (e = cudaGetSymbolAddress((void**)&a.status, g_scratch_status)) != cudaSuccess ||
+        (e = cudaGetSymbolAddress((void**)&a.hist, g_scratch_hist)) != cudaSuccess) {
+        char buf[256];
+        std::snprintf(buf, sizeof(buf), "luc_sort_u32_static: cudaGetSymbolAddress failed: %s",
+                      cudaGetErrorString(e));
+        set_err(msg, len, buf);
+        return LUC_ERR_LAUNCH;
     }
-    out = a;
     return LUC_OK;
+}
+
+// Launch with the launch's own status as the result (not the thread's
+// last-error word, which may hold an earlier, unrelated failure).
+template <typename... Params, typename... Args>
+cudaError_t launch(void (*kernel)(Params...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = s;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 }  // namespace
@@ -91,35 +92,30 @@ extern "C" int32_t luc_sort_u32_static(void* keys_dev, void* vals_dev, uint32_t 
         set_err(err_msg, err_len, "luc_sort_u32_static: null device array");
         return LUC_ERR_VALIDATION;
     }
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
-        set_err(err_msg, err_len, "luc_sort_u32_static: no current CUDA device");
-        return LUC_ERR_NO_DEVICE;
-    }
     ScratchAddr sa;
-    int32_t rc = scratch_for_device(dev, sa, err_msg, err_len);
+    int32_t rc = scratch_addresses(sa, err_msg, err_len);
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
     const uint32_t tiles = (n + kTile - 1) / kTile;
     uint32_t* hist = sa.hist;
     uint32_t* offs = hist + 1024;
     uint32_t* tcount = hist + 2048;
-    // The scratch keeps the previous call's contents: clear what must start at zero.
-    cudaMemsetAsync(hist, 0, kHistWords * sizeof(uint32_t), s);
-    int grid = (int)std::min<uint32_t>((n + 255) / 256, 148 * 32);
-    k_hist4<<<grid, 256, 0, s>>>((const uint32_t*)keys_dev, n, hist);
-    k_hist_scan<<<1, 256, 0, s>>>(hist, offs);
+    const unsigned grid = std::min<uint32_t>((n + 255) / 256, 148 * 32);
     uint32_t *ka = (uint32_t*)keys_dev, *va = (uint32_t*)vals_dev, *kb = sa.keys, *vb = sa.vals;
-    for (int p = 0; p < 4; ++p) {
-        cudaMemsetAsync(sa.status, 0, (size_t)tiles * 256 * sizeof(uint32_t), s);
-        k_onesweep<<<tiles, kSortThreads, 0, s>>>(ka, va, kb, vb, n, 8 * p, offs + 256 * p, sa.status, tcount + p,
-                                                   tcount + 4);
+    // The scratch keeps the previous call's contents: clear what must start at zero.
+    cudaError_t e = cudaMemsetAsync(hist, 0, kHistWords * sizeof(uint32_t), s);
+    if (e == cudaSuccess) e = launch(k_hist4, grid, 256, s, (const uint32_t*)keys_dev, n, hist);
+    if (e == cudaSuccess) e = launch(k_hist_scan, 1, 256, s, (const uint32_t*)hist, offs);
+    for (int p = 0; p < 4 && e == cudaSuccess; ++p) {
+        e = cudaMemsetAsync(sa.status, 0, (size_t)tiles * 256 * sizeof(uint32_t), s);
+        if (e == cudaSuccess)
+            e = launch(k_onesweep, tiles, kSortThreads, s, (const uint32_t*)ka, (const uint32_t*)va, kb, vb, n,
+                       8 * p, (const uint32_t*)(offs + 256 * p), sa.status, tcount + p, tcount + 4);
         std::swap(ka, kb);
         std::swap(va, vb);
     }
     // After four passes the sorted pairs are back in the caller's arrays.
     uint32_t flag = 0;
-    cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, tcount + 4, sizeof(flag), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {

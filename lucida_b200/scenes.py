@@ -12,7 +12,9 @@
 
 "Lambertian" is Lucida's GpuMaterial::diffuse (gpu_layout.rs:77-84): a
 diffuse base under a roughness-1, IOR-1.5 GGX coat. The value-noise lattice
-hash and the sphere layout are defined here and documented in DESIGN.md.
+hash and the sphere layout are defined here: a 32-bit avalanche hash of the
+integer cell and the octave seed, trilinear with smoothstep, octaves at
+frequency 2, 4, 8 with weights 1, 1/2, 1/4.
 """
 from __future__ import annotations
 
@@ -80,7 +82,7 @@ def icosphere_unit(levels: int):
 
 def _lattice_hash(ix, iy, iz, seed):
     """Integer lattice hash -> [0, 1): a 32-bit avalanche of the cell
-    coordinates and the octave seed (the value-noise lattice of DESIGN.md)."""
+    coordinates and the octave seed."""
     h = (ix.astype(np.uint32) * np.uint32(0x8DA6B343) ^ iy.astype(np.uint32) * np.uint32(0xD8163841)
          ^ iz.astype(np.uint32) * np.uint32(0xCB1AB31F) ^ np.uint32(seed & 0xFFFFFFFF))
     h ^= h >> np.uint32(16)
