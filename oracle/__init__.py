@@ -88,6 +88,9 @@ def lib():
         L.orc_instance_world_bounds.argtypes = [vp, vp, vp]
         L.orc_build_uniforms.argtypes = [vp, u32, u32, u32, u32, u32, u32, u32, u32, vp]
         L.orc_render_sums.argtypes = [vp, vp, u32, u32, u32, u32, vp]
+        L.orc_set_libm_mode.argtypes = [i32]
+        L.orc_get_libm_mode.restype = i32
+        L.orc_sample_traces.argtypes = [vp, vp, vp, u32, u32, vp, vp]
         L.orc_intersect_batch.argtypes = [vp, vp, u32, vp]
         for f in ("orc_pcg_hash", "orc_hash_u32", "orc_expand_bits"):
             getattr(L, f).restype = u32
@@ -263,13 +266,29 @@ class Scene:
                                  sampler, C.byref(u))
         return u
 
-    def render_sums(self, u: Uniforms, threads: int = 0, rows=None, band: int = 32) -> np.ndarray:
+    def render_sums(self, u: Uniforms, threads: int = 0, rows=None, band: int = 32,
+                    libm: str = "glibc") -> np.ndarray:
         """Per-pixel [radiance sum 3, radiance^2 sum 3, albedo 3, normal 3, depth 1] in sample order,
-        rows [r0, r1) handed to `threads` workers in `band`-row bands (integrator.rs:635-699 uses 32)."""
+        rows [r0, r1) handed to `threads` workers in `band`-row bands (integrator.rs:635-699 uses 32).
+        `libm`: "glibc" (the reference's f32 transcendentals) or "double" (evaluated in double and
+        rounded once, as the CUDA integrator rounds them)."""
         r0, r1 = (0, u.height) if rows is None else rows
         out = np.zeros(((r1 - r0) * u.width, 13), np.float32)
-        lib().orc_render_sums(self._h, C.byref(u), threads, r0, r1, band, _p(out))
+        with libm_mode(libm):
+            lib().orc_render_sums(self._h, C.byref(u), threads, r0, r1, band, _p(out))
         return out
+
+    def sample_traces(self, u: Uniforms, pixels, libm: str = "glibc", threads: int = 0):
+        """Every sample of the listed pixels (indices y * width + x) traced on its own: radiance
+        (n, spp, 3) and path signatures (n, spp) u64 — a hash of the path's discrete events (the
+        primitive each ray hit, shadow-ray outcomes, BSDF lobe choices and rejections, light picks)."""
+        pixels = np.ascontiguousarray(pixels, np.uint32).reshape(-1)
+        n, spp = len(pixels), u.samples_per_launch
+        rad = np.zeros((n, spp, 3), np.float32)
+        sig = np.zeros((n, spp), np.uint64)
+        with libm_mode(libm):
+            lib().orc_sample_traces(self._h, C.byref(u), _p(pixels), n, threads, _p(rad), _p(sig))
+        return rad, sig
 
     def intersect(self, rays: np.ndarray) -> np.ndarray:
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
@@ -283,6 +302,24 @@ class Scene:
         d, r, p = np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32), np.zeros(n, np.float32)
         lib().orc_env_sample_batch(self._h, _p(u2), n, _p(d), _p(r), _p(p))
         return d, r, p
+
+
+class libm_mode:
+    """Context manager: render-time transcendentals as glibc's f32 functions ("glibc", the
+    reference's) or evaluated in double and rounded once ("double", the CUDA integrator's)."""
+
+    def __init__(self, mode: str):
+        if mode not in ("glibc", "double"):
+            raise ValueError(mode)
+        self.mode = 1 if mode == "double" else 0
+
+    def __enter__(self):
+        self.prev = lib().orc_get_libm_mode()
+        lib().orc_set_libm_mode(self.mode)
+        return self
+
+    def __exit__(self, *exc):
+        lib().orc_set_libm_mode(self.prev)
 
 
 def sampler_stream(kind, frame_seed, pixel, sample, pattern: str) -> np.ndarray:

@@ -1,6 +1,8 @@
 // ORACLE — test infrastructure only (see oracle_core.hpp). A C ABI over the
 // restatement so tests/ (through oracle/__init__.py) can drive it with ctypes.
 #include "oracle_scene.hpp"
+#include <atomic>
+#include <thread>
 
 using namespace oracle;
 
@@ -216,6 +218,38 @@ void orc_render_sums(void* h, const GpuUniforms* u, uint32_t threads, uint32_t r
         ps[i].normal.to(o + 9);
         o[12] = ps[i].depth;
     }
+}
+
+// Render-time transcendental rounding: 0 = glibc f32 (the reference), 1 =
+// double evaluation rounded once (the CUDA integrator's). Call between renders.
+void orc_set_libm_mode(int mode) { g_libm_mode = mode ? 1 : 0; }
+int orc_get_libm_mode(void) { return g_libm_mode; }
+
+// Every sample of the listed pixels traced on its own: radiance (3 floats)
+// and path signature per (pixel, sample), pixel-major. Threads split pixels.
+void orc_sample_traces(void* h, const GpuUniforms* u, const uint32_t* pixels, uint32_t n, uint32_t threads,
+                       float* rad_out, uint64_t* sig_out) {
+    const Scene& s = *(Scene*)h;
+    const uint32_t spp = u->samples_per_launch;
+    std::atomic<uint32_t> next{0};
+    auto worker = [&] {
+        for (;;) {
+            uint32_t i = next.fetch_add(1);
+            if (i >= n) break;
+            uint32_t x = pixels[i] % u->width, y = pixels[i] / u->width;
+            for (uint32_t k = 0; k < spp; ++k) {
+                uint64_t sig;
+                Vec3 r = trace_sample(s, *u, x, y, k, sig);
+                r.to(rad_out + 3 * ((size_t)i * spp + k));
+                sig_out[(size_t)i * spp + k] = sig;
+            }
+        }
+    };
+    if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < threads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
 }
 
 // Closest hit for a batch of rays (origin3, dir3): t, material, front_face,

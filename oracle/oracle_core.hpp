@@ -58,6 +58,38 @@ inline float clampf(float x, float lo, float hi) {
     return x;
 }
 inline uint32_t bits(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+
+// ---------------------------------------------------------------- libm mode
+// How the render-time transcendentals round. 0 (the default): glibc's f32
+// functions, what the reference's Rust calls. 1: evaluated in double and
+// rounded once to f32, the rounding the CUDA integrator uses. Scene
+// construction and the tables the device receives from the host (energy
+// table, environment row sines, camera uniforms) always use glibc. Set only
+// between renders (orc_set_libm_mode); render threads read it.
+extern int g_libm_mode;
+inline float m_sin(float x) { return g_libm_mode ? (float)std::sin((double)x) : std::sin(x); }
+inline float m_cos(float x) { return g_libm_mode ? (float)std::cos((double)x) : std::cos(x); }
+inline float m_acos(float x) { return g_libm_mode ? (float)std::acos((double)x) : std::acos(x); }
+inline float m_atan2(float y, float x) {
+    return g_libm_mode ? (float)std::atan2((double)y, (double)x) : std::atan2(y, x);
+}
+inline float m_pow(float x, float y) { return g_libm_mode ? (float)std::pow((double)x, (double)y) : std::pow(x, y); }
+
+// ---------------------------------------------------------------- path signature
+// A per-thread hash of a path's discrete events (which primitive each ray
+// hit, each shadow ray's outcome, each BSDF lobe choice and rejection, each
+// light pick), filled only while g_path_sig points somewhere. Two traces of
+// one sample with equal signatures took the same branches everywhere; their
+// radiance can differ only by rounding carried along the same path.
+extern thread_local uint64_t* g_path_sig;
+inline void sig_event(uint32_t kind, uint64_t value) {
+    if (!g_path_sig) return;
+    uint64_t h = *g_path_sig ^ (((uint64_t)kind << 56) + value + 0x9E3779B97F4A7C15ull);
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+    *g_path_sig = h;
+}
 inline float from_bits(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
 inline uint32_t reverse_bits(uint32_t x) {
     x = ((x >> 1) & 0x55555555u) | ((x & 0x55555555u) << 1);
@@ -118,7 +150,7 @@ struct Vec3 {
     Vec3 abs() const { return Vec3(std::fabs(x), std::fabs(y), std::fabs(z)); }
     // glam 0.33: self * (1 - s) + rhs * s
     Vec3 lerp(Vec3 o, float s) const { return *this * (1.0f - s) + o * s; }
-    Vec3 powf(float e) const { return Vec3(std::pow(x, e), std::pow(y, e), std::pow(z, e)); }
+    Vec3 powf(float e) const { return Vec3(m_pow(x, e), m_pow(y, e), m_pow(z, e)); }
     bool is_finite() const { return std::isfinite(x) && std::isfinite(y) && std::isfinite(z); }
 };
 inline Vec3 operator*(float s, Vec3 v) { return Vec3(s * v.x, s * v.y, s * v.z); }
@@ -258,7 +290,7 @@ inline Vec2 concentric_sample_disk(Vec2 u) {  // :87-99
         r = o.y;
         theta = PI / 2.0f - (PI / 4.0f) * (o.x / o.y);
     }
-    return Vec2(r * std::cos(theta), r * std::sin(theta));
+    return Vec2(r * m_cos(theta), r * m_sin(theta));
 }
 inline Vec3 sample_cosine_hemisphere(Vec2 u) {  // :68-74
     Vec2 d = concentric_sample_disk(u);
@@ -367,8 +399,8 @@ inline Vec3 sample_ggx_vndf(Vec3 wo, float alpha, Vec2 u) {  // :187-216
     Vec3 t2 = v.cross(t1);
     float r = std::sqrt(u.x);
     float phi = 2.0f * PI * u.y;
-    float p1 = r * std::cos(phi);
-    float p2 = r * std::sin(phi);
+    float p1 = r * m_cos(phi);
+    float p2 = r * m_sin(phi);
     float s = 0.5f * (1.0f + v.z);
     p2 = (1.0f - s) * std::sqrt(fmax_(1.0f - p1 * p1, 0.0f)) + s * p2;
     Vec3 nh = p1 * t1 + p2 * t2 + std::sqrt(fmax_(1.0f - p1 * p1 - p2 * p2, 0.0f)) * v;

@@ -6,6 +6,13 @@
 
 namespace oracle {
 
+int g_libm_mode = 0;
+thread_local uint64_t* g_path_sig = nullptr;
+static inline bool sig_bool(uint32_t kind, bool b) {
+    sig_event(kind, b ? 1 : 0);
+    return b;
+}
+
 // scene.rs:76-97
 bool intersect_sphere(const GpuPrimitive& s, const Ray& ray, float tmin, float tmax, float& out) {
     Vec3 center = Vec3::from(s.position);
@@ -101,6 +108,7 @@ bool Scene::intersect(const Ray& ray, Hit& out) const {
         // Instances instead of the single-level path (scene.rs:489-501).
         uint32_t inst = 0;
         if (intersect_instances(ray, T_MIN, best_t, st, th, inst)) {
+            sig_event(1, ((uint64_t)inst + 1) << 32 | th.triangle);
             out = shade_instanced_triangle(th, inst, ray);
             out.steps = st.node_visits;
             return true;
@@ -111,12 +119,14 @@ bool Scene::intersect(const Ray& ray, Hit& out) const {
                                                    T_MIN, best_t, th)
                            : bvh.intersect(triangles.data(), positions.data(), ray, T_MIN, best_t, st, th);
         if (tri_hit) {
+            sig_event(1, th.triangle);
             out = shade_triangle(th, ray);
             out.steps = st.node_visits;
             return true;
         }
     }
-    if (best < 0) return false;
+    if (best < 0) return sig_event(1, ~0ull), false;
+    sig_event(1, (1ull << 62) | (uint64_t)best);
     const GpuPrimitive& prim = primitives[best];
     Vec3 position = ray.origin + best_t * ray.dir;
     bool quad = prim.kind == PRIM_KIND_QUAD;
@@ -141,15 +151,15 @@ bool Scene::occluded(const Ray& ray, float tmax) const {
         float t;
         bool h = p.kind == PRIM_KIND_QUAD ? intersect_quad(p, ray, T_MIN, tmax, t)
                                           : intersect_sphere(p, ray, T_MIN, tmax, t);
-        if (h) return true;
+        if (h) return sig_bool(2, true);
     }
-    if (!instances.empty() && !reference_instance_shadows) return occluded_instances(ray, T_MIN, tmax);
+    if (!instances.empty() && !reference_instance_shadows) return sig_bool(2, occluded_instances(ray, T_MIN, tmax));
     if (bvh.empty()) {
         TriHit th;
-        return brute_force_intersect(triangles.data(), triangles.size(), positions.data(), ray, T_MIN,
-                                     tmax, th);
+        return sig_bool(2, brute_force_intersect(triangles.data(), triangles.size(), positions.data(), ray,
+                                                 T_MIN, tmax, th));
     }
-    return bvh.occluded(triangles.data(), positions.data(), ray, T_MIN, tmax);
+    return sig_bool(2, bvh.occluded(triangles.data(), positions.data(), ray, T_MIN, tmax));
 }
 
 // integrator.rs:153-178
@@ -187,6 +197,7 @@ static Vec3 direct_light(const Scene& scene, const Surface& surf, const Hit& hit
     uint32_t total = scene.light_strategy_count();
     if (total == 0) return Vec3();
     uint32_t pick = std::min(f2u(u_select * (float)total), total - 1);
+    sig_event(5, pick);
     Vec3 wi_world, radiance;
     float distance, pdf;
     if (pick < n_lights) {
@@ -303,18 +314,26 @@ Vec3 radiance_with_guide(const Scene& scene, Ray ray, Sampler& rng, uint32_t max
             guide.steps = (float)hit.steps;
         }
         Vec3 wo = to_local(-ray.dir, hit.normal);
-        if (wo.z <= 0.0f) break;
+        if (wo.z <= 0.0f) {
+            sig_event(8, 0);
+            break;
+        }
         bool has_env = !scene.env.is_empty();
         if ((mode == LUC_SAMPLING_NEE || mode == LUC_SAMPLING_MIS) && depth + 1 < max_depth &&
             (!scene.lights.empty() || has_env)) {
-            radiance += throughput * direct_light(scene, surf, hit, wo, rng, mode);
+            Vec3 dl = direct_light(scene, surf, hit, wo, rng, mode);
+            sig_event(6, dl.max_element() > 0.0f);
+            radiance += throughput * dl;
         }
         float u_lobe = rng.next_f32();
         Vec2 u = rng.next_vec2();
         BsdfSample smp = surface_sample(surf, wo, u_lobe, u);
         if (!smp.valid()) break;
         throughput *= smp.weight;
-        if (throughput.max_element() <= 0.0f) break;
+        if (throughput.max_element() <= 0.0f) {
+            sig_event(7, 0);
+            break;
+        }
         prev_bsdf_pdf = smp.pdf;
         prev_position = hit.position;
         Vec3 dir = to_world(smp.wi, hit.normal);
@@ -368,6 +387,24 @@ void render_sums(const Scene& s, const GpuUniforms& u, uint32_t threads, std::ve
     for (uint32_t t = 1; t < threads; ++t) pool.emplace_back(worker);
     worker();
     for (auto& t : pool) t.join();
+}
+
+// One sample (pixel x, y; sample index k of the uniforms' range) traced as
+// render_sums traces it, with its path signature (g_path_sig events).
+Vec3 trace_sample(const Scene& s, const GpuUniforms& u, uint32_t x, uint32_t y, uint32_t k, uint64_t& sig) {
+    uint32_t mode = u.sampling_mode == 0 ? LUC_SAMPLING_BSDF : (u.sampling_mode == 1 ? LUC_SAMPLING_NEE : LUC_SAMPLING_MIS);
+    uint32_t kind = u.sampler_kind == LUC_SAMPLER_SOBOL ? LUC_SAMPLER_SOBOL : LUC_SAMPLER_INDEPENDENT;
+    uint32_t pixel = y * u.width + x;
+    Sampler rng(kind, u.frame_seed, pixel, u.sample_offset + k);
+    Vec2 puv = rng.next_vec2();
+    Vec2 luv = rng.next_vec2();
+    Ray ray = generate_ray(u, x, y, puv, luv);
+    GuideSample g;
+    sig = 0;
+    g_path_sig = &sig;
+    Vec3 r = radiance_with_guide(s, ray, rng, u.max_depth, mode, g);
+    g_path_sig = nullptr;
+    return r;
 }
 
 }  // namespace oracle

@@ -239,6 +239,7 @@ struct PixelSums {
 };
 void render_sums(const Scene& s, const GpuUniforms& u, uint32_t threads, std::vector<PixelSums>& out,
                  uint32_t row0, uint32_t row1, uint32_t band = 32);
+Vec3 trace_sample(const Scene& s, const GpuUniforms& u, uint32_t x, uint32_t y, uint32_t k, uint64_t& sig);
 
 // ---------------------------------------------------------------- denoise.rs
 struct DenoiseParams {

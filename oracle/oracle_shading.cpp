@@ -103,24 +103,27 @@ BsdfSample surface_sample(const Surface& s, Vec3 wo, float u_lobe, Vec2 u) {
     float alpha = roughness_to_alpha(s.roughness);
     Vec3 wi;
     if (u_lobe < p_spec) {
+        sig_event(3, 0);
         Vec3 m = sample_ggx_vndf(wo, alpha, u);
         Vec3 r = reflect(wo, m);
-        if (r.z <= 0.0f) return BsdfSample::invalid();
+        if (r.z <= 0.0f) return sig_event(4, 1), BsdfSample::invalid();
         wi = r;
     } else if (u_lobe < p_spec + (1.0f - p_spec) * s.transmission) {
+        sig_event(3, 1);
         Vec3 m = sample_ggx_vndf(wo, alpha, u);
         Vec3 wt;
-        if (!refract(wo, m, s.relative_ior, wt)) return BsdfSample::invalid();
-        if (wt.z >= 0.0f) return BsdfSample::invalid();
+        if (!refract(wo, m, s.relative_ior, wt)) return sig_event(4, 2), BsdfSample::invalid();
+        if (wt.z >= 0.0f) return sig_event(4, 3), BsdfSample::invalid();
         wi = wt;
     } else {
+        sig_event(3, 2);
         wi = sample_cosine_hemisphere(u);
     }
-    if (wi.z == 0.0f || wi == Vec3()) return BsdfSample::invalid();
-    if (wi.z < 0.0f && s.transmission <= 0.0f) return BsdfSample::invalid();
+    if (wi.z == 0.0f || wi == Vec3()) return sig_event(4, 4), BsdfSample::invalid();
+    if (wi.z < 0.0f && s.transmission <= 0.0f) return sig_event(4, 5), BsdfSample::invalid();
     Vec3 f = surface_eval(s, wo, wi);
     float pdf = surface_pdf(s, wo, wi);
-    if (pdf <= 0.0f) return BsdfSample::invalid();
+    if (pdf <= 0.0f) return sig_event(4, 6), BsdfSample::invalid();
     return BsdfSample{wi, f * (std::fabs(wi.z) / pdf), pdf};
 }
 
@@ -175,12 +178,12 @@ std::vector<GpuLight> build_lights(const std::vector<GpuMaterial>& mats,
 Vec3 EnvMap::direction_from_uv(float u, float v) {  // envmap.rs:93-99
     float theta = v * PI;
     float phi = u * TAU;
-    float st = std::sin(theta), ct = std::cos(theta);
-    return Vec3(st * std::cos(phi), ct, st * std::sin(phi));
+    float st = m_sin(theta), ct = m_cos(theta);
+    return Vec3(st * m_cos(phi), ct, st * m_sin(phi));
 }
 Vec2 EnvMap::uv_from_direction(Vec3 d) {  // :103-111
-    float theta = std::acos(clampf(d.y, -1.0f, 1.0f));
-    float a = std::atan2(d.z, d.x);
+    float theta = m_acos(clampf(d.y, -1.0f, 1.0f));
+    float a = m_atan2(d.z, d.x);
     float r = std::fmod(a, TAU);  // rem_euclid
     float phi = r < 0.0f ? r + std::fabs(TAU) : r;
     return Vec2(phi / TAU, theta / PI);

@@ -14,7 +14,7 @@ import pytest
 
 import lucida_b200 as lb
 from lucida_b200 import scenes
-from tests.bridge import compare, oracle_from_scene
+from tests.bridge import oracle_from_scene, parity
 import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -48,10 +48,7 @@ def _render_check(gpu, s, osc, label, ref_shadows=False):
     params = lb.RenderParams(width=64, height=48, samples=8, max_depth=6, sampling="mis", sampler="sobol")
     acc = lb.render_accum(gpu, s, params, uniforms=lb.layout.uniforms_from_bytes(bytes(u)),
                           reference_shadows=ref_shadows).reshape(-1)
-    st = compare(acc["radiance"], osc.render_sums(u)[:, 0:3])
-    print(label, st)
-    assert st["frac_within_1e3"] >= 0.999 and st["mean_rel"] < 1e-4, (label, st)
-    assert abs(st["energy_ratio"] - 1.0) < 1e-4, (label, st)
+    parity(acc["radiance"], osc, u, label)
 
 
 def test_device_build_is_bit_exact_and_renders_match(gpu):

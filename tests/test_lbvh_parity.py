@@ -99,13 +99,10 @@ def test_lbvh_render_matches_sah_render(gpu):
     """An acceleration structure changes speed, not the picture: the device
     LBVH (triangles compacted into its leaf order) renders the same image as
     the oracle's SAH tree (scene.rs BvhBuilder note)."""
-    from tests.bridge import compare, oracle_from_scene
+    from tests.bridge import oracle_from_scene, parity
     s = scenes.displaced_spheres(count=24, level=3, env_size=(256, 128))
     osc = oracle_from_scene(s)
     u = osc.uniforms(64, 48, 4, 5, sampler=1)
     acc = lb.render_accum(gpu, s, lb.RenderParams(width=64, height=48, samples=4, max_depth=5),
                           uniforms=lb.layout.uniforms_from_bytes(bytes(u))).reshape(-1)
-    ref = osc.render_sums(u)
-    st = compare(acc["radiance"], ref[:, 0:3])
-    print(st)
-    assert st["frac_within_1e3"] >= 0.995 and st["mean_rel"] < 5e-4, st
+    parity(acc["radiance"], osc, u, "lbvh vs sah")

@@ -10,7 +10,7 @@ import pytest
 import lucida_b200 as lb
 from lucida_b200 import scenes
 import oracle as O
-from tests.bridge import compare, scene_from_oracle
+from tests.bridge import parity, scene_from_oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -63,9 +63,7 @@ def test_megakernel_matches_the_oracle(gpu):
     u = osc.uniforms(64, 48, 16, 8, frame_seed=0x5EED1234, sampling=2, sampler=0)
     acc = lb.render_accum(gpu, s, lb.RenderParams(width=64, height=48, samples=16, max_depth=8),
                           uniforms=lb.layout.uniforms_from_bytes(bytes(u)), architecture="megakernel").reshape(-1)
-    st = compare(acc["radiance"], osc.render_sums(u)[:, 0:3])
-    print(st)
-    assert st["frac_within_1e3"] >= 0.999 and st["mean_rel"] < 1e-4, st
+    parity(acc["radiance"], osc, u, "megakernel/cornell-box")
 
 
 def test_megakernel_rejects_the_guide(gpu):

@@ -4,15 +4,16 @@ Both sides trace the same scene with the same uniforms (camera, seed,
 sampler) and the same counter-seeded streams, so they agree to float
 rounding rather than to Monte Carlo noise (crates/gpu/tests/
 cpu_gpu_agreement.rs pattern). The accumulators are compared directly
-(radiance sums in sample order, no 1/spp), with the reference's metric
-(mean relative error, image.rs:178-216) and per-pixel relative error.
+(radiance sums in sample order, no 1/spp).
 
-Tolerance: per-pixel relative error <= 1e-3 on at least 99.9% of pixels,
-mean relative error < 1e-4 (the reference asserts < 2e-3,
-cpu_gpu_agreement.rs:83-87), energy ratio within 1e-4. The residue comes
-from transcendentals: the device rounds sin/cos/acos/atan2 from a double
-evaluation, while glibc's f32 versions (which Rust calls) misround the last
-bit on ~1% of inputs; a path that grazes a silhouette can then diverge.
+Tolerance (tests.bridge.parity): per-pixel relative error <= 1e-3 on every
+pixel against the oracle whose transcendentals round like the device's
+(double evaluation, one rounding); against the oracle with glibc's f32
+functions (the reference's), the reference's metrics (mean relative error
+< 1e-4 where cpu_gpu_agreement.rs:83-87 asserts < 2e-3, energy within
+1e-4, >= 99.9% of pixels within 1e-3), every pixel beyond 1e-3 explained by
+the libm rounding alone and classified as a path flip or an amplified
+rounding from the oracle's per-sample path signatures.
 """
 import numpy as np
 import pytest
@@ -20,7 +21,7 @@ import pytest
 import oracle as O
 import lucida_b200 as lb
 from lucida_b200 import scenes
-from tests.bridge import compare, oracle_from_scene, scene_from_oracle
+from tests.bridge import oracle_from_scene, parity, scene_from_oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -40,26 +41,20 @@ def _render_both(gpu, osc, width, height, spp, depth, sampling="mis", sampler="s
     params = lb.RenderParams(width=width, height=height, samples=spp, max_depth=depth, frame_seed=seed,
                              sample_offset=offset, sampling=sampling, sampler=sampler)
     acc = lb.render_accum(gpu, s, params, uniforms=lb.layout.uniforms_from_bytes(bytes(u)))
-    ref = osc.render_sums(u)
-    return acc.reshape(-1), ref
+    return acc.reshape(-1), u
 
 
-def _check(acc, ref, label, strict=True):
-    st = compare(acc["radiance"], ref[:, 0:3])
-    print(label, st)
-    assert np.all(np.isfinite(acc["radiance"]))
-    assert st["frac_within_1e3"] >= 0.999, (label, st)
-    assert st["mean_rel"] < 1e-4, (label, st)
-    assert abs(st["energy_ratio"] - 1.0) < 1e-4, (label, st)
-    return st
+def _check(acc, osc, u, label, ref=None):
+    return parity(acc["radiance"], osc, u, label, ref_glibc=ref)
 
 
 @pytest.mark.parametrize("sampler", ["independent", "sobol"])
 def test_cornell_analytic_config(gpu, sampler):
     s = scenes.cornell_analytic()
     osc = oracle_from_scene(s)
-    acc, ref = _render_both(gpu, osc, 96, 96, 16, 8, sampler=sampler, scene=s)
-    _check(acc, ref, f"cornell-analytic/{sampler}")
+    acc, u = _render_both(gpu, osc, 96, 96, 16, 8, sampler=sampler, scene=s)
+    ref = osc.render_sums(u)
+    _check(acc, osc, u, f"cornell-analytic/{sampler}", ref)
     # The guide channels (first-hit albedo/normal/depth sums) follow the same streams.
     np.testing.assert_allclose(acc["albedo"].reshape(-1, 3), ref[:, 6:9], rtol=1e-5, atol=1e-5)
     np.testing.assert_allclose(acc["depth"].reshape(-1), ref[:, 12], rtol=1e-5, atol=1e-5)
@@ -71,8 +66,8 @@ def test_cornell_analytic_config(gpu, sampler):
 @pytest.mark.parametrize("mode", ["bsdf", "nee", "mis"])
 def test_reference_scenes(gpu, name, mode):
     osc = O.Scene.builtin(name)
-    acc, ref = _render_both(gpu, osc, 64, 48, 8, 6, sampling=mode)
-    _check(acc, ref, f"{name}/{mode}")
+    acc, u = _render_both(gpu, osc, 64, 48, 8, 6, sampling=mode)
+    _check(acc, osc, u, f"{name}/{mode}")
 
 
 @pytest.mark.parametrize("which", ["displaced-spheres", "guided-room"])
@@ -85,8 +80,8 @@ def test_triangle_workload_scenes(gpu, which):
     else:
         s = scenes.guided_room(count=24, level=3)
     osc = oracle_from_scene(s)
-    acc, ref = _render_both(gpu, osc, 64, 48, 8, 8, scene=s)
-    _check(acc, ref, which)
+    acc, u = _render_both(gpu, osc, 64, 48, 8, 8, scene=s)
+    _check(acc, osc, u, which)
 
 
 @pytest.mark.parametrize("mode", ["bsdf", "nee", "mis"])
@@ -105,7 +100,7 @@ def test_instanced_scene(gpu, mode, shadows):
     params = lb.RenderParams(width=64, height=48, samples=8, max_depth=6, sampling=mode, sampler="sobol")
     acc = lb.render_accum(gpu, s, params, uniforms=lb.layout.uniforms_from_bytes(bytes(u)),
                           reference_shadows=ref_shadows).reshape(-1)
-    _check(acc, osc.render_sums(u), f"instance-forest/{mode}/{shadows}")
+    _check(acc, osc, u, f"instance-forest/{mode}/{shadows}")
 
 
 def test_instanced_shadow_modes_differ(gpu):
@@ -145,14 +140,16 @@ def test_progressive_equals_one_shot(gpu):
 @pytest.mark.parametrize("depth", [1, 2, 4, 8, 16])
 def test_agreement_across_path_lengths(gpu, depth):
     """cpu_gpu_agreement.rs:93-117: cornell-box at max_depth 1, 2, 4, 8, 16."""
-    acc, ref = _render_both(gpu, O.Scene.builtin("cornell-box"), 48, 48, 8, depth)
-    _check(acc, ref, f"depth {depth}")
+    osc = O.Scene.builtin("cornell-box")
+    acc, u = _render_both(gpu, osc, 48, 48, 8, depth)
+    _check(acc, osc, u, f"depth {depth}")
 
 
 def test_deep_dielectric_paths(gpu):
     """cpu_gpu_agreement.rs:521-569: glass-box at max_depth 24."""
-    acc, ref = _render_both(gpu, O.Scene.builtin("glass-box"), 64, 48, 8, 24)
-    _check(acc, ref, "glass-box d24")
+    osc = O.Scene.builtin("glass-box")
+    acc, u = _render_both(gpu, osc, 64, 48, 8, 24)
+    _check(acc, osc, u, "glass-box d24")
 
 
 def test_empty_primitive_arrays(gpu):
@@ -169,7 +166,8 @@ def test_empty_primitive_arrays(gpu):
                                camera=dict(eye=s.camera.eye, look_at=s.camera.look_at, vfov_deg=s.camera.vfov_deg,
                                            up=s.camera.up, aperture=s.camera.aperture,
                                            focus_distance=s.camera.focus_distance), bvh="sah")
-    acc, ref = _render_both(gpu, bare, 48, 48, 8, 3, scene=empty)
+    acc, u = _render_both(gpu, bare, 48, 48, 8, 3, scene=empty)
+    ref = bare.render_sums(u)
     assert np.array_equal(acc["radiance"], ref[:, 0:3].reshape(acc["radiance"].shape))
 
 
