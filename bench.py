@@ -7,8 +7,8 @@ materials, lit by a procedural 1024 x 512 sky with a 0.5-degree sun of peak
 1e4 (2-D CDF importance sampling); LBVH built on the device; 1024 x 1024, 16
 spp, 8 bounces, Owen-scrambled Sobol, NEE + MIS. Synthetic, seeded inputs.
 
-One step = one full frame (1024*1024*16 = 16.8M paths) through the wavefront
-integrator into a device accumulator. `value` is device-timed (CUDA events on
+One step = one full frame (1024*1024*16 = 16.8M paths per GPU) through the
+wavefront integrator into a cleared device accumulator. `value` is device-timed (CUDA events on
 the library's stream, which is torch's current stream), L2 flushed with a
 256 MiB write before every timed step. `e2e` is the same metric through the
 public API with host buffers: every step uploads the scene from pinned host
@@ -17,9 +17,12 @@ back into pinned host memory, exactly what pt_gpu::render_with does per call.
 The roofline's per-stage times come from profiled repeats of the timed frames
 (stage events, stages in sequence), run after the timed region.
 
-Multi-GPU (--gpus N under torchrun): each rank renders the same frame with a
-disjoint sample range (sample_offset = rank * spp) — independent replicas, no
-collective on the data path; value = all ranks' paths / max-over-ranks time.
+Multi-GPU (--gpus N under torchrun): each rank renders its own sample range
+of the frame (lucida_b200.shards.shard_params: samples [rank*spp,
+(rank+1)*spp) of every pixel) and every frame the ranks' accumulators are
+merged into the frame's (merge_accumulators: an all-gather over NCCL and a
+rank-order sum) inside the timed region; value = all ranks' paths /
+max-over-ranks time.
 
 --impl reference times the reference's CPU tracer — here the oracle's C++
 restatement of crates/core's integrator, banded over every host core — on a
@@ -169,36 +172,47 @@ def build_scene(args):
     return scenes.displaced_spheres(count=args.spheres, level=args.level)
 
 
-def cpu_baseline(scene, args, target_s: float):
-    """Time the oracle (C++ restatement of the reference's CPU tracer) on a band
-    of rows of the same frame, banded over every host core. Returns a dict."""
-    import numpy as np
-    from tests.bridge import oracle_from_scene
-    t0 = time.time()
-    osc = oracle_from_scene(scene, bvh="sah")  # Scene::finalize builds the binned-SAH tree
-    prep = time.time() - t0
-    w = args.width
-    threads = os.cpu_count() or 1
-    # Calibrate on a small band of rows (one row per worker), then size the
-    # sample for ~target_s seconds. Rows go to workers one at a time so every
-    # core stays busy on a bounded sample (the reference hands out 32-row
-    # bands over a full frame; band height changes load balance, not work).
-    u = osc.uniforms(w, w, args.spp, args.depth, sampler=1)
-    y0 = w // 4
-    rows = min(threads, w - y0)
-    osc.render_sums(u, threads=threads, rows=(y0, y0 + 1), band=1)  # warms the energy table
-    t0 = time.time()
-    osc.render_sums(u, threads=threads, rows=(y0, y0 + rows), band=1)
-    dt = max(time.time() - t0, 1e-3)
-    rows = int(max(rows, min(w - y0, 0.5 * rows * target_s / dt)))
-    t0 = time.time()
-    osc.render_sums(u, threads=threads, rows=(y0, y0 + rows), band=1)
-    dt = time.time() - t0
-    paths = rows * w * args.spp
-    return {"value": paths / dt / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": "port",
-            "sample": f"rows {y0}..{y0 + rows} of the {w}x{w} frame ({paths} paths, {args.spp} spp, "
-                      f"depth {args.depth}), C++ restatement of the reference's banded CPU tracer, "
-                      f"{threads} threads, 1-row bands, SAH BVH (build {prep:.1f}s untimed)", "seconds": dt}
+class CpuBaseline:
+    """The oracle (C++ restatement of the reference's CPU tracer) on a
+    bounded sample of the same frame: image rows spaced evenly over the whole
+    height, each row one work item for a pool of every host core (the
+    reference hands 32-row bands of a full frame to its threads through an
+    atomic counter, integrator.rs:635-699; on a sample of a few dozen rows,
+    one-row items keep every core busy). The binned-SAH tree is built once,
+    untimed (Scene::finalize)."""
+
+    def __init__(self, scene, args):
+        from tests.bridge import oracle_from_scene
+        t0 = time.time()
+        self.osc = oracle_from_scene(scene, bvh="sah")
+        self.prep = time.time() - t0
+        self.args = args
+        self.threads = os.cpu_count() or 1
+        w = args.width
+        self.u = self.osc.uniforms(w, w, args.spp, args.depth, sampler=1)
+        self.osc.render_rows(self.u, [w // 2], threads=1)  # warms the energy table
+        t0 = time.time()
+        self.osc.render_rows(self.u, self.rows(self.threads), threads=self.threads)
+        self.row_s = max(time.time() - t0, 1e-3) / self.threads  # wall seconds per row on the pool
+
+    def rows(self, n):
+        import numpy as np
+        h = self.args.width
+        n = max(1, min(h, int(n)))
+        return np.unique(np.round(np.linspace(0, h - 1, n)).astype(np.uint32))
+
+    def run(self, target_s: float):
+        rows = self.rows(target_s / self.row_s)
+        t0 = time.time()
+        self.osc.render_rows(self.u, rows, threads=self.threads)
+        dt = time.time() - t0
+        a, w = self.args, self.args.width
+        paths = len(rows) * w * a.spp
+        return {"value": paths / dt / 1e6, "unit": "Mpaths/s", "cores": self.threads, "kind": "port",
+                "sample": f"{len(rows)} rows spaced evenly over the {w}x{w} frame ({paths} paths, {a.spp} spp, "
+                          f"depth {a.depth}), C++ restatement of the reference's CPU tracer on {self.threads} "
+                          f"threads, one row per work item, binned-SAH BVH (build {self.prep:.1f}s untimed)",
+                "seconds": dt}
 
 
 def config_block(args, n_tris, world):
@@ -206,7 +220,9 @@ def config_block(args, n_tris, world):
                         f"sky 1024x512 + sun, LBVH on device, {args.width}x{args.width}, {args.spp} spp, "
                         f"{args.depth} bounces, Sobol, NEE+MIS",
             "width": args.width, "height": args.width, "spp": args.spp, "max_depth": args.depth,
-            "triangles": n_tris, "parallelism": f"replicas x{world} (disjoint sample ranges)",
+            "triangles": n_tris,
+            "parallelism": f"sample-range shards x{world}" + (", accumulators merged every frame (all-gather + "
+                                                             "rank-order sum)" if world > 1 else ""),
             "l2": "flushed (256 MiB write) before every timed step; path pool of 3.5 GB streamed per bounce"}
 
 
@@ -217,14 +233,15 @@ def run_reference(args):
         return
     scene = build_scene(args)
     n_tris = len(scene.triangles)
-    # Each step: a bounded band sized so the whole run stays within minutes.
-    per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+    # Each step: a bounded sample sized so the whole run stays within minutes.
+    per_step = max(2.0, min(12.0, 90.0 / max(1, args.steps)))
+    base = CpuBaseline(scene, args)
     for _ in range(args.warmup):
-        cpu_baseline(scene, args, per_step / 4)
+        base.run(per_step / 4)
     vals, secs = [], []
     cb = None
     for _ in range(args.steps):
-        cb = cpu_baseline(scene, args, per_step)
+        cb = base.run(per_step)
         vals.append(cb["value"])
         secs.append(cb["seconds"])
     v = statistics.median(vals)
@@ -237,7 +254,8 @@ def run_reference(args):
                              "sample": cb["sample"]},
             "e2e": {"value": v, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference's Rust tracer cannot be built here (no cargo); timed is the oracle's C++ "
-                    "restatement of crates/core/src/integrator.rs with its 32-row band scheduler"}
+                    "restatement of crates/core/src/integrator.rs over every host core, on rows spaced evenly "
+                    "over the frame, one row per work item"}
     print(json.dumps(line), flush=True)
 
 
@@ -253,7 +271,8 @@ def main():
 
     import lucida_b200 as lb
     from lucida_b200 import layout as L
-    from lucida_b200.native import LUC_FLAG_NO_GUIDES, LUC_FLAG_PROFILE, check, lib
+    from lucida_b200.native import LUC_FLAG_PROFILE, check, lib
+    from lucida_b200.shards import merge_accumulators, shard_params
 
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
@@ -261,8 +280,8 @@ def main():
     n_tris = len(scene.triangles)
     W = H = args.width
     P = W * H
-    params = lb.RenderParams(width=W, height=H, samples=args.spp, max_depth=args.depth, sampler="sobol",
-                             sampling="mis", sample_offset=rank * args.spp)
+    params = shard_params(lb.RenderParams(width=W, height=H, samples=args.spp, max_depth=args.depth,
+                                          sampler="sobol", sampling="mis"), rank)
     u = lb.build_uniforms(scene, params)
 
     gpu = lb.Gpu(local)
@@ -280,8 +299,16 @@ def main():
     def render_dev(flags=0):
         check(h, lib().luc_render(h, C.byref(u), args.spp, args.depth, flags, None, C.c_void_p(acc.data_ptr())))
 
+    def frame(flags=0):
+        """One frame: this rank's sample range into a cleared accumulator,
+        then (N > 1) the ranks' accumulators merged into the frame's."""
+        acc.zero_()
+        render_dev(flags)
+        if world > 1:
+            merge_accumulators(acc, gpu)
+
     for _ in range(args.warmup):
-        render_dev()
+        frame()
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
@@ -293,7 +320,7 @@ def main():
         for k in range(args.steps):
             flush.fill_(float(k))
             ev[k][0].record(stream)
-            render_dev()
+            frame()
             ev[k][1].record(stream)
             s = gpu.stats()
             for key in counts:
@@ -327,6 +354,7 @@ def main():
                          camera=scene.camera, env_pixels=pinned(scene.env_pixels), env_cdf=pinned(scene.env_cdf),
                          env_total_weight=scene.env_total_weight)
     out_host = pinned(np.zeros(P, L.ACCUM))
+    out_t = torch.from_numpy(out_host.view(np.float32).reshape(-1))
     h2d = sum(a.nbytes for a in (pscene.materials, pscene.primitives, pscene.lights, pscene.positions,
                                  pscene.vertex_attrs, pscene.triangles, pscene.env_pixels, pscene.env_cdf))
     d2h = out_host.nbytes
@@ -336,13 +364,35 @@ def main():
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         gpu.upload(pscene, force=True)
-        check(h, lib().luc_render(h, C.byref(u), args.spp, args.depth, 0, out_host.ctypes.data_as(C.c_void_p), None))
+        if world == 1:  # pt_gpu::render_with: render and read the accumulator back
+            check(h, lib().luc_render(h, C.byref(u), args.spp, args.depth, 0, out_host.ctypes.data_as(C.c_void_p),
+                                      None))
+        else:  # this rank's samples, the merge, and the merged frame read back
+            frame()
+            out_t.copy_(acc, non_blocking=True)
         b.record(stream)
         torch.cuda.synchronize()
         if k > 0:  # the first call warms the pinned-path allocations
             e2e_ms.append(a.elapsed_time(b))
     e2e_step = max_over_ranks(statistics.median(e2e_ms), world)
     e2e_value = world * P * args.spp / (e2e_step / 1e3) / 1e6
+
+    # --- bandwidth references measured on this GPU, now: a streaming read of
+    # a 64 MiB buffer that stays L2-resident across passes (the peak the
+    # traversal's node and triangle traffic, mostly L2 hits, is set against).
+    l2_buf = torch.empty(64 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda").fill_(1.0)
+    sink = torch.zeros(148 * 8, dtype=torch.int32, device="cuda")
+    check(h, lib().luc_read_sweep(h, C.c_void_p(l2_buf.data_ptr()), l2_buf.numel() * 4, 3,
+                                  C.c_void_p(sink.data_ptr())))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    passes = 50
+    a.record(stream)
+    check(h, lib().luc_read_sweep(h, C.c_void_p(l2_buf.data_ptr()), l2_buf.numel() * 4, passes,
+                                  C.c_void_p(sink.data_ptr())))
+    b.record(stream)
+    torch.cuda.synchronize()
+    l2_gbs = l2_buf.numel() * 4 * passes / (a.elapsed_time(b) / 1e3) / 1e9
+    del l2_buf
 
     # --- roofline of the dominant kernel (EXTEND: closest-hit traversal)
     hbm, peak_kind = peaks()
@@ -352,23 +402,68 @@ def main():
     bytes_per_launch = (counts["nodes_extend"] * node_b + counts["tris_extend"] * tri_b +
                         counts["rays_extend"] * RAY_IO_BYTES) / launches_extend
     achieved = bytes_per_launch / (ext_ms / 1e3) / 1e9
-    roofline = {"kernel": "k_extend (closest-hit BVH traversal)", "bound": "hbm", "achieved": achieved,
-                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_kind,
-                "traffic": EXTEND_DRAM_BYTES_PER_RAY * counts["rays_extend"] / launches_extend if wide else None,
+    traffic = EXTEND_DRAM_BYTES_PER_RAY * counts["rays_extend"] / launches_extend if wide else None
+    dram_gbs = traffic / (ext_ms / 1e3) / 1e9 if traffic else None
+    roofline = {"kernel": "k_extend (closest-hit BVH traversal)", "bound": "l2", "achieved": achieved,
+                "peak": l2_gbs, "unit": "GB/s", "frac": achieved / l2_gbs,
+                "peak_source": "measured in this run: luc_read_sweep, 128-bit streaming reads of a 64 MiB "
+                               "L2-resident buffer, 50 passes, CUDA events",
+                "frac_l2": achieved / l2_gbs, "frac_dram": dram_gbs / hbm if dram_gbs else None,
+                "dram_gbs": dram_gbs, "frac_hbm_of_logical_bytes": achieved / hbm, "hbm_peak": hbm,
+                "hbm_peak_source": peak_kind,
+                "limiter": "instruction issue: ncu on a 512x512x4-spp frame of this scene shows 67-71% issue "
+                           "active, the ALU pipe at 47-50%, 15-18 of 32 threads active per warp instruction, "
+                           "71-76% L2 hit rate (profiles/k_extend_wide_small_case.md)",
+                "traffic": traffic,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per EXTEND ray on a 512x512x4-spp "
                                   "frame of this scene, scaled by this launch size's rays",
                 "model": f"{'wide' if wide else 'binary'} tree: node visits x {node_b} B + triangle tests x "
-                         f"{tri_b} B + rays x {RAY_IO_BYTES} B per launch (measured counters); most node bytes "
-                         "are L2 hits",
+                         f"{tri_b} B + rays x {RAY_IO_BYTES} B per launch (measured counters), against the L2 "
+                         "read bandwidth since most of those bytes are L2 hits",
                 "ms_per_launch": ext_ms, "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
                 "stage_source": "CUDA events between stages on profiled repeats of the timed frames (stages in "
                                 "sequence; the timed frames overlap each CONNECT with the next EXTEND)",
                 "per_ray": {"nodes": counts["nodes_extend"] / max(1, counts["rays_extend"]),
                             "tris": counts["tris_extend"] / max(1, counts["rays_extend"]),
                             "rays_per_path": counts["rays_extend"] / (args.steps * P * args.spp)}}
+
+    # --- wavefront queue/state traffic against HBM: the SoA path-pool fields
+    # each stage reads and writes per live path (one 16-byte float4 per
+    # field, a 4-byte queue entry), from the frame's own counters.
+    paths = args.steps * P * args.spp
+    re, rs = counts["rays_extend"], counts["rays_shadow"]
+    survivors = re - paths  # every path extended after the first bounce survived a SHADE
+    state = {
+        # o_pdf, dir, thr, rad, prev (+ galb, gnrm: first-hit guides) written
+        "generate": paths * (5 * 16 + 2 * 16),
+        # queue entry (not at depth 0) + origin + direction read, hit written
+        "extend": re * RAY_IO_BYTES - paths * 4,
+        # read: queue, o_pdf, dir, hit, thr, rad; written: rad, and for
+        # survivors o_pdf, dir, thr, prev + next-queue entry; guides at the
+        # first hit; each shadow ray's origin, direction, contribution
+        "shade": (re * (4 + 5 * 16) - paths * 4) + re * 16 + survivors * (4 * 16 + 4) + paths * 32 + rs * 48,
+        # shadow origin + direction read (lower bound: an unoccluded ray also
+        # reads its contribution and adds it to the path's radiance, 48 B)
+        "connect": rs * 32,
+        # per path radiance + guides read; per pixel the accumulator r/w
+        "resolve": paths * 48 + args.steps * P * 128,
+    }
+    stage_state = {"unit": "GB/s", "hbm_peak": hbm,
+                   "bytes_per_live_path_bounce": sum(state.values()) / max(1, re),
+                   "model": "SoA path-pool fields read and written per live path by each stage (16 B per float4 "
+                            "field, 4 B queue entries), from the frame's ray counters; CONNECT counts only the "
+                            "shadow ray read (a lower bound)"}
+    for k, v in state.items():
+        t = stage[k] / 1e3
+        stage_state[k] = {"bytes_per_step": v / args.steps, "gbs": v / t / 1e9 if t > 0 else None,
+                          "frac_hbm": v / t / 1e9 / hbm if t > 0 else None}
+    frame_s = sum(stage.values()) / 1e3
+    stage_state["frame"] = {"bytes_per_step": sum(state.values()) / args.steps,
+                            "gbs": sum(state.values()) / frame_s / 1e9,
+                            "frac_hbm": sum(state.values()) / frame_s / 1e9 / hbm}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline(scene, args, args.cpu_seconds)
+        cb = CpuBaseline(scene, args).run(args.cpu_seconds)
         cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
@@ -378,9 +473,12 @@ def main():
                 "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_step,
                         "includes": "scene upload from pinned host memory + device LBVH rebuild + render + "
-                                    "accumulator readback (pt_gpu::render_with per call)"},
+                                    "accumulator readback (pt_gpu::render_with per call); with N > 1 each "
+                                    "rank's sample range, the accumulator merge (all-gather + rank-order "
+                                    "sum), then the merged frame read back"},
                 "gpu_launches": int(counts["launches"]),
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
+                "roofline": roofline, "stage_state": stage_state, "cpu_baseline": cpu,
+                "clocks": clocks.summary(),
                 "scene_upload_s": upload_s}
         print(json.dumps(line), flush=True)
     gpu.close()

@@ -67,6 +67,11 @@ extern "C" {
  * crates/gpu/src/lib.rs:86-97). */
 #define LUC_FLAG_MEASURE 0x1000u
 
+/* Test hooks for the bounded device waits (luc_debug_waits). */
+#define LUC_DEBUG_NONE 0u
+#define LUC_DEBUG_SORT_ORPHAN_TILE 1u /* next radix sort: tile 0 never runs, tile 1's look-back waits on it */
+#define LUC_DEBUG_TC_NO_COMMIT 2u     /* next tensor-core guide forward: no MMA issued, no commit to the mbarrier */
+
 typedef struct luc_ctx luc_ctx;
 
 /* The SceneBlob upload (crates/core/src/gpu_layout.rs:706-770 plus the
@@ -231,6 +236,28 @@ int32_t luc_intersect(luc_ctx* ctx, const float* rays8, uint32_t n, int32_t mode
  * pixels with >= 2 samples and mean luminance > 1e-3 (-1 if none). Assumes
  * independent samples: with Sobol it over-reports. */
 int32_t luc_convergence(luc_ctx* ctx, const void* accum_dev, uint32_t pixels, float* out);
+/* Bandwidth reference (no reference counterpart; the benchmark's roofline
+ * denominator for L2-resident traffic): `passes` streaming reads of `bytes`
+ * (a multiple of 16, 16-byte aligned) of caller device memory on the ctx's
+ * stream, asynchronous. sink_dev: 148 * 8 u32 the kernel XORs into. Over a
+ * buffer that fits and stays in L2 it measures L2 read bandwidth. */
+int32_t luc_read_sweep(luc_ctx* ctx, const void* buf_dev, uint64_t bytes, uint32_t passes, void* sink_dev);
+/* Test hook (no reference counterpart): make the next call of one kind wait
+ * on a flag nothing sets, so its bounded wait runs out after `limit` polls
+ * and the call returns its error status (a radix sort: LUC_ERR_VALIDATION,
+ * "look-back wait gave up"; luc_guide_forward: LUC_ERR_LAUNCH, "a
+ * tensor-core wait ran out"), with the context usable afterwards. Nothing
+ * faults or hangs: the waits are the kernels' own bounded loops, and no
+ * tensor-core work is left in flight. One-shot; LUC_DEBUG_NONE cancels. */
+int32_t luc_debug_waits(luc_ctx* ctx, uint32_t mode, uint32_t limit);
+/* Sample-range shards (crates/gpu/tests/cpu_gpu_agreement.rs:119-168: a
+ * progressive render equals a one-shot one, so per-rank accumulators over
+ * disjoint sample ranges sum to the frame's): out[px] = parts[0][px] +
+ * parts[1][px] + ... field by field, in rank order, on the ctx's stream
+ * (asynchronous). parts_dev: nparts consecutive arrays of `pixels` GpuAccum
+ * (device, 16-byte aligned), e.g. the output of an all-gather; out_dev may
+ * alias parts_dev's first array. */
+int32_t luc_accum_merge(luc_ctx* ctx, const void* parts_dev, uint32_t nparts, uint32_t pixels, void* out_dev);
 
 /* Sort without allocating: the variant of luc_sort_u32_dev for callers that
  * cannot call cudaMalloc (a host that reserves all device memory up front, or

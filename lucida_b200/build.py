@@ -20,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "liblucida_cuda.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["capi.cu", "wavefront.cu", "lbvh.cu", "denoise.cu", "sort_static.cu", "eval.cu", "guide.cu", "instances.cu", "batch.cu", "wide.cu", "megakernel.cu", "stats.cu", "guide_tc.cu"]
+SOURCES = ["capi.cu", "wavefront.cu", "lbvh.cu", "denoise.cu", "sort_static.cu", "eval.cu", "guide.cu", "instances.cu", "batch.cu", "wide.cu", "megakernel.cu", "stats.cu", "guide_tc.cu", "shards.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
          "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-warn-spills"]

@@ -185,6 +185,15 @@ void luc_destroy(luc_ctx* c) {
 
 const char* luc_last_error(const luc_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
+int32_t luc_debug_waits(luc_ctx* c, uint32_t mode, uint32_t limit) {
+    if (!c) return LUC_ERR_VALIDATION;
+    if (mode != LUC_DEBUG_NONE && mode != LUC_DEBUG_SORT_ORPHAN_TILE && mode != LUC_DEBUG_TC_NO_COMMIT)
+        return luc_fail(c, LUC_ERR_VALIDATION, "debug waits: unknown mode");
+    c->dbg_mode = mode;
+    c->dbg_limit = limit;
+    return LUC_OK;
+}
+
 int32_t luc_set_stream(luc_ctx* c, void* stream) {
     if (!c) return LUC_ERR_VALIDATION;
     c->stream = stream ? (cudaStream_t)stream : c->own_stream;

@@ -38,6 +38,10 @@ struct FrameGraph {
 
 struct luc_ctx {
     int device = 0;
+    // Test hook (luc_debug_waits): the next radix sort's or tensor-core
+    // forward's bounded wait is made to run out after dbg_limit polls of a
+    // flag nothing sets. One-shot: the call that uses it clears dbg_mode.
+    uint32_t dbg_mode = 0, dbg_limit = 0;
     FrameGraph graph;
     bool use_graphs = true;
     cudaStream_t own_stream = nullptr;

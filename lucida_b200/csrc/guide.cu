@@ -818,6 +818,8 @@ GuideDev luc_guide_dev(const luc_ctx* c) {
     GuideDev g{};
     g.wbf = c->g_wbf.as<uint16_t>();
     g.bias = c->g_bias.as<float>();
+    g.tc_wait_limit = kTcWaitLimit;
+    g.tc_no_issue = 0;
     for (int a = 0; a < 3; ++a) {
         g.lo[a] = c->guide_lo[a];
         g.ext[a] = c->guide_hi[a] > c->guide_lo[a] ? c->guide_hi[a] - c->guide_lo[a] : 1.0f;
@@ -973,8 +975,14 @@ int32_t luc_guide_forward_ex(luc_ctx* c, const float* in9, uint32_t n, int32_t p
     LUC_CUDA(c, cudaMemcpyAsync(din, in9, (size_t)n * 9 * sizeof(float), cudaMemcpyHostToDevice, s), "upload");
     uint32_t* err = c->g_misc.as<uint32_t>() + kGmTcError;
     if (path == 0) {
+        GuideDev g = luc_guide_dev(c);
+        if (c->dbg_mode == LUC_DEBUG_TC_NO_COMMIT) {  // test hook: a wait that runs out
+            g.tc_no_issue = 1;
+            g.tc_wait_limit = c->dbg_limit;
+            c->dbg_mode = 0;
+        }
         LUC_CUDA(c, cudaMemsetAsync(err, 0, 4, s), "clear error word");
-        LUC_CUDA(c, launch_guide_forward_tc(din, n, luc_guide_dev(c), dout, err, c->num_sms, s), "guide forward");
+        LUC_CUDA(c, launch_guide_forward_tc(din, n, g, dout, err, c->num_sms, s), "guide forward");
     } else {
         int grid = (int)std::min<uint64_t>((n + 16 * kInferWarps - 1) / (16 * kInferWarps), (uint64_t)c->num_sms * 2);
         k_guide_forward<<<grid, kInferWarps * 32, sizeof(InferSmem), s>>>(din, n, luc_guide_dev(c), dout);

@@ -45,10 +45,15 @@ constexpr int kGmWords = 16;
 //   [3] sampled direction (world), throughput .z
 //   [4] path radiance when the continuation started, mixture pdf p(wi)
 
+// Polls of a tensor-core kernel's mbarrier before its wait gives up.
+constexpr uint32_t kTcWaitLimit = 1u << 22;
+
 struct GuideDev {
     const uint16_t* wbf;   // packed bf16 weights
     const float* bias;     // packed fp32 biases
     float lo[3], ext[3];  // scene box for the position encoding (ext = hi - lo, or 1)
+    uint32_t tc_wait_limit;  // kTcWaitLimit (a test hook lowers it)
+    uint32_t tc_no_issue;    // test hook: issue no MMA and no commit, so the wait runs out
 };
 
 // 32-bit integer mix (Wellons' "lowbias32" constants) for record selection.

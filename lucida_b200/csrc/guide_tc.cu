@@ -35,7 +35,6 @@ constexpr uint32_t kLboH = kGHid * 16;         // B tiles of 64 output units
 constexpr uint32_t kLboO = kGOutPad * 16;      // B tile of the 48 (40 used) output units
 constexpr uint32_t kSbo = 128;                 // 8 rows of 16 B
 constexpr uint32_t kTmemCols = 64;
-constexpr uint32_t kWaitLimit = 1u << 22;
 
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -62,8 +61,8 @@ __device__ __forceinline__ void commit(uint32_t mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                  : "memory");
 }
-__device__ __forceinline__ bool wait_phase(uint32_t mbar, uint32_t phase) {
-    for (uint32_t i = 0; i < kWaitLimit; ++i) {
+__device__ __forceinline__ bool wait_phase(uint32_t mbar, uint32_t phase, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i) {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred P1;\n\t"
@@ -208,13 +207,13 @@ __device__ void forward_teams(uint32_t n, const GuideDev& g, uint32_t* err, Load
         fence_before();
         team_sync(team);
         fence_after();
-        if (tt == 0) {
+        if (tt == 0 && !g.tc_no_issue) {
             for (int ks = 0; ks < ksteps; ++ks)
                 mma(tcol, desc(saddr(region) + 2 * ks * kLboA, kLboA), desc(saddr(w) + 2 * ks * lbw, lbw), idesc(nout),
                     (fresh && ks == 0) ? 0u : 1u);
             commit(mbar);
         }
-        const bool ok = wait_phase(mbar, phase);
+        const bool ok = wait_phase(mbar, phase, g.tc_wait_limit);
         phase ^= 1u;
         fence_after();
         // The team votes on the outcome (threads time out independently),

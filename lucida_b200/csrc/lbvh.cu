@@ -177,7 +177,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint32_t* __
                                                            const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
                                                            uint32_t* __restrict__ vout, uint32_t n, int shift,
                                                            const uint32_t* __restrict__ digit_offsets,
-                                                           uint32_t* status, uint32_t* tile_counter, uint32_t* err) {
+                                                           uint32_t* status, uint32_t* tile_counter, uint32_t* err,
+                                                           uint32_t spin_limit) {
     __shared__ uint32_t s_tile;
     __shared__ uint32_t whist[kSortThreads / 32][256];
     __shared__ uint32_t s_base[256];   // global start of each digit's run from this tile
@@ -226,7 +227,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint32_t* __
             uint32_t s = st[(size_t)j * 256 + tid];
             uint32_t flag = s & ~kCountMask;
             if (flag == 0) {
-                if (++spins > kSpinLimit) {  // bounded wait: report, never hang
+                if (++spins > spin_limit) {  // bounded wait: report, never hang
                     atomicExch(err, 1u);
                     break;
                 }
@@ -441,19 +442,32 @@ int32_t luc_radix_sort_device(luc_ctx* c, uint32_t n) {
     LUC_CUDA(c, c->lb_keys2.ensure((size_t)n * 4), "alloc sort");
     LUC_CUDA(c, c->lb_vals2.ensure((size_t)n * 4), "alloc sort");
     LUC_CUDA(c, c->lb_hist.ensure((4 * 256 + 4 * 256 + 8) * 4), "alloc sort");
-    LUC_CUDA(c, c->lb_look.ensure((size_t)tiles * 256 * 4), "alloc sort");
+    // One status row more than the tiles: the look-back test hook (below)
+    // numbers the tiles from 1.
+    LUC_CUDA(c, c->lb_look.ensure((size_t)(tiles + 1) * 256 * 4), "alloc sort");
     uint32_t* hist = c->lb_hist.as<uint32_t>();
     uint32_t* offs = hist + 1024;
     uint32_t* tcount = hist + 2048;  // [0..3] one tile counter per pass, [4] error flag
     cudaMemsetAsync(hist, 0, (2048 + 8) * 4, s);
+    // Test hook (luc_debug_waits, LUC_DEBUG_SORT_ORPHAN_TILE): the first
+    // pass's tile counter starts at 1, so tile 0 never runs and tile 1's
+    // look-back waits on a flag nothing sets until `spin` polls run out.
+    uint32_t spin = kSpinLimit;
+    if (c->dbg_mode == LUC_DEBUG_SORT_ORPHAN_TILE) {
+        const uint32_t one = 1;
+        LUC_CUDA(c, cudaMemcpyAsync(tcount, &one, 4, cudaMemcpyHostToDevice, s), "debug tile counter");
+        LUC_CUDA(c, cudaStreamSynchronize(s), "debug tile counter");
+        spin = c->dbg_limit;
+        c->dbg_mode = 0;
+    }
     k_hist4<<<grid_for(n, 256, c->num_sms), 256, 0, s>>>(c->lb_keys.as<uint32_t>(), n, hist);
     k_hist_scan<<<1, 256, 0, s>>>(hist, offs);
     uint32_t *ka = c->lb_keys.as<uint32_t>(), *va = c->lb_vals.as<uint32_t>();
     uint32_t *kb = c->lb_keys2.as<uint32_t>(), *vb = c->lb_vals2.as<uint32_t>();
     for (int p = 0; p < 4; ++p) {
-        cudaMemsetAsync(c->lb_look.p, 0, (size_t)tiles * 256 * 4, s);
+        cudaMemsetAsync(c->lb_look.p, 0, (size_t)(tiles + 1) * 256 * 4, s);
         k_onesweep<<<tiles, kSortThreads, 0, s>>>(ka, va, kb, vb, n, 8 * p, offs + 256 * p, c->lb_look.as<uint32_t>(),
-                                                   tcount + p, tcount + 4);
+                                                   tcount + p, tcount + 4, p == 0 ? spin : kSpinLimit);
         std::swap(ka, kb);
         std::swap(va, vb);
     }

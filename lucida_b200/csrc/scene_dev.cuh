@@ -713,6 +713,20 @@ LUC_D void analytic_closest(const DevScene& s, V3 o, V3 d, float& best_t, uint32
     }
 }
 
+// Any hit among the analytic primitives in (kTMin, tmax): the first loop of
+// Scene::occluded (scene.rs:577-606).
+LUC_D bool analytic_any(const DevScene& s, V3 o, V3 d, float tmax) {
+    for (uint32_t i = 0; i < s.num_prims; ++i) {
+        const GpuPrimitive& p = s.prims[i];
+        float th;
+        bool h = p.kind == PRIM_KIND_QUAD
+                     ? hit_quad(ld3(p.position), ld3(p.edge_u), ld3(p.edge_v), ld3(p.normal), o, d, kTMin, tmax, th)
+                     : hit_sphere(ld3(p.position), p.radius, o, d, kTMin, tmax, th);
+        if (h) return true;
+    }
+    return false;
+}
+
 template <bool kInst, int kWide = 2>
 LUC_D uint32_t closest_hit(const DevScene& s, V3 o, V3 d, float& t, float& u, float& v, uint32_t& inst,
                            TravCount& tc) {

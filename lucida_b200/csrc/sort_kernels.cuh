@@ -16,10 +16,12 @@ __global__ void k_hist4(const uint32_t* __restrict__ keys, uint32_t n, uint32_t*
 // Exclusive scan of each pass's 256 counts into offsets (one block of 256 threads).
 __global__ void k_hist_scan(const uint32_t* __restrict__ hist, uint32_t* __restrict__ offsets);
 // One stable pass over digit (key >> shift) & 255; `status` (tiles x 256) and
-// `tile_counter` must be zero on entry; *err is set if a look-back wait gives up.
+// `tile_counter` must be zero on entry; *err is set if a look-back wait gives
+// up after `spin_limit` polls of a predecessor that has not published
+// (kSpinLimit in every product call).
 __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                            uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t n, int shift,
                            const uint32_t* __restrict__ digit_offsets, uint32_t* status, uint32_t* tile_counter,
-                           uint32_t* err);
+                           uint32_t* err, uint32_t spin_limit);
 
 }  // namespace luc

@@ -110,7 +110,7 @@ extern "C" int32_t luc_sort_u32_static(void* keys_dev, void* vals_dev, uint32_t 
         e = cudaMemsetAsync(sa.status, 0, (size_t)tiles * 256 * sizeof(uint32_t), s);
         if (e == cudaSuccess)
             e = launch(k_onesweep, tiles, kSortThreads, s, (const uint32_t*)ka, (const uint32_t*)va, kb, vb, n,
-                       8 * p, (const uint32_t*)(offs + 256 * p), sa.status, tcount + p, tcount + 4);
+                       8 * p, (const uint32_t*)(offs + 256 * p), sa.status, tcount + p, tcount + 4, kSpinLimit);
         std::swap(ka, kb);
         std::swap(va, vb);
     }

@@ -206,6 +206,61 @@ __global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_extend_
     flush_counts(ps.stat, rays, tc);
 }
 
+// CONNECT on the wide tree of a single-level scene with the same dynamic
+// ray fetch as k_extend_dyn: any-hit walks end at their first hit, so their
+// lengths vary even more than closest-hit walks, and a warp that waited for
+// its longest shadow ray idled most of its lanes. Each ray's walk is
+// wide_trace<true>'s (WideWalk), after the analytic primitives (occluded()'s
+// order), so the visibility and the counters are the same.
+template <int kThreads, int kRefill>
+__global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_connect_dyn(PathState ps,
+                                                                                     const __grid_constant__ DevScene sc,
+                                                                                     uint32_t depth) {
+    const uint32_t len = ps.ctr[depth * kCtrStride + kCtrShadow];
+    uint32_t* pull = ps.ctr + depth * kCtrStride + kCtrPullConnect;
+    const uint32_t lane = threadIdx.x & 31u, below = (1u << lane) - 1u;
+    TravCount tc;
+    uint32_t rays = 0, slot = 0;
+    bool live = false, exhausted = false;
+    WideWalk w;
+    auto finish = [&](bool occluded) {
+        if (!occluded) {
+            const uint32_t p = __float_as_uint(ld4(ps.sh_d + slot).w);
+            const float4 c4 = ld4(ps.sh_c + slot), r4 = ld4(ps.rad + p);
+            __stcs(ps.rad + p, make_float4(r4.x + c4.x, r4.y + c4.y, r4.z + c4.z, 0.0f));
+        }
+        ++rays;
+        live = false;
+    };
+    for (;;) {
+        const uint32_t need = __ballot_sync(0xFFFFFFFFu, !live);
+        if (!exhausted && __popc(need) >= kRefill) {
+            const uint32_t leader = __ffs(need) - 1u, n = __popc(need);
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(pull, n);
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            exhausted = base + n >= len;
+            if (!live) {
+                const uint32_t i = base + __popc(need & below);
+                if (i < len) {
+                    slot = i;
+                    const float4 o4 = ld4(ps.sh_o + i), d4 = ld4(ps.sh_d + i);
+                    const V3 o = xyz(o4), d = xyz(d4);
+                    live = true;
+                    if (analytic_any(sc, o, d, o4.w)) finish(true);
+                    else w.begin(0u, o, d, o4.w);
+                }
+            }
+        }
+        if (__ballot_sync(0xFFFFFFFFu, live) == 0) {
+            if (exhausted) break;
+            continue;
+        }
+        if (live && w.step<true>(sc, kTMin, tc)) finish(w.found);
+    }
+    flush_counts(ps.stat + 3, rays, tc);
+}
+
 // Warp-aggregated append: one atomicAdd per warp. Every lane of the warp must
 // call this (it uses full-warp ballots).
 __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
@@ -530,7 +585,7 @@ void query_occupancy(RenderState& rs) {
         return b > 0 ? b : 8;
     };
     rs.extend_blocks = occ((const void*)k_extend_dyn<128, kExtendRefill>);
-    rs.connect_blocks = occ((const void*)k_connect<false, false, 128, 1>);
+    rs.connect_blocks = occ((const void*)k_connect_dyn<128, kExtendRefill>);
     rs.extend_blocks_bin = occ((const void*)k_extend<false, false, 128, 0>);
     rs.connect_blocks_bin = occ((const void*)k_connect<false, false, 128, 0>);
     rs.shade_blocks = occ((const void*)k_shade<false, false>);
@@ -621,7 +676,7 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
                 k_connect<true, false, 128, 0><<<sms * rs.connect_blocks_inst_bin, 128, 0, cs>>>(rs.ps, sc,
                                                                                                  BatchDev{}, d);
             else if (wide)
-                k_connect<false, false, 128, 1><<<sms * rs.connect_blocks, 128, 0, cs>>>(rs.ps, sc, BatchDev{}, d);
+                k_connect_dyn<128, kExtendRefill><<<sms * rs.connect_blocks, 128, 0, cs>>>(rs.ps, sc, d);
             else
                 k_connect<false, false, 128, 0><<<sms * rs.connect_blocks_bin, 128, 0, cs>>>(rs.ps, sc, BatchDev{}, d);
             rs.launches++;

@@ -6,7 +6,20 @@ room lit by two 0.2 x 0.2 emitters of radiance 200), 1024 x 1024, 8 bounces.
                                       [--ref-cache PATH] [--out JSON]
 
 The reference is a plain render of --ref-spp samples per pixel (Sobol, its
-own scrambling seed), cached as .npy at --ref-cache. Then, for every time
+own scrambling seed), cached as .npy at --ref-cache.
+
+Time to target (--target-spp, default 64): the wall-clock time plain
+rendering takes to accumulate --target-spp samples per pixel, and its MSE
+against the reference (the target); then, from a fresh guide, the wall-clock
+time guided rendering (1-spp batches, one Adam step after each) takes until
+its accumulated image first reaches that MSE. The error is evaluated after
+every batch on the device, with the clock stopped. Optionally the guide first
+trains on --warmup-frames guided frames at --warmup-res x --warmup-res (they
+produce records, not image samples), which counts toward the guided time.
+The ratio plain / guided is the speed-up to equal error (>= 2 is the target
+the guided form is measured against).
+
+Then, for every time
 budget T (seconds of wall clock, each call synchronised), a plain render and a
 guided render (a fresh guide, one Adam step on up to 2^18 path vertices after
 every 1-spp batch) run until T has elapsed; both accumulate on the device and
@@ -35,7 +48,7 @@ def parse(argv=None):
     ap.add_argument("--width", type=int, default=1024)
     ap.add_argument("--height", type=int, default=1024)
     ap.add_argument("--depth", type=int, default=8)
-    ap.add_argument("--budgets", type=float, nargs="+", default=[2.0, 8.0, 32.0])
+    ap.add_argument("--budgets", type=float, nargs="*", default=[2.0, 8.0, 32.0])
     ap.add_argument("--ref-spp", type=int, default=65536)
     ap.add_argument("--ref-batch", type=int, default=16)
     ap.add_argument("--ref-cache", default=None)
@@ -45,6 +58,11 @@ def parse(argv=None):
     ap.add_argument("--lr", type=float, default=1e-2)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--level", type=int, default=4)
+    ap.add_argument("--target-spp", type=int, default=64)
+    ap.add_argument("--target-max-factor", type=float, default=8.0,
+                    help="give up on the guided run after this multiple of plain's time to target")
+    ap.add_argument("--warmup-frames", type=int, default=0)
+    ap.add_argument("--warmup-res", type=int, default=256)
     ap.add_argument("--out", default=None)
     return ap.parse_args(argv)
 
@@ -86,6 +104,67 @@ def _timed(frame, budget, batch, flags):
     return n, time.perf_counter() - t0
 
 
+def _device_mse(frame, ref_dev):
+    """MSE of the frame's accumulated image against the reference, on the device."""
+    a = frame.acc.view(frame.pixels, 16)
+    img = a[:, 0:3] / a[:, 3:4].clamp(min=1.0)
+    return float(((img.double() - ref_dev) ** 2).mean())
+
+
+def _time_to_target(args, scene, gpu, ft, ref, guide):
+    import torch
+    ref_dev = torch.from_numpy(ref.reshape(-1, 3)).cuda()
+    # Plain: --target-spp samples in the plain batches, timed, then its error.
+    ft.clear()
+    t0 = time.perf_counter()
+    n = 0
+    while n < args.target_spp:
+        b = min(args.plain_batch, args.target_spp - n)
+        ft.render(b, n, 0)
+        n += b
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    target = _device_mse(ft, ref_dev)
+    # Guided: a fresh guide; optional low-resolution training frames first.
+    guide.reset(seed=args.seed)
+    guide.configure(train=True, records_per_step=args.records, lr=args.lr)
+    warm = None
+    if args.warmup_frames > 0:
+        wp = RenderParams(width=args.warmup_res, height=args.warmup_res, samples=1, max_depth=args.depth,
+                          sampler="sobol", frame_seed=0x0BADCAFE)
+        warm = _Frame(gpu, build_uniforms(scene, wp), args.warmup_res, args.warmup_res, args.depth)
+        warm.render(1, 0, LUC_FLAG_GUIDED)  # capture the graph outside the clock
+        guide.reset(seed=args.seed)
+        guide.configure(train=True, records_per_step=args.records, lr=args.lr)
+    ft.clear()
+    elapsed, n, trace = 0.0, 0, []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(args.warmup_frames):
+        warm.render(1, k, LUC_FLAG_GUIDED)
+    torch.cuda.synchronize()
+    warm_s = time.perf_counter() - t0
+    elapsed += warm_s
+    reached = None
+    while elapsed < args.target_max_factor * t_plain:
+        t0 = time.perf_counter()
+        ft.render(args.guided_batch, n, LUC_FLAG_GUIDED)
+        torch.cuda.synchronize()
+        elapsed += time.perf_counter() - t0
+        n += args.guided_batch
+        e = _device_mse(ft, ref_dev)  # clock stopped
+        trace.append((round(elapsed, 4), n, e))
+        if e <= target:
+            reached = elapsed
+            break
+    return {"target_spp": args.target_spp, "plain_seconds": round(t_plain, 4), "target_mse": target,
+            "guided_seconds": None if reached is None else round(reached, 4), "guided_spp": n,
+            "warmup_frames": args.warmup_frames, "warmup_res": args.warmup_res, "warmup_seconds": round(warm_s, 4),
+            "speedup_plain_over_guided": None if reached is None else t_plain / reached,
+            "gave_up_after_s": None if reached is not None else round(elapsed, 4),
+            "trace_every_8": trace[::8]}
+
+
 def _errors(img, ref):
     d = (img.astype(np.float64) - ref) ** 2
     return {"mse": float(d.mean()), "relmse": float((d / (ref * ref + 1e-2)).mean())}
@@ -124,6 +203,10 @@ def main(argv=None):
     # Warm both paths once (graph capture, allocations) outside the budgets.
     ft.render(args.plain_batch, 0, 0)
     ft.render(args.guided_batch, 0, LUC_FLAG_GUIDED)
+    ttt = _time_to_target(args, scene, gpu, ft, ref, guide) if args.target_spp > 0 else None
+    if ttt:
+        print(json.dumps({"time_to_target": {k: v for k, v in ttt.items() if k != "trace_every_8"}}),
+              file=sys.stderr)
     rows = []
     for T in args.budgets:
         n_p, t_p = _timed(ft, T, args.plain_batch, 0)
@@ -142,7 +225,7 @@ def main(argv=None):
         print(json.dumps(rows[-1]), file=sys.stderr)
     out = {"workload": f"guided-room {args.width}x{args.height} d{args.depth} ({len(scene.triangles)} triangles)",
            "ref_spp": args.ref_spp, "ref_seconds": ref_seconds, "ref_mean": float(ref.mean()),
-           "records_per_step": args.records, "lr": args.lr, "budgets": rows}
+           "records_per_step": args.records, "lr": args.lr, "time_to_target": ttt, "budgets": rows}
     line = json.dumps(out)
     print(line)
     if args.out:

@@ -22,6 +22,7 @@ LUC_FLAG_PROFILE = 0x200
 LUC_FLAG_GUIDED = 0x400
 LUC_FLAG_REFERENCE_SHADOWS = 0x800
 LUC_FLAG_MEASURE = 0x1000
+LUC_DEBUG_NONE, LUC_DEBUG_SORT_ORPHAN_TILE, LUC_DEBUG_TC_NO_COMMIT = 0, 1, 2
 LUC_ARCH_WAVEFRONT = 0x0
 LUC_ARCH_MEGAKERNEL = 0x1
 LUC_DENOISE_HALF_GUIDES = 0x1
@@ -107,6 +108,9 @@ _SIGS = {
                                  C.c_void_p]),
     "luc_intersect": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p]),
     "luc_convergence": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "luc_read_sweep": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
+    "luc_accum_merge": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
+    "luc_debug_waits": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "luc_sort_u32_static": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_char_p,
                                         C.c_uint32]),
     "luc_sort_u32_static_max": (C.c_uint32, []),

@@ -88,6 +88,7 @@ def lib():
         L.orc_instance_world_bounds.argtypes = [vp, vp, vp]
         L.orc_build_uniforms.argtypes = [vp, u32, u32, u32, u32, u32, u32, u32, u32, vp]
         L.orc_render_sums.argtypes = [vp, vp, u32, u32, u32, u32, vp]
+        L.orc_render_row_list.argtypes = [vp, vp, u32, vp, u32, vp]
         L.orc_set_libm_mode.argtypes = [i32]
         L.orc_get_libm_mode.restype = i32
         L.orc_sample_traces.argtypes = [vp, vp, vp, u32, u32, vp, vp]
@@ -276,6 +277,15 @@ class Scene:
         out = np.zeros(((r1 - r0) * u.width, 13), np.float32)
         with libm_mode(libm):
             lib().orc_render_sums(self._h, C.byref(u), threads, r0, r1, band, _p(out))
+        return out
+
+    def render_rows(self, u: Uniforms, rows, threads: int = 0) -> np.ndarray:
+        """render_sums over an explicit list of image rows, one row per work item over `threads`
+        workers (0 = every core); (len(rows) * width, 13), rows in list order."""
+        rows = np.ascontiguousarray(rows, np.uint32).reshape(-1)
+        assert rows.size == 0 or int(rows.max()) < u.height
+        out = np.zeros((len(rows) * u.width, 13), np.float32)
+        lib().orc_render_row_list(self._h, C.byref(u), threads, _p(rows), len(rows), _p(out))
         return out
 
     def sample_traces(self, u: Uniforms, pixels, libm: str = "glibc", threads: int = 0):

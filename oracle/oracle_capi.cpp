@@ -220,6 +220,36 @@ void orc_render_sums(void* h, const GpuUniforms* u, uint32_t threads, uint32_t r
     }
 }
 
+// render_sums over an explicit list of image rows (each row one work item,
+// handed to `threads` workers through an atomic counter): a bounded sample
+// of a frame spread over its whole height. Output rows in list order.
+void orc_render_row_list(void* h, const GpuUniforms* u, uint32_t threads, const uint32_t* rows, uint32_t nrows,
+                         float* out) {
+    const Scene& s = *(Scene*)h;
+    std::atomic<uint32_t> next{0};
+    auto worker = [&] {
+        std::vector<PixelSums> ps;
+        for (;;) {
+            uint32_t i = next.fetch_add(1);
+            if (i >= nrows) break;
+            render_sums(s, *u, 1, ps, rows[i], rows[i] + 1, 1);
+            for (uint32_t x = 0; x < u->width; ++x) {
+                float* o = out + 13 * ((size_t)i * u->width + x);
+                ps[x].radiance.to(o);
+                ps[x].radiance_sq.to(o + 3);
+                ps[x].albedo.to(o + 6);
+                ps[x].normal.to(o + 9);
+                o[12] = ps[x].depth;
+            }
+        }
+    };
+    if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < threads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+}
+
 // Render-time transcendental rounding: 0 = glibc f32 (the reference), 1 =
 // double evaluation rounded once (the CUDA integrator's). Call between renders.
 void orc_set_libm_mode(int mode) { g_libm_mode = mode ? 1 : 0; }

@@ -1,14 +1,18 @@
 """Two ranks over gloo on the CPU: the sample-range sharding `bench.py
 --gpus N` runs (one process per GPU, rank r renders samples
-[r*spp, (r+1)*spp) of every pixel, no exchange on the data path).
+[r*spp, (r+1)*spp) of every pixel) and the product's one exchange,
+lucida_b200.shards.merge_accumulators (all-gather of the accumulators, then
+a rank-order sum).
 
 The reference's RNG is a pure function of (frame, pixel, sample)
 (crates/core/src/rng.rs:18-21) and a progressive render equals a one-shot
 render (crates/gpu/tests/cpu_gpu_agreement.rs:119-168), so the ranks'
-accumulators summed equal one render of world*spp samples. The oracle plays
-each rank's renderer here; the GPU renderer's offset handling is pinned
-against the oracle in test_render_parity. Also covers bench.py's timing
-helpers (barrier, max over ranks) on a gloo group.
+accumulators summed equal one render of world*spp samples. With no GPU here
+the oracle plays each rank's renderer and the rank-order sum runs on the
+host; the device sum (luc_accum_merge) is pinned in test_shards_merge on a
+GPU, and the GPU renderer's offset handling against the oracle in
+test_render_parity. Also covers bench.py's timing helpers (barrier, max over
+ranks) on a gloo group.
 """
 import datetime
 import os
@@ -28,6 +32,24 @@ def _free_port():
         return s.getsockname()[1]
 
 
+def _as_accum(sums, spp):
+    """The oracle's per-pixel sums packed as GpuAccum records."""
+    import lucida_b200 as lb
+    a = np.zeros(len(sums), lb.layout.ACCUM)
+    a["radiance"], a["radiance_sq"], a["albedo"] = sums[:, 0:3], sums[:, 3:6], sums[:, 6:9]
+    a["normal"], a["depth"], a["samples"] = sums[:, 9:12], sums[:, 12], spp
+    return a
+
+
+def _rank_order_sum(parts, out):
+    """The device merge's arithmetic on the host: parts[0] + parts[1] + ...,
+    float32, rank order."""
+    acc = parts[0].numpy().copy()
+    for r in range(1, parts.shape[0]):
+        acc += parts[r].numpy()
+    out.copy_(__import__("torch").from_numpy(acc))
+
+
 def _rank_main(rank, port, out_dir):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
                       WORLD_SIZE=str(WORLD), LOCAL_RANK=str(rank))
@@ -37,13 +59,18 @@ def _rank_main(rank, port, out_dir):
     try:
         import bench
         import oracle as O
+        import lucida_b200 as lb
+        from lucida_b200.shards import merge_accumulators, shard_params
         osc = O.Scene.builtin("cornell-box")
-        u = osc.uniforms(W, H, SPP, DEPTH, sample_offset=rank * SPP, sampler=1)
-        part = torch.from_numpy(osc.render_sums(u, threads=2)[:, :6].astype(np.float64))
-        dist.all_reduce(part)  # what a user merging the replicas would run once, after the frames
+        p = shard_params(lb.RenderParams(width=W, height=H, samples=SPP, max_depth=DEPTH), rank)
+        assert p.sample_offset == rank * SPP
+        u = osc.uniforms(W, H, SPP, DEPTH, sample_offset=p.sample_offset, sampler=1)
+        acc = torch.from_numpy(_as_accum(osc.render_sums(u, threads=2), SPP).view(np.float32).reshape(-1).copy())
+        np.save(os.path.join(out_dir, f"part{rank}.npy"), acc.numpy())
+        merge_accumulators(acc, sum_parts=_rank_order_sum)
         bench.barrier(WORLD)
         slowest = bench.max_over_ranks(10.0 + rank, WORLD)
-        np.save(os.path.join(out_dir, f"rank{rank}.npy"), part.numpy())
+        np.save(os.path.join(out_dir, f"rank{rank}.npy"), acc.numpy())
         with open(os.path.join(out_dir, f"rank{rank}.txt"), "w") as f:
             f.write(repr(slowest))
     finally:
@@ -66,13 +93,21 @@ def test_sample_range_shards_sum_to_the_one_shot_render(tmp_path):
     assert [p.exitcode for p in procs] == [0] * WORLD
 
     import oracle as O
+    import lucida_b200 as lb
     osc = O.Scene.builtin("cornell-box")
-    whole = osc.render_sums(osc.uniforms(W, H, WORLD * SPP, DEPTH, sampler=1), threads=2)[:, :6].astype(np.float64)
+    whole = _as_accum(osc.render_sums(osc.uniforms(W, H, WORLD * SPP, DEPTH, sampler=1), threads=2), WORLD * SPP)
+    parts = [np.load(tmp_path / f"part{r}.npy") for r in range(WORLD)]
+    expect = parts[0].copy()
+    for r in range(1, WORLD):
+        expect += parts[r]
     for r in range(WORLD):
         merged = np.load(tmp_path / f"rank{r}.npy")
-        # float32 partial sums in two halves vs one sequential float32 sum
-        np.testing.assert_allclose(merged, whole, rtol=1e-5, atol=1e-6)
+        assert np.array_equal(merged, expect)  # every rank holds the same rank-order sum
+        m = merged.view(lb.layout.ACCUM)
+        assert np.all(m["samples"] == WORLD * SPP)
+        for f in ("radiance", "radiance_sq", "albedo", "normal", "depth"):
+            # float32 partial sums in two halves vs one sequential float32 sum
+            np.testing.assert_allclose(m[f], whole[f], rtol=1e-5, atol=1e-6)
         assert float((tmp_path / f"rank{r}.txt").read_text()) == 10.0 + WORLD - 1
     # the shards are disjoint: each rank alone is not the whole
-    half = osc.render_sums(osc.uniforms(W, H, SPP, DEPTH, sampler=1), threads=2)[:, :6]
-    assert not np.allclose(half, whole)
+    assert not np.allclose(parts[0].view(lb.layout.ACCUM)["radiance"], whole["radiance"])
