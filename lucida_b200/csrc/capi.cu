@@ -143,6 +143,7 @@ int32_t luc_create(int32_t device, luc_ctx** out) {
     if (const char* g = std::getenv("LUC_NO_GRAPHS")) c->use_graphs = g[0] == '\0' || g[0] == '0';
     if (const char* g = std::getenv("LUC_BINARY_BVH")) c->use_wide = g[0] == '\0' || g[0] == '0';
     if (const char* g = std::getenv("LUC_GUIDE_TC")) c->rs.guide_tc = g[0] != '\0' && g[0] != '0';
+    if (const char* w = std::getenv("LUC_WIDE_STAGE")) c->rs.wide_stage = std::atoi(w) == 73 ? 73 : 0;
     const std::vector<float>& et = energy_table_cached();
     if (upload(c->energy, et.data(), et.size(), c->stream) != cudaSuccess ||
         luc_init_sobol_tables(c->stream) != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) {
@@ -511,6 +512,7 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     d.soup = c->soup.as<float4>();
     d.wnodes = c->wide_nodes ? c->wnodes.as<float4>() : nullptr;
     d.wsoup = c->wide_nodes ? c->wsoup.as<float4>() : nullptr;
+    d.num_wnodes = c->wide_nodes;
     d.blas_wide = c->wide_nodes && (ni || meshes) ? c->blas_wide.as<uint32_t>() : nullptr;
     d.root_first = 0;
     d.root_count = 0;

@@ -145,6 +145,11 @@ cudaError_t launch_guide_forward_tc(const float* in9, uint32_t n, const luc::Gui
 void launch_guide_infer_tc(const luc::RenderState& rs, const luc::DevScene& sc, const luc::FrameParams& fp,
                            uint32_t depth, cudaStream_t s);
 cudaError_t guide_tc_setup();
+// guide_tc.cu: one gradient evaluation over `cap` records on tcgen05 (the
+// per-CTA slices go to `part`, the biases and loss to grad / gmisc); returns
+// the number of slices.
+uint32_t launch_guide_gradient_tc(const float4* rec, uint32_t cap, uint32_t* gmisc, const luc::GuideDev& g,
+                                  float* grad, float* part, int num_sms, cudaStream_t s);
 // stats.cu: record the convergence meter over a device accumulator on `s`;
 // the figure lands in c->conv_scratch after 64 float2 partials.
 int32_t luc_record_convergence(luc_ctx* c, const GpuAccum* accum, uint32_t pixels, cudaStream_t s);

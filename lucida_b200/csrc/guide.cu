@@ -85,7 +85,6 @@ __device__ __forceinline__ void load_net(NetSmem& s, const uint16_t* __restrict_
     for (int i = t; i < kGBias; i += nt) s.b[i] = bias[i];
 }
 
-__device__ __forceinline__ float softplus_f(float x) { return x > 20.0f ? x : log1pf(expf(x)); }
 
 // Raw outputs -> (mu, kappa) x 8 and softmax weights.
 __device__ __forceinline__ void decode_row(const float* __restrict__ o, float4* __restrict__ lobes, float* __restrict__ w) {
@@ -350,9 +349,6 @@ struct TrainSmem {
     float loss;
 };
 static_assert(sizeof(TrainSmem) <= 113 * 1024, "two training CTAs per SM");
-// Per-CTA weight-gradient slice: dW1 | dW2 | dW3 | dW4 (kGOutPad rows).
-constexpr int kPartW1 = 0, kPartW2 = kGHid * kGIn, kPartW3 = kPartW2 + kGHid * kGHid,
-              kPartW4 = kPartW3 + kGHid * kGHid, kPartFloats = kPartW4 + kGOutPad * kGHid;
 
 // dW[m][n] += sum_r G[r][m] H[r][n] over the tile's 64 rows for the 16 output
 // rows m0..m0+15. G is [64][SG] (m contiguous), H is [64][SH]; both operands
@@ -420,49 +416,6 @@ __device__ void input_grad(const uint16_t* __restrict__ G, const uint16_t* __res
             atomicAdd(db + n + 1, s1);
         }
     }
-}
-
-// Loss term of one row, -F/S log q(d), and its gradient w.r.t. the raw
-// outputs (the same closed forms as the oracle).
-__device__ __forceinline__ float row_loss_grad(const float* __restrict__ o, V3 d, float F, float invS, float* __restrict__ go) {
-    float mx = -INFINITY;
-    for (int j = 0; j < kGLobes; ++j) mx = fmaxf(mx, o[5 * j + 4]);
-    float w[kGLobes], pj[kGLobes];
-    float ws = 0.f;
-    for (int j = 0; j < kGLobes; ++j) {
-        w[j] = expf(o[5 * j + 4] - mx);
-        ws += w[j];
-    }
-    float q = 0.f;
-    for (int j = 0; j < kGLobes; ++j) {
-        w[j] /= ws;
-        float x = o[5 * j], y = o[5 * j + 1], z = o[5 * j + 2];
-        float ln = fmaxf(sqrtf(x * x + y * y + z * z), 1e-30f);
-        float c = (x * d.x + y * d.y + z * d.z) / ln;
-        float kap = fminf(1.0f + softplus_f(o[5 * j + 3]), kGKappaMax);
-        pj[j] = kap / (2.0f * kPi * (1.0f - expf(-2.0f * kap))) * expf(kap * (c - 1.0f));
-        q += w[j] * pj[j];
-    }
-    q = fmaxf(q, 1e-30f);
-    const float scale = -F * invS;
-    for (int j = 0; j < kGLobes; ++j) {
-        float x = o[5 * j], y = o[5 * j + 1], z = o[5 * j + 2];
-        float ln = fmaxf(sqrtf(x * x + y * y + z * z), 1e-30f);
-        float mu[3] = {x / ln, y / ln, z / ln};
-        float c = mu[0] * d.x + mu[1] * d.y + mu[2] * d.z;
-        float kr = 1.0f + softplus_f(o[5 * j + 3]);
-        float kap = fminf(kr, kGKappaMax);
-        float ex = expf(-2.0f * kap);
-        float r = w[j] * pj[j] / q;
-        go[5 * j + 4] = scale * (r - w[j]);
-        float dk = r * (1.0f / kap - 2.0f * ex / (1.0f - ex) + c - 1.0f);
-        float sig = 1.0f / (1.0f + expf(-fminf(fmaxf(o[5 * j + 3], -60.f), 60.f)));
-        go[5 * j + 3] = kr >= kGKappaMax ? 0.0f : scale * dk * sig;
-        float gm[3] = {r * kap * d.x, r * kap * d.y, r * kap * d.z};
-        float dotm = gm[0] * mu[0] + gm[1] * mu[1] + gm[2] * mu[2];
-        for (int a = 0; a < 3; ++a) go[5 * j + a] = scale * (gm[a] - dotm * mu[a]) / ln;
-    }
-    return scale * logf(q);
 }
 
 // One gradient evaluation over the records (count gmisc[kGmRecords], capped
@@ -592,11 +545,17 @@ size_t guide_part_bytes(int num_sms) { return (size_t)2 * num_sms * kPartFloats 
 
 // One gradient evaluation over records rec[0, min(count, cap)) into grad
 // (zeroed here) and the loss word.
+// tc: the tcgen05 kernel (guide_tc.cu), else the mma.sync one.
 void launch_guide_gradient(const float4* rec, uint32_t cap, uint32_t* gmisc, const GuideDev& g, float* grad,
-                           float* part, int num_sms, cudaStream_t s) {
-    const uint32_t grid = guide_train_grid(cap, num_sms);
+                           float* part, int num_sms, bool tc, cudaStream_t s) {
     cudaMemsetAsync(grad, 0, kGParams * sizeof(float), s);
-    k_guide_train<<<grid, kGuideThreads, sizeof(TrainSmem), s>>>(rec, cap, gmisc, g, grad, part);
+    uint32_t grid;
+    if (tc) {
+        grid = launch_guide_gradient_tc(rec, cap, gmisc, g, grad, part, num_sms, s);
+    } else {
+        grid = guide_train_grid(cap, num_sms);
+        k_guide_train<<<grid, kGuideThreads, sizeof(TrainSmem), s>>>(rec, cap, gmisc, g, grad, part);
+    }
     k_guide_fold<<<(kPartFloats + 255) / 256, 256, 0, s>>>(part, grid, grad);
 }
 
@@ -794,7 +753,7 @@ void launch_guide_finalize(const RenderState& rs, const FrameParams& fp, cudaStr
 }
 
 void launch_guide_step(const RenderState& rs, uint32_t cap, const GuideDev& g, const GuideTrain& gt, cudaStream_t s) {
-    launch_guide_gradient(rs.ps.rec, cap, rs.ps.gmisc, g, gt.grad, gt.part, rs.num_sms, s);
+    launch_guide_gradient(rs.ps.rec, cap, rs.ps.gmisc, g, gt.grad, gt.part, rs.num_sms, rs.guide_tc, s);
     k_guide_adam<<<(kGParams + 255) / 256, 256, 0, s>>>(gt.params, gt.m, gt.v, gt.grad, rs.ps.gmisc, gt.lr);
     k_guide_pack<<<(kGBf16 + 255) / 256, 256, 0, s>>>(gt.params, gt.wbf, gt.bias, rs.ps.gmisc, cap, 1u);
 }
@@ -880,6 +839,11 @@ int32_t luc_guide_init(luc_ctx* c, const float* params, uint64_t seed, const flo
     std::vector<float> p(kGParams, 0.0f);
     if (params) {
         std::memcpy(p.data(), params, kGParams * sizeof(float));
+        // W1's padding columns multiply features that are always zero; they
+        // are held at zero (the tensor-core training kernel sets padding
+        // feature 127 to 1 to read b1's gradient out of its dW1 product).
+        for (int r = 0; r < kGHid; ++r)
+            for (int k = kGFeatures; k < kGIn; ++k) p[(size_t)r * kGIn + k] = 0.0f;
     } else {
         // Uniform +-sqrt(6 / (fan_in + fan_out)) weights, zero biases, W1's
         // padding columns zero.
@@ -1021,7 +985,7 @@ int32_t luc_guide_train_records(luc_ctx* c, const float* records, uint32_t n, ui
         LUC_CUDA(c, cudaMemsetAsync(gm + kGmWeightSum, 0, 2 * sizeof(uint32_t), s), "clear sums");
         k_guide_weight_sum<<<c->num_sms * 2, 256, 0, s>>>(rec, n, gm);
         launch_guide_gradient(rec, n, gm, luc_guide_dev(c), c->g_grad.as<float>(), c->g_part.as<float>(),
-                              c->num_sms, s);
+                              c->num_sms, c->rs.guide_tc, s);
         if (steps > 0) {
             k_guide_adam<<<(kGParams + 255) / 256, 256, 0, s>>>(c->g_params.as<float>(), c->g_m.as<float>(),
                                                                 c->g_v.as<float>(), c->g_grad.as<float>(), gm,

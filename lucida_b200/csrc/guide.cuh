@@ -45,6 +45,11 @@ constexpr int kGmWords = 16;
 //   [3] sampled direction (world), throughput .z
 //   [4] path radiance when the continuation started, mixture pdf p(wi)
 
+// Per-CTA weight-gradient slice of the training kernels (mma.sync and
+// tcgen05 alike): dW1 | dW2 | dW3 | dW4 (kGOutPad rows), each [out][in].
+constexpr int kPartW1 = 0, kPartW2 = kGHid * kGIn, kPartW3 = kPartW2 + kGHid * kGHid,
+              kPartW4 = kPartW3 + kGHid * kGHid, kPartFloats = kPartW4 + kGOutPad * kGHid;
+
 // Polls of a tensor-core kernel's mbarrier before its wait gives up.
 constexpr uint32_t kTcWaitLimit = 1u << 22;
 
@@ -55,6 +60,51 @@ struct GuideDev {
     uint32_t tc_wait_limit;  // kTcWaitLimit (a test hook lowers it)
     uint32_t tc_no_issue;    // test hook: issue no MMA and no commit, so the wait runs out
 };
+
+LUC_D float softplus_f(float x) { return x > 20.0f ? x : log1pf(expf(x)); }
+
+// Loss term of one row, -F/S log q(d), and its gradient w.r.t. the raw
+// outputs (the same closed forms as the oracle).
+LUC_D float row_loss_grad(const float* __restrict__ o, V3 d, float F, float invS, float* __restrict__ go) {
+    float mx = -INFINITY;
+    for (int j = 0; j < kGLobes; ++j) mx = fmaxf(mx, o[5 * j + 4]);
+    float w[kGLobes], pj[kGLobes];
+    float ws = 0.f;
+    for (int j = 0; j < kGLobes; ++j) {
+        w[j] = expf(o[5 * j + 4] - mx);
+        ws += w[j];
+    }
+    float q = 0.f;
+    for (int j = 0; j < kGLobes; ++j) {
+        w[j] /= ws;
+        float x = o[5 * j], y = o[5 * j + 1], z = o[5 * j + 2];
+        float ln = fmaxf(sqrtf(x * x + y * y + z * z), 1e-30f);
+        float c = (x * d.x + y * d.y + z * d.z) / ln;
+        float kap = fminf(1.0f + softplus_f(o[5 * j + 3]), kGKappaMax);
+        pj[j] = kap / (2.0f * kPi * (1.0f - expf(-2.0f * kap))) * expf(kap * (c - 1.0f));
+        q += w[j] * pj[j];
+    }
+    q = fmaxf(q, 1e-30f);
+    const float scale = -F * invS;
+    for (int j = 0; j < kGLobes; ++j) {
+        float x = o[5 * j], y = o[5 * j + 1], z = o[5 * j + 2];
+        float ln = fmaxf(sqrtf(x * x + y * y + z * z), 1e-30f);
+        float mu[3] = {x / ln, y / ln, z / ln};
+        float c = mu[0] * d.x + mu[1] * d.y + mu[2] * d.z;
+        float kr = 1.0f + softplus_f(o[5 * j + 3]);
+        float kap = fminf(kr, kGKappaMax);
+        float ex = expf(-2.0f * kap);
+        float r = w[j] * pj[j] / q;
+        go[5 * j + 4] = scale * (r - w[j]);
+        float dk = r * (1.0f / kap - 2.0f * ex / (1.0f - ex) + c - 1.0f);
+        float sig = 1.0f / (1.0f + expf(-fminf(fmaxf(o[5 * j + 3], -60.f), 60.f)));
+        go[5 * j + 3] = kr >= kGKappaMax ? 0.0f : scale * dk * sig;
+        float gm[3] = {r * kap * d.x, r * kap * d.y, r * kap * d.z};
+        float dotm = gm[0] * mu[0] + gm[1] * mu[1] + gm[2] * mu[2];
+        for (int a = 0; a < 3; ++a) go[5 * j + a] = scale * (gm[a] - dotm * mu[a]) / ln;
+    }
+    return scale * logf(q);
+}
 
 // 32-bit integer mix (Wellons' "lowbias32" constants) for record selection.
 LUC_D uint32_t mix32(uint32_t x) {

@@ -44,9 +44,22 @@ __device__ __forceinline__ uint64_t desc(uint32_t a, uint32_t lbo) {
     return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
            ((uint64_t)((kSbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
+// The same with an explicit stride byte offset: the stride between 8-row
+// groups (K-major) or between 8-element MN groups (MN-major, where `lbo` is
+// the stride between 8-row K groups).
+__device__ __forceinline__ uint64_t desc2(uint32_t a, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
 // Instruction descriptor, kind::f16: D F32, A and B BF16, both K-major.
 __host__ __device__ constexpr uint32_t idesc(int n) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
+}
+// With A and/or B read MN-major (bit 15: A, bit 16: B): the operand's
+// elements are contiguous along M (N) instead of K, so a tile stored K-major
+// for one product is read transposed by another.
+__host__ __device__ constexpr uint32_t idesc_mn(int n, bool a_mn, bool b_mn) {
+    return idesc(n) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16);
 }
 
 __device__ __forceinline__ void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
@@ -366,6 +379,317 @@ __global__ void __launch_bounds__(kTeamCta, 1) k_infer_tc(PathState ps, const __
         });
 }
 
+// ---------------------------------------------------------------- training
+// One gradient evaluation on the tensor cores: the tcgen05 counterpart of
+// k_guide_train (guide.cu) over the same records, with the same loss, output
+// gradient and parameter-gradient layout. One CTA of 128 threads per SM (one
+// thread per tile row, its TMEM lane) walks 128-row tiles of records:
+//   forward   X -> H1 -> H2 -> H3 -> Y as inference computes it, the BF16
+//             activations kept in shared memory in the canonical K-major
+//             layout;
+//   loss      each thread turns its row's outputs into dL/dY (row_loss_grad),
+//             rounded to BF16;
+//   backward  dH(l-1) = (dY(l) W(l)) * (H(l-1) > 0), the weights read
+//             transposed through MN-major descriptors of their forward
+//             layout, and dW(l)^T += H(l-1)^T dY(l) accumulated in TMEM over
+//             all of the CTA's tiles, the activation and gradient tiles read
+//             transposed the same way (the batch rows are the contraction).
+// Bias gradients come out of the same products: each hidden activation tile
+// carries a constant upper half (features 64..127) whose feature 64 is 1, so
+// row 64 of dW(l)^T (l = 2, 3, 4) is the column sum of dY(l), the gradient
+// of b(l); the input tile's padding feature 127 is 1, so row 127 of dW1^T is
+// the gradient of b1 (W1's padding columns are zero, so the forward does not
+// change). TMEM: columns 0-63 the layer product, 64-127 dW1^T, 128-191
+// dW2^T, 192-255 dW3^T, 256-303 dW4^T. At the end each thread reads its
+// rows of the gradients into the CTA's slice of `part` (k_guide_fold sums the
+// slices in CTA order) and the bias gradients into `grad`.
+// A wait that runs out sets gmisc[kGmTcError]; the CTA's slice is zeroed.
+struct TrainTcSmem {
+    uint8_t x[16 * kLboA];     // 128 rows x 128 features
+    uint8_t h[3][16 * kLboA];  // 128 rows x (64 features + the constant half)
+    uint8_t dy[6 * kLboA];     // 128 rows x 48 output gradients
+    uint8_t dh[2][8 * kLboA];  // 128 rows x 64 hidden gradients, ping-pong
+    uint8_t w1[(kGIn / 8) * kLboH], w2[(kGHid / 8) * kLboH], w3[(kGHid / 8) * kLboH], w4[(kGHid / 8) * kLboO];
+    float b[kGBias];
+    unsigned long long mbar;
+    uint32_t tmem;
+    float loss;
+};
+constexpr uint32_t kTrainTmemCols = 512;
+constexpr uint32_t kColS = 0, kColW1 = 64, kColW2 = 128, kColW3 = 192, kColW4 = 256;
+
+__global__ void __launch_bounds__(kM, 1) k_guide_train_tc(const float4* __restrict__ rec, uint32_t cap,
+                                                          uint32_t* __restrict__ gmisc, GuideDev g,
+                                                          float* __restrict__ grad, float* __restrict__ part) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    TrainTcSmem& S = *reinterpret_cast<TrainTcSmem*>(smem_raw);
+    const int t = threadIdx.x, warp = t >> 5, r = t;
+    const uint32_t n = min(gmisc[kGmRecords], cap);
+    const float wsum = __uint_as_float(gmisc[kGmWeightSum]);
+    const float invS = wsum > 0.0f ? 1.0f / wsum : 0.0f;
+    float* P = part + (size_t)blockIdx.x * kPartFloats;
+    if (blockIdx.x * (uint32_t)kM >= n) {  // no tile: an all-zero slice
+        for (int i = t; i < kPartFloats / 4; i += blockDim.x)
+            reinterpret_cast<float4*>(P)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    {
+        auto load_w = [&](uint8_t* dst, const uint16_t* src, int nn, int k, uint32_t lbo) {
+            const int chunks = nn * (k / 8);
+            for (int i = t; i < chunks; i += blockDim.x) {
+                const int row = i / (k / 8), c = i % (k / 8);
+                *reinterpret_cast<uint4*>(dst + c * lbo + (row >> 3) * kSbo + (row & 7) * 16) =
+                    *reinterpret_cast<const uint4*>(src + row * k + c * 8);
+            }
+        };
+        load_w(S.w1, g.wbf, kGHid, kGIn, kLboH);
+        load_w(S.w2, g.wbf + kGHid * kGIn, kGHid, kGHid, kLboH);
+        load_w(S.w3, g.wbf + kGHid * kGIn + kGHid * kGHid, kGHid, kGHid, kLboH);
+        load_w(S.w4, g.wbf + kGHid * kGIn + 2 * kGHid * kGHid, kGOutPad, kGHid, kLboO);
+        for (int i = t; i < kGBias; i += blockDim.x) S.b[i] = g.bias[i];
+        // The hidden tiles' constant upper half: feature 64 = 1, 65..127 = 0.
+        for (int l = 0; l < 3; ++l)
+            for (int c = 8; c < 16; ++c)
+                *chunk(S.h[l], c, r) = make_uint4(c == 8 ? 0x3F80u : 0u, 0u, 0u, 0u);
+    }
+    if (t == 0) {
+        S.loss = 0.0f;
+        asm volatile("mbarrier.init.shared::cta.b64 [%1], %0;" ::"r"(1u), "r"(saddr(&S.mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&S.tmem)),
+                     "r"(kTrainTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tm = S.tmem;
+    const uint32_t lane_off = (uint32_t)(32 * warp) << 16;
+    const uint32_t mbar = saddr(&S.mbar);
+    uint32_t phase = 0;
+    bool failed = false, first = true;
+    float loss = 0.0f;
+    // One product chain: D[M=128][N] (+)= sum over ksteps of A x B^T.
+    auto chain = [&](uint32_t dcol, uint32_t a, uint32_t a_lbo, uint32_t a_sbo, uint32_t a_step, uint32_t b,
+                     uint32_t b_lbo, uint32_t b_sbo, uint32_t b_step, int ksteps, uint32_t id, bool fresh) {
+        for (int ks = 0; ks < ksteps; ++ks)
+            mma(tm + dcol, desc2(a + ks * a_step, a_lbo, a_sbo), desc2(b + ks * b_step, b_lbo, b_sbo), id,
+                (fresh && ks == 0) ? 0u : 1u);
+    };
+    // Issue (one thread), commit, bounded wait; the CTA learns the outcome.
+    auto run = [&](auto issue) {
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        fence_after();
+        if (t == 0 && !g.tc_no_issue) {
+            issue();
+            commit(mbar);
+        }
+        const bool ok = wait_phase(mbar, phase, g.tc_wait_limit);
+        phase ^= 1u;
+        fence_after();
+        return __syncthreads_or(ok ? 0 : 1) == 0;
+    };
+    // Forward products: A = activations (K-major), B = weights (K-major).
+    auto fwd = [&](const uint8_t* act, int ksteps, const uint8_t* w, uint32_t lbw, int nout) {
+        return run([&] {
+            chain(kColS, saddr(act), kLboA, kSbo, 2 * kLboA, saddr(w), lbw, kSbo, 2 * lbw, ksteps, idesc(nout), true);
+        });
+    };
+    // bias + ReLU of the 64 product columns into hidden tile `hout`.
+    auto epi_hidden = [&](const float* b, uint8_t* hout) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float v[16];
+            ld16(tm + kColS + lane_off + 16 * q, v);
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                uint32_t w[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int k = 8 * cc + 2 * j, nn = 16 * q + k;
+                    w[j] = pack2(fmaxf(v[k] + b[nn], 0.0f), fmaxf(v[k + 1] + b[nn + 1], 0.0f));
+                }
+                *chunk(hout, 2 * q + cc, r) = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+        }
+    };
+    // The product (dY W) masked by the forward activation (> 0), into `gout`.
+    auto epi_grad = [&](const uint8_t* hprev, uint8_t* gout) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float v[16];
+            ld16(tm + kColS + lane_off + 16 * q, v);
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const uint4 hp = *chunk(const_cast<uint8_t*>(hprev), 2 * q + cc, r);
+                const uint32_t hw[4] = {hp.x, hp.y, hp.z, hp.w};
+                uint32_t w[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int k = 8 * cc + 2 * j;
+                    const float h0 = __uint_as_float(hw[j] << 16), h1 = __uint_as_float(hw[j] & 0xFFFF0000u);
+                    w[j] = pack2(h0 > 0.0f ? v[k] : 0.0f, h1 > 0.0f ? v[k + 1] : 0.0f);
+                }
+                *chunk(gout, 2 * q + cc, r) = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+        }
+    };
+    const uint32_t sx = saddr(S.x), sh0 = saddr(S.h[0]), sh1 = saddr(S.h[1]), sh2 = saddr(S.h[2]);
+    const uint32_t sdy = saddr(S.dy), sd0 = saddr(S.dh[0]), sd1 = saddr(S.dh[1]);
+    // Backward pair: dH = dY x W (B = W read MN-major: K = output units in
+    // 8-row groups 128 B apart, N = input units in groups lbw apart) and
+    // dW^T += Hprev^T x dY (both read MN-major: M = Hprev's 128 features in
+    // groups kLboA apart, N = dY's units, K = the 128 rows in groups 128 B
+    // apart).
+    auto back = [&](uint32_t g_tile, int gk, uint32_t w, uint32_t lbw, uint32_t hprev, uint32_t dwcol, int nout) {
+        return run([&] {
+            chain(kColS, g_tile, kLboA, kSbo, 2 * kLboA, w, kSbo, lbw, 2 * kSbo, gk, idesc_mn(kGHid, false, true),
+                  true);
+            chain(dwcol, hprev, kSbo, kLboA, 2 * kSbo, g_tile, kSbo, kLboA, 2 * kSbo, kM / 16,
+                  idesc_mn(nout, true, true), first);
+        });
+    };
+    for (uint32_t base = blockIdx.x * kM; base < n && !failed; base += gridDim.x * kM) {
+        const uint32_t i = base + r;
+        const bool mine = i < n;
+        float in[9] = {0, 0, 0, 0, 0, 1, 0, 0, 1};
+        float4 a4{0, 0, 0, 0}, d4{0, 0, 0, 0};
+        if (mine) {
+            a4 = rec[kGRecF4 * (size_t)i];
+            const float4 b4 = rec[kGRecF4 * (size_t)i + 1], c4 = rec[kGRecF4 * (size_t)i + 2];
+            d4 = rec[kGRecF4 * (size_t)i + 3];
+            in[0] = a4.x;
+            in[1] = a4.y;
+            in[2] = a4.z;
+            in[3] = b4.x;
+            in[4] = b4.y;
+            in[5] = b4.z;
+            in[6] = c4.x;
+            in[7] = c4.y;
+            in[8] = c4.z;
+        }
+        write_feature_half(S.x, r, 0, in, g);
+        write_feature_half(S.x, r, 1, in, g);
+        *chunk(S.x, 15, r) = make_uint4(0u, 0u, 0u, 0x3F800000u);  // feature 127 = 1 (bias gradient of b1)
+        bool ok = fwd(S.x, 8, S.w1, kLboH, kGHid);
+        if (ok) {
+            epi_hidden(S.b, S.h[0]);
+            ok = fwd(S.h[0], 4, S.w2, kLboH, kGHid);
+        }
+        if (ok) {
+            epi_hidden(S.b + kGHid, S.h[1]);
+            ok = fwd(S.h[1], 4, S.w3, kLboH, kGHid);
+        }
+        if (ok) {
+            epi_hidden(S.b + 2 * kGHid, S.h[2]);
+            ok = fwd(S.h[2], 4, S.w4, kLboO, kGOutPad);
+        }
+        if (ok) {
+            // Loss epilogue: this row's outputs -> dL/dY (BF16) and its loss term.
+            float o[kGOutPad], go[kGOut];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                float v[16];
+                ld16(tm + kColS + lane_off + 16 * q, v);
+#pragma unroll
+                for (int k = 0; k < 16; ++k) o[16 * q + k] = v[k] + S.b[3 * kGHid + 16 * q + k];
+            }
+            if (mine && a4.w > 0.0f) loss += row_loss_grad(o, V3{d4.x, d4.y, d4.z}, a4.w, invS, go);
+            else
+#pragma unroll
+                for (int k = 0; k < kGOut; ++k) go[k] = 0.0f;
+#pragma unroll
+            for (int c = 0; c < kGOutPad / 8; ++c) {
+                uint32_t w[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int k = 8 * c + 2 * j;
+                    w[j] = pack2(k < kGOut ? go[k] : 0.0f, k + 1 < kGOut ? go[k + 1] : 0.0f);
+                }
+                *chunk(S.dy, c, r) = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+            ok = back(sdy, kGOutPad / 16, saddr(S.w4), kLboO, sh2, kColW4, kGOutPad);
+        }
+        if (ok) {
+            epi_grad(S.h[2], S.dh[0]);
+            ok = back(sd0, kGHid / 16, saddr(S.w3), kLboH, sh1, kColW3, kGHid);
+        }
+        if (ok) {
+            epi_grad(S.h[1], S.dh[1]);
+            ok = back(sd1, kGHid / 16, saddr(S.w2), kLboH, sh0, kColW2, kGHid);
+        }
+        if (ok) {
+            epi_grad(S.h[0], S.dh[0]);
+            ok = run([&] {
+                chain(kColW1, sx, kSbo, kLboA, 2 * kSbo, sd0, kSbo, kLboA, 2 * kSbo, kM / 16,
+                      idesc_mn(kGHid, true, true), first);
+            });
+        }
+        if (!ok) failed = true;
+        first = false;
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (!failed) {
+        float* gb1 = grad + kGHid * kGIn;
+        float* gb2 = gb1 + kGHid + kGHid * kGHid;
+        float* gb3 = gb2 + kGHid + kGHid * kGHid;
+        float* gb4 = gb3 + kGHid + kGOut * kGHid;
+        // dW1^T: row r = input feature r; row 127 = the gradient of b1.
+#pragma unroll 1
+        for (int q = 0; q < 4; ++q) {
+            float v[16];
+            ld16(tm + kColW1 + lane_off + 16 * q, v);
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const int h = 16 * q + k;
+                P[kPartW1 + h * kGIn + r] = r < kGFeatures ? v[k] : 0.0f;
+                if (r == kGIn - 1) atomicAdd(gb1 + h, v[k]);
+            }
+        }
+        // dW2^T, dW3^T, dW4^T: row r < 64 = input unit r; row 64 = the bias gradient.
+        float* const gbs[3] = {gb2, gb3, gb4};
+        const int pw[3] = {kPartW2, kPartW3, kPartW4};
+        const uint32_t cols[3] = {kColW2, kColW3, kColW4};
+#pragma unroll 1
+        for (int l = 0; l < 3; ++l) {
+            const int nout = l == 2 ? kGOutPad : kGHid, nreal = l == 2 ? kGOut : kGHid;
+#pragma unroll 1
+            for (int q = 0; q < nout / 16; ++q) {
+                float v[16];
+                ld16(tm + cols[l] + lane_off + 16 * q, v);
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+                    const int o = 16 * q + k;
+                    if (r < kGHid) P[pw[l] + o * kGHid + r] = v[k];
+                    else if (r == kGHid && o < nreal) atomicAdd(gbs[l] + o, v[k]);
+                }
+            }
+        }
+    } else {
+        for (int i = t; i < kPartFloats / 4; i += blockDim.x)
+            reinterpret_cast<float4*>(P)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (t == 0) atomicOr(gmisc + kGmTcError, 1u);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, off);
+    if ((t & 31) == 0) atomicAdd(&S.loss, loss);
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (t == 0 && !failed) atomicAdd(reinterpret_cast<float*>(gmisc + kGmLoss), S.loss);
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(kTrainTmemCols)
+                     : "memory");
+}
+
 }  // namespace tcg
 }  // namespace luc
 
@@ -378,7 +702,22 @@ cudaError_t guide_tc_setup() {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(tcg::k_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sizeof(tcg::TeamSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(tcg::k_guide_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(tcg::TrainTcSmem));
     return e;
+}
+
+// One gradient evaluation on the tensor cores: one CTA per SM at most (512
+// TMEM columns and 211 KB of shared memory each), one per 128-row tile of
+// `cap` records; returns the grid (the number of gradient slices to fold).
+uint32_t launch_guide_gradient_tc(const float4* rec, uint32_t cap, uint32_t* gmisc, const luc::GuideDev& g,
+                                  float* grad, float* part, int num_sms, cudaStream_t s) {
+    using namespace luc;
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>((cap + tcg::kM - 1) / tcg::kM, (uint64_t)num_sms));
+    tcg::k_guide_train_tc<<<grid, tcg::kM, sizeof(tcg::TrainTcSmem), s>>>(rec, cap, gmisc, g, grad, part);
+    return grid;
 }
 
 void launch_guide_infer_tc(const luc::RenderState& rs, const luc::DevScene& sc, const luc::FrameParams& fp,

@@ -107,6 +107,10 @@ struct RenderState {
     int extend_blocks_bin = 0, connect_blocks_bin = 0;  // single-level scenes on the binary tree
     int extend_blocks_inst_bin = 0, connect_blocks_inst_bin = 0;  // two-level scenes on binary BLASes
     bool guide_tc = true;  // guide inference on tcgen05 (LUC_GUIDE_TC=0: the mma.sync kernel)
+    // Closest-hit traversal of single-level wide trees with the top 73
+    // nodes (root and two levels) staged in shared memory (LUC_WIDE_STAGE=73).
+    int wide_stage = 0;
+    int extend_blocks_stage = 8;
     uint64_t launches = 0;
 };
 

@@ -24,6 +24,7 @@ struct DevScene {
     // scene traverses the binary tree (instanced scenes, LUC_BINARY_BVH=1).
     const float4* wnodes;  // 5 float4 per wide node, root = node 0
     const float4* wsoup;   // (p0 | leaf-order index in p0.w, e1, e2) per triangle, wide-node order
+    uint32_t num_wnodes;
     // Two-level scenes: the wide trees are the BLASes'; blas_wide maps a BLAS's
     // binary root (an instance row's blas_root) to its wide root.
     const uint32_t* blas_wide;
@@ -398,14 +399,32 @@ LUC_D uint32_t xor_permute8(uint32_t x, uint32_t oct) {
 // Slab tests of the 8 child boxes of wide node `node`. Returns the node group
 // (first child, internal mask << 8 | hit bits at positions slot ^ oct) and
 // the triangle group (first triangle, mask of hit triangle bits, count mask).
+LUC_D void wide_slabs(const float4 a, const uint4 b, const uint4 c, const uint4 d, const uint4 e, V3 o, V3 inv,
+                      uint32_t oct, float tmin, float tmax, uint2& ng, uint3& tg);
 LUC_D void wide_node(const float4* __restrict__ wn, uint32_t node, V3 o, V3 inv, uint32_t oct, float tmin,
                      float tmax, uint2& ng, uint3& tg) {
     const float4* q = wn + 5 * (size_t)node;
-    const float4 a = __ldg(q);
-    const uint4 b = __ldg(reinterpret_cast<const uint4*>(q + 1));
-    const uint4 c = __ldg(reinterpret_cast<const uint4*>(q + 2));
-    const uint4 d = __ldg(reinterpret_cast<const uint4*>(q + 3));
-    const uint4 e = __ldg(reinterpret_cast<const uint4*>(q + 4));
+    wide_slabs(__ldg(q), __ldg(reinterpret_cast<const uint4*>(q + 1)), __ldg(reinterpret_cast<const uint4*>(q + 2)),
+               __ldg(reinterpret_cast<const uint4*>(q + 3)), __ldg(reinterpret_cast<const uint4*>(q + 4)), o, inv,
+               oct, tmin, tmax, ng, tg);
+}
+// The same node test with the top `kStage` nodes of the tree (the first
+// levels: the builder numbers nodes level by level) read from a copy in
+// shared memory, `stage`, and the rest from global memory.
+template <int kStage>
+LUC_D void wide_node_staged(const float4* __restrict__ wn, const float4* stage, uint32_t node, V3 o, V3 inv,
+                            uint32_t oct, float tmin, float tmax, uint2& ng, uint3& tg) {
+    if (kStage > 0 && node < (uint32_t)kStage) {
+        const float4* q = stage + 5 * node;
+        wide_slabs(q[0], *reinterpret_cast<const uint4*>(q + 1), *reinterpret_cast<const uint4*>(q + 2),
+                   *reinterpret_cast<const uint4*>(q + 3), *reinterpret_cast<const uint4*>(q + 4), o, inv, oct, tmin,
+                   tmax, ng, tg);
+    } else {
+        wide_node(wn, node, o, inv, oct, tmin, tmax, ng, tg);
+    }
+}
+LUC_D void wide_slabs(const float4 a, const uint4 b, const uint4 c, const uint4 d, const uint4 e, V3 o, V3 inv,
+                      uint32_t oct, float tmin, float tmax, uint2& ng, uint3& tg) {
     const uint32_t ew = __float_as_uint(a.w);
     const float sx = __uint_as_float((ew & 0xFFu) << 23) * inv.x;
     const float sy = __uint_as_float(((ew >> 8) & 0xFFu) << 23) * inv.y;
@@ -475,8 +494,8 @@ struct WideWalk {
     // stack is empty, or (kAny) a hit was found. Each node and triangle is
     // visited at most once per ray in a tree; the step limit only bounds the
     // walk should the arrays ever not form one.
-    template <bool kAny>
-    LUC_D bool step(const DevScene& s, float tmin, TravCount& tc) {
+    template <bool kAny, int kStage = 0>
+    LUC_D bool step(const DevScene& s, float tmin, TravCount& tc, const float4* stage = nullptr) {
         if (g.y & 0xFFu) {
             const uint32_t k = __ffs(g.y & 0xFFu) - 1u;
             g.y &= ~(1u << k);
@@ -484,7 +503,7 @@ struct WideWalk {
             const uint32_t child = g.x + __popc((g.y >> 8) & ((1u << slot) - 1u));
             if ((g.y & 0xFFu) && sp < kWideStack) stack[sp++] = g;
             uint3 t;
-            wide_node(s.wnodes, child, o, inv, oct, tmin, tmax, g, t);
+            wide_node_staged<kStage>(s.wnodes, stage, child, o, inv, oct, tmin, tmax, g, t);
             tc.nodes++;
             while (t.y) {
                 const uint32_t bit = __ffs(t.y) - 1u;

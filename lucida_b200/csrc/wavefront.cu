@@ -158,10 +158,18 @@ __global__ void __launch_bounds__(kThreads, kWide == 1 ? (kInst ? 7 * 128 / kThr
 // refills them with the next rays of the queue (one atomic per refill), so
 // lanes do not idle until the warp's longest ray ends. Each ray's walk is
 // wide_trace's (WideWalk), so the hits are the same.
-template <int kThreads, int kRefill>
+// kStage > 0: the first kStage wide nodes (the top levels) are copied into
+// shared memory when the block starts and read from there.
+template <int kThreads, int kRefill, int kStage = 0>
 __global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_extend_dyn(PathState ps,
                                                                                     const __grid_constant__ DevScene sc,
                                                                                     FrameParams fp, uint32_t depth) {
+    __shared__ float4 stage[kStage > 0 ? 5 * kStage : 1];
+    if (kStage > 0) {
+        const uint32_t nf4 = 5 * min((uint32_t)kStage, sc.num_wnodes);
+        for (uint32_t i = threadIdx.x; i < nf4; i += kThreads) stage[i] = __ldg(sc.wnodes + i);
+        __syncthreads();
+    }
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
     const uint32_t* queue = ps.queue[depth & 1];
     uint32_t* pull = ps.ctr + depth * kCtrStride + kCtrPullExtend;
@@ -196,7 +204,7 @@ __global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_extend_
             continue;
         }
         // One node per refill check (measured best against 4, 8 and 16).
-        if (live && w.step<false>(sc, kTMin, tc)) {
+        if (live && w.step<false, kStage>(sc, kTMin, tc, stage)) {
             __stcs(ps.hit + p, make_float4(w.tmax, w.found ? w.bu : 0.0f, w.found ? w.bv : 0.0f,
                                            __uint_as_float(w.found ? w.btri : pid)));
             ++rays;
@@ -585,6 +593,7 @@ void query_occupancy(RenderState& rs) {
         return b > 0 ? b : 8;
     };
     rs.extend_blocks = occ((const void*)k_extend_dyn<128, kExtendRefill>);
+    rs.extend_blocks_stage = occ((const void*)k_extend_dyn<128, kExtendRefill, 73>);
     rs.connect_blocks = occ((const void*)k_connect_dyn<128, kExtendRefill>);
     rs.extend_blocks_bin = occ((const void*)k_extend<false, false, 128, 0>);
     rs.connect_blocks_bin = occ((const void*)k_connect<false, false, 128, 0>);
@@ -640,6 +649,8 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
         else if (inst)
             k_extend<true, false, 128, 0><<<sms * rs.extend_blocks_inst_bin, 128, 0, stream>>>(rs.ps, sc, fp,
                                                                                                BatchDev{}, d);
+        else if (wide && rs.wide_stage == 73)
+            k_extend_dyn<128, kExtendRefill, 73><<<sms * rs.extend_blocks_stage, 128, 0, stream>>>(rs.ps, sc, fp, d);
         else if (wide)
             k_extend_dyn<128, kExtendRefill><<<sms * rs.extend_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
         else

@@ -172,8 +172,44 @@ def test_device_mixture_sampler_matches_its_pdf(gpu):
 
 
 @pytest.mark.gpu
-def test_device_training_tracks_the_oracle(gpu):
+@pytest.mark.parametrize("n", [3000, 100_000])
+def test_tensor_core_gradient_matches_mma_sync(gpu, gpu_mma, n):
+    """The tcgen05 training kernel (the default) and the mma.sync one give
+    the same gradient and loss up to summation order and the bias gradients'
+    BF16 operands (3000 records: 24 tiles, one per CTA; 100,000: several
+    tiles accumulated per CTA in tensor memory), and both match the oracle."""
     from lucida_b200 import Guide, records_array
+    p = _params(5)
+    x, nrm, wo, wi, F = _records(n, 6)
+    rec = records_array(x, nrm, wo, wi, F)
+    g_tc, l_tc = Guide(gpu, params=p, lo=LO, hi=HI).gradient(rec)
+    g_mm, l_mm = Guide(gpu_mma, params=p, lo=LO, hi=HI).gradient(rec)
+    X = OG.encode(x, nrm, wo, LO, HI)
+    o, acts = OG.forward(p, X)
+    loss, go = OG.loss_and_grad_outputs(o, wi, F)
+    g_ref = OG.backward(p, acts, go)
+    assert abs(l_tc - l_mm) < 1e-4 * abs(l_mm) + 1e-6, (l_tc, l_mm)
+    assert abs(l_tc - loss) < 1e-3 * abs(loss) + 1e-4, (l_tc, loss)
+    off = 0
+    for name, shape in OG.SHAPES:
+        k = int(np.prod(shape))
+        a, b, c = (v[off:off + k].astype(np.float64) for v in (g_tc, g_mm, g_ref))
+        off += k
+        if name == "W1":
+            assert np.all(a.reshape(shape)[:, 120:] == 0)
+            a, b, c = (v.reshape(shape)[:, :120].ravel() for v in (a, b, c))
+        rel_mm = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
+        rel_ref = np.linalg.norm(a - c) / max(np.linalg.norm(c), 1e-12)
+        print(f"grad {name}: tcgen05 vs mma.sync {rel_mm:.2e}, vs oracle {rel_ref:.2e}")
+        assert rel_mm < 1e-2, (name, rel_mm)
+        assert rel_ref < 3e-2, (name, rel_ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", ["tcgen05", "mma.sync"])
+def test_device_training_tracks_the_oracle(request, kernel):
+    from lucida_b200 import Guide, records_array
+    gpu = request.getfixturevalue("gpu" if kernel == "tcgen05" else "gpu_mma")
     p0 = OG.init_params(11)
     guide = Guide(gpu, params=p0, lo=LO, hi=HI)
     n = 2048
