@@ -574,8 +574,8 @@ __global__ void __launch_bounds__(kM, 1) k_guide_train_tc(const float4* __restri
             in[7] = c4.y;
             in[8] = c4.z;
         }
-        write_feature_half(S.x, r, 0, in, g);
-        write_feature_half(S.x, r, 1, in, g);
+        write_feature_half(S.x, r, 0, in, g);               // features 0..63: chunks 0..7
+        write_feature_half(S.x + 8 * kLboA, r, 1, in, g);   // features 64..127: chunks 8..15
         *chunk(S.x, 15, r) = make_uint4(0u, 0u, 0u, 0x3F800000u);  // feature 127 = 1 (bias gradient of b1)
         bool ok = fwd(S.x, 8, S.w1, kLboH, kGHid);
         if (ok) {

@@ -414,14 +414,29 @@ LUC_D void wide_node(const float4* __restrict__ wn, uint32_t node, V3 o, V3 inv,
 template <int kStage>
 LUC_D void wide_node_staged(const float4* __restrict__ wn, const float4* stage, uint32_t node, V3 o, V3 inv,
                             uint32_t oct, float tmin, float tmax, uint2& ng, uint3& tg) {
-    if (kStage > 0 && node < (uint32_t)kStage) {
-        const float4* q = stage + 5 * node;
-        wide_slabs(q[0], *reinterpret_cast<const uint4*>(q + 1), *reinterpret_cast<const uint4*>(q + 2),
-                   *reinterpret_cast<const uint4*>(q + 3), *reinterpret_cast<const uint4*>(q + 4), o, inv, oct, tmin,
-                   tmax, ng, tg);
-    } else {
+    if (kStage == 0) {
         wide_node(wn, node, o, inv, oct, tmin, tmax, ng, tg);
+        return;
     }
+    // Only the five loads branch; the slab tests run once for either source.
+    float4 a;
+    uint4 b, c, d, e;
+    if (node < (uint32_t)kStage) {
+        const float4* q = stage + 5 * node;
+        a = q[0];
+        b = *reinterpret_cast<const uint4*>(q + 1);
+        c = *reinterpret_cast<const uint4*>(q + 2);
+        d = *reinterpret_cast<const uint4*>(q + 3);
+        e = *reinterpret_cast<const uint4*>(q + 4);
+    } else {
+        const float4* q = wn + 5 * (size_t)node;
+        a = __ldg(q);
+        b = __ldg(reinterpret_cast<const uint4*>(q + 1));
+        c = __ldg(reinterpret_cast<const uint4*>(q + 2));
+        d = __ldg(reinterpret_cast<const uint4*>(q + 3));
+        e = __ldg(reinterpret_cast<const uint4*>(q + 4));
+    }
+    wide_slabs(a, b, c, d, e, o, inv, oct, tmin, tmax, ng, tg);
 }
 LUC_D void wide_slabs(const float4 a, const uint4 b, const uint4 c, const uint4 d, const uint4 e, V3 o, V3 inv,
                       uint32_t oct, float tmin, float tmax, uint2& ng, uint3& tg) {
