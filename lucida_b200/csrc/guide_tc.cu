@@ -655,24 +655,22 @@ __global__ void __launch_bounds__(kM, 1) k_guide_train_tc(const float4* __restri
             }
         }
         // dW2^T, dW3^T, dW4^T: row r < 64 = input unit r; row 64 = the bias gradient.
-        float* const gbs[3] = {gb2, gb3, gb4};
-        const int pw[3] = {kPartW2, kPartW3, kPartW4};
-        const uint32_t cols[3] = {kColW2, kColW3, kColW4};
-#pragma unroll 1
-        for (int l = 0; l < 3; ++l) {
-            const int nout = l == 2 ? kGOutPad : kGHid, nreal = l == 2 ? kGOut : kGHid;
+        auto read_dw = [&](uint32_t col, int poff, int nout, int nreal, float* gb) {
 #pragma unroll 1
             for (int q = 0; q < nout / 16; ++q) {
                 float v[16];
-                ld16(tm + cols[l] + lane_off + 16 * q, v);
+                ld16(tm + col + lane_off + 16 * q, v);
 #pragma unroll
                 for (int k = 0; k < 16; ++k) {
                     const int o = 16 * q + k;
-                    if (r < kGHid) P[pw[l] + o * kGHid + r] = v[k];
-                    else if (r == kGHid && o < nreal) atomicAdd(gbs[l] + o, v[k]);
+                    if (r < kGHid) P[poff + o * kGHid + r] = v[k];
+                    else if (r == kGHid && o < nreal) atomicAdd(gb + o, v[k]);
                 }
             }
-        }
+        };
+        read_dw(kColW2, kPartW2, kGHid, kGHid, gb2);
+        read_dw(kColW3, kPartW3, kGHid, kGHid, gb3);
+        read_dw(kColW4, kPartW4, kGOutPad, kGOut, gb4);
     } else {
         for (int i = t; i < kPartFloats / 4; i += blockDim.x)
             reinterpret_cast<float4*>(P)[i] = make_float4(0.f, 0.f, 0.f, 0.f);

@@ -1,7 +1,7 @@
 """What the trained guide gains over rendering without it.
 
 On a small guided room (24 displaced spheres in the half-closed room lit by
-two small emitters facing the ceiling; 96 x 96, 8 bounces) the guide is
+two small emitters facing the ceiling; 128 x 128, 8 bounces) the guide is
 trained online on the tracer's own records (guided 1-spp frames, one Adam
 step each), then frozen; guided and plain renders of the same sample count
 (their own seeds) are compared with a 4096-spp plain reference by mean
@@ -17,10 +17,10 @@ from lucida_b200 import Guide, scenes
 
 pytestmark = pytest.mark.gpu
 
-W = H = 96
+W = H = 128
 DEPTH = 8
-TRAIN_FRAMES = 400
-SPP = 64
+TRAIN_FRAMES = 1500
+SPP = 128
 MARGIN = 1.3
 
 
@@ -46,7 +46,7 @@ def test_trained_guide_lowers_error_at_equal_samples():
     guide.configure(train=False)
     untrained = _mse(_image(lb.render_accum(g, s, test, guided=True)), ref)
 
-    guide.configure(train=True, records_per_step=1 << 15, lr=1e-2)
+    guide.configure(train=True, records_per_step=1 << 16, lr=1e-2)
     train = lb.RenderParams(width=W, height=H, samples=1, max_depth=DEPTH, frame_seed=0x0BADCAFE)
     for k in range(TRAIN_FRAMES):
         train.sample_offset = k
