@@ -144,10 +144,6 @@ int32_t luc_create(int32_t device, luc_ctx** out) {
     if (const char* g = std::getenv("LUC_BINARY_BVH")) c->use_wide = g[0] == '\0' || g[0] == '0';
     if (const char* g = std::getenv("LUC_GUIDE_TC")) c->rs.guide_tc = g[0] != '\0' && g[0] != '0';
     if (const char* w = std::getenv("LUC_WIDE_STAGE")) c->rs.wide_stage = std::atoi(w) == 73 ? 73 : 0;
-    if (const char* v = std::getenv("LUC_SORT_VARIANT")) {
-        const int k = std::atoi(v);
-        c->sort_variant = k >= 0 && k <= 5 ? k : 0;
-    }
     const std::vector<float>& et = energy_table_cached();
     if (upload(c->energy, et.data(), et.size(), c->stream) != cudaSuccess ||
         luc_init_sobol_tables(c->stream) != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) {

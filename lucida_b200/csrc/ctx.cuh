@@ -42,8 +42,6 @@ struct luc_ctx {
     // forward's bounded wait is made to run out after dbg_limit polls of a
     // flag nothing sets. One-shot: the call that uses it clears dbg_mode.
     uint32_t dbg_mode = 0, dbg_limit = 0;
-    // Radix-sort block shape (lbvh.cu, kSortVariants; LUC_SORT_VARIANT).
-    int sort_variant = 0;
     FrameGraph graph;
     bool use_graphs = true;
     cudaStream_t own_stream = nullptr;

@@ -284,155 +284,6 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint32_t* __
     }
 }
 
-// The onesweep pass as a template over the block shape: T threads (>= 256;
-// thread d < 256 owns digit d in the look-back and the scans), K keys per
-// thread, MINB blocks per SM. Same algorithm and results as k_onesweep (the
-// tile is T*K keys; equal keys keep their input order); values are read at
-// the scatter instead of being held in registers through the ranking.
-template <int T, int K, int MINB>
-__global__ void __launch_bounds__(T, MINB) k_onesweep_t(const uint32_t* __restrict__ kin,
-                                                        const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
-                                                        uint32_t* __restrict__ vout, uint32_t n, int shift,
-                                                        const uint32_t* __restrict__ digit_offsets, uint32_t* status,
-                                                        uint32_t* tile_counter, uint32_t* err, uint32_t spin_limit) {
-    constexpr uint32_t TILE = (uint32_t)T * K, WARPS = T / 32;
-    __shared__ uint32_t s_tile;
-    extern __shared__ __align__(16) uint32_t s_dyn[];  // onesweep_smem<T, K>() bytes
-    uint32_t(*whist)[256] = reinterpret_cast<uint32_t(*)[256]>(s_dyn);
-    uint32_t* s_base = s_dyn + WARPS * 256;
-    uint32_t* s_start = s_base + 256;
-    uint32_t* s_keys = s_start + 256;
-    uint32_t* s_vals = s_keys + TILE;
-    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    for (uint32_t t = tid; t < WARPS * 256; t += T) (&whist[0][0])[t] = 0;
-    if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    const uint32_t wbase = tile * TILE + warp * (32u * K);
-    const uint32_t lt = (1u << lane) - 1u;
-    uint32_t key[K], rank[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        const uint32_t idx = wbase + k * 32u + lane;
-        key[k] = idx < n ? kin[idx] : 0u;
-    }
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        const uint32_t idx = wbase + k * 32u + lane;
-        const bool valid = idx < n;
-        const uint32_t digit = valid ? (key[k] >> shift) & 255u : 256u;
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, digit);
-        const uint32_t before = valid ? whist[warp][digit] : 0u;
-        __syncwarp();
-        if (valid && lane == (uint32_t)(__ffs(peers) - 1)) whist[warp][digit] = before + __popc(peers);
-        __syncwarp();
-        rank[k] = valid ? before + __popc(peers & lt) : kNone;
-    }
-    __syncthreads();
-    uint32_t total = 0, excl = 0;
-    if (tid < 256) {
-        for (uint32_t w = 0; w < WARPS; ++w) {
-            const uint32_t c = whist[w][tid];
-            whist[w][tid] = total;
-            total += c;
-        }
-        volatile uint32_t* st = status;
-        if (tile == 0) {
-            atomicExch(status + tid, total | kFlagInc);
-        } else {
-            atomicExch(status + (size_t)tile * 256 + tid, total | kFlagAgg);
-            int64_t j = (int64_t)tile - 1;
-            uint32_t spins = 0;
-            while (j >= 0) {
-                const uint32_t sv = st[(size_t)j * 256 + tid];
-                const uint32_t flag = sv & ~kCountMask;
-                if (flag == 0) {
-                    if (++spins > spin_limit) {  // bounded wait: report, never hang
-                        atomicExch(err, 1u);
-                        break;
-                    }
-                    continue;
-                }
-                excl += sv & kCountMask;
-                if (flag == kFlagInc) break;
-                --j;
-            }
-            __threadfence();
-            atomicExch(status + (size_t)tile * 256 + tid, (excl + total) | kFlagInc);
-        }
-        s_base[tid] = digit_offsets[tid] + excl;
-        s_start[tid] = total;
-    }
-    __syncthreads();
-    for (uint32_t off = 1; off < 256; off <<= 1) {
-        const uint32_t tt = (tid < 256 && tid >= off) ? s_start[tid - off] : 0u;
-        __syncthreads();
-        if (tid < 256) s_start[tid] += tt;
-        __syncthreads();
-    }
-    if (tid < 256) s_start[tid] -= total;
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        if (rank[k] == kNone) continue;
-        const uint32_t digit = (key[k] >> shift) & 255u;
-        const uint32_t local = s_start[digit] + whist[warp][digit] + rank[k];
-        s_keys[local] = key[k];
-        s_vals[local] = vin[wbase + k * 32u + lane];
-    }
-    __syncthreads();
-    const uint32_t first_key = tile * TILE;
-    const uint32_t count = first_key < n ? min(TILE, n - first_key) : 0u;
-    for (uint32_t i = tid; i < count; i += T) {
-        const uint32_t kk = s_keys[i];
-        const uint32_t digit = (kk >> shift) & 255u;
-        const uint32_t dst = s_base[digit] + (i - s_start[digit]);
-        if (dst < n) {
-            kout[dst] = kk;
-            vout[dst] = s_vals[i];
-        }
-    }
-}
-
-// The block shapes measured for the sort (LUC_SORT_VARIANT selects one for
-// a context; 0 = k_onesweep). tile keys = threads x keys per thread.
-struct SortVariant {
-    int threads, kpt;
-};
-constexpr SortVariant kSortVariants[] = {{256, 16}, {256, 16}, {512, 8}, {512, 8}, {256, 8}, {1024, 4}};
-inline uint32_t sort_variant_tile(int v) {
-    return (uint32_t)kSortVariants[v].threads * kSortVariants[v].kpt;
-}
-template <int T, int K>
-constexpr size_t onesweep_smem() {
-    return ((size_t)(T / 32) * 256 + 512 + 2 * (size_t)T * K) * sizeof(uint32_t);
-}
-template <int T, int K, int MINB>
-cudaError_t launch_onesweep_t(uint32_t tiles, cudaStream_t s, const uint32_t* ka, const uint32_t* va, uint32_t* kb,
-                              uint32_t* vb, uint32_t n, int shift, const uint32_t* offs, uint32_t* status,
-                              uint32_t* tcount, uint32_t* err, uint32_t spin) {
-    constexpr size_t bytes = onesweep_smem<T, K>();
-    cudaError_t e = cudaFuncSetAttribute(k_onesweep_t<T, K, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)bytes);
-    if (e != cudaSuccess) return e;
-    k_onesweep_t<T, K, MINB><<<tiles, T, bytes, s>>>(ka, va, kb, vb, n, shift, offs, status, tcount, err, spin);
-    return cudaGetLastError();
-}
-cudaError_t launch_onesweep(int v, uint32_t tiles, cudaStream_t s, const uint32_t* ka, const uint32_t* va,
-                            uint32_t* kb, uint32_t* vb, uint32_t n, int shift, const uint32_t* offs,
-                            uint32_t* status, uint32_t* tcount, uint32_t* err, uint32_t spin) {
-    switch (v) {
-        case 1: return launch_onesweep_t<256, 16, 3>(tiles, s, ka, va, kb, vb, n, shift, offs, status, tcount, err, spin);
-        case 2: return launch_onesweep_t<512, 8, 2>(tiles, s, ka, va, kb, vb, n, shift, offs, status, tcount, err, spin);
-        case 3: return launch_onesweep_t<512, 8, 3>(tiles, s, ka, va, kb, vb, n, shift, offs, status, tcount, err, spin);
-        case 4: return launch_onesweep_t<256, 8, 4>(tiles, s, ka, va, kb, vb, n, shift, offs, status, tcount, err, spin);
-        case 5: return launch_onesweep_t<1024, 4, 1>(tiles, s, ka, va, kb, vb, n, shift, offs, status, tcount, err, spin);
-        default:
-            k_onesweep<<<tiles, kSortThreads, 0, s>>>(ka, va, kb, vb, n, shift, offs, status, tcount, err, spin);
-            return cudaGetLastError();
-    }
-}
-
 // ---------------------------------------------------------------- Karras
 __device__ __forceinline__ int lcp(const uint32_t* __restrict__ c, int64_t n, int32_t i, int32_t j) {
     if (j < 0 || j >= n) return -1;
@@ -594,8 +445,7 @@ int32_t luc_radix_sort_device(luc_ctx* c, uint32_t n) {
     if (n <= 1) return LUC_OK;
     if (n > kCountMask) return luc_fail(c, LUC_ERR_VALIDATION, "sort: more than 2^30-1 keys");
     cudaStream_t s = c->stream;
-    const int variant = c->sort_variant;
-    uint32_t tiles = (n + sort_variant_tile(variant) - 1) / sort_variant_tile(variant);
+    uint32_t tiles = (n + kTile - 1) / kTile;
     LUC_CUDA(c, c->lb_keys2.ensure((size_t)n * 4), "alloc sort");
     LUC_CUDA(c, c->lb_vals2.ensure((size_t)n * 4), "alloc sort");
     LUC_CUDA(c, c->lb_hist.ensure((4 * 256 + 4 * 256 + 8) * 4), "alloc sort");
@@ -627,9 +477,8 @@ int32_t luc_radix_sort_device(luc_ctx* c, uint32_t n) {
     const int passes = orphan ? 1 : 4;
     for (int p = 0; p < passes; ++p) {
         cudaMemsetAsync(c->lb_look.p, 0, (size_t)(tiles + 1) * 256 * 4, s);
-        LUC_CUDA(c, launch_onesweep(variant, tiles, s, ka, va, kb, vb, n, 8 * p, offs + 256 * p,
-                                    c->lb_look.as<uint32_t>(), tcount + p, tcount + 4, p == 0 ? spin : kSpinLimit),
-                 "radix sort pass");
+        k_onesweep<<<tiles, kSortThreads, 0, s>>>(ka, va, kb, vb, n, 8 * p, offs + 256 * p, c->lb_look.as<uint32_t>(),
+                                                   tcount + p, tcount + 4, p == 0 ? spin : kSpinLimit);
         std::swap(ka, kb);
         std::swap(va, vb);
     }

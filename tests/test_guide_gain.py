@@ -21,7 +21,7 @@ W = H = 128
 DEPTH = 8
 TRAIN_FRAMES = 1500
 SPP = 128
-MARGIN = 1.3
+MARGIN = 3.0
 
 
 def _image(acc):
