@@ -144,6 +144,7 @@ int32_t luc_create(int32_t device, luc_ctx** out) {
     if (const char* g = std::getenv("LUC_BINARY_BVH")) c->use_wide = g[0] == '\0' || g[0] == '0';
     if (const char* g = std::getenv("LUC_GUIDE_TC")) c->rs.guide_tc = g[0] != '\0' && g[0] != '0';
     if (const char* w = std::getenv("LUC_WIDE_STAGE")) c->rs.wide_stage = std::atoi(w) == 73 ? 73 : 0;
+    if (const char* sp = std::getenv("LUC_SPLIT_ESCAPES")) c->rs.split = sp[0] != '\0' && sp[0] != '0';
     const std::vector<float>& et = energy_table_cached();
     if (upload(c->energy, et.data(), et.size(), c->stream) != cudaSuccess ||
         luc_init_sobol_tables(c->stream) != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) {
@@ -570,7 +571,7 @@ int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth) {
     paths = std::max(paths, rs.capacity);
     ctrs = std::max(ctrs, rs.ctr_capacity);
     const size_t f4 = sizeof(float4);
-    size_t bytes = paths * (11 * f4 + 4 * sizeof(uint32_t)) + ctrs * sizeof(uint32_t) + 16 * 256;
+    size_t bytes = paths * (11 * f4 + 6 * sizeof(uint32_t)) + ctrs * sizeof(uint32_t) + 18 * 256;
     LUC_CUDA(c, c->pool.ensure(bytes), "allocate path pool");
     char* p = (char*)c->pool.p;
     auto take = [&](size_t n) {
@@ -593,6 +594,8 @@ int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth) {
     ps.queue[0] = (uint32_t*)take(paths * 4);
     ps.queue[1] = (uint32_t*)take(paths * 4);
     ps.hinst = (uint32_t*)take(paths * 4);
+    ps.hitq = (uint32_t*)take(paths * 4);
+    ps.missq = (uint32_t*)take(paths * 4);
     ps.seg = (uint32_t*)take(paths * 4);
     ps.ctr = (uint32_t*)take(ctrs * 4);
     ps.stat = (unsigned long long*)take(8 * sizeof(unsigned long long));
@@ -672,6 +675,7 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     fp.sampling = u->sampling_mode;
     fp.max_depth = max_depth;
     fp.guides = (flags & LUC_FLAG_NO_GUIDES) ? 0u : 1u;
+    fp.split = c->rs.split ? 1u : 0u;
     if (guided) {
         fp.guided = 1u;
         fp.rec_cap = c->guide_train ? c->guide_rec_cap : 0u;

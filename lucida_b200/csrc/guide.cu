@@ -252,8 +252,7 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(PathState ps, 
     InferSmem& S = *reinterpret_cast<InferSmem*>(smem_raw);
     load_net(S.net, fp.guide.wbf, fp.guide.bias);
     __syncthreads();
-    const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
-    const uint32_t* queue = ps.queue[depth & 1];
+    const uint32_t len = shaded_count(ps, fp, depth);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float* o = S.o[warp];
     const uint32_t nwarps = gridDim.x * kInferWarps;
@@ -262,7 +261,7 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_guide_infer(PathState ps, 
         bool hit_row = false;
         if (base + lane < len) {
             const uint32_t i = base + lane;
-            const uint32_t q = depth == 0 ? i : queue[i];
+            const uint32_t q = shaded_path(ps, fp, depth, i);
             const float4 h4 = ps.hit[q];
             const uint32_t id = __float_as_uint(h4.w);
             if (id != kMiss) {

@@ -330,12 +330,11 @@ __global__ void __launch_bounds__(kTeamCta, 1) k_forward_tc(const float* __restr
 // same operation order (the softmax sum is the two half-sums added).
 __global__ void __launch_bounds__(kTeamCta, 1) k_infer_tc(PathState ps, const __grid_constant__ DevScene sc,
                                                  const __grid_constant__ FrameParams fp, uint32_t depth) {
-    const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
-    const uint32_t* queue = ps.queue[depth & 1];
+    const uint32_t len = shaded_count(ps, fp, depth);
     forward_teams(
         len, fp.guide, ps.gmisc + kGmTcError,
         [&](uint32_t i, float (&in)[9]) {
-            const uint32_t q = depth == 0 ? i : queue[i];
+            const uint32_t q = shaded_path(ps, fp, depth, i);
             const float4 h4 = ps.hit[q];
             const uint32_t id = __float_as_uint(h4.w);
             if (id == kMiss) return false;

@@ -10,11 +10,13 @@ namespace luc {
 
 // Per-depth device counters: queue length entering the depth, shadow rays
 // appended at the depth.
-constexpr uint32_t kCtrStride = 4;
+constexpr uint32_t kCtrStride = 8;
 constexpr uint32_t kCtrQueue = 0;
 constexpr uint32_t kCtrShadow = 1;
 constexpr uint32_t kCtrPullExtend = 2;  // ray-pull cursor of EXTEND at this depth
 constexpr uint32_t kCtrPullConnect = 3;  // ray-pull cursor of CONNECT at this depth
+constexpr uint32_t kCtrHit = 4;   // split frames: extended paths whose ray hit a surface
+constexpr uint32_t kCtrMiss = 5;  // split frames: extended paths whose ray escaped
 
 // SoA path pool, one float4 per field per path (128-bit accesses).
 struct PathState {
@@ -31,6 +33,8 @@ struct PathState {
     float4* sh_d;   // shadow ray direction, path id (u32 bits)
     float4* sh_c;   // shadow ray contribution
     uint32_t* queue[2];
+    // Split frames: this depth's extended paths by outcome (k_classify).
+    uint32_t *hitq, *missq;
     uint32_t* ctr;
     // [0] extend rays, [1] extend node visits, [2] extend triangle tests,
     // [3] shadow rays, [4] shadow node visits, [5] shadow triangle tests.
@@ -55,10 +59,25 @@ struct FrameParams {
     uint32_t guides;
     uint32_t guided;   // one-sample MIS with the learned proposal
     uint32_t rec_cap;  // training records per batch (0: no recording)
+    // Hits and escaped rays shaded apart (hit queue for SHADE and the guide,
+    // k_escape for the rest); single-scene frames.
+    uint32_t split;
     GuideDev guide;
     float lens_radius;
     V3 cam_origin, cam_upper_left, cam_horizontal, cam_vertical;
 };
+
+// The paths SHADE and the guide's inference visit at `depth`, and the i-th
+// of them: the hit queue in split frames, else every extended path (all
+// paths at depth 0, the survivor queue after).
+LUC_D uint32_t shaded_count(const PathState& ps, const FrameParams& fp, uint32_t depth) {
+    if (fp.split) return ps.ctr[depth * kCtrStride + kCtrHit];
+    return depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
+}
+LUC_D uint32_t shaded_path(const PathState& ps, const FrameParams& fp, uint32_t depth, uint32_t i) {
+    if (fp.split) return ps.hitq[i];
+    return depth == 0 ? i : ps.queue[depth & 1][i];
+}
 
 // CUDA-event marks between stages, accumulated per stage.
 struct StageTimer {
@@ -110,6 +129,9 @@ struct RenderState {
     // Closest-hit traversal of single-level wide trees with the top 73
     // nodes (root and two levels) staged in shared memory (LUC_WIDE_STAGE=73).
     int wide_stage = 0;
+    // Hits and escaped rays shaded apart (k_classify, k_escape, SHADE over
+    // the hit queue); LUC_SPLIT_ESCAPES=0 shades every extended path in SHADE.
+    bool split = true;
     int extend_blocks_stage = 8;
     uint64_t launches = 0;
 };

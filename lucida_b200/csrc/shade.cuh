@@ -52,6 +52,35 @@ LUC_D void camera_ray(const FrameParams& fp, uint32_t pixel, Sampler& smp, V3& o
 // `rad` is updated in place (the return value says whether it changed);
 // `lob` / `lobe_stride` locate the path's guide mixture (guided frames). The
 // sampler advances in place.
+// An escaped ray (integrator.rs:228-263): the environment through its MIS
+// weight (full credit at depth 0 and for BSDF-only sampling, none for
+// NEE-only), or the background. `rad` is updated in place; the return value
+// says whether it changed. SHADE runs it for a miss; split frames run it in
+// k_escape for the escaped queue.
+template <bool kSkyMis>
+LUC_D bool escape_vertex(const DevScene& sc, const FrameParams& fp, uint32_t depth, V3 dir, V3 thr, V3& rad,
+                         float prev_pdf) {
+    const uint32_t sampling = kSkyMis ? LUC_SAMPLING_MIS : fp.sampling;
+    if (kSkyMis || sc.has_env) {
+        float epdf;
+        V3 l = env_radiance_pdf(sc, dir, epdf);
+        float weight;
+        if (depth == 0 || sampling == LUC_SAMPLING_BSDF) weight = 1.0f;
+        else if (sampling == LUC_SAMPLING_NEE) weight = 0.0f;
+        else {
+            uint32_t total = max(sc.light_strategies, 1u);
+            weight = power_heuristic(prev_pdf, epdf / (float)total);
+        }
+        if (weight > 0.0f) {
+            rad = rad + thr * l * weight;
+            return true;
+        }
+        return false;
+    }
+    rad = rad + thr * sc.background;
+    return true;
+}
+
 template <bool kGuided, bool kInst, bool kSkyMis = false, typename Sink>
 LUC_D bool shade_vertex(const DevScene& sc, const FrameParams& fp, uint32_t depth, Sampler& smp, V3 org, V3 dir,
                         V3 thr, V3& rad, float prev_pdf, float4 h4, uint32_t inst, const float4* lob,
@@ -60,28 +89,7 @@ LUC_D bool shade_vertex(const DevScene& sc, const FrameParams& fp, uint32_t dept
     const uint32_t sampling = kSkyMis ? LUC_SAMPLING_MIS : fp.sampling;
     const uint32_t id = __float_as_uint(h4.w);
     bool rad_changed = false;
-    if (id == kMiss) {
-        // Escaped (integrator.rs:228-263).
-        if (kSkyMis || sc.has_env) {
-            float epdf;
-            V3 l = env_radiance_pdf(sc, dir, epdf);
-            float weight;
-            if (depth == 0 || sampling == LUC_SAMPLING_BSDF) weight = 1.0f;
-            else if (sampling == LUC_SAMPLING_NEE) weight = 0.0f;
-            else {
-                uint32_t total = max(sc.light_strategies, 1u);
-                weight = power_heuristic(prev_pdf, epdf / (float)total);
-            }
-            if (weight > 0.0f) {
-                rad = rad + thr * l * weight;
-                rad_changed = true;
-            }
-        } else {
-            rad = rad + thr * sc.background;
-            rad_changed = true;
-        }
-        return rad_changed;
-    }
+    if (id == kMiss) return escape_vertex<kSkyMis>(sc, fp, depth, dir, thr, rad, prev_pdf);
     const SurfaceHit hit = surface_hit_t<kInst>(sc, id, inst, h4.x, h4.y, h4.z, org, dir);
     const GpuMaterial m = sc.materials[hit.material];
     const V3 emissive = ld3(m.emissive);

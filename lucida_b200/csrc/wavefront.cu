@@ -373,10 +373,9 @@ template <bool kGuided, bool kInst, bool kBatch = false, bool kSobol = false, bo
 __global__ void __launch_bounds__(128, 8) k_shade(PathState ps, const __grid_constant__ DevScene sc_arg,
                                                   const __grid_constant__ FrameParams fp_arg, BatchDev bd,
                                                   uint32_t depth) {
-    const uint32_t len = depth == 0 ? (uint32_t)fp_arg.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
+    const uint32_t len = shaded_count(ps, fp_arg, depth);
     const uint32_t rec_threshold = kGuided ? ps.gmisc[kGmThreshold] : 65536u;
     const uint32_t sbase_arg = kBatch ? 0u : *fp_arg.sbase;
-    const uint32_t* queue = ps.queue[depth & 1];
     uint32_t* next_queue = ps.queue[(depth + 1) & 1];
     uint32_t* next_len = ps.ctr + (depth + 1) * kCtrStride + kCtrQueue;
     uint32_t* shadow_len = ps.ctr + depth * kCtrStride + kCtrShadow;
@@ -391,7 +390,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(PathState ps, const __grid_con
         V3 sh_o{0, 0, 0}, sh_d{0, 0, 0}, sh_c{0, 0, 0};
         float sh_t = 0.0f;
         if (active) {
-            p = depth == 0 ? i : queue[i];
+            p = shaded_path(ps, fp_arg, depth, i);
             const BatchSegDev* seg = kBatch ? bd.segs + ps.seg[p] : nullptr;
             const BatchJobDev* job = kBatch ? bd.jobs + seg->job : nullptr;
             const DevScene& sc = kBatch ? bd.scenes[job->scene] : sc_arg;
@@ -440,6 +439,58 @@ __global__ void __launch_bounds__(128, 8) k_shade(PathState ps, const __grid_con
             store4(ps.sh_d + sslot, sh_d, __uint_as_float(p));
             store4(ps.sh_c + sslot, sh_c, 0.0f);
         }
+    }
+}
+
+// Split frames: this depth's extended paths into the hit queue and the
+// escaped queue (warp-aggregated appends), so that SHADE's warps run hits
+// only and escaped rays are shaded apart (k_escape): a warp mixing the two
+// ran the short escape code and the long surface code one after the other.
+__global__ void __launch_bounds__(256) k_classify(PathState ps, FrameParams fp, uint32_t depth) {
+    const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
+    const uint32_t* queue = ps.queue[depth & 1];
+    uint32_t* nhit = ps.ctr + depth * kCtrStride + kCtrHit;
+    uint32_t* nmiss = ps.ctr + depth * kCtrStride + kCtrMiss;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // Warp-uniform trip count so the appends' ballots see every lane.
+    const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;
+    for (uint32_t base = warp0; base < len; base += stride) {
+        const uint32_t i = base + (threadIdx.x & 31u);
+        const bool active = i < len;
+        uint32_t p = 0;
+        bool hit = false;
+        if (active) {
+            p = depth == 0 ? i : queue[i];
+            hit = __float_as_uint(__ldcs(&ps.hit[p].w)) != kMiss;
+        }
+        const uint32_t hs = warp_append(nhit, active && hit);
+        if (active && hit) ps.hitq[hs] = p;
+        const uint32_t ms = warp_append(nmiss, active && !hit);
+        if (active && !hit) ps.missq[ms] = p;
+    }
+}
+
+// Split frames: the escaped paths of this depth, shaded as SHADE shades a
+// miss (escape_vertex), and in guided frames the training record of the
+// previous vertex opened as SHADE opens it.
+template <bool kGuided, bool kSkyMis>
+__global__ void __launch_bounds__(256) k_escape(PathState ps, const __grid_constant__ DevScene sc,
+                                                const __grid_constant__ FrameParams fp, uint32_t depth) {
+    const uint32_t n = ps.ctr[depth * kCtrStride + kCtrMiss];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t p = ps.missq[i];
+        const float4 o4 = ld4(ps.o_pdf + p), d4 = ld4(ps.dir + p), t4 = ld4(ps.thr + p), r4 = ld4(ps.rad + p);
+        V3 rad = xyz(r4);
+        if (kGuided) {
+            const uint32_t slot1 = __float_as_uint(ps.prev[p].w);
+            if (slot1 != 0u) {
+                float* rs = reinterpret_cast<float*>(ps.rec + kGRecF4 * (size_t)(slot1 - 1u) + 4);
+                rs[0] = rad.x;
+                rs[1] = rad.y;
+                rs[2] = rad.z;
+            }
+        }
+        if (escape_vertex<kSkyMis>(sc, fp, depth, xyz(d4), xyz(t4), rad, o4.w)) store4(ps.rad + p, rad, 0.0f);
     }
 }
 
@@ -655,6 +706,10 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
             k_extend_dyn<128, kExtendRefill><<<sms * rs.extend_blocks, 128, 0, stream>>>(rs.ps, sc, fp, d);
         else
             k_extend<false, false, 128, 0><<<sms * rs.extend_blocks_bin, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
+        if (fp.split) {
+            k_classify<<<sms * 8, 256, 0, stream>>>(rs.ps, fp, d);
+            rs.launches++;
+        }
         if (d == 0 && gt && gt->join) cudaStreamWaitEvent(stream, gt->join, 0);  // the previous frame's step
         if (fp.guided && d + 1 < fp.max_depth) {
             if (timer) timer->mark(stream, StageTimer::kGuide);
@@ -663,6 +718,14 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
         }
         join_connect();
         if (timer) timer->mark(stream, StageTimer::kShade);
+        if (fp.split) {
+            const bool sky_mis = fp.sampling == LUC_SAMPLING_MIS && sc.num_lights == 0 && sc.has_env;
+            if (fp.guided && sky_mis) k_escape<true, true><<<sms * 8, 256, 0, stream>>>(rs.ps, sc, fp, d);
+            else if (fp.guided) k_escape<true, false><<<sms * 8, 256, 0, stream>>>(rs.ps, sc, fp, d);
+            else if (sky_mis) k_escape<false, true><<<sms * 8, 256, 0, stream>>>(rs.ps, sc, fp, d);
+            else k_escape<false, false><<<sms * 8, 256, 0, stream>>>(rs.ps, sc, fp, d);
+            rs.launches++;
+        }
         if (fp.guided && inst)
             launch_shade<true, true>(rs, sms * rs.shade_blocks_guided_inst, sc, fp, d, stream);
         else if (fp.guided)
