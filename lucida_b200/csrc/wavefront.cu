@@ -443,30 +443,62 @@ __global__ void __launch_bounds__(128, 8) k_shade(PathState ps, const __grid_con
 }
 
 // Split frames: this depth's extended paths into the hit queue and the
-// escaped queue (warp-aggregated appends), so that SHADE's warps run hits
-// only and escaped rays are shaded apart (k_escape): a warp mixing the two
-// ran the short escape code and the long surface code one after the other.
+// escaped queue, so that SHADE's warps run hits only and escaped rays are
+// shaded apart (k_escape): a warp mixing the two ran the short escape code
+// and the long surface code one after the other. Appends are aggregated per
+// block of kClassifyItems x 256 paths (one atomic per queue per block): with
+// one per warp the two counters' atomics bounded the kernel.
+constexpr int kClassifyItems = 8;
 __global__ void __launch_bounds__(256) k_classify(PathState ps, FrameParams fp, uint32_t depth) {
+    constexpr uint32_t kPerBlock = 256u * kClassifyItems;
+    __shared__ uint32_t s_cnt[2][8];  // per warp: hits, escapes
+    __shared__ uint32_t s_base[2];
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
     const uint32_t* queue = ps.queue[depth & 1];
     uint32_t* nhit = ps.ctr + depth * kCtrStride + kCtrHit;
     uint32_t* nmiss = ps.ctr + depth * kCtrStride + kCtrMiss;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    // Warp-uniform trip count so the appends' ballots see every lane.
-    const uint32_t warp0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;
-    for (uint32_t base = warp0; base < len; base += stride) {
-        const uint32_t i = base + (threadIdx.x & 31u);
-        const bool active = i < len;
-        uint32_t p = 0;
-        bool hit = false;
-        if (active) {
-            p = depth == 0 ? i : queue[i];
-            hit = __float_as_uint(__ldcs(&ps.hit[p].w)) != kMiss;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, lt = (1u << lane) - 1u;
+    for (uint32_t base = blockIdx.x * kPerBlock; base < len; base += gridDim.x * kPerBlock) {
+        uint32_t p[kClassifyItems], hb[kClassifyItems], mb[kClassifyItems];
+        uint32_t nh = 0, nm = 0;
+#pragma unroll
+        for (int k = 0; k < kClassifyItems; ++k) {
+            const uint32_t i = base + (uint32_t)k * 256u + tid;
+            const bool active = i < len;
+            p[k] = active ? (depth == 0 ? i : queue[i]) : 0u;
+            const bool hit = active && __float_as_uint(__ldcs(&ps.hit[p[k]].w)) != kMiss;
+            hb[k] = __ballot_sync(0xFFFFFFFFu, hit);
+            mb[k] = __ballot_sync(0xFFFFFFFFu, active && !hit);
+            nh += __popc(hb[k]);
+            nm += __popc(mb[k]);
         }
-        const uint32_t hs = warp_append(nhit, active && hit);
-        if (active && hit) ps.hitq[hs] = p;
-        const uint32_t ms = warp_append(nmiss, active && !hit);
-        if (active && !hit) ps.missq[ms] = p;
+        if (lane == 0) {
+            s_cnt[0][warp] = nh;
+            s_cnt[1][warp] = nm;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t th = 0, tm = 0;
+            for (int w = 0; w < 8; ++w) {
+                const uint32_t h = s_cnt[0][w], m = s_cnt[1][w];
+                s_cnt[0][w] = th;
+                s_cnt[1][w] = tm;
+                th += h;
+                tm += m;
+            }
+            s_base[0] = th ? atomicAdd(nhit, th) : 0u;
+            s_base[1] = tm ? atomicAdd(nmiss, tm) : 0u;
+        }
+        __syncthreads();
+        uint32_t oh = s_base[0] + s_cnt[0][warp], om = s_base[1] + s_cnt[1][warp];
+#pragma unroll
+        for (int k = 0; k < kClassifyItems; ++k) {
+            if (hb[k] >> lane & 1u) ps.hitq[oh + __popc(hb[k] & lt)] = p[k];
+            if (mb[k] >> lane & 1u) ps.missq[om + __popc(mb[k] & lt)] = p[k];
+            oh += __popc(hb[k]);
+            om += __popc(mb[k]);
+        }
+        __syncthreads();  // s_cnt / s_base are rewritten by the next round
     }
 }
 
@@ -707,7 +739,7 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
         else
             k_extend<false, false, 128, 0><<<sms * rs.extend_blocks_bin, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
         if (fp.split) {
-            k_classify<<<sms * 8, 256, 0, stream>>>(rs.ps, fp, d);
+            k_classify<<<sms * 4, 256, 0, stream>>>(rs.ps, fp, d);
             rs.launches++;
         }
         if (d == 0 && gt && gt->join) cudaStreamWaitEvent(stream, gt->join, 0);  // the previous frame's step
