@@ -571,7 +571,7 @@ int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth) {
     paths = std::max(paths, rs.capacity);
     ctrs = std::max(ctrs, rs.ctr_capacity);
     const size_t f4 = sizeof(float4);
-    size_t bytes = paths * (11 * f4 + 6 * sizeof(uint32_t)) + ctrs * sizeof(uint32_t) + 18 * 256;
+    size_t bytes = paths * (11 * f4 + 8 * sizeof(uint32_t)) + ctrs * sizeof(uint32_t) + 20 * 256;
     LUC_CUDA(c, c->pool.ensure(bytes), "allocate path pool");
     char* p = (char*)c->pool.p;
     auto take = [&](size_t n) {
@@ -594,7 +594,7 @@ int32_t ensure_pool(luc_ctx* c, uint64_t paths, uint32_t max_depth) {
     ps.queue[0] = (uint32_t*)take(paths * 4);
     ps.queue[1] = (uint32_t*)take(paths * 4);
     ps.hinst = (uint32_t*)take(paths * 4);
-    ps.hitq = (uint32_t*)take(paths * 4);
+    for (int k = 0; k < 3; ++k) ps.hitq[k] = (uint32_t*)take(paths * 4);
     ps.missq = (uint32_t*)take(paths * 4);
     ps.seg = (uint32_t*)take(paths * 4);
     ps.ctr = (uint32_t*)take(ctrs * 4);

@@ -15,8 +15,14 @@ constexpr uint32_t kCtrQueue = 0;
 constexpr uint32_t kCtrShadow = 1;
 constexpr uint32_t kCtrPullExtend = 2;  // ray-pull cursor of EXTEND at this depth
 constexpr uint32_t kCtrPullConnect = 3;  // ray-pull cursor of CONNECT at this depth
-constexpr uint32_t kCtrHit = 4;   // split frames: extended paths whose ray hit a surface
-constexpr uint32_t kCtrMiss = 5;  // split frames: extended paths whose ray escaped
+// Split frames: extended paths whose ray hit a surface, by material class
+// (kCtrHit + class slot: 4 = reflective non-metal, 6 = metal, 7 =
+// transmissive), and those whose ray escaped (5).
+constexpr uint32_t kCtrHit = 4;
+constexpr uint32_t kCtrMiss = 5;
+constexpr uint32_t kCtrHit1 = 6;
+constexpr uint32_t kCtrHit2 = 7;
+__host__ __device__ constexpr uint32_t hit_slot(uint32_t cls) { return cls == 0 ? kCtrHit : (cls == 1 ? kCtrHit1 : kCtrHit2); }
 
 // SoA path pool, one float4 per field per path (128-bit accesses).
 struct PathState {
@@ -33,8 +39,9 @@ struct PathState {
     float4* sh_d;   // shadow ray direction, path id (u32 bits)
     float4* sh_c;   // shadow ray contribution
     uint32_t* queue[2];
-    // Split frames: this depth's extended paths by outcome (k_classify).
-    uint32_t *hitq, *missq;
+    // Split frames: this depth's extended paths by outcome (k_classify):
+    // hits by material class, escaped rays.
+    uint32_t *hitq[3], *missq;
     uint32_t* ctr;
     // [0] extend rays, [1] extend node visits, [2] extend triangle tests,
     // [3] shadow rays, [4] shadow node visits, [5] shadow triangle tests.
@@ -71,11 +78,20 @@ struct FrameParams {
 // of them: the hit queue in split frames, else every extended path (all
 // paths at depth 0, the survivor queue after).
 LUC_D uint32_t shaded_count(const PathState& ps, const FrameParams& fp, uint32_t depth) {
-    if (fp.split) return ps.ctr[depth * kCtrStride + kCtrHit];
-    return depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
+    const uint32_t* c = ps.ctr + depth * kCtrStride;
+    if (fp.split) return c[kCtrHit] + c[kCtrHit1] + c[kCtrHit2];
+    return depth == 0 ? (uint32_t)fp.num_paths : c[kCtrQueue];
 }
+// In split frames the three class queues one after the other, so a warp's
+// 32 consecutive paths share a material class except at two boundaries.
 LUC_D uint32_t shaded_path(const PathState& ps, const FrameParams& fp, uint32_t depth, uint32_t i) {
-    if (fp.split) return ps.hitq[i];
+    if (fp.split) {
+        const uint32_t* c = ps.ctr + depth * kCtrStride;
+        const uint32_t n0 = c[kCtrHit], n1 = c[kCtrHit1];
+        if (i < n0) return ps.hitq[0][i];
+        i -= n0;
+        return i < n1 ? ps.hitq[1][i] : ps.hitq[2][i - n1];
+    }
     return depth == 0 ? i : ps.queue[depth & 1][i];
 }
 

@@ -442,61 +442,81 @@ __global__ void __launch_bounds__(128, 8) k_shade(PathState ps, const __grid_con
     }
 }
 
-// Split frames: this depth's extended paths into the hit queue and the
-// escaped queue, so that SHADE's warps run hits only and escaped rays are
-// shaded apart (k_escape): a warp mixing the two ran the short escape code
-// and the long surface code one after the other. Appends are aggregated per
-// block of kClassifyItems x 256 paths (one atomic per queue per block): with
-// one per warp the two counters' atomics bounded the kernel.
+// Split frames: this depth's extended paths into hit queues by material
+// class and the escaped queue, so that SHADE's warps run hits only, mostly
+// of one class (the BSDF's lobe choice and sampling code follow the class),
+// and escaped rays are shaded apart (k_escape): a warp mixing the two ran
+// the short escape code and the long surface code one after the other.
+// Appends are aggregated per block of kClassifyItems x 256 paths (one atomic
+// per queue per block): with one per warp the counters' atomics bounded the
+// kernel.
 constexpr int kClassifyItems = 8;
-__global__ void __launch_bounds__(256) k_classify(PathState ps, FrameParams fp, uint32_t depth) {
+// Material class of a hit: 0 reflective non-metal, 1 metal, 2 transmissive
+// (the lobes make_surface enables).
+LUC_D uint32_t hit_class(const DevScene& sc, const PathState& ps, uint32_t p, uint32_t id) {
+    uint32_t m;
+    if (id & kAnalytic) {
+        m = __ldg(&sc.prims[id & ~kAnalytic].material);
+    } else {
+        m = __ldg(&sc.tris[id].material);
+        if (sc.num_instances) {
+            const uint32_t o = __ldg(&sc.inst[ps.hinst[p]].material);
+            if (o != 0xFFFFFFFFu) m = o;
+        }
+    }
+    const float metallic = clampf(__ldg(&sc.materials[m].metallic), 0.0f, 1.0f);
+    const float transmission = clampf(__ldg(&sc.materials[m].transmission), 0.0f, 1.0f) * (1.0f - metallic);
+    return transmission > 0.0f ? 2u : (metallic >= 0.5f ? 1u : 0u);
+}
+__global__ void __launch_bounds__(256) k_classify(PathState ps, const __grid_constant__ DevScene sc, FrameParams fp,
+                                                  uint32_t depth) {
     constexpr uint32_t kPerBlock = 256u * kClassifyItems;
-    __shared__ uint32_t s_cnt[2][8];  // per warp: hits, escapes
-    __shared__ uint32_t s_base[2];
+    __shared__ uint32_t s_cnt[4][8];  // per warp: hits of class 0, 1, 2, escapes
+    __shared__ uint32_t s_base[4];
     const uint32_t len = depth == 0 ? (uint32_t)fp.num_paths : ps.ctr[depth * kCtrStride + kCtrQueue];
     const uint32_t* queue = ps.queue[depth & 1];
-    uint32_t* nhit = ps.ctr + depth * kCtrStride + kCtrHit;
-    uint32_t* nmiss = ps.ctr + depth * kCtrStride + kCtrMiss;
+    uint32_t* ctr = ps.ctr + depth * kCtrStride;
+    uint32_t* out[4] = {ps.hitq[0], ps.hitq[1], ps.hitq[2], ps.missq};
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, lt = (1u << lane) - 1u;
     for (uint32_t base = blockIdx.x * kPerBlock; base < len; base += gridDim.x * kPerBlock) {
-        uint32_t p[kClassifyItems], hb[kClassifyItems], mb[kClassifyItems];
-        uint32_t nh = 0, nm = 0;
+        uint32_t p[kClassifyItems], cls[kClassifyItems];
+        uint32_t n[4] = {0, 0, 0, 0};
 #pragma unroll
         for (int k = 0; k < kClassifyItems; ++k) {
             const uint32_t i = base + (uint32_t)k * 256u + tid;
             const bool active = i < len;
             p[k] = active ? (depth == 0 ? i : queue[i]) : 0u;
-            const bool hit = active && __float_as_uint(__ldcs(&ps.hit[p[k]].w)) != kMiss;
-            hb[k] = __ballot_sync(0xFFFFFFFFu, hit);
-            mb[k] = __ballot_sync(0xFFFFFFFFu, active && !hit);
-            nh += __popc(hb[k]);
-            nm += __popc(mb[k]);
-        }
-        if (lane == 0) {
-            s_cnt[0][warp] = nh;
-            s_cnt[1][warp] = nm;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            uint32_t th = 0, tm = 0;
-            for (int w = 0; w < 8; ++w) {
-                const uint32_t h = s_cnt[0][w], m = s_cnt[1][w];
-                s_cnt[0][w] = th;
-                s_cnt[1][w] = tm;
-                th += h;
-                tm += m;
+            cls[k] = 4u;  // inactive
+            if (active) {
+                const uint32_t id = __float_as_uint(__ldcs(&ps.hit[p[k]].w));
+                cls[k] = id == kMiss ? 3u : hit_class(sc, ps, p[k], id);
             }
-            s_base[0] = th ? atomicAdd(nhit, th) : 0u;
-            s_base[1] = tm ? atomicAdd(nmiss, tm) : 0u;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) n[q] += __popc(__ballot_sync(0xFFFFFFFFu, cls[k] == (uint32_t)q));
+        }
+        if (lane < 4) s_cnt[lane][warp] = n[lane];
+        __syncthreads();
+        if (tid < 4) {
+            uint32_t t = 0;
+            for (int w = 0; w < 8; ++w) {
+                const uint32_t c = s_cnt[tid][w];
+                s_cnt[tid][w] = t;
+                t += c;
+            }
+            s_base[tid] = t ? atomicAdd(ctr + (tid < 3 ? hit_slot(tid) : kCtrMiss), t) : 0u;
         }
         __syncthreads();
-        uint32_t oh = s_base[0] + s_cnt[0][warp], om = s_base[1] + s_cnt[1][warp];
+        uint32_t off[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) off[q] = s_base[q] + s_cnt[q][warp];
 #pragma unroll
         for (int k = 0; k < kClassifyItems; ++k) {
-            if (hb[k] >> lane & 1u) ps.hitq[oh + __popc(hb[k] & lt)] = p[k];
-            if (mb[k] >> lane & 1u) ps.missq[om + __popc(mb[k] & lt)] = p[k];
-            oh += __popc(hb[k]);
-            om += __popc(mb[k]);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t b = __ballot_sync(0xFFFFFFFFu, cls[k] == (uint32_t)q);
+                if (cls[k] == (uint32_t)q) out[q][off[q] + __popc(b & lt)] = p[k];
+                off[q] += __popc(b);
+            }
         }
         __syncthreads();  // s_cnt / s_base are rewritten by the next round
     }
@@ -739,7 +759,7 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
         else
             k_extend<false, false, 128, 0><<<sms * rs.extend_blocks_bin, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
         if (fp.split) {
-            k_classify<<<sms * 4, 256, 0, stream>>>(rs.ps, fp, d);
+            k_classify<<<sms * 4, 256, 0, stream>>>(rs.ps, sc, fp, d);
             rs.launches++;
         }
         if (d == 0 && gt && gt->join) cudaStreamWaitEvent(stream, gt->join, 0);  // the previous frame's step
