@@ -145,6 +145,7 @@ int32_t luc_create(int32_t device, luc_ctx** out) {
     if (const char* g = std::getenv("LUC_GUIDE_TC")) c->rs.guide_tc = g[0] != '\0' && g[0] != '0';
     if (const char* w = std::getenv("LUC_WIDE_STAGE")) c->rs.wide_stage = std::atoi(w) == 73 ? 73 : 0;
     if (const char* sp = std::getenv("LUC_SPLIT_ESCAPES")) c->rs.split = sp[0] != '\0' && sp[0] != '0';
+    if (const char* ic = std::getenv("LUC_INST_CULL")) c->inst_cull = ic[0] != '\0' && ic[0] != '0';
     const std::vector<float>& et = energy_table_cached();
     if (upload(c->energy, et.data(), et.size(), c->stream) != cudaSuccess ||
         luc_init_sobol_tables(c->stream) != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) {
@@ -504,6 +505,7 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     d.nodes = c->nodes.as<float4>();
     d.num_nodes = v->num_triangles ? num_nodes : 0;
     d.inst = reinterpret_cast<const GpuInstance*>(c->prims.as<GpuPrimitive>() + np_);
+    d.inst_box = nullptr;  // caller-built instancing (SceneBlob layout): no per-instance boxes
     d.num_instances = v->num_triangles ? ni : 0;
     d.tlas_root = v->tlas_root;
     d.blas_roots = c->blas_roots.as<uint32_t>();

@@ -63,6 +63,10 @@ struct luc_ctx {
     // node total (= the TLAS's first node), the analytic primitives, and the
     // instance capacity the buffers are sized for.
     DevBuf mesh_root, mesh_bounds, inst_in, inst_tmp;
+    // Device-built instancing: each instance's padded world box in TLAS-leaf
+    // order (two float4), tested before its BLAS is entered.
+    DevBuf inst_box;
+    bool inst_cull = true;  // LUC_INST_CULL=0 enters every BLAS of a TLAS leaf
     std::vector<uint32_t> host_mesh_root;
     std::vector<GpuPrimitive> host_prims;
     uint32_t blas_nodes = 0, inst_capacity = 0, num_meshes = 0;

@@ -122,6 +122,16 @@ __global__ void k_gather_instances(const GpuInstance* __restrict__ src, const ui
                                    GpuInstance* __restrict__ dst) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[order[i]];
 }
+// The instances' padded world boxes (the TLAS build's inputs) in TLAS-leaf
+// order, lo and hi as two float4 per instance.
+__global__ void k_gather_boxes(const float* __restrict__ boxes6, const uint32_t* __restrict__ order, uint32_t n,
+                               float4* __restrict__ dst) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* b = boxes6 + 6 * (size_t)order[i];
+        dst[2 * (size_t)i] = make_float4(b[0], b[1], b[2], 0.0f);
+        dst[2 * (size_t)i + 1] = make_float4(b[3], b[4], b[5], 0.0f);
+    }
+}
 
 // Object-space bounds of one mesh: the root of its freshly built LBVH.
 __global__ void k_mesh_bounds(const float4* __restrict__ root, float* __restrict__ out6) {
@@ -224,6 +234,7 @@ int32_t luc_set_instances(luc_ctx* c, const float* object_to_world, const uint32
         LUC_CUDA(c, c->prims.ensure(((size_t)np_ + n) * sizeof(GpuPrimitive)), "grow primitives");
         LUC_CUDA(c, cudaMemcpyAsync(c->prims.p, c->host_prims.data(), (size_t)np_ * sizeof(GpuPrimitive),
                                     cudaMemcpyHostToDevice, s), "upload primitives");
+        LUC_CUDA(c, c->inst_box.ensure((size_t)n * 2 * sizeof(float4)), "grow instance boxes");
         c->inst_capacity = n;  // moved arrays change the DevScene bytes, which key the frame graph
     }
     LUC_CUDA(c, c->inst_in.ensure((size_t)n * 56), "alloc instance input");
@@ -246,6 +257,8 @@ int32_t luc_set_instances(luc_ctx* c, const float* object_to_world, const uint32
                                                          c->nodes.as<float4>() + 2 * (size_t)bn);
     k_gather_instances<<<grid_n(n, c->num_sms), 256, 0, s>>>(c->inst_tmp.as<GpuInstance>(), c->lb_vals.as<uint32_t>(), n,
                                                             reinterpret_cast<GpuInstance*>(c->prims.as<GpuPrimitive>() + np_));
+    k_gather_boxes<<<grid_n(n, c->num_sms), 256, 0, s>>>(c->lb_boxes.as<float>(), c->lb_vals.as<uint32_t>(), n,
+                                                        c->inst_box.as<float4>());
     LUC_CUDA(c, cudaGetLastError(), "tlas");
     rc = luc_build_tnodes_range(c, bn, bn + tn);
     if (rc) return rc;
@@ -283,6 +296,7 @@ int32_t luc_set_instances(luc_ctx* c, const float* object_to_world, const uint32
     d.blas_wide = c->wide_nodes ? c->blas_wide.as<uint32_t>() : nullptr;
     d.num_nodes = bn + 2 * c->inst_capacity;  // fixed while the capacity holds, so frame graphs keep replaying
     d.inst = reinterpret_cast<const GpuInstance*>(d.prims + np_);
+    d.inst_box = c->inst_cull ? c->inst_box.as<float4>() : nullptr;
     d.num_instances = n;
     d.tlas_root = bn;
     d.blas_roots = c->mesh_root.as<uint32_t>();

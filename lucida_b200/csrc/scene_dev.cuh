@@ -33,6 +33,10 @@ struct DevScene {
     // primitives, in TLAS-leaf order; the TLAS's first node in `nodes`; the
     // distinct BLAS roots (for the reference's shadow-ray behaviour).
     const GpuInstance* inst;
+    // Device-built instancing: world box of each instance row (lo.xyz, hi.xyz
+    // in two float4), null otherwise; a ray enters an instance's BLAS only if
+    // it crosses the box.
+    const float4* inst_box;
     uint32_t num_instances, tlas_root;
     const uint32_t* blas_roots;
     uint32_t num_blas;
@@ -198,6 +202,16 @@ constexpr uint32_t kNoNode = 0xFFFFFFFFu;
 // ULPs; boxes are padded by 1e-6 relative (bvh.rs:100-111), far above that,
 // so no hit is ever culled. Only the visiting order of equal-entry boxes can
 // change, which matters solely for exactly tied triangle distances.
+// The slab test of test_pair on one box (lo in b[0].xyz, hi in b[1].xyz).
+LUC_D bool test_box(const float4* __restrict__ b, V3 oi, V3 inv, float tmin, float tmax) {
+    const float4 lo = __ldg(b), hi = __ldg(b + 1);
+    const float lx = __fmaf_rn(lo.x, inv.x, -oi.x), hx = __fmaf_rn(hi.x, inv.x, -oi.x);
+    const float ly = __fmaf_rn(lo.y, inv.y, -oi.y), hy = __fmaf_rn(hi.y, inv.y, -oi.y);
+    const float lz = __fmaf_rn(lo.z, inv.z, -oi.z), hz = __fmaf_rn(hi.z, inv.z, -oi.z);
+    const float e = fmaxf(fmaxf(fminf(lx, hx), fminf(ly, hy)), fmaxf(fminf(lz, hz), tmin));
+    const float x = fminf(fminf(fmaxf(lx, hx), fmaxf(ly, hy)), fminf(fmaxf(lz, hz), tmax));
+    return e <= x;
+}
 LUC_D void test_pair(const float4* __restrict__ tn, V3 oi, V3 inv, float tmin, float tmax, bool& h0, bool& h1,
                      float& e0, float& e1, TRef& r0, TRef& r1) {
     float4 a = __ldg(tn), b = __ldg(tn + 1), c = __ldg(tn + 2);
@@ -664,6 +678,7 @@ LUC_D bool instances_closest(const DevScene& s, V3 o, V3 d, float tmin, float& c
         } else {
             for (uint32_t ii = cur.a; ii < cur.a + cur.cnt; ++ii) {
                 const uint32_t k = ii - s.num_prims;
+                if (s.inst_box && !test_box(s.inst_box + 2 * (size_t)k, oi, inv, tmin, closest)) continue;
                 const GpuInstance g = s.inst[k];
                 const bool h = kWide ? wide_trace<false>(s, __ldg(s.blas_wide + g.blas_root), inst_point(g, o),
                                                          inst_vector(g, d), tmin, closest, bu, bv, btri, tc)
@@ -709,6 +724,8 @@ LUC_D bool instances_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax, 
             }
         } else {
             for (uint32_t ii = cur.a; ii < cur.a + cur.cnt; ++ii) {
+                if (s.inst_box && !test_box(s.inst_box + 2 * (size_t)(ii - s.num_prims), oi, inv, tmin, tmax))
+                    continue;
                 const GpuInstance g = s.inst[ii - s.num_prims];
                 float tm = tmax, bu, bv;
                 uint32_t bt;
