@@ -121,11 +121,11 @@ __global__ void k_morton(const float* __restrict__ boxes, uint32_t n, const floa
 
 // ---------------------------------------------------------------- onesweep sort
 // Stable LSD radix sort of (u32 key, u32 value), 8-bit digits, 4 passes.
-// One histogram pass counts all four digits at once; each pass then ranks a
-// 4096-key tile per block (warp-level __match_any_sync ranking keeps ties in
-// input order), publishes per-digit tile counts, and resolves its global
-// prefix by decoupled look-back over the preceding tiles. Tile ids come from
-// an atomic counter, so every tile a block waits on has already started.
+// One histogram pass counts all four digits at once; each pass then sorts a
+// 4096-key tile per block by digit in shared memory (stable), publishes the
+// tile's per-digit counts, and resolves each digit's global start by
+// decoupled look-back over the preceding tiles. Tile ids come from an atomic
+// counter, so every tile a block waits on has already started.
 
 __global__ void k_hist4(const uint32_t* __restrict__ keys, uint32_t n, uint32_t* __restrict__ hist) {
     __shared__ uint32_t sh[4][256];
@@ -173,107 +173,162 @@ __global__ void k_hist_scan(const uint32_t* __restrict__ hist, uint32_t* __restr
     }
 }
 
-__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint32_t* __restrict__ kin,
+// Look-back status words are read and written at GPU scope (past the
+// incoherent L1). A word packs its flag with its count, so it is seen whole.
+__device__ __forceinline__ uint32_t ld_status(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_status(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// The exclusive prefix of digit `tid` over the tiles before `tile`: walks
+// back from tile - 1, kLookWin status rows per round trip (each read is one
+// coalesced row segment per warp), adding aggregates until an inclusive
+// prefix ends the walk; an unpublished word stops the round and the next
+// round re-reads from there. Publishes this tile's inclusive prefix.
+__device__ __forceinline__ uint32_t look_back(uint32_t* status, uint32_t tile, uint32_t tid, uint32_t total,
+                                              uint32_t spin_limit, uint32_t* err) {
+    if (tile == 0) return 0;  // published inclusive with the aggregate
+    uint32_t excl = 0, spins = 0;
+    int64_t j = (int64_t)tile - 1;  // the next predecessor to account for
+    while (j >= 0) {
+        const int64_t j0 = j;
+        uint32_t e[kLookWin];
+#pragma unroll
+        for (int v = 0; v < kLookWin; ++v) e[v] = j0 - v >= 0 ? ld_status(status + (size_t)(j0 - v) * 256 + tid) : 0u;
+        bool stop = false, done = false;
+#pragma unroll
+        for (int v = 0; v < kLookWin; ++v) {
+            const uint32_t flag = e[v] & ~kCountMask;
+            if (!stop && j0 - v >= 0) {
+                if (flag == 0) {
+                    stop = true;
+                } else {
+                    excl += e[v] & kCountMask;
+                    j = j0 - v - 1;
+                    if (flag == kFlagInc) stop = done = true;
+                }
+            }
+        }
+        if (done) break;
+        if (stop && ++spins > spin_limit) {  // bounded wait: report, never hang
+            atomicExch(err, 1u);
+            break;
+        }
+    }
+    st_status(status + (size_t)tile * 256 + tid, (excl + total) | kFlagInc);
+    return excl;
+}
+
+// One pass. Per 4096-key tile (one block, 16 keys a thread in warp-striped
+// order): load the keys and values; count the tile's digits per warp and
+// publish the tile's per-digit aggregate at once, so that later tiles'
+// look-backs find it early; scan the counts into each (warp, digit)'s first
+// position in the digit-sorted tile; rank every key into the shared-memory
+// tile (lanes holding the same digit find one another through a per-digit
+// lane mask that each sets a bit in, which keeps ties in input order); look
+// back for the digits' global starts; write each digit's run out
+// contiguously. 64 registers and 45 KB of shared memory hold four blocks per
+// SM.
+__global__ void __launch_bounds__(kSortThreads, 4) k_onesweep(const uint32_t* __restrict__ kin,
                                                            const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
                                                            uint32_t* __restrict__ vout, uint32_t n, int shift,
                                                            const uint32_t* __restrict__ digit_offsets,
                                                            uint32_t* status, uint32_t* tile_counter, uint32_t* err,
                                                            uint32_t spin_limit) {
+    constexpr uint32_t kWarps = kSortThreads / 32;
     __shared__ uint32_t s_tile;
-    __shared__ uint32_t whist[kSortThreads / 32][256];
-    __shared__ uint32_t s_base[256];   // global start of each digit's run from this tile
-    __shared__ uint32_t s_start[256];  // start of each digit's run within the tile
+    __shared__ uint16_t s_next[kWarps][256];  // next tile position of each (warp, digit) while ranking
+    __shared__ uint32_t s_lanes[kWarps][256]; // lanes of one key slot holding each digit (zero between slots)
+    __shared__ uint32_t s_base[256];          // global destination minus tile position, per digit
+    __shared__ uint32_t s_wsum[kWarps];
     __shared__ uint32_t s_keys[kTile], s_vals[kTile];
+    uint32_t(*s_count)[256] = reinterpret_cast<uint32_t(*)[256]>(s_vals);  // digit counts, before the ranking
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    for (uint32_t t = tid; t < (kSortThreads / 32) * 256; t += kSortThreads) (&whist[0][0])[t] = 0;
+    for (uint32_t t = tid; t < kWarps * 256; t += kSortThreads) {
+        (&s_lanes[0][0])[t] = 0;
+        (&s_count[0][0])[t] = 0;
+    }
     if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
     const uint32_t wbase = tile * kTile + warp * (32u * kSortKpt);
-    const uint32_t lt = (1u << lane) - 1u;
-    uint32_t key[kSortKpt], val[kSortKpt], rank[kSortKpt];
+    uint32_t key[kSortKpt], val[kSortKpt];
 #pragma unroll
     for (int k = 0; k < kSortKpt; ++k) {
-        uint32_t idx = wbase + k * 32u + lane;
-        bool valid = idx < n;
+        const uint32_t idx = wbase + k * 32u + lane;
+        const bool valid = idx < n;
         key[k] = valid ? kin[idx] : 0u;
         val[k] = valid ? vin[idx] : 0u;
-        uint32_t digit = valid ? (key[k] >> shift) & 255u : 256u;
-        uint32_t peers = __match_any_sync(0xFFFFFFFFu, digit);
-        uint32_t before = valid ? whist[warp][digit] : 0u;
-        __syncwarp();
-        if (valid && lane == (uint32_t)(__ffs(peers) - 1)) whist[warp][digit] = before + __popc(peers);
-        __syncwarp();
-        rank[k] = valid ? before + __popc(peers & lt) : kNone;
+    }
+#pragma unroll
+    for (int k = 0; k < kSortKpt; ++k)
+        if (wbase + k * 32u + lane < n) atomicAdd(&s_count[warp][(key[k] >> shift) & 255u], 1u);
+    __syncthreads();
+    // Thread `tid` owns digit `tid`: its count per warp and in the tile; the
+    // aggregate goes out before anything else.
+    uint32_t wc[kWarps], total = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < kWarps; ++w) {
+        wc[w] = s_count[w][tid];
+        total += wc[w];
+    }
+    st_status(status + (size_t)tile * 256 + tid, total | (tile == 0 ? kFlagInc : kFlagAgg));
+    // Exclusive scan of the digit totals over the tile: where each digit's
+    // run starts in the digit-sorted tile.
+    uint32_t x = total;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) s_wsum[warp] = x;
+    __syncthreads();  // also: every count is read before the values overwrite them
+    uint32_t start = x - total;
+#pragma unroll
+    for (uint32_t w = 0; w < kWarps; ++w) start += w < warp ? s_wsum[w] : 0u;
+    uint32_t run = start;
+#pragma unroll
+    for (uint32_t w = 0; w < kWarps; ++w) {
+        s_next[w][tid] = (uint16_t)run;
+        run += wc[w];
     }
     __syncthreads();
-    // Thread `tid` owns digit `tid`: warp-exclusive offsets and the tile total.
-    uint32_t total = 0;
-    for (uint32_t w = 0; w < kSortThreads / 32; ++w) {
-        uint32_t c = whist[w][tid];
-        whist[w][tid] = total;
-        total += c;
-    }
-    // Decoupled look-back for this digit.
-    volatile uint32_t* st = status;
-    uint32_t excl = 0;
-    if (tile == 0) {
-        atomicExch(status + tid, total | kFlagInc);
-    } else {
-        atomicExch(status + (size_t)tile * 256 + tid, total | kFlagAgg);
-        int64_t j = (int64_t)tile - 1;
-        uint32_t spins = 0;
-        while (j >= 0) {
-            uint32_t s = st[(size_t)j * 256 + tid];
-            uint32_t flag = s & ~kCountMask;
-            if (flag == 0) {
-                if (++spins > spin_limit) {  // bounded wait: report, never hang
-                    atomicExch(err, 1u);
-                    break;
-                }
-                continue;
-            }
-            excl += s & kCountMask;
-            if (flag == kFlagInc) break;
-            --j;
-        }
-        __threadfence();
-        atomicExch(status + (size_t)tile * 256 + tid, (excl + total) | kFlagInc);
-    }
-    s_base[tid] = digit_offsets[tid] + excl;
-    // Exclusive scan of the tile's digit totals: where each digit's run
-    // starts inside the tile (Hillis-Steele over 256 threads in s_start).
-    s_start[tid] = total;
-    __syncthreads();
-    for (uint32_t off = 1; off < 256; off <<= 1) {
-        uint32_t t = tid >= off ? s_start[tid - off] : 0u;
-        __syncthreads();
-        s_start[tid] += t;
-        __syncthreads();
-    }
-    const uint32_t incl = s_start[tid];
-    __syncthreads();
-    s_start[tid] = incl - total;
-    __syncthreads();
-    // Sort the tile by digit in shared memory (stable: tile order within a
-    // digit), then write each digit's run out contiguously, so consecutive
-    // threads store to consecutive addresses.
+    // Rank each key slot: its lanes holding one digit are numbered in lane
+    // order after the warp's earlier slots; the key lands in its position.
+    const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
     for (int k = 0; k < kSortKpt; ++k) {
-        if (rank[k] == kNone) continue;
-        uint32_t digit = (key[k] >> shift) & 255u;
-        uint32_t local = s_start[digit] + whist[warp][digit] + rank[k];
-        s_keys[local] = key[k];
-        s_vals[local] = val[k];
+        const bool valid = wbase + k * 32u + lane < n;
+        const uint32_t digit = (key[k] >> shift) & 255u;
+        if (valid) atomicOr(&s_lanes[warp][digit], 1u << lane);
+        __syncwarp();
+        const uint32_t peers = valid ? s_lanes[warp][digit] : 0u;
+        const uint32_t before = valid ? s_next[warp][digit] : 0u;
+        __syncwarp();
+        if (valid && lane == (uint32_t)(__ffs(peers) - 1)) {
+            s_next[warp][digit] = (uint16_t)(before + __popc(peers));
+            s_lanes[warp][digit] = 0u;
+        }
+        __syncwarp();
+        const uint32_t local = before + __popc(peers & lt);
+        if (valid) {
+            s_keys[local] = key[k];
+            s_vals[local] = val[k];
+        }
     }
+    const uint32_t excl = look_back(status, tile, tid, total, spin_limit, err);
+    s_base[tid] = digit_offsets[tid] + excl - start;
     __syncthreads();
     // A tile past the last (only the look-back test hook numbers one) writes nothing.
     const uint32_t first_key = tile * kTile;
     const uint32_t count = first_key < n ? min(kTile, n - first_key) : 0u;
     for (uint32_t i = tid; i < count; i += kSortThreads) {
-        uint32_t kk = s_keys[i];
-        uint32_t digit = (kk >> shift) & 255u;
-        uint32_t dst = s_base[digit] + (i - s_start[digit]);
+        const uint32_t kk = s_keys[i];
+        const uint32_t dst = s_base[(kk >> shift) & 255u] + i;
         // In bounds whenever the pass's input matches the histogram; a pass
         // after one whose look-back gave up may not, and writes nothing
         // outside the arrays.

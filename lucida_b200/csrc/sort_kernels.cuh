@@ -10,6 +10,7 @@ constexpr int kSortKpt = 16;
 constexpr uint32_t kTile = kSortThreads * kSortKpt;  // keys per block tile
 constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kCountMask = (1u << 30) - 1u;
 constexpr uint32_t kSpinLimit = 1u << 24;
+constexpr int kLookWin = 4;  // look-back predecessors read per round trip
 
 // Digit histograms of all four 8-bit passes (hist: 4 x 256, zeroed by the caller).
 __global__ void k_hist4(const uint32_t* __restrict__ keys, uint32_t n, uint32_t* __restrict__ hist);
@@ -19,7 +20,7 @@ __global__ void k_hist_scan(const uint32_t* __restrict__ hist, uint32_t* __restr
 // `tile_counter` must be zero on entry; *err is set if a look-back wait gives
 // up after `spin_limit` polls of a predecessor that has not published
 // (kSpinLimit in every product call).
-__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+__global__ void __launch_bounds__(kSortThreads, 4) k_onesweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                            uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t n, int shift,
                            const uint32_t* __restrict__ digit_offsets, uint32_t* status, uint32_t* tile_counter,
                            uint32_t* err, uint32_t spin_limit);
