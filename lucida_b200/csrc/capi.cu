@@ -188,6 +188,13 @@ void luc_destroy(luc_ctx* c) {
 
 const char* luc_last_error(const luc_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
+int32_t luc_set_tlas_leaf(luc_ctx* c, uint32_t max_leaf) {
+    if (!c) return LUC_ERR_VALIDATION;
+    if (max_leaf < 1 || max_leaf > 64) return luc_fail(c, LUC_ERR_VALIDATION, "tlas leaf size must be 1..64");
+    c->tlas_leaf = max_leaf;
+    return LUC_OK;
+}
+
 int32_t luc_debug_waits(luc_ctx* c, uint32_t mode, uint32_t limit) {
     if (!c) return LUC_ERR_VALIDATION;
     if (mode != LUC_DEBUG_NONE && mode != LUC_DEBUG_SORT_ORPHAN_TILE && mode != LUC_DEBUG_TC_NO_COMMIT)
@@ -832,6 +839,8 @@ int32_t luc_render(luc_ctx* c, const GpuUniforms* u, uint32_t spp, uint32_t max_
     c->stats.rays_shadow = counts[3];
     c->stats.nodes_shadow = counts[4];
     c->stats.tris_shadow = counts[5];
+    c->stats.blas_extend = counts[6];
+    c->stats.blas_shadow = counts[7];
     if (tp) {
         double st[StageTimer::kCount] = {0};
         if (one_batch && c->use_graphs) c->graph.timer.accumulate(st);

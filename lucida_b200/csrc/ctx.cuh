@@ -36,6 +36,8 @@ struct FrameGraph {
     bool profiled = false;
 };
 
+constexpr uint32_t kLbvhMaxLeaf = 4;  // LBVH_MAX_LEAF (lbvh.rs:185)
+
 struct luc_ctx {
     int device = 0;
     // Test hook (luc_debug_waits): the next radix sort's or tensor-core
@@ -67,6 +69,7 @@ struct luc_ctx {
     // order (two float4), tested before its BLAS is entered.
     DevBuf inst_box;
     bool inst_cull = true;  // LUC_INST_CULL=0 enters every BLAS of a TLAS leaf
+    uint32_t tlas_leaf = 1;  // instances per TLAS leaf at most (luc_set_tlas_leaf)
     std::vector<uint32_t> host_mesh_root;
     std::vector<GpuPrimitive> host_prims;
     uint32_t blas_nodes = 0, inst_capacity = 0, num_meshes = 0;
@@ -128,7 +131,9 @@ int32_t luc_cuda_fail(luc_ctx* c, cudaError_t e, const char* what);
 // resident at lb_boxes (min xyz, max xyz as 6 floats each), leaving the
 // relaid-out tree in lb_nodes (count in *num_nodes) and the sorted order
 // (leaf primitive order) in lb_vals.
-int32_t luc_lbvh_device(luc_ctx* c, uint32_t n, uint32_t* num_nodes);
+// max_leaf: the collapse keeps subtrees of at most this many primitives as
+// one leaf (kLbvhMaxLeaf for the reference's builds).
+int32_t luc_lbvh_device(luc_ctx* c, uint32_t n, uint32_t* num_nodes, uint32_t max_leaf = kLbvhMaxLeaf);
 // Triangle boxes (padded as bvh.rs:100-111) from resident triangles/positions
 // into lb_boxes.
 int32_t luc_triangle_boxes_device(luc_ctx* c, const GpuTriangle* tris_dev, const float4* pos_dev, uint32_t n);

@@ -251,7 +251,7 @@ int32_t luc_set_instances(luc_ctx* c, const float* object_to_world, const uint32
                                                              c->lb_boxes.as<float>());
     LUC_CUDA(c, cudaGetLastError(), "prepare instances");
     uint32_t tn = 0;
-    int32_t rc = luc_lbvh_device(c, n, &tn);
+    int32_t rc = luc_lbvh_device(c, n, &tn, c->tlas_leaf);
     if (rc) return rc;
     k_rebase_nodes<<<grid_n(tn, c->num_sms), 256, 0, s>>>(c->lb_nodes.as<float4>(), tn, bn, np_,
                                                          c->nodes.as<float4>() + 2 * (size_t)bn);

@@ -22,7 +22,6 @@
 
 namespace luc {
 
-constexpr uint32_t kMaxLeaf = 4;  // LBVH_MAX_LEAF (lbvh.rs:185)
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 
 // ---------------------------------------------------------------- bounds
@@ -382,10 +381,10 @@ __global__ void k_karras(const uint32_t* __restrict__ codes, uint32_t n, uint32_
 
 // Bottom-up fit (lbvh.rs:490-525): the second child to arrive at a node
 // unions both boxes and continues upward. Also counts, per node, how many
-// nodes of its subtree stay internal after the <= kMaxLeaf collapse.
+// nodes of its subtree stay internal after the <= max_leaf collapse.
 __global__ void k_fit(const float* __restrict__ boxes, const uint32_t* __restrict__ order, uint32_t n,
                       const uint32_t* __restrict__ karras, const uint32_t* __restrict__ parent, float* nbounds,
-                      uint32_t* subtree, uint32_t* icount, uint32_t* visits, uint32_t* err) {
+                      uint32_t* subtree, uint32_t* icount, uint32_t* visits, uint32_t* err, uint32_t max_leaf) {
     const uint32_t leaf_base = n - 1;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const float* b = boxes + 6 * (size_t)order[k];
@@ -411,7 +410,7 @@ __global__ void k_fit(const float* __restrict__ boxes, const uint32_t* __restric
             uint32_t il = l >= leaf_base ? 0u : __ldcg(icount + l), ir = r >= leaf_base ? 0u : __ldcg(icount + r);
             uint32_t size = sl + sr;
             subtree[node] = size;
-            icount[node] = size > kMaxLeaf ? 1u + il + ir : 0u;
+            icount[node] = size > max_leaf ? 1u + il + ir : 0u;
             node = parent[node];
         }
     }
@@ -428,10 +427,10 @@ __global__ void k_fit(const float* __restrict__ boxes, const uint32_t* __restric
 __global__ void k_relayout(const uint32_t* __restrict__ karras, const uint32_t* __restrict__ parent,
                            const uint32_t* __restrict__ first_of, const uint32_t* __restrict__ subtree,
                            const uint32_t* __restrict__ icount, const float* __restrict__ nbounds, uint32_t n,
-                           float4* __restrict__ nodes, uint32_t* err) {
+                           float4* __restrict__ nodes, uint32_t* err, uint32_t max_leaf) {
     const uint32_t leaf_base = n - 1;
     for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < n - 1; x += gridDim.x * blockDim.x) {
-        if (subtree[x] <= kMaxLeaf) continue;
+        if (subtree[x] <= max_leaf) continue;
         uint32_t r = 0, cur = x, steps = 0;
         while (cur != 0) {
             uint32_t p = parent[cur];
@@ -455,7 +454,7 @@ __global__ void k_relayout(const uint32_t* __restrict__ karras, const uint32_t* 
             uint32_t size = leaf ? 1u : subtree[c];
             const float* b = nbounds + 6 * (size_t)c;
             uint32_t lf, cnt;
-            if (leaf || size <= kMaxLeaf) {
+            if (leaf || size <= max_leaf) {
                 lf = leaf ? c - leaf_base : first_of[c];
                 cnt = size;
             } else {
@@ -469,7 +468,7 @@ __global__ void k_relayout(const uint32_t* __restrict__ karras, const uint32_t* 
         }
     }
 }
-// Root collapsed into one leaf (n <= kMaxLeaf) or n == 1.
+// Root collapsed into one leaf (n <= max_leaf) or n == 1.
 __global__ void k_root_leaf(const float* __restrict__ b, uint32_t n, float4* __restrict__ nodes) {
     nodes[0] = make_float4(b[0], b[1], b[2], __uint_as_float(0u));
     nodes[1] = make_float4(b[3], b[4], b[5], __uint_as_float(n));
@@ -549,7 +548,7 @@ int32_t luc_radix_sort_device(luc_ctx* c, uint32_t n) {
 // LBVH over the n boxes in lb_boxes -> lb_nodes (tree), lb_vals (order),
 // lb_codes (codes in input order), lb_karras / lb_parent / lb_nbounds /
 // lb_subtree, lb_misc[0..6) centroid bounds.
-int32_t luc_lbvh_device(luc_ctx* c, uint32_t n, uint32_t* num_nodes) {
+int32_t luc_lbvh_device(luc_ctx* c, uint32_t n, uint32_t* num_nodes, uint32_t max_leaf) {
     cudaStream_t s = c->stream;
     *num_nodes = 0;
     if (n == 0) return LUC_OK;
@@ -568,7 +567,7 @@ int32_t luc_lbvh_device(luc_ctx* c, uint32_t n, uint32_t* num_nodes) {
     LUC_CUDA(c, cudaGetLastError(), "morton");
     int32_t rc = luc_radix_sort_device(c, n);
     if (rc) return rc;
-    if (n <= kMaxLeaf) {
+    if (n <= max_leaf) {
         // The whole tree collapses into the root leaf (Lbvh::build n == 1, or
         // relayout with count <= max_leaf at the root). Its bounds are the
         // union of every box, which the fit computes for n > 1.
@@ -597,15 +596,16 @@ int32_t luc_lbvh_device(luc_ctx* c, uint32_t n, uint32_t* num_nodes) {
     k_fit<<<grid_for(n, 256, sms), 256, 0, s>>>(c->lb_boxes.as<float>(), c->lb_vals.as<uint32_t>(), n,
                                                 c->lb_karras.as<uint32_t>(), c->lb_parent.as<uint32_t>(),
                                                 c->lb_nbounds.as<float>(), c->lb_subtree.as<uint32_t>(),
-                                                c->lb_icount.as<uint32_t>(), c->lb_flags.as<uint32_t>(), errp);
-    if (n <= kMaxLeaf) {
+                                                c->lb_icount.as<uint32_t>(), c->lb_flags.as<uint32_t>(), errp,
+                                                max_leaf);
+    if (n <= max_leaf) {
         k_root_leaf<<<1, 1, 0, s>>>(c->lb_nbounds.as<float>(), n, c->lb_nodes.as<float4>());
         *num_nodes = 1;
     } else {
         k_relayout<<<grid_for(n - 1, 256, sms), 256, 0, s>>>(
             c->lb_karras.as<uint32_t>(), c->lb_parent.as<uint32_t>(), c->lb_rank.as<uint32_t>(),
             c->lb_subtree.as<uint32_t>(), c->lb_icount.as<uint32_t>(), c->lb_nbounds.as<float>(), n,
-            c->lb_nodes.as<float4>(), errp);
+            c->lb_nodes.as<float4>(), errp, max_leaf);
         uint32_t root_internal = 0;
         LUC_CUDA(c, cudaMemcpyAsync(&root_internal, c->lb_icount.p, 4, cudaMemcpyDeviceToHost, s), "lbvh count");
         *num_nodes = 1u + 2u * root_internal;

@@ -101,9 +101,9 @@ __global__ void __launch_bounds__(128, 4) k_megakernel(PathState ps, const __gri
     }
     // One atomic per warp per counter (every lane reaches here: the loop
     // above has no early exit).
-    unsigned long long v[6] = {rays_e, tce.nodes, tce.tris, rays_s, tcs.nodes, tcs.tris};
+    unsigned long long v[8] = {rays_e, tce.nodes, tce.tris, rays_s, tcs.nodes, tcs.tris, tce.blas, tcs.blas};
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
+    for (int k = 0; k < 8; ++k) {
         unsigned long long x = v[k];
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xFFFFFFFFu, x, o);
         if ((threadIdx.x & 31u) == 0) atomicAdd(ps.stat + k, x);

@@ -181,6 +181,7 @@ constexpr uint32_t kMiss = 0xFFFFFFFFu;
 
 struct TravCount {
     uint32_t nodes = 0, tris = 0;
+    uint32_t blas = 0;  // two-level scenes: instances whose BLAS the walk entered
 };
 
 // Traversal layout, derived on the device from the GpuBvhNode tree:
@@ -680,6 +681,7 @@ LUC_D bool instances_closest(const DevScene& s, V3 o, V3 d, float tmin, float& c
                 const uint32_t k = ii - s.num_prims;
                 if (s.inst_box && !test_box(s.inst_box + 2 * (size_t)k, oi, inv, tmin, closest)) continue;
                 const GpuInstance g = s.inst[k];
+                tc.blas++;
                 const bool h = kWide ? wide_trace<false>(s, __ldg(s.blas_wide + g.blas_root), inst_point(g, o),
                                                          inst_vector(g, d), tmin, closest, bu, bv, btri, tc)
                                      : bvh_closest(s, node_ref(s, g.blas_root), inst_point(g, o), inst_vector(g, d),
@@ -727,6 +729,7 @@ LUC_D bool instances_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax, 
                 if (s.inst_box && !test_box(s.inst_box + 2 * (size_t)(ii - s.num_prims), oi, inv, tmin, tmax))
                     continue;
                 const GpuInstance g = s.inst[ii - s.num_prims];
+                tc.blas++;
                 float tm = tmax, bu, bv;
                 uint32_t bt;
                 if (kWide ? wide_trace<true>(s, __ldg(s.blas_wide + g.blas_root), inst_point(g, o), inst_vector(g, d),

@@ -30,17 +30,21 @@ __device__ __forceinline__ void store4(float4* p, V3 v, float w) { __stcs(p, mak
 __device__ __forceinline__ float4 ld4(const float4* p) { return __ldcs(p); }
 
 // One atomic per warp: fold this thread's traversal counters into stat[k..k+2].
-__device__ __forceinline__ void flush_counts(unsigned long long* stat, uint32_t rays, const TravCount& tc) {
-    unsigned long long r = rays, nv = tc.nodes, tt = tc.tris;
+// stat: rays, node visits, triangle tests; blas_slot: BLAS entries.
+__device__ __forceinline__ void flush_counts(unsigned long long* stat, unsigned long long* blas_slot, uint32_t rays,
+                                             const TravCount& tc) {
+    unsigned long long r = rays, nv = tc.nodes, tt = tc.tris, nb = tc.blas;
     for (int off = 16; off > 0; off >>= 1) {
         r += __shfl_down_sync(0xFFFFFFFFu, r, off);
         nv += __shfl_down_sync(0xFFFFFFFFu, nv, off);
         tt += __shfl_down_sync(0xFFFFFFFFu, tt, off);
+        nb += __shfl_down_sync(0xFFFFFFFFu, nb, off);
     }
     if ((threadIdx.x & 31u) == 0 && r) {
         atomicAdd(stat + 0, r);
         atomicAdd(stat + 1, nv);
         atomicAdd(stat + 2, tt);
+        if (nb) atomicAdd(blas_slot, nb);
     }
 }
 __device__ __forceinline__ V3 xyz(float4 a) { return V3{a.x, a.y, a.z}; }
@@ -149,7 +153,7 @@ __global__ void __launch_bounds__(kThreads, kWide == 1 ? (kInst ? 7 * 128 / kThr
             __syncwarp();
         }
     }
-    flush_counts(ps.stat, rays, tc);
+    flush_counts(ps.stat, ps.stat + 6, rays, tc);
 }
 
 // EXTEND on the wide tree of a single-level scene, with dynamic ray fetch
@@ -211,7 +215,7 @@ __global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_extend_
             live = false;
         }
     }
-    flush_counts(ps.stat, rays, tc);
+    flush_counts(ps.stat, ps.stat + 6, rays, tc);
 }
 
 // CONNECT on the wide tree of a single-level scene with the same dynamic
@@ -266,7 +270,7 @@ __global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_connect
         }
         if (live && w.step<true>(sc, kTMin, tc)) finish(w.found);
     }
-    flush_counts(ps.stat + 3, rays, tc);
+    flush_counts(ps.stat + 3, ps.stat + 7, rays, tc);
 }
 
 // Warp-aggregated append: one atomicAdd per warp. Every lane of the warp must
@@ -589,7 +593,7 @@ __global__ void __launch_bounds__(kThreads, kWide == 1 || kInst ? wide_min_block
             __syncwarp();
         }
     }
-    flush_counts(ps.stat + 3, rays, tc);
+    flush_counts(ps.stat + 3, ps.stat + 7, rays, tc);
 }
 
 // RESOLVE (shaders/wavefront/resolve.wgsl:14-48): per pixel, this batch's

@@ -152,7 +152,14 @@ def main(argv=None):
         torch.cuda.synchronize()
         st = gpu.stats()
         stages.append({"extend_ms": st.ms_extend, "shade_ms": st.ms_shade, "connect_ms": st.ms_connect,
-                       "guide_ms": st.ms_guide, "train_ms": st.ms_train, "total_ms": st.ms_total})
+                       "guide_ms": st.ms_guide, "train_ms": st.ms_train, "total_ms": st.ms_total,
+                       "nodes_per_ray": st.nodes_extend / max(st.rays_extend, 1),
+                       "tris_per_ray": st.tris_extend / max(st.rays_extend, 1),
+                       "nodes_per_shadow_ray": st.nodes_shadow / max(st.rays_shadow, 1),
+                       "tris_per_shadow_ray": st.tris_shadow / max(st.rays_shadow, 1),
+                       "blas_per_ray": st.blas_extend / max(st.rays_extend, 1),
+                       "blas_per_shadow_ray": st.blas_shadow / max(st.rays_shadow, 1),
+                       "shadow_rays": st.rays_shadow})
     stage_med = {k: float(np.median([r[k] for r in stages])) for k in stages[0]} if stages else {}
     out = {"metric": "Mpaths/s", "value": paths / total_ms / 1e3, "unit": "Mpaths/s",
            "workload": f"instanced field {args.meshes} meshes ({len(scene.triangles)} triangles) x "

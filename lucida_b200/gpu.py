@@ -190,6 +190,12 @@ class Gpu:
             check(self._h, self._lib.luc_upload_scene(self._h, C.byref(v)))
         self._scene = scene
 
+    def set_tlas_leaf(self, max_leaf: int):
+        """Leaf size of the TLAS the next instance placement builds
+        (luc_set_tlas_leaf): 4 reproduces the reference's node layout, the
+        default 1 renders the same image faster."""
+        check(self._h, self._lib.luc_set_tlas_leaf(self._h, int(max_leaf)))
+
     def set_instances(self, object_to_world, mesh, material=None):
         """Place the uploaded meshes (luc_set_instances): rebuilds the TLAS on
         the device. object_to_world (N, 3, 4) row-major; material None keeps

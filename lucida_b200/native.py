@@ -66,7 +66,8 @@ class RenderStats(C.Structure):
                 ("launches", C.c_uint64), ("rays_extend", C.c_uint64), ("rays_shadow", C.c_uint64),
                 ("paths", C.c_uint64), ("nodes_extend", C.c_uint64), ("tris_extend", C.c_uint64),
                 ("nodes_shadow", C.c_uint64), ("tris_shadow", C.c_uint64), ("ms_guide", C.c_double),
-                ("ms_train", C.c_double), ("convergence", C.c_double)]
+                ("ms_train", C.c_double), ("convergence", C.c_double), ("blas_extend", C.c_uint64),
+                ("blas_shadow", C.c_uint64)]
 
 
 class BatchJob(C.Structure):
@@ -111,6 +112,7 @@ _SIGS = {
     "luc_read_sweep": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]),
     "luc_accum_merge": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
     "luc_debug_waits": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32]),
+    "luc_set_tlas_leaf": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "luc_sort_u32_static": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_char_p,
                                         C.c_uint32]),
     "luc_sort_u32_static_max": (C.c_uint32, []),

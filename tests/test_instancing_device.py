@@ -53,6 +53,7 @@ def _render_check(gpu, s, osc, label, ref_shadows=False):
 
 def test_device_build_is_bit_exact_and_renders_match(gpu):
     s = _small()
+    gpu.set_tlas_leaf(4)  # the reference's LBVH_MAX_LEAF: its node layout bit for bit
     gpu.upload(s, force=True)
     osc = oracle_from_scene(s)
     _same_arrays(gpu, osc)
@@ -60,8 +61,24 @@ def test_device_build_is_bit_exact_and_renders_match(gpu):
     _render_check(gpu, s, osc, "instanced-field/reference-shadows", ref_shadows=True)
 
 
+def test_single_instance_tlas_leaves_render_the_same(gpu):
+    """The default TLAS (one instance per leaf) differs from the reference's
+    node layout but not in what a ray hits: the renders meet the same bar
+    against the oracle's leaf-4 build."""
+    s = _small()
+    gpu.set_tlas_leaf(1)
+    gpu.upload(s, force=True)
+    osc = oracle_from_scene(s)
+    tlas = gpu.read_scene("nodes")[-(2 * 40 - 1):]
+    counts = tlas.view(np.uint32).reshape(-1, 8)[:, 7]
+    assert counts.max() == 1  # every leaf holds one instance
+    _render_check(gpu, s, osc, "instanced-field/leaf-1")
+    _render_check(gpu, s, osc, "instanced-field/leaf-1/reference-shadows", ref_shadows=True)
+
+
 def test_tlas_rebuild_after_the_instances_move(gpu):
     s = _small()
+    gpu.set_tlas_leaf(4)
     gpu.upload(s, force=True)
     o2w, mesh, material = s.placements
     rng = np.random.default_rng(7)
