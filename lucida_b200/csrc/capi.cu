@@ -171,7 +171,7 @@ void luc_destroy(luc_ctx* c) {
                       &c->lb_icount, &c->lb_look, &c->lb_codes, &c->dn_in,  &c->dn_out,    &c->dn_a,      &c->dn_b,
                       &c->dn_dev,    &c->g_params, &c->g_m,     &c->g_v,       &c->g_grad,    &c->g_wbf,
                       &c->g_bias,    &c->g_misc,   &c->g_lobes, &c->g_rec,     &c->g_io,
-                      &c->g_part};
+                      &c->g_part,    &c->twnodes,  &c->twsoup};
     for (DevBuf* b : bufs) b->release();
     if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
     c->graph.timer.release();
@@ -513,6 +513,8 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
     d.num_nodes = v->num_triangles ? num_nodes : 0;
     d.inst = reinterpret_cast<const GpuInstance*>(c->prims.as<GpuPrimitive>() + np_);
     d.inst_box = nullptr;  // caller-built instancing (SceneBlob layout): no per-instance boxes
+    d.twnodes = nullptr;   // nor a wide TLAS
+    d.twsoup = nullptr;
     d.num_instances = v->num_triangles ? ni : 0;
     d.tlas_root = v->tlas_root;
     d.blas_roots = c->blas_roots.as<uint32_t>();

@@ -54,6 +54,7 @@ struct luc_ctx {
     DevBuf materials, prims, lights, positions, attrs, tris, nodes, env_px, env_cond, env_marg, env_row_sin, energy;
     DevBuf tnodes, soup;  // traversal layout derived from nodes / tris
     DevBuf wnodes, wsoup, wtasks, wctr;  // compressed 8-wide tree (wide.cu)
+    DevBuf twnodes, twsoup;              // the TLAS's 8-wide tree, rebuilt with it
     DevBuf wroots, blas_wide;            // its roots; BLAS binary root -> wide root (two-level scenes)
     DevBuf conv_scratch;                 // convergence meter partials + result (stats.cu)
     DevBuf upload_scratch;               // upload: validation word, vertex-bound keys
@@ -169,6 +170,10 @@ int32_t luc_build_wide(luc_ctx* c, uint32_t num_nodes, uint32_t num_tris);
 // tree); with `map`, fills c->blas_wide (binary root -> wide root).
 int32_t luc_build_wide_roots(luc_ctx* c, const uint32_t* roots, uint32_t nroots, bool map, uint32_t num_nodes,
                              uint32_t num_tris);
+// The TLAS (binary nodes [root, num_nodes), leaves of <= 4 instances) into
+// c->twnodes / c->twsoup; *ok false when it keeps the binary walk.
+int32_t luc_build_wide_tlas(luc_ctx* c, uint32_t root, uint32_t num_nodes, uint32_t prim_bound, uint32_t ninst,
+                            bool* ok);
 int32_t luc_build_tnodes_range(luc_ctx* c, uint32_t begin, uint32_t end);
 // Implemented in instances.cu: one LBVH per mesh range of the triangles in
 // lb_tris into c->nodes / c->tris (see luc_upload_meshes).

@@ -262,6 +262,11 @@ int32_t luc_set_instances(luc_ctx* c, const float* object_to_world, const uint32
     LUC_CUDA(c, cudaGetLastError(), "tlas");
     rc = luc_build_tnodes_range(c, bn, bn + tn);
     if (rc) return rc;
+    bool wide_tlas = false;
+    if (c->wide_nodes) {
+        rc = luc_build_wide_tlas(c, bn, bn + tn, np_ + n, n, &wide_tlas);
+        if (rc) return rc;
+    }
     GpuBvhNode root;
     LUC_CUDA(c, cudaMemcpyAsync(&root, c->nodes.as<GpuBvhNode>() + bn, sizeof(root), cudaMemcpyDeviceToHost, s), "read tlas root");
     LUC_CUDA(c, cudaStreamSynchronize(s), "set instances");
@@ -294,6 +299,8 @@ int32_t luc_set_instances(luc_ctx* c, const float* object_to_world, const uint32
     d.wnodes = c->wide_nodes ? c->wnodes.as<float4>() : nullptr;
     d.wsoup = c->wide_nodes ? c->wsoup.as<float4>() : nullptr;
     d.blas_wide = c->wide_nodes ? c->blas_wide.as<uint32_t>() : nullptr;
+    d.twnodes = wide_tlas ? c->twnodes.as<float4>() : nullptr;
+    d.twsoup = wide_tlas ? c->twsoup.as<uint32_t>() : nullptr;
     d.num_nodes = bn + 2 * c->inst_capacity;  // fixed while the capacity holds, so frame graphs keep replaying
     d.inst = reinterpret_cast<const GpuInstance*>(d.prims + np_);
     d.inst_box = c->inst_cull ? c->inst_box.as<float4>() : nullptr;

@@ -33,6 +33,11 @@ struct DevScene {
     // primitives, in TLAS-leaf order; the TLAS's first node in `nodes`; the
     // distinct BLAS roots (for the reference's shadow-ray behaviour).
     const GpuInstance* inst;
+    // Device-built instancing: the TLAS collapsed into the 8-wide format
+    // (root = wide node 0; a leaf slot's entries in twsoup are primitive
+    // indices, instance row = index - num_prims), null for the binary walk.
+    const float4* twnodes;
+    const uint32_t* twsoup;
     // Device-built instancing: world box of each instance row (lo.xyz, hi.xyz
     // in two float4), null otherwise; a ray enters an instance's BLAS only if
     // it crosses the box.
@@ -642,6 +647,229 @@ LUC_D V3 inst_normal(const GpuInstance& g, V3 n) {
     return normalize_or(t, V3{0.0f, 0.0f, 1.0f});
 }
 
+// A resumable walk of one ray through a two-level scene whose BLASes have
+// wide trees: the TLAS's child pairs and, for each instance whose world box
+// the ray enters, that instance's wide BLAS with the ray in object space.
+// One step is one TLAS pair test, one instance (its box test and, on a hit,
+// the entry into its BLAS) or one BLAS node visit, so kernels can walk a
+// warp's rays in lock step and refill finished lanes. The order is
+// instances_closest's (kAny = false: nearer pair child first, a leaf's
+// instances in order, each BLAS walked whole before the next) or
+// instances_any's (kAny: first child first; ends at the first hit), so the
+// results are theirs.
+template <bool kAny>
+struct InstWalk {
+    V3 o, d, inv, oi;  // the world ray
+    float tmax, bu, bv;
+    uint32_t btri, binst;
+    bool found, in_blas, tlas_done;
+    TRef cur;          // TLAS position: a child pair (cnt == 0) or a leaf's instances
+    uint32_t next;     // the leaf's next instance
+    uint32_t inst_k;   // the instance whose BLAS is being walked
+    int sp;
+    uint32_t steps;
+    TRef stack[32];
+    WideWalk w;
+
+    LUC_D void enter(const DevScene& s, TRef r) {
+        cur = r;
+        next = r.a;
+    }
+    LUC_D void begin(const DevScene& s, V3 o_, V3 d_, float tmax_) {
+        o = o_;
+        d = d_;
+        inv = safe_inv_dir(d_);
+        oi = V3{o.x * inv.x, o.y * inv.y, o.z * inv.z};
+        tmax = tmax_;
+        bu = bv = 0.0f;
+        btri = binst = 0u;
+        found = in_blas = tlas_done = false;
+        sp = 0;
+        steps = 0;
+        enter(s, node_ref(s, s.tlas_root));
+    }
+    // The TLAS walk moves to the next subtree on its stack (or ends).
+    LUC_D void pop(const DevScene& s) {
+        if (sp == 0) tlas_done = true;
+        else enter(s, stack[--sp]);
+    }
+    // True when the walk is over (kAny: also at the first hit).
+    LUC_D bool step(const DevScene& s, float tmin, TravCount& tc) {
+        if (++steps >= (1u << 24)) return true;  // bounds a walk over arrays that do not form trees
+        if (in_blas) {
+            if (w.step<kAny>(s, tmin, tc)) {
+                in_blas = false;
+                if (w.found) {
+                    found = true;
+                    if (kAny) return true;
+                    tmax = w.tmax;
+                    bu = w.bu;
+                    bv = w.bv;
+                    btri = w.btri;
+                    binst = inst_k;
+                }
+                return tlas_done;
+            }
+            return false;
+        }
+        if (tlas_done) return true;
+        if (cur.cnt == 0) {
+            bool h0, h1;
+            float e0, e1;
+            TRef r0, r1;
+            test_pair(s.tnodes + 4 * (size_t)cur.a, oi, inv, tmin, tmax, h0, h1, e0, e1, r0, r1);
+            tc.nodes++;
+            if (h0 && h1) {
+                const bool first = kAny || e0 <= e1;
+                if (sp < 32) stack[sp++] = first ? r1 : r0;
+                enter(s, first ? r0 : r1);
+            } else if (h0) {
+                enter(s, r0);
+            } else if (h1) {
+                enter(s, r1);
+            } else {
+                pop(s);
+            }
+            return tlas_done;
+        }
+        // A leaf: one instance per step.
+        const uint32_t k = next - s.num_prims;
+        ++next;
+        if (!s.inst_box || test_box(s.inst_box + 2 * (size_t)k, oi, inv, tmin, tmax)) {
+            const GpuInstance g = s.inst[k];
+            tc.blas++;
+            w.begin(__ldg(s.blas_wide + g.blas_root), inst_point(g, o), inst_vector(g, d), tmax);
+            in_blas = true;
+            inst_k = k;
+        }
+        if (next >= cur.a + cur.cnt) pop(s);
+        return !in_blas && tlas_done;
+    }
+};
+
+// The two-level walk when the TLAS has an 8-wide tree too (s.twnodes): a
+// TLAS node visit and a BLAS node visit are the same wide-node test, on the
+// world ray or the entered instance's object-space ray, so the lanes of a
+// warp run them together whichever level each is in. A TLAS node's leaf
+// slots (instances) are entered one per step, in slot order, before its
+// internal children; each BLAS is walked whole before the next instance.
+// Hits update the walk's nearest distance as they are found (kAny: the walk
+// ends at the first).
+constexpr int kTlasStack = 24;
+template <bool kAny>
+struct InstWalkW {
+    V3 o, d, inv, oi;   // world ray
+    V3 bo, bd, binv;    // the entered instance's object-space ray
+    uint32_t oct, boct;
+    float tmax, bu, bv;
+    uint32_t btri, binst, inst_k;
+    bool found, in_blas;
+    uint2 gt, gb;       // current node groups of the TLAS and the BLAS walks
+    uint3 pend;         // TLAS leaf entries still to enter: (first, entry bits, count mask)
+    int spt, spb;
+    uint32_t steps;
+    uint2 stt[kTlasStack];
+    uint2 stb[kWideStack];
+
+    LUC_D void begin(const DevScene& s, V3 o_, V3 d_, float tmax_) {
+        o = o_;
+        d = d_;
+        inv = safe_inv_dir(d_);
+        oi = V3{o.x * inv.x, o.y * inv.y, o.z * inv.z};
+        oct = (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) | (inv.z < 0.0f ? 4u : 0u);
+        tmax = tmax_;
+        bu = bv = 0.0f;
+        btri = binst = inst_k = 0u;
+        found = in_blas = false;
+        gt = make_uint2(0u, (1u << 8) | (1u << oct));  // a virtual parent of TLAS wide node 0
+        gb = make_uint2(0u, 0u);
+        pend = make_uint3(0u, 0u, 0u);
+        spt = spb = 0;
+        steps = 0;
+        boct = 0u;
+    }
+    // True when the walk is over (kAny: also at the first hit).
+    LUC_D bool step(const DevScene& s, float tmin, TravCount& tc) {
+        if (++steps >= (1u << 24)) return true;  // bounds a walk over arrays that do not form trees
+        if (!in_blas && pend.y) {
+            // Enter the next instance of the last TLAS node's leaf slots.
+            const uint32_t bit = __ffs(pend.y) - 1u;
+            pend.y &= pend.y - 1u;
+            const uint32_t k = __ldg(s.twsoup + pend.x + __popc(pend.z & ((1u << bit) - 1u))) - s.num_prims;
+            if (!s.inst_box || test_box(s.inst_box + 2 * (size_t)k, oi, inv, tmin, tmax)) {
+                const GpuInstance g = s.inst[k];
+                tc.blas++;
+                bo = inst_point(g, o);
+                bd = inst_vector(g, d);
+                binv = safe_inv_dir(bd);
+                boct = (binv.x < 0.0f ? 1u : 0u) | (binv.y < 0.0f ? 2u : 0u) | (binv.z < 0.0f ? 4u : 0u);
+                gb = make_uint2(__ldg(s.blas_wide + g.blas_root), (1u << 8) | (1u << boct));
+                spb = 0;
+                in_blas = true;
+                inst_k = k;
+            }
+            return false;
+        }
+        uint2 g = in_blas ? gb : gt;
+        if (g.y & 0xFFu) {
+            const uint32_t oc = in_blas ? boct : oct;
+            const uint32_t kk = __ffs(g.y & 0xFFu) - 1u;
+            g.y &= ~(1u << kk);
+            const uint32_t slot = kk ^ oc;
+            const uint32_t child = g.x + __popc((g.y >> 8) & ((1u << slot) - 1u));
+            if (g.y & 0xFFu) {
+                if (in_blas) {
+                    if (spb < kWideStack) stb[spb++] = g;
+                } else if (spt < kTlasStack) {
+                    stt[spt++] = g;
+                }
+            }
+            uint3 t;
+            wide_node(in_blas ? s.wnodes : s.twnodes, child, in_blas ? bo : o, in_blas ? binv : inv, oc, tmin, tmax,
+                      g, t);
+            tc.nodes++;
+            if (!in_blas) {
+                pend = t;
+            } else {
+                while (t.y) {
+                    const uint32_t tb = __ffs(t.y) - 1u;
+                    t.y &= t.y - 1u;
+                    const uint32_t kt = t.x + __popc(t.z & ((1u << tb) - 1u));
+                    tc.tris++;
+                    float th, uh, vh;
+                    if (hit_soup(s.wsoup, kt, bo, bd, tmin, tmax, th, uh, vh)) {
+                        found = true;
+                        if (kAny) return true;
+                        tmax = th;
+                        bu = uh;
+                        bv = vh;
+                        btri = __float_as_uint(__ldg(s.wsoup + 3 * (size_t)kt).w);
+                        binst = inst_k;
+                    }
+                }
+            }
+        }
+        if (!(g.y & 0xFFu)) {
+            if (in_blas) {
+                if (spb > 0) {
+                    g = stb[--spb];
+                } else {
+                    in_blas = false;  // this instance is done: back to the TLAS walk
+                    return !pend.y && !(gt.y & 0xFFu) && spt == 0;
+                }
+            } else if (spt > 0) {
+                g = stt[--spt];
+            } else {
+                gt = g;
+                return !pend.y;
+            }
+        }
+        if (in_blas) gb = g;
+        else gt = g;
+        return false;
+    }
+};
+
 // InstanceSet::intersect (instance.rs:342-421): walk the TLAS in world space
 // with the child-pair records (near child first; leaves hold instance
 // rows), and at each instance walk its BLAS with the ray in object space and
@@ -651,6 +879,20 @@ LUC_D V3 inst_normal(const GpuInstance& g, V3 n) {
 template <int kWide>
 LUC_D bool instances_closest(const DevScene& s, V3 o, V3 d, float tmin, float& closest, float& bu, float& bv,
                              uint32_t& btri, uint32_t& binst, TravCount& tc) {
+    if (kWide && s.twnodes) {  // the 8-wide TLAS: the wavefront's walk, run whole
+        InstWalkW<false> w;
+        w.begin(s, o, d, closest);
+        while (!w.step(s, tmin, tc)) {
+        }
+        if (w.found) {
+            closest = w.tmax;
+            bu = w.bu;
+            bv = w.bv;
+            btri = w.btri;
+            binst = w.binst;
+        }
+        return w.found;
+    }
     const V3 inv = safe_inv_dir(d);
     const V3 oi = V3{o.x * inv.x, o.y * inv.y, o.z * inv.z};
     bool found = false;
@@ -701,6 +943,13 @@ LUC_D bool instances_closest(const DevScene& s, V3 o, V3 d, float tmin, float& c
 // Any hit through the two levels (the default for shadow rays).
 template <int kWide>
 LUC_D bool instances_any(const DevScene& s, V3 o, V3 d, float tmin, float tmax, TravCount& tc) {
+    if (kWide && s.twnodes) {
+        InstWalkW<true> w;
+        w.begin(s, o, d, tmax);
+        while (!w.step(s, tmin, tc)) {
+        }
+        return w.found;
+    }
     const V3 inv = safe_inv_dir(d);
     const V3 oi = V3{o.x * inv.x, o.y * inv.y, o.z * inv.z};
     TRef stack[32];

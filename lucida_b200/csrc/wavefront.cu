@@ -18,6 +18,8 @@
 //     the CPU's accumulation order: emission(d), NEE(d), emission(d+1), ...;
 //   * RESOLVE sums a pixel's samples in sample order onto the accumulator,
 //     which makes batched and progressive renders bit-identical to one shot.
+#include <type_traits>
+
 #include "ctx.cuh"
 #include "shade.cuh"
 
@@ -109,6 +111,9 @@ constexpr int wide_min_blocks(int threads) { return 1024 / threads; }
 // k_extend_dyn refills a warp's finished lanes once this many are idle
 // (measured best against 1, 16 and 32).
 constexpr int kExtendRefill = 8;
+// Blocks of 128 threads per SM for the two-level dynamic-fetch walks (their
+// state: the world ray, the TLAS stack and a BLAS walk).
+constexpr int kInstDynBlocks = 6;
 
 // Two-level closest-hit walks (kInst) at 28 warps per SM (72 registers): the
 // instanced frame's EXTEND took 602 ms at 32 warps (spilling) and 574 at 28.
@@ -164,10 +169,11 @@ __global__ void __launch_bounds__(kThreads, kWide == 1 ? (kInst ? 7 * 128 / kThr
 // wide_trace's (WideWalk), so the hits are the same.
 // kStage > 0: the first kStage wide nodes (the top levels) are copied into
 // shared memory when the block starts and read from there.
-template <int kThreads, int kRefill, int kStage = 0>
-__global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_extend_dyn(PathState ps,
-                                                                                    const __grid_constant__ DevScene sc,
-                                                                                    FrameParams fp, uint32_t depth) {
+// kInst: a two-level scene whose BLASes have wide trees, walked a step at a
+// time: 1 by InstWalk (binary TLAS), 2 by InstWalkW (8-wide TLAS).
+template <int kThreads, int kRefill, int kStage = 0, int kInst = 0>
+__global__ void __launch_bounds__(kThreads, kInst ? kInstDynBlocks * 128 / kThreads : wide_min_blocks(kThreads))
+    k_extend_dyn(PathState ps, const __grid_constant__ DevScene sc, FrameParams fp, uint32_t depth) {
     __shared__ float4 stage[kStage > 0 ? 5 * kStage : 1];
     if (kStage > 0) {
         const uint32_t nf4 = 5 * min((uint32_t)kStage, sc.num_wnodes);
@@ -181,7 +187,7 @@ __global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_extend_
     TravCount tc;
     uint32_t rays = 0, p = 0, pid = kMiss;
     bool live = false, exhausted = false;
-    WideWalk w;
+    std::conditional_t<kInst == 2, InstWalkW<false>, std::conditional_t<kInst == 1, InstWalk<false>, WideWalk>> w;
     for (;;) {
         const uint32_t need = __ballot_sync(0xFFFFFFFFu, !live);
         if (!exhausted && __popc(need) >= kRefill) {
@@ -198,7 +204,8 @@ __global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_extend_
                     float best_t = kTMax;
                     pid = kMiss;
                     analytic_closest(sc, o, d, best_t, pid);  // Scene::intersect: primitives first
-                    w.begin(0u, o, d, best_t);
+                    if constexpr (kInst != 0) w.begin(sc, o, d, best_t);
+                    else w.begin(0u, o, d, best_t);
                     live = true;
                 }
             }
@@ -208,9 +215,13 @@ __global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_extend_
             continue;
         }
         // One node per refill check (measured best against 4, 8 and 16).
-        if (live && w.step<false, kStage>(sc, kTMin, tc, stage)) {
+        bool over = false;
+        if constexpr (kInst != 0) over = live && w.step(sc, kTMin, tc);
+        else over = live && w.template step<false, kStage>(sc, kTMin, tc, stage);
+        if (over) {
             __stcs(ps.hit + p, make_float4(w.tmax, w.found ? w.bu : 0.0f, w.found ? w.bv : 0.0f,
                                            __uint_as_float(w.found ? w.btri : pid)));
+            if constexpr (kInst != 0) ps.hinst[p] = w.found ? w.binst : 0u;
             ++rays;
             live = false;
         }
@@ -224,17 +235,16 @@ __global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_extend_
 // its longest shadow ray idled most of its lanes. Each ray's walk is
 // wide_trace<true>'s (WideWalk), after the analytic primitives (occluded()'s
 // order), so the visibility and the counters are the same.
-template <int kThreads, int kRefill>
-__global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_connect_dyn(PathState ps,
-                                                                                     const __grid_constant__ DevScene sc,
-                                                                                     uint32_t depth) {
+template <int kThreads, int kRefill, int kInst = 0>
+__global__ void __launch_bounds__(kThreads, kInst ? kInstDynBlocks * 128 / kThreads : wide_min_blocks(kThreads))
+    k_connect_dyn(PathState ps, const __grid_constant__ DevScene sc, uint32_t depth) {
     const uint32_t len = ps.ctr[depth * kCtrStride + kCtrShadow];
     uint32_t* pull = ps.ctr + depth * kCtrStride + kCtrPullConnect;
     const uint32_t lane = threadIdx.x & 31u, below = (1u << lane) - 1u;
     TravCount tc;
     uint32_t rays = 0, slot = 0;
     bool live = false, exhausted = false;
-    WideWalk w;
+    std::conditional_t<kInst == 2, InstWalkW<true>, std::conditional_t<kInst == 1, InstWalk<true>, WideWalk>> w;
     auto finish = [&](bool occluded) {
         if (!occluded) {
             const uint32_t p = __float_as_uint(ld4(ps.sh_d + slot).w);
@@ -260,6 +270,7 @@ __global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_connect
                     const V3 o = xyz(o4), d = xyz(d4);
                     live = true;
                     if (analytic_any(sc, o, d, o4.w)) finish(true);
+                    else if constexpr (kInst != 0) w.begin(sc, o, d, o4.w);
                     else w.begin(0u, o, d, o4.w);
                 }
             }
@@ -268,7 +279,10 @@ __global__ void __launch_bounds__(kThreads, wide_min_blocks(kThreads)) k_connect
             if (exhausted) break;
             continue;
         }
-        if (live && w.step<true>(sc, kTMin, tc)) finish(w.found);
+        bool over = false;
+        if constexpr (kInst != 0) over = live && w.step(sc, kTMin, tc);
+        else over = live && w.template step<true>(sc, kTMin, tc);
+        if (over) finish(w.found);
     }
     flush_counts(ps.stat + 3, ps.stat + 7, rays, tc);
 }
@@ -706,8 +720,8 @@ void query_occupancy(RenderState& rs) {
     rs.connect_blocks_bin = occ((const void*)k_connect<false, false, 128, 0>);
     rs.shade_blocks = occ((const void*)k_shade<false, false>);
     rs.shade_blocks_guided = occ((const void*)k_shade<true, false>);
-    rs.extend_blocks_inst = occ((const void*)k_extend<true, false, 128, 1>);
-    rs.connect_blocks_inst = occ((const void*)k_connect<true, false, 128, 1>);
+    rs.extend_blocks_inst = occ((const void*)k_extend_dyn<128, kExtendRefill, 0, 2>);
+    rs.connect_blocks_inst = occ((const void*)k_connect_dyn<128, kExtendRefill, 2>);
     rs.extend_blocks_inst_bin = occ((const void*)k_extend<true, false, 128, 0>);
     rs.connect_blocks_inst_bin = occ((const void*)k_connect<true, false, 128, 0>);
     rs.shade_blocks_inst = occ((const void*)k_shade<false, true>);
@@ -751,8 +765,10 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
     for (uint32_t d = 0; d < fp.max_depth; ++d) {
         if (timer) timer->mark(stream, StageTimer::kExtend);
         const bool inst = sc.num_instances > 0, wide = inst ? sc.blas_wide != nullptr : sc.wnodes != nullptr;
-        if (inst && wide)
-            k_extend<true, false, 128, 1><<<sms * rs.extend_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, BatchDev{}, d);
+        if (inst && wide && sc.twnodes)
+            k_extend_dyn<128, kExtendRefill, 0, 2><<<sms * rs.extend_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, d);
+        else if (inst && wide)
+            k_extend_dyn<128, kExtendRefill, 0, 1><<<sms * rs.extend_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, d);
         else if (inst)
             k_extend<true, false, 128, 0><<<sms * rs.extend_blocks_inst_bin, 128, 0, stream>>>(rs.ps, sc, fp,
                                                                                                BatchDev{}, d);
@@ -800,9 +816,14 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
                 cudaStreamWaitEvent(ov->side, ov->ready, 0);
                 cs = ov->side;
             }
-            // Two-level shadow rays walk the binary BLASes: measured faster
-            // than the wide ones for any-hit (C5: 133 against 153 ms / frame).
-            if (inst)
+            // Two-level shadow rays walk the wide BLASes in lock step
+            // (InstWalk); the reference's object-space shadow rays and
+            // binary-only scenes keep the nested any-hit walk.
+            if (inst && wide && sc.twnodes && !sc.reference_shadows)
+                k_connect_dyn<128, kExtendRefill, 2><<<sms * rs.connect_blocks_inst, 128, 0, cs>>>(rs.ps, sc, d);
+            else if (inst && wide && !sc.reference_shadows)
+                k_connect_dyn<128, kExtendRefill, 1><<<sms * rs.connect_blocks_inst, 128, 0, cs>>>(rs.ps, sc, d);
+            else if (inst)
                 k_connect<true, false, 128, 0><<<sms * rs.connect_blocks_inst_bin, 128, 0, cs>>>(rs.ps, sc,
                                                                                                  BatchDev{}, d);
             else if (wide)

@@ -183,13 +183,17 @@ __global__ void k_wide_advance(uint32_t* __restrict__ ctr) {
     ctr[kWcEnd] = ctr[kWcAlloc];
 }
 
+// kTlas: the binary tree is a TLAS whose leaves hold at most kSmallLeaf
+// instances (primitive indices); leaf slots are never split and the soup is
+// `isoup`, one primitive index per entry, instead of triangle records.
+template <bool kTlas>
 __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ nodes, uint32_t num_nodes,
                                                     const float4* __restrict__ soup, uint32_t num_tris,
                                                     const GpuTriangle* __restrict__ tri_idx,
                                                     const float4* __restrict__ tri_pos, float leaf_weight,
                                                     uint4* __restrict__ tasks, float4* __restrict__ wnodes,
-                                                    float4* __restrict__ wsoup, uint32_t cap,
-                                                    uint32_t* __restrict__ ctr) {
+                                                    float4* __restrict__ wsoup, uint32_t* __restrict__ isoup,
+                                                    uint32_t cap, uint32_t* __restrict__ ctr) {
     if (ctr[kWcErr]) return;  // a failed level ends the build
     // Claims past the capacity failed (and flagged); never read beyond it.
     const uint32_t begin = ctr[kWcBegin], end = min(ctr[kWcEnd], cap);
@@ -252,6 +256,19 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
                 ch[best] = l;
                 ch[n++] = r;
             }
+        } else if (kTlas) {
+            // A TLAS whose root is a leaf: one slot under the leaf's box.
+            if (task.z == 0 || task.z > kSmallLeaf) {
+                atomicOr(ctr + kWcErr, kErrTree);
+                continue;
+            }
+            node_box(nodes, task.x, ch[0]);
+            ch[0].node = task.x;
+            ch[0].first = task.y;
+            ch[0].count = task.z;
+            ch[0].kind = 2u;
+            ch[0].sub = (1u << task.z) - 1u;
+            n = 1;
         } else {
             // Leaf chunk: up to 7 (or 8, for the last) slots of 4 triangles,
             // every slot with the binary leaf's box; the rest chains on.
@@ -279,6 +296,8 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
                 ++n;
             }
         }
+        if (kTlas)
+            for (uint32_t k = 0; k < n; ++k) ok = ok && ch[k].kind != kKindChunk;  // leaves of <= 4 instances only
         if (!ok) {
             atomicOr(ctr + kWcErr, kErrTree);
             continue;
@@ -396,6 +415,10 @@ __global__ void __launch_bounds__(128) k_wide_level(const float4* __restrict__ n
                     uint32_t i = 0;
                     for (uint32_t bits = ch[k].sub; bits; bits &= bits - 1u, ++i) {
                         const uint32_t t = ch[k].first + (uint32_t)(__ffs(bits) - 1);
+                        if (kTlas) {
+                            isoup[tbase + off + i] = t;
+                            continue;
+                        }
                         const size_t src = 3 * (size_t)t, dst = 3 * (size_t)(tbase + off + i);
                         float4 q0 = soup[src];
                         q0.w = __uint_as_float(t);
@@ -465,10 +488,10 @@ int32_t luc_build_wide_roots(luc_ctx* c, const uint32_t* roots, uint32_t nroots,
     uint32_t h[kWcWords] = {};
     for (int level = 0; level < kMaxLevels; level += kLevelsPerSync) {
         for (int k = 0; k < kLevelsPerSync; ++k) {
-            k_wide_level<<<grid, 128, 0, s>>>(c->nodes.as<float4>(), num_nodes, c->soup.as<float4>(), num_tris,
+            k_wide_level<false><<<grid, 128, 0, s>>>(c->nodes.as<float4>(), num_nodes, c->soup.as<float4>(), num_tris,
                                               c->tris.as<GpuTriangle>(), c->positions.as<float4>(),
                                               map ? kBlasLeafSplitWeight : kLeafSplitWeight, c->wtasks.as<uint4>(), c->wnodes.as<float4>(), c->wsoup.as<float4>(),
-                                              (uint32_t)cap, ctr);
+                                              nullptr, (uint32_t)cap, ctr);
             k_wide_advance<<<1, 1, 0, s>>>(ctr);
         }
         LUC_CUDA(c, cudaGetLastError(), "wide build");
@@ -480,6 +503,43 @@ int32_t luc_build_wide_roots(luc_ctx* c, const uint32_t* roots, uint32_t nroots,
     }
     if (h[kWcBegin] != h[kWcEnd] || h[kWcSoup] != num_tris) return LUC_OK;  // too deep: binary traversal
     c->wide_nodes = h[kWcAlloc];
+    return LUC_OK;
+}
+
+// Collapse the TLAS (binary nodes [root, num_nodes) of c->nodes, leaves of at
+// most 4 instances whose primitive indices lie below prim_bound) into
+// c->twnodes / c->twsoup (one primitive index per leaf entry), the same
+// 8-wide format as the BLASes' trees. *ok is false (binary TLAS traversal)
+// when the leaves are larger or the tree is deeper than the level budget.
+int32_t luc_build_wide_tlas(luc_ctx* c, uint32_t root, uint32_t num_nodes, uint32_t prim_bound, uint32_t ninst,
+                            bool* ok) {
+    using namespace luc;
+    *ok = false;
+    if (!ninst || c->tlas_leaf > kSmallLeaf || root >= num_nodes) return LUC_OK;
+    const uint64_t cap = 2ull * (num_nodes - root) + 8;
+    cudaStream_t s = c->stream;
+    LUC_CUDA(c, c->twnodes.ensure(cap * 80), "alloc wide tlas");
+    LUC_CUDA(c, c->twsoup.ensure((size_t)prim_bound * 4), "alloc wide tlas soup");
+    LUC_CUDA(c, c->wtasks.ensure(cap * 16), "alloc wide tasks");
+    LUC_CUDA(c, c->wctr.ensure(kWcWords * 4), "alloc wide counters");
+    LUC_CUDA(c, upload(c->wroots, &root, 1, s), "upload wide roots");
+    uint32_t* ctr = c->wctr.as<uint32_t>();
+    k_wide_init<<<1, 128, 0, s>>>(c->nodes.as<float4>(), num_nodes, c->wroots.as<uint32_t>(), 1,
+                                  c->wtasks.as<uint4>(), nullptr, ctr);
+    const int grid = c->num_sms * 2;
+    constexpr int kLevels = 16;  // 4^16 instances deep at 2 children per level: far beyond any TLAS here
+    for (int level = 0; level < kLevels; ++level) {
+        k_wide_level<true><<<grid, 128, 0, s>>>(c->nodes.as<float4>(), num_nodes, nullptr, prim_bound, nullptr,
+                                                nullptr, -1.0f, c->wtasks.as<uint4>(), c->twnodes.as<float4>(),
+                                                nullptr, c->twsoup.as<uint32_t>(), (uint32_t)cap, ctr);
+        k_wide_advance<<<1, 1, 0, s>>>(ctr);
+    }
+    LUC_CUDA(c, cudaGetLastError(), "wide tlas");
+    uint32_t h[kWcWords] = {};
+    LUC_CUDA(c, cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, s), "wide tlas counters");
+    LUC_CUDA(c, cudaStreamSynchronize(s), "wide tlas");
+    if (h[kWcErr] & kErrTree) return luc_fail(c, LUC_ERR_VALIDATION, "TLAS: malformed tree (wide collapse)");
+    *ok = h[kWcErr] == 0 && h[kWcBegin] == h[kWcEnd] && h[kWcSoup] == ninst;
     return LUC_OK;
 }
 

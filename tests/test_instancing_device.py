@@ -61,19 +61,24 @@ def test_device_build_is_bit_exact_and_renders_match(gpu):
     _render_check(gpu, s, osc, "instanced-field/reference-shadows", ref_shadows=True)
 
 
-def test_single_instance_tlas_leaves_render_the_same(gpu):
-    """The default TLAS (one instance per leaf) differs from the reference's
-    node layout but not in what a ray hits: the renders meet the same bar
-    against the oracle's leaf-4 build."""
+@pytest.mark.parametrize("leaf", [1, 8])
+def test_other_tlas_leaf_sizes_render_the_same(gpu, leaf):
+    """TLASes other than the reference's (leaf size 4) differ in node layout
+    but not in what a ray hits: the renders meet the same bar against the
+    oracle's leaf-4 build. Leaf size 1 (the default) is walked through its
+    8-wide collapse, leaf size 8 (too large for a wide leaf slot) through the
+    binary child pairs."""
     s = _small()
-    gpu.set_tlas_leaf(1)
+    gpu.set_tlas_leaf(leaf)
     gpu.upload(s, force=True)
     osc = oracle_from_scene(s)
-    tlas = gpu.read_scene("nodes")[-(2 * 40 - 1):]
-    counts = tlas.view(np.uint32).reshape(-1, 8)[:, 7]
-    assert counts.max() == 1  # every leaf holds one instance
-    _render_check(gpu, s, osc, "instanced-field/leaf-1")
-    _render_check(gpu, s, osc, "instanced-field/leaf-1/reference-shadows", ref_shadows=True)
+    if leaf == 1:
+        tlas = gpu.read_scene("nodes")[-(2 * 40 - 1):]
+        counts = tlas.view(np.uint32).reshape(-1, 8)[:, 7]
+        assert counts.max() == 1  # every leaf holds one instance
+    _render_check(gpu, s, osc, f"instanced-field/leaf-{leaf}")
+    _render_check(gpu, s, osc, f"instanced-field/leaf-{leaf}/reference-shadows", ref_shadows=True)
+    gpu.set_tlas_leaf(1)
 
 
 def test_tlas_rebuild_after_the_instances_move(gpu):
