@@ -792,23 +792,30 @@ struct InstWalkW {
     LUC_D bool step(const DevScene& s, float tmin, TravCount& tc) {
         if (++steps >= (1u << 24)) return true;  // bounds a walk over arrays that do not form trees
         if (!in_blas && pend.y) {
-            // Enter the next instance of the last TLAS node's leaf slots.
+            // Enter the next instance of the last TLAS node's leaf slots: its
+            // world box, then (ray in object space) its BLAS's root box, which
+            // a rotated instance's world box bounds loosely.
             const uint32_t bit = __ffs(pend.y) - 1u;
             pend.y &= pend.y - 1u;
             const uint32_t k = __ldg(s.twsoup + pend.x + __popc(pend.z & ((1u << bit) - 1u))) - s.num_prims;
             if (!s.inst_box || test_box(s.inst_box + 2 * (size_t)k, oi, inv, tmin, tmax)) {
                 const GpuInstance g = s.inst[k];
-                tc.blas++;
                 bo = inst_point(g, o);
                 bd = inst_vector(g, d);
                 binv = safe_inv_dir(bd);
-                boct = (binv.x < 0.0f ? 1u : 0u) | (binv.y < 0.0f ? 2u : 0u) | (binv.z < 0.0f ? 4u : 0u);
-                gb = make_uint2(__ldg(s.blas_wide + g.blas_root), (1u << 8) | (1u << boct));
-                spb = 0;
-                in_blas = true;
-                inst_k = k;
+                const V3 boi{bo.x * binv.x, bo.y * binv.y, bo.z * binv.z};
+                if (test_box(s.nodes + 2 * (size_t)g.blas_root, boi, binv, tmin, tmax)) {
+                    tc.blas++;
+                    boct = (binv.x < 0.0f ? 1u : 0u) | (binv.y < 0.0f ? 2u : 0u) | (binv.z < 0.0f ? 4u : 0u);
+                    gb = make_uint2(__ldg(s.blas_wide + g.blas_root), (1u << 8) | (1u << boct));
+                    spb = 0;
+                    in_blas = true;
+                    inst_k = k;
+                }
             }
-            return false;
+            // Entered: its root is visited in this same step. Otherwise the
+            // node's next instance, or its children once none is left.
+            if (!in_blas && pend.y) return false;
         }
         uint2 g = in_blas ? gb : gt;
         if (g.y & 0xFFu) {
