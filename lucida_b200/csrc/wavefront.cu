@@ -111,9 +111,13 @@ constexpr int wide_min_blocks(int threads) { return 1024 / threads; }
 // k_extend_dyn refills a warp's finished lanes once this many are idle
 // (measured best against 1, 16 and 32).
 constexpr int kExtendRefill = 8;
-// Blocks of 128 threads per SM for the two-level dynamic-fetch walks (their
-// state: the world ray, the TLAS stack and a BLAS walk).
-constexpr int kInstDynBlocks = 6;
+// Blocks of 128 threads per SM for the two-level dynamic-fetch walks (64
+// registers) and their refill threshold: the instanced frame (4096
+// instances, 8 frames) ran 64.4 / 64.6 / 70.2 / 73.0 / 68.0 Mpaths/s at 6 / 5
+// / 7 / 8 / 10 blocks, and at 8 blocks 73.5 refilling at 4 idle lanes (8:
+// 73.0; 16 at 6 blocks: 61.6).
+constexpr int kInstDynBlocks = 8;
+constexpr int kInstRefill = 4;
 
 // Two-level closest-hit walks (kInst) at 28 warps per SM (72 registers): the
 // instanced frame's EXTEND took 602 ms at 32 warps (spilling) and 574 at 28.
@@ -720,8 +724,8 @@ void query_occupancy(RenderState& rs) {
     rs.connect_blocks_bin = occ((const void*)k_connect<false, false, 128, 0>);
     rs.shade_blocks = occ((const void*)k_shade<false, false>);
     rs.shade_blocks_guided = occ((const void*)k_shade<true, false>);
-    rs.extend_blocks_inst = occ((const void*)k_extend_dyn<128, kExtendRefill, 0, 2>);
-    rs.connect_blocks_inst = occ((const void*)k_connect_dyn<128, kExtendRefill, 2>);
+    rs.extend_blocks_inst = occ((const void*)k_extend_dyn<128, kInstRefill, 0, 2>);
+    rs.connect_blocks_inst = occ((const void*)k_connect_dyn<128, kInstRefill, 2>);
     rs.extend_blocks_inst_bin = occ((const void*)k_extend<true, false, 128, 0>);
     rs.connect_blocks_inst_bin = occ((const void*)k_connect<true, false, 128, 0>);
     rs.shade_blocks_inst = occ((const void*)k_shade<false, true>);
@@ -766,9 +770,9 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
         if (timer) timer->mark(stream, StageTimer::kExtend);
         const bool inst = sc.num_instances > 0, wide = inst ? sc.blas_wide != nullptr : sc.wnodes != nullptr;
         if (inst && wide && sc.twnodes)
-            k_extend_dyn<128, kExtendRefill, 0, 2><<<sms * rs.extend_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, d);
+            k_extend_dyn<128, kInstRefill, 0, 2><<<sms * rs.extend_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, d);
         else if (inst && wide)
-            k_extend_dyn<128, kExtendRefill, 0, 1><<<sms * rs.extend_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, d);
+            k_extend_dyn<128, kInstRefill, 0, 1><<<sms * rs.extend_blocks_inst, 128, 0, stream>>>(rs.ps, sc, fp, d);
         else if (inst)
             k_extend<true, false, 128, 0><<<sms * rs.extend_blocks_inst_bin, 128, 0, stream>>>(rs.ps, sc, fp,
                                                                                                BatchDev{}, d);
@@ -820,9 +824,9 @@ void record_batch(RenderState& rs, const DevScene& sc, const FrameParams& fp, Gp
             // (InstWalk); the reference's object-space shadow rays and
             // binary-only scenes keep the nested any-hit walk.
             if (inst && wide && sc.twnodes && !sc.reference_shadows)
-                k_connect_dyn<128, kExtendRefill, 2><<<sms * rs.connect_blocks_inst, 128, 0, cs>>>(rs.ps, sc, d);
+                k_connect_dyn<128, kInstRefill, 2><<<sms * rs.connect_blocks_inst, 128, 0, cs>>>(rs.ps, sc, d);
             else if (inst && wide && !sc.reference_shadows)
-                k_connect_dyn<128, kExtendRefill, 1><<<sms * rs.connect_blocks_inst, 128, 0, cs>>>(rs.ps, sc, d);
+                k_connect_dyn<128, kInstRefill, 1><<<sms * rs.connect_blocks_inst, 128, 0, cs>>>(rs.ps, sc, d);
             else if (inst)
                 k_connect<true, false, 128, 0><<<sms * rs.connect_blocks_inst_bin, 128, 0, cs>>>(rs.ps, sc,
                                                                                                  BatchDev{}, d);
