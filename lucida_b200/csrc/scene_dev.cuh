@@ -497,11 +497,44 @@ LUC_D void wide_slabs(const float4 a, const uint4 b, const uint4 c, const uint4 
 // one triangle per step (after Ylitie, Karras and Laine 2017, compressed
 // wide BVHs; their deferral of triangle groups while few lanes have one
 // measured slower here).
+// A walk's stack of node groups, kCap entries: the first kShared in shared
+// memory, in this thread's column of a [kShared][kThreads] array (`col`
+// points at row 0, so a warp's accesses at any depths fall in distinct bank
+// pairs), the rest in local memory.
+template <int kShared, int kThreads, int kCap>
+struct GroupStack {
+    uint32_t col = 0;  // shared-window address of this thread's row-0 entry
+    uint2 deep[kCap > kShared ? kCap - kShared : 1];
+    LUC_D void bind(uint2* p) { col = (uint32_t)__cvta_generic_to_shared(p); }
+    LUC_D void put(int i, uint2 v) {
+        if (kShared > 0 && i < kShared)
+            asm("st.shared.v2.u32 [%0], {%1, %2};" ::"r"(col + (uint32_t)i * (uint32_t)(kThreads * 8)), "r"(v.x),
+                "r"(v.y)
+                : "memory");
+        else
+            deep[i - kShared] = v;
+    }
+    LUC_D uint2 get(int i) const {
+        if (kShared > 0 && i < kShared) {
+            uint2 v;
+            asm("ld.shared.v2.u32 {%0, %1}, [%2];"
+                : "=r"(v.x), "=r"(v.y)
+                : "r"(col + (uint32_t)i * (uint32_t)(kThreads * 8))
+                : "memory");
+            return v;
+        }
+        return deep[i - kShared];
+    }
+};
+template <int kCap>
+using LocalStack = GroupStack<0, 1, kCap>;
+
 // A resumable walk of one ray through a wide tree: begin() then step()
 // until it reports the end. Used whole by wide_trace and one node at a time
 // by kernels that refill finished lanes with new rays (k_extend_dyn): both
 // visit the same nodes and triangles in the same order.
-struct WideWalk {
+template <class Stack = LocalStack<kWideStack>>
+struct WideWalkT {
     V3 o, d, inv;
     uint32_t oct, btri;
     float tmax, bu, bv;
@@ -509,8 +542,10 @@ struct WideWalk {
     uint2 g;
     int sp;
     uint32_t steps;
-    uint2 stack[kWideStack];
+    Stack stack;
 
+    // This thread's shared-memory stack column (used when Stack keeps entries there).
+    LUC_D void bind(uint2* shared_col, uint2*) { stack.bind(shared_col); }
     LUC_D void begin(uint32_t root, V3 o_, V3 d_, float tmax_) {
         o = o_;
         d = d_;
@@ -536,7 +571,7 @@ struct WideWalk {
             g.y &= ~(1u << k);
             const uint32_t slot = k ^ oct;
             const uint32_t child = g.x + __popc((g.y >> 8) & ((1u << slot) - 1u));
-            if ((g.y & 0xFFu) && sp < kWideStack) stack[sp++] = g;
+            if ((g.y & 0xFFu) && sp < kWideStack) stack.put(sp++, g);
             uint3 t;
             wide_node_staged<kStage>(s.wnodes, stage, child, o, inv, oct, tmin, tmax, g, t);
             tc.nodes++;
@@ -558,11 +593,12 @@ struct WideWalk {
         }
         if (!(g.y & 0xFFu)) {
             if (sp == 0) return true;
-            g = stack[--sp];
+            g = stack.get(--sp);
         }
         return ++steps >= (1u << 24);
     }
 };
+using WideWalk = WideWalkT<>;
 
 // Closest hit (kAny = false) or any hit (kAny = true) through the wide tree
 // whose root is wide node `root`. The triangle test and its operands are
@@ -671,6 +707,7 @@ struct InstWalk {
     TRef stack[32];
     WideWalk w;
 
+    LUC_D void bind(uint2*, uint2*) {}  // local-memory stacks only
     LUC_D void enter(const DevScene& s, TRef r) {
         cur = r;
         next = r.a;
@@ -756,7 +793,7 @@ struct InstWalk {
 // Hits update the walk's nearest distance as they are found (kAny: the walk
 // ends at the first).
 constexpr int kTlasStack = 24;
-template <bool kAny>
+template <bool kAny, class TStack = LocalStack<kTlasStack>, class BStack = LocalStack<kWideStack>>
 struct InstWalkW {
     V3 o, d, inv, oi;   // world ray
     V3 bo, bd, binv;    // the entered instance's object-space ray
@@ -768,9 +805,14 @@ struct InstWalkW {
     uint3 pend;         // TLAS leaf entries still to enter: (first, entry bits, count mask)
     int spt, spb;
     uint32_t steps;
-    uint2 stt[kTlasStack];
-    uint2 stb[kWideStack];
+    TStack stt;
+    BStack stb;
 
+    // This thread's shared-memory stack columns, BLAS walk and TLAS walk.
+    LUC_D void bind(uint2* blas_col, uint2* tlas_col) {
+        stb.bind(blas_col);
+        stt.bind(tlas_col);
+    }
     LUC_D void begin(const DevScene& s, V3 o_, V3 d_, float tmax_) {
         o = o_;
         d = d_;
@@ -826,9 +868,9 @@ struct InstWalkW {
             const uint32_t child = g.x + __popc((g.y >> 8) & ((1u << slot) - 1u));
             if (g.y & 0xFFu) {
                 if (in_blas) {
-                    if (spb < kWideStack) stb[spb++] = g;
+                    if (spb < kWideStack) stb.put(spb++, g);
                 } else if (spt < kTlasStack) {
-                    stt[spt++] = g;
+                    stt.put(spt++, g);
                 }
             }
             uint3 t;
@@ -859,13 +901,13 @@ struct InstWalkW {
         if (!(g.y & 0xFFu)) {
             if (in_blas) {
                 if (spb > 0) {
-                    g = stb[--spb];
+                    g = stb.get(--spb);
                 } else {
                     in_blas = false;  // this instance is done: back to the TLAS walk
                     return !pend.y && !(gt.y & 0xFFu) && spt == 0;
                 }
             } else if (spt > 0) {
-                g = stt[--spt];
+                g = stt.get(--spt);
             } else {
                 gt = g;
                 return !pend.y;

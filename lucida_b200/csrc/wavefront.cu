@@ -118,6 +118,22 @@ constexpr int kExtendRefill = 8;
 // 73.0; 16 at 6 blocks: 61.6).
 constexpr int kInstDynBlocks = 8;
 constexpr int kInstRefill = 4;
+// Entries of the walks' node-group stacks kept in shared memory (the rest in
+// local memory, which competes with the tree for L1). Single-level walks: the
+// displaced-sphere frame ran 394.0 / 428.6 / 430.9 / 428.8 Mpaths/s with 0 /
+// 4 / 8 / 16 entries. Two-level walks keep theirs in local memory: with 4 /
+// 8 / 16 BLAS entries in shared memory the instanced frame ran 69.4 / 68.3 /
+// 67.2 Mpaths/s against 72.3 (its three-million-triangle BLASes need the L1),
+// and a TLAS stack in shared memory spilled registers.
+constexpr int kWalkSharedStack = 8;
+constexpr int kBlasSharedStack = 0;
+constexpr int kTlasSharedStack = 0;
+template <int kThreads, bool kAny, int kInst>
+using DynWalk = std::conditional_t<
+    kInst == 2,
+    InstWalkW<kAny, GroupStack<kTlasSharedStack, kThreads, kTlasStack>, GroupStack<kBlasSharedStack, kThreads, kWideStack>>,
+    std::conditional_t<kInst == 1, InstWalk<kAny>, WideWalkT<GroupStack<kWalkSharedStack, kThreads, kWideStack>>>>;
+
 
 // Two-level closest-hit walks (kInst) at 28 warps per SM (72 registers): the
 // instanced frame's EXTEND took 602 ms at 32 warps (spilling) and 574 at 28.
@@ -191,7 +207,11 @@ __global__ void __launch_bounds__(kThreads, kInst ? kInstDynBlocks * 128 / kThre
     TravCount tc;
     uint32_t rays = 0, p = 0, pid = kMiss;
     bool live = false, exhausted = false;
-    std::conditional_t<kInst == 2, InstWalkW<false>, std::conditional_t<kInst == 1, InstWalk<false>, WideWalk>> w;
+    constexpr int kShared = kInst == 0 ? kWalkSharedStack : kInst == 2 ? kBlasSharedStack : 0;
+    __shared__ uint2 s_stack[kShared > 0 ? kShared : 1][kThreads];
+    __shared__ uint2 s_tstack[kInst == 2 && kTlasSharedStack > 0 ? kTlasSharedStack : 1][kThreads];
+    DynWalk<kThreads, false, kInst> w;
+    w.bind(&s_stack[0][threadIdx.x], &s_tstack[0][threadIdx.x]);
     for (;;) {
         const uint32_t need = __ballot_sync(0xFFFFFFFFu, !live);
         if (!exhausted && __popc(need) >= kRefill) {
@@ -248,7 +268,11 @@ __global__ void __launch_bounds__(kThreads, kInst ? kInstDynBlocks * 128 / kThre
     TravCount tc;
     uint32_t rays = 0, slot = 0;
     bool live = false, exhausted = false;
-    std::conditional_t<kInst == 2, InstWalkW<true>, std::conditional_t<kInst == 1, InstWalk<true>, WideWalk>> w;
+    constexpr int kShared = kInst == 0 ? kWalkSharedStack : kInst == 2 ? kBlasSharedStack : 0;
+    __shared__ uint2 s_stack[kShared > 0 ? kShared : 1][kThreads];
+    __shared__ uint2 s_tstack[kInst == 2 && kTlasSharedStack > 0 ? kTlasSharedStack : 1][kThreads];
+    DynWalk<kThreads, true, kInst> w;
+    w.bind(&s_stack[0][threadIdx.x], &s_tstack[0][threadIdx.x]);
     auto finish = [&](bool occluded) {
         if (!occluded) {
             const uint32_t p = __float_as_uint(ld4(ps.sh_d + slot).w);
