@@ -411,9 +411,9 @@ def main():
                 "frac_l2": achieved / l2_gbs, "frac_dram": dram_gbs / hbm if dram_gbs else None,
                 "dram_gbs": dram_gbs, "frac_hbm_of_logical_bytes": achieved / hbm, "hbm_peak": hbm,
                 "hbm_peak_source": peak_kind,
-                "limiter": "instruction issue: ncu on a 512x512x4-spp frame of this scene shows 67-71% issue "
-                           "active, the ALU pipe at 47-50%, 15-18 of 32 threads active per warp instruction, "
-                           "71-76% L2 hit rate (profiles/k_extend_wide_small_case.md)",
+                "limiter": "instruction issue: ncu on a 512x512x4-spp frame of this scene shows 72-74% issue "
+                           "active, the ALU pipe at 52-54%, 15-18 of 32 threads active per warp instruction, "
+                           "68-79% L2 hit rate (profiles/k_extend_wide_small_case.md)",
                 "traffic": traffic,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per EXTEND ray on a 512x512x4-spp "
                                   "frame of this scene, scaled by this launch size's rays",
