@@ -222,16 +222,17 @@ __device__ __forceinline__ uint32_t look_back(uint32_t* status, uint32_t tile, u
     return excl;
 }
 
-// One pass. Per 4096-key tile (one block, 16 keys a thread in warp-striped
-// order): load the keys and values; count the tile's digits per warp and
-// publish the tile's per-digit aggregate at once, so that later tiles'
-// look-backs find it early; scan the counts into each (warp, digit)'s first
-// position in the digit-sorted tile; rank every key into the shared-memory
-// tile (lanes holding the same digit find one another through a per-digit
-// lane mask that each sets a bit in, which keeps ties in input order); look
-// back for the digits' global starts; write each digit's run out
-// contiguously. 64 registers and 45 KB of shared memory hold four blocks per
-// SM.
+// One pass, by persistent blocks that take tiles from the counter in turn.
+// Per 4096-key tile (16 keys a thread in warp-striped order): count the
+// tile's digits per warp and publish the tile's per-digit aggregate at once,
+// so that later tiles' look-backs find it early; scan the counts into each
+// (warp, digit)'s first position in the digit-sorted tile; rank every key
+// into the shared-memory tile (lanes holding the same digit find one another
+// through a per-digit lane mask that each sets a bit in, which keeps ties in
+// input order); then take the next tile and load its keys and values into
+// the registers the ranking freed, while this tile looks back for its
+// digits' global starts and writes each digit's run out contiguously. 64
+// registers and 45 KB of shared memory hold four blocks per SM.
 __global__ void __launch_bounds__(kSortThreads, 4) k_onesweep(const uint32_t* __restrict__ kin,
                                                            const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
                                                            uint32_t* __restrict__ vout, uint32_t n, int shift,
@@ -239,7 +240,7 @@ __global__ void __launch_bounds__(kSortThreads, 4) k_onesweep(const uint32_t* __
                                                            uint32_t* status, uint32_t* tile_counter, uint32_t* err,
                                                            uint32_t spin_limit) {
     constexpr uint32_t kWarps = kSortThreads / 32;
-    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_tile, s_next_tile;
     __shared__ uint16_t s_next[kWarps][256];  // next tile position of each (warp, digit) while ranking
     __shared__ uint32_t s_lanes[kWarps][256]; // lanes of one key slot holding each digit (zero between slots)
     __shared__ uint32_t s_base[256];          // global destination minus tile position, per digit
@@ -247,94 +248,107 @@ __global__ void __launch_bounds__(kSortThreads, 4) k_onesweep(const uint32_t* __
     __shared__ uint32_t s_keys[kTile], s_vals[kTile];
     uint32_t(*s_count)[256] = reinterpret_cast<uint32_t(*)[256]>(s_vals);  // digit counts, before the ranking
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    for (uint32_t t = tid; t < kWarps * 256; t += kSortThreads) {
-        (&s_lanes[0][0])[t] = 0;
-        (&s_count[0][0])[t] = 0;
-    }
+    const uint32_t tiles = (n + kTile - 1) / kTile;
+    const uint32_t offs = digit_offsets[tid];
+    for (uint32_t t = tid; t < kWarps * 256; t += kSortThreads) (&s_lanes[0][0])[t] = 0;
     if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
     __syncthreads();
-    const uint32_t tile = s_tile;
-    const uint32_t wbase = tile * kTile + warp * (32u * kSortKpt);
+    uint32_t tile = s_tile;
     uint32_t key[kSortKpt], val[kSortKpt];
+    auto load = [&](uint32_t t) {
+        const uint32_t base = t * kTile + warp * (32u * kSortKpt);
 #pragma unroll
-    for (int k = 0; k < kSortKpt; ++k) {
-        const uint32_t idx = wbase + k * 32u + lane;
-        const bool valid = idx < n;
-        key[k] = valid ? kin[idx] : 0u;
-        val[k] = valid ? vin[idx] : 0u;
-    }
-#pragma unroll
-    for (int k = 0; k < kSortKpt; ++k)
-        if (wbase + k * 32u + lane < n) atomicAdd(&s_count[warp][(key[k] >> shift) & 255u], 1u);
-    __syncthreads();
-    // Thread `tid` owns digit `tid`: its count per warp and in the tile; the
-    // aggregate goes out before anything else.
-    uint32_t wc[kWarps], total = 0;
-#pragma unroll
-    for (uint32_t w = 0; w < kWarps; ++w) {
-        wc[w] = s_count[w][tid];
-        total += wc[w];
-    }
-    st_status(status + (size_t)tile * 256 + tid, total | (tile == 0 ? kFlagInc : kFlagAgg));
-    // Exclusive scan of the digit totals over the tile: where each digit's
-    // run starts in the digit-sorted tile.
-    uint32_t x = total;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-        if (lane >= (uint32_t)o) x += y;
-    }
-    if (lane == 31) s_wsum[warp] = x;
-    __syncthreads();  // also: every count is read before the values overwrite them
-    uint32_t start = x - total;
-#pragma unroll
-    for (uint32_t w = 0; w < kWarps; ++w) start += w < warp ? s_wsum[w] : 0u;
-    uint32_t run = start;
-#pragma unroll
-    for (uint32_t w = 0; w < kWarps; ++w) {
-        s_next[w][tid] = (uint16_t)run;
-        run += wc[w];
-    }
-    __syncthreads();
-    // Rank each key slot: its lanes holding one digit are numbered in lane
-    // order after the warp's earlier slots; the key lands in its position.
-    const uint32_t lt = (1u << lane) - 1u;
-#pragma unroll
-    for (int k = 0; k < kSortKpt; ++k) {
-        const bool valid = wbase + k * 32u + lane < n;
-        const uint32_t digit = (key[k] >> shift) & 255u;
-        if (valid) atomicOr(&s_lanes[warp][digit], 1u << lane);
-        __syncwarp();
-        const uint32_t peers = valid ? s_lanes[warp][digit] : 0u;
-        const uint32_t before = valid ? s_next[warp][digit] : 0u;
-        __syncwarp();
-        if (valid && lane == (uint32_t)(__ffs(peers) - 1)) {
-            s_next[warp][digit] = (uint16_t)(before + __popc(peers));
-            s_lanes[warp][digit] = 0u;
+        for (int k = 0; k < kSortKpt; ++k) {
+            const uint32_t idx = base + k * 32u + lane;
+            const bool valid = idx < n;
+            key[k] = valid ? kin[idx] : 0u;
+            val[k] = valid ? vin[idx] : 0u;
         }
-        __syncwarp();
-        const uint32_t local = before + __popc(peers & lt);
-        if (valid) {
-            s_keys[local] = key[k];
-            s_vals[local] = val[k];
+    };
+    if (tile < tiles) load(tile);
+    while (tile < tiles) {
+        const uint32_t wbase = tile * kTile + warp * (32u * kSortKpt);
+        for (uint32_t t = tid; t < kWarps * 256; t += kSortThreads) (&s_count[0][0])[t] = 0;
+        if (tid == 0) s_next_tile = atomicAdd(tile_counter, 1u);  // read after the ranking
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kSortKpt; ++k)
+            if (wbase + k * 32u + lane < n) atomicAdd(&s_count[warp][(key[k] >> shift) & 255u], 1u);
+        __syncthreads();
+        // Thread `tid` owns digit `tid`: its count per warp and in the tile;
+        // the aggregate goes out before anything else.
+        uint32_t wc[kWarps], total = 0;
+#pragma unroll
+        for (uint32_t w = 0; w < kWarps; ++w) {
+            wc[w] = s_count[w][tid];
+            total += wc[w];
         }
-    }
-    const uint32_t excl = look_back(status, tile, tid, total, spin_limit, err);
-    s_base[tid] = digit_offsets[tid] + excl - start;
-    __syncthreads();
-    // A tile past the last (only the look-back test hook numbers one) writes nothing.
-    const uint32_t first_key = tile * kTile;
-    const uint32_t count = first_key < n ? min(kTile, n - first_key) : 0u;
-    for (uint32_t i = tid; i < count; i += kSortThreads) {
-        const uint32_t kk = s_keys[i];
-        const uint32_t dst = s_base[(kk >> shift) & 255u] + i;
-        // In bounds whenever the pass's input matches the histogram; a pass
-        // after one whose look-back gave up may not, and writes nothing
-        // outside the arrays.
-        if (dst < n) {
-            kout[dst] = kk;
-            vout[dst] = s_vals[i];
+        st_status(status + (size_t)tile * 256 + tid, total | (tile == 0 ? kFlagInc : kFlagAgg));
+        // Exclusive scan of the digit totals over the tile: where each
+        // digit's run starts in the digit-sorted tile.
+        uint32_t x = total;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= (uint32_t)o) x += y;
         }
+        if (lane == 31) s_wsum[warp] = x;
+        __syncthreads();  // also: every count is read before the values overwrite them
+        uint32_t start = x - total;
+#pragma unroll
+        for (uint32_t w = 0; w < kWarps; ++w) start += w < warp ? s_wsum[w] : 0u;
+        uint32_t run = start;
+#pragma unroll
+        for (uint32_t w = 0; w < kWarps; ++w) {
+            s_next[w][tid] = (uint16_t)run;
+            run += wc[w];
+        }
+        __syncthreads();
+        // Rank each key slot: its lanes holding one digit are numbered in
+        // lane order after the warp's earlier slots; the key lands in its
+        // position.
+        const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+        for (int k = 0; k < kSortKpt; ++k) {
+            const bool valid = wbase + k * 32u + lane < n;
+            const uint32_t digit = (key[k] >> shift) & 255u;
+            if (valid) atomicOr(&s_lanes[warp][digit], 1u << lane);
+            __syncwarp();
+            const uint32_t peers = valid ? s_lanes[warp][digit] : 0u;
+            const uint32_t before = valid ? s_next[warp][digit] : 0u;
+            __syncwarp();
+            if (valid && lane == (uint32_t)(__ffs(peers) - 1)) {
+                s_next[warp][digit] = (uint16_t)(before + __popc(peers));
+                s_lanes[warp][digit] = 0u;
+            }
+            __syncwarp();
+            const uint32_t local = before + __popc(peers & lt);
+            if (valid) {
+                s_keys[local] = key[k];
+                s_vals[local] = val[k];
+            }
+        }
+        // The next tile's keys and values load while this tile looks back.
+        const uint32_t next = s_next_tile;
+        if (next < tiles) load(next);
+        const uint32_t excl = look_back(status, tile, tid, total, spin_limit, err);
+        s_base[tid] = offs + excl - start;
+        __syncthreads();
+        const uint32_t first_key = tile * kTile;
+        const uint32_t count = min(kTile, n - first_key);
+        for (uint32_t i = tid; i < count; i += kSortThreads) {
+            const uint32_t kk = s_keys[i];
+            const uint32_t dst = s_base[(kk >> shift) & 255u] + i;
+            // In bounds whenever the pass's input matches the histogram; a
+            // pass after one whose look-back gave up may not, and writes
+            // nothing outside the arrays.
+            if (dst < n) {
+                kout[dst] = kk;
+                vout[dst] = s_vals[i];
+            }
+        }
+        __syncthreads();  // the tile's shared memory is read before the next tile's counts reuse it
+        tile = next;
     }
 }
 
@@ -531,8 +545,9 @@ int32_t luc_radix_sort_device(luc_ctx* c, uint32_t n) {
     const int passes = orphan ? 1 : 4;
     for (int p = 0; p < passes; ++p) {
         cudaMemsetAsync(c->lb_look.p, 0, (size_t)(tiles + 1) * 256 * 4, s);
-        k_onesweep<<<tiles, kSortThreads, 0, s>>>(ka, va, kb, vb, n, 8 * p, offs + 256 * p, c->lb_look.as<uint32_t>(),
-                                                   tcount + p, tcount + 4, p == 0 ? spin : kSpinLimit);
+        k_onesweep<<<onesweep_grid(tiles, c->num_sms), kSortThreads, 0, s>>>(
+            ka, va, kb, vb, n, 8 * p, offs + 256 * p, c->lb_look.as<uint32_t>(), tcount + p, tcount + 4,
+            p == 0 ? spin : kSpinLimit);
         std::swap(ka, kb);
         std::swap(va, vb);
     }

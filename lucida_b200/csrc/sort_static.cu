@@ -102,6 +102,13 @@ extern "C" int32_t luc_sort_u32_static(void* keys_dev, void* vals_dev, uint32_t 
     uint32_t* tcount = hist + 2048;
     const unsigned grid = std::min<uint32_t>((n + 255) / 256, 148 * 32);
     uint32_t *ka = (uint32_t*)keys_dev, *va = (uint32_t*)vals_dev, *kb = sa.keys, *vb = sa.vals;
+    int dev = 0, sms = 0;
+    cudaError_t ae = cudaGetDevice(&dev);
+    if (ae == cudaSuccess) ae = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (ae != cudaSuccess || sms <= 0) {
+        set_err(err_msg, err_len, "luc_sort_u32_static: cannot query the device");
+        return LUC_ERR_LAUNCH;
+    }
     // The scratch keeps the previous call's contents: clear what must start at zero.
     cudaError_t e = cudaMemsetAsync(hist, 0, kHistWords * sizeof(uint32_t), s);
     if (e == cudaSuccess) e = launch(k_hist4, grid, 256, s, (const uint32_t*)keys_dev, n, hist);
@@ -109,7 +116,7 @@ extern "C" int32_t luc_sort_u32_static(void* keys_dev, void* vals_dev, uint32_t 
     for (int p = 0; p < 4 && e == cudaSuccess; ++p) {
         e = cudaMemsetAsync(sa.status, 0, (size_t)tiles * 256 * sizeof(uint32_t), s);
         if (e == cudaSuccess)
-            e = launch(k_onesweep, tiles, kSortThreads, s, (const uint32_t*)ka, (const uint32_t*)va, kb, vb, n,
+            e = launch(k_onesweep, onesweep_grid(tiles, sms), kSortThreads, s, (const uint32_t*)ka, (const uint32_t*)va, kb, vb, n,
                        8 * p, (const uint32_t*)(offs + 256 * p), sa.status, tcount + p, tcount + 4, kSpinLimit);
         std::swap(ka, kb);
         std::swap(va, vb);
