@@ -20,8 +20,9 @@ The roofline's per-stage times come from profiled repeats of the timed frames
 Multi-GPU (--gpus N under torchrun): each rank renders its own sample range
 of the frame (lucida_b200.shards.shard_params: samples [rank*spp,
 (rank+1)*spp) of every pixel) and every frame the ranks' accumulators are
-merged into the frame's (merge_accumulators: an all-gather over NCCL and a
-rank-order sum) inside the timed region; value = all ranks' paths /
+merged into the frame's (merge_accumulators: an all-to-all of pixel slices
+over NCCL, a rank-order sum of each slice, an all-gather of the sums) inside
+the timed region; value = all ranks' paths /
 max-over-ranks time.
 
 --impl reference times the reference's CPU tracer — here the oracle's C++
@@ -221,8 +222,9 @@ def config_block(args, n_tris, world):
                         f"{args.depth} bounces, Sobol, NEE+MIS",
             "width": args.width, "height": args.width, "spp": args.spp, "max_depth": args.depth,
             "triangles": n_tris,
-            "parallelism": f"sample-range shards x{world}" + (", accumulators merged every frame (all-gather + "
-                                                             "rank-order sum)" if world > 1 else ""),
+            "parallelism": f"sample-range shards x{world}" + (", accumulators merged every frame (all-to-all of "
+                                                             "pixel slices, rank-order sums, all-gather)"
+                                                             if world > 1 else ""),
             "l2": "flushed (256 MiB write) before every timed step; path pool of 3.5 GB streamed per bounce"}
 
 
@@ -474,8 +476,8 @@ def main():
                         "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_step,
                         "includes": "scene upload from pinned host memory + device LBVH rebuild + render + "
                                     "accumulator readback (pt_gpu::render_with per call); with N > 1 each "
-                                    "rank's sample range, the accumulator merge (all-gather + rank-order "
-                                    "sum), then the merged frame read back"},
+                                    "rank's sample range, the accumulator merge (all-to-all of pixel "
+                                    "slices, rank-order sums, all-gather), then the merged frame read back"},
                 "gpu_launches": int(counts["launches"]),
                 "roofline": roofline, "stage_state": stage_state, "cpu_baseline": cpu,
                 "clocks": clocks.summary(),

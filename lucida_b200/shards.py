@@ -5,10 +5,14 @@ accumulator: `shard_params` sets that range (RenderParams.sample_offset).
 The RNG is a pure function of (frame, pixel, sample) (crates/core/src/
 rng.rs:18-21) and accumulation is additive (crates/gpu/tests/
 cpu_gpu_agreement.rs:119-168), so the frame's accumulator is the field-wise
-sum of the ranks'. `merge_accumulators` is that one exchange: an all-gather
-of the W*H*64-byte accumulators (torch.distributed; NCCL over NVLink on
-GPUs) and a fixed rank-order sum (luc_accum_merge), so the merged image does
-not depend on the collective's reduction schedule.
+sum of the ranks'. `merge_accumulators` is that exchange, done as a
+reduce-scatter then an all-gather so that each rank moves about two
+accumulators' worth of bytes whatever N is (all-gathering every rank's whole
+accumulator moves N - 1): an all-to-all gives rank r the r-th pixel slice of
+every rank's accumulator (torch.distributed; NCCL over NVLink on GPUs),
+rank r sums them in rank order (luc_accum_merge), and an all-gather of the
+summed slices gives every rank the frame. The fixed rank-order sum keeps
+the merged image independent of the collectives' schedules.
 """
 from __future__ import annotations
 
@@ -55,7 +59,17 @@ def merge_accumulators(accum, gpu=None, group=None, sum_parts=None):
         if not accum.is_cuda or gpu is None:
             raise ValueError("the device merge needs a CUDA accumulator and its Gpu")
         sum_parts = lambda parts, out: _sum_on_device(gpu, parts, out)  # noqa: E731
-    flat = torch.empty(world * accum.numel(), dtype=accum.dtype, device=accum.device)
-    dist.all_gather_into_tensor(flat, accum.view(-1), group=group)
-    sum_parts(flat.view(world, accum.numel()), accum.view(-1))
+    pixels = accum.numel() // 16
+    per = -(-pixels // world)  # pixels of each rank's slice (the last padded with zero records)
+    whole = accum.view(-1)
+    if per * world != pixels:
+        whole = torch.zeros(per * world * 16, dtype=accum.dtype, device=accum.device)
+        whole[:accum.numel()].copy_(accum.view(-1))
+    parts = torch.empty(world * per * 16, dtype=accum.dtype, device=accum.device)
+    dist.all_to_all_single(parts, whole, group=group)  # parts[k] = rank k's copy of this rank's slice
+    mine = torch.empty(per * 16, dtype=accum.dtype, device=accum.device)
+    sum_parts(parts.view(world, per * 16), mine)
+    dist.all_gather_into_tensor(whole, mine, group=group)
+    if whole.data_ptr() != accum.data_ptr():
+        accum.view(-1).copy_(whole[:accum.numel()])
     return accum

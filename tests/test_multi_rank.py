@@ -1,8 +1,8 @@
 """Two ranks over gloo on the CPU: the sample-range sharding `bench.py
 --gpus N` runs (one process per GPU, rank r renders samples
 [r*spp, (r+1)*spp) of every pixel) and the product's one exchange,
-lucida_b200.shards.merge_accumulators (all-gather of the accumulators, then
-a rank-order sum).
+lucida_b200.shards.merge_accumulators (an all-to-all of pixel slices, each
+rank's rank-order sum of its slice, an all-gather of the sums).
 
 The reference's RNG is a pure function of (frame, pixel, sample)
 (crates/core/src/rng.rs:18-21) and a progressive render equals a one-shot
@@ -111,3 +111,44 @@ def test_sample_range_shards_sum_to_the_one_shot_render(tmp_path):
         assert float((tmp_path / f"rank{r}.txt").read_text()) == 10.0 + WORLD - 1
     # the shards are disjoint: each rank alone is not the whole
     assert not np.allclose(parts[0].view(lb.layout.ACCUM)["radiance"], whole["radiance"])
+
+
+def _merge_only_main(rank, world, port, pixels, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    import torch
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        from lucida_b200.shards import merge_accumulators
+        rng = np.random.default_rng(100 + rank)
+        acc = torch.from_numpy(rng.standard_normal(pixels * 16).astype(np.float32))
+        np.save(os.path.join(out_dir, f"in{rank}.npy"), acc.numpy())
+        merge_accumulators(acc, sum_parts=_rank_order_sum)
+        np.save(os.path.join(out_dir, f"out{rank}.npy"), acc.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,pixels", [(3, 7), (3, 1), (4, 12)])
+def test_merge_with_slices_that_do_not_divide_the_frame(tmp_path, world, pixels):
+    """Pixel counts that leave the last rank's slice short (or some ranks
+    with none): every rank still ends with the exact rank-order sum."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_merge_only_main, args=(r, world, port, pixels, str(tmp_path))) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+            p.join()
+    assert [p.exitcode for p in procs] == [0] * world
+    expect = np.load(tmp_path / "in0.npy")
+    for r in range(1, world):
+        expect = expect + np.load(tmp_path / f"in{r}.npy")
+    for r in range(world):
+        assert np.array_equal(np.load(tmp_path / f"out{r}.npy"), expect)
