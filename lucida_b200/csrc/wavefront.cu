@@ -405,18 +405,19 @@ struct PoolSink {
 // kBatch: the path's scene and frame parameters come from its wave segment
 // (luc_render_batch) instead of the kernel arguments.
 //
-// 8 blocks of 128 per SM (64 registers, about 700 bytes spilled to L1): SHADE
-// is bound by the latency of its path-state, triangle and material loads, and
-// the extra warps hide more of it than the spills cost (measured against 4,
-// 5, 6 and 7 blocks; 7 -> 8 took the displaced-sphere frame's SHADE from
-// 16.0 to 15.5 ms).
+// 6 blocks of 128 per SM (80 registers, about 450 bytes spilled). SHADE is bound by the latency of its
+// path-state, triangle and material loads. When it shaded escaped rays too,
+// 8 blocks (64 registers, about 700 bytes spilled to L1) ran best (7 -> 8:
+// 16.0 -> 15.5 ms per displaced-sphere frame); with the hits alone, split by
+// material class, and the traversal stacks partly in shared memory, 6 blocks
+// run 9.42 ms against 9.78 at 8 and 9.58 at 7.
 // kSobol (launched only for Sobol frames) and kSkyMis (MIS frames of scenes
 // lit only by an environment map): the code of the other cases is compiled
 // out of the kernel whose top stall is instruction fetch (displaced-sphere
 // frame: SHADE 15.6 ms generic, 14.7 with kSobol and no light sampling,
 // 14.4 with MIS and the environment fixed too).
 template <bool kGuided, bool kInst, bool kBatch = false, bool kSobol = false, bool kSkyMis = false>
-__global__ void __launch_bounds__(128, 8) k_shade(PathState ps, const __grid_constant__ DevScene sc_arg,
+__global__ void __launch_bounds__(128, 6) k_shade(PathState ps, const __grid_constant__ DevScene sc_arg,
                                                   const __grid_constant__ FrameParams fp_arg, BatchDev bd,
                                                   uint32_t depth) {
     const uint32_t len = shaded_count(ps, fp_arg, depth);
