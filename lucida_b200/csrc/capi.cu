@@ -479,8 +479,9 @@ static int32_t upload_scene(luc_ctx* c, const luc_scene_view* v, const MeshSpec*
             rc2 = luc_build_wide(c, num_nodes, v->num_triangles);
             if (rc2) return rc2;
         } else if (c->use_wide) {
-            // Two-level scenes: one wide tree per BLAS (the TLAS stays binary,
-            // rebuilt per frame); instances reach theirs through blas_wide.
+            // Two-level scenes: one wide tree per BLAS; instances reach theirs
+            // through blas_wide. Device-built TLASes (luc_set_instances) get
+            // their own wide tree each frame; a caller's TLAS stays binary.
             const std::vector<uint32_t>& br = meshes ? c->host_mesh_root : roots;
             rc2 = luc_build_wide_roots(c, br.data(), (uint32_t)br.size(), true, num_nodes, v->num_triangles);
             if (rc2) return rc2;

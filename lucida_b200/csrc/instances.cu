@@ -295,7 +295,8 @@ int32_t luc_set_instances(luc_ctx* c, const float* object_to_world, const uint32
     d.num_prims = np_;
     d.nodes = c->nodes.as<float4>();
     d.tnodes = c->tnodes.as<float4>();
-    // The BLASes' wide trees (built at upload) stay; the TLAS is binary.
+    // The BLASes' wide trees (built at upload) stay; the TLAS's wide tree is
+    // this frame's (null: the binary child pairs are walked).
     d.wnodes = c->wide_nodes ? c->wnodes.as<float4>() : nullptr;
     d.wsoup = c->wide_nodes ? c->wsoup.as<float4>() : nullptr;
     d.blas_wide = c->wide_nodes ? c->blas_wide.as<uint32_t>() : nullptr;

@@ -594,9 +594,11 @@ __global__ void __launch_bounds__(256) k_escape(PathState ps, const __grid_const
 }
 
 // CONNECT (shaders/wavefront/connect.wgsl:58-84): any-hit shadow rays, with
-// the same persistent ray pull as EXTEND. Two-level any-hit walks (kInst,
-// binary BLASes) run at 32 warps per SM too: the instanced frame's CONNECT
-// took 133 ms unbounded (82 registers, 24 warps), 110 at 28 warps, 103 at 32.
+// the same persistent ray pull as EXTEND. Two-level scenes use it when their
+// walk cannot be stepped (binary BLASes, or the reference's object-space
+// shadow rays); it runs at 32 warps per SM there too (the instanced frame's
+// CONNECT took 133 ms unbounded with 82 registers at 24 warps, 110 at 28
+// warps, 103 at 32, when it walked every instanced shadow ray).
 template <bool kInst, bool kBatch, int kThreads, int kWide>
 __global__ void __launch_bounds__(kThreads, kWide == 1 || kInst ? wide_min_blocks(kThreads) : 1) k_connect(PathState ps, const __grid_constant__ DevScene sc_arg, BatchDev bd,
                                                       uint32_t depth) {
