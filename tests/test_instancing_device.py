@@ -61,6 +61,40 @@ def test_device_build_is_bit_exact_and_renders_match(gpu):
     _render_check(gpu, s, osc, "instanced-field/reference-shadows", ref_shadows=True)
 
 
+@pytest.mark.parametrize("leaf", [1, 4, 8])
+def test_ray_queries_match_the_oracle(gpu, leaf):
+    """Closest hits of single rays (luc_intersect: the integrator's
+    two-level walk, whole) against the oracle's Scene::intersect on its
+    leaf-4 build: the same distance bit for bit, whichever TLAS the device
+    walks (leaf 1 and 4: the 8-wide TLAS; leaf 8: the binary child pairs);
+    and occlusion queries consistent with those distances."""
+    s = _small()
+    gpu.set_tlas_leaf(leaf)
+    gpu.upload(s, force=True)
+    osc = oracle_from_scene(s)
+    rng = np.random.default_rng(31 + leaf)
+    n = 20_000
+    o = np.stack([rng.uniform(-12, 12, n), rng.uniform(0.2, 6, n), rng.uniform(-12, 12, n)], 1).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    t, _, _, ids = gpu.intersect(o, d)
+    ref = osc.intersect(np.concatenate([o, d], 1))
+    hit_ref = ref[:, 0] >= 0
+    hit_dev = ids != 0xFFFFFFFF
+    assert hit_ref.sum() > n // 4 and (~hit_ref).sum() > n // 20  # both kinds of ray occur
+    same = (hit_ref == hit_dev) & (~hit_ref | (t.view(np.uint32) == ref[:, 0].view(np.uint32)))
+    assert same.mean() >= 0.9999, same.mean()
+    # Occluded within (1e-4, tmax) exactly when the nearest hit lies inside.
+    tmax = np.where(hit_ref, ref[:, 0], 10.0).astype(np.float32)
+    half = (0.5 * tmax).astype(np.float32)
+    occ_half = gpu.intersect(o, d, half)
+    occ_far = gpu.intersect(o, d, (tmax * 1.01 + 1e-3).astype(np.float32))
+    clear = half > 1e-3
+    assert np.mean(occ_half[clear] == False) >= 0.9999  # noqa: E712 — nothing nearer than the nearest hit
+    assert np.mean(occ_far[hit_ref] == True) >= 0.9999  # noqa: E712 — the nearest hit itself occludes
+    gpu.set_tlas_leaf(1)
+
+
 @pytest.mark.parametrize("leaf", [1, 8])
 def test_other_tlas_leaf_sizes_render_the_same(gpu, leaf):
     """TLASes other than the reference's (leaf size 4) differ in node layout
