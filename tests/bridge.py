@@ -82,8 +82,9 @@ def _px_rel(a, b):
 
 
 def parity(acc_radiance, osc: "O.Scene", u, label: str, ref_glibc=None, ref_double=None) -> dict:
-    """The north star's per-pixel bar on a device render, against the oracle
-    run both ways its transcendentals can round.
+    """The per-pixel parity bar (relative error <= 1e-3 per pixel) on a
+    device render, against the oracle run both ways its transcendentals can
+    round.
 
     * Against the oracle with transcendentals evaluated in double and rounded
       once (the rounding the CUDA integrator uses, so the two differ only
